@@ -1,0 +1,254 @@
+"""Generate golden vectors by running the reference implementation itself.
+
+Run from the repository root in a container where the reference checkout is
+available (default path below, or SIMULON_REFERENCE=<dir>):
+
+    python tests/golden/make_golden.py
+
+The reference is imported unmodified; two third-party imports it makes at
+module level but does not use on this path (pymatgen.core and
+torch_geometric.data.Data) are replaced by minimal stand-ins.  Inputs come
+from the seeded generators in ``oracle.inputs``.  Each case is written as a
+small .npz next to this script; the tests read only those files.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+import types
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+REF = os.environ.get("SIMULON_REFERENCE", "/root/reference")
+
+from oracle import inputs as oin  # noqa: E402
+from oracle.philox import langevin_normals  # noqa: E402
+
+
+def _stub_imports():
+    pm = types.ModuleType("pymatgen")
+    pmc = types.ModuleType("pymatgen.core")
+
+    class _Placeholder:  # never instantiated on the hot path
+        pass
+
+    pmc.Structure = _Placeholder
+    pmc.Lattice = _Placeholder
+    sys.modules.setdefault("pymatgen", pm)
+    sys.modules.setdefault("pymatgen.core", pmc)
+    tg = types.ModuleType("torch_geometric")
+    tgd = types.ModuleType("torch_geometric.data")
+
+    class Data:
+        def __init__(self, **kw):
+            for k, v in kw.items():
+                setattr(self, k, v)
+
+        def get(self, k, default=None):
+            return getattr(self, k, default)
+
+    tgd.Data = Data
+    sys.modules.setdefault("torch_geometric", tg)
+    sys.modules.setdefault("torch_geometric.data", tgd)
+    sys.path.insert(0, REF)
+
+
+def _reader(tmp, name, coords, symbol, box, cutoff, skin, params=None, is_fs=False):
+    from io_utils.reader import AtomFileReader
+    path = oin.write_xyz(os.path.join(tmp, name + ".xyz"), coords, symbol)
+    H = np.asarray(box, dtype=np.float64)
+    kw = {}
+    if H.ndim == 2:
+        kw["box_vectors"] = torch.tensor(H)
+        bl = float(np.linalg.norm(H[0]))
+    else:
+        bl = float(H) if H.ndim == 0 else H.tolist()
+    return AtomFileReader(filename=path, box_length=bl, cutoff=cutoff, device=torch.device("cpu"),
+                          parameter=params, skin_thickness=skin, is_fs=is_fs, **kw)
+
+
+def _save(name, **arrays):
+    out = {k: (v.detach().cpu().numpy() if torch.is_tensor(v) else np.asarray(v)) for k, v in arrays.items()}
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"wrote {name}.npz  ({', '.join(f'{k}{list(np.shape(v))}' for k, v in out.items())})")
+
+
+def neighbor_cases(tmp):
+    cases = []
+    x, L = oin.fcc_lattice(3)
+    cases.append(("nbr_ar108_f64", oin.jitter(x, 0.05, 0), L, 7.0, 0.5, torch.float64))
+    x, L = oin.bcc_lattice(5)
+    cases.append(("nbr_w250_f32", oin.jitter(x, 0.05, 2), L, 4.4, 0.5, torch.float32))
+    x, H = oin.bcc_triclinic(6)
+    cases.append(("nbr_wtri432_f32", oin.jitter(x, 0.05, 3), H, 4.4, 0.5, torch.float32))
+    cases.append(("nbr_wtri432_f64", oin.jitter(x, 0.05, 3), H, 4.4, 0.5, torch.float64))
+    rng = np.random.default_rng(4)
+    box = np.array([20.0, 22.0, 25.0])
+    gas = rng.uniform(-0.5, 1.5, size=(300, 3)) * box      # unwrapped, partly outside the box
+    cases.append(("nbr_gas300_orth_f32", gas, np.diag(box), 4.0, 1.0, torch.float32))
+    cases.append(("nbr_pair2_f64", np.array([[0.1, 0.2, 0.3], [9.9, 0.2, 0.3]]), 10.0, 3.0, 0.5, torch.float64))
+    cases.append(("nbr_far3_f32", np.array([[0.0, 0.0, 0.0], [5.0, 5.0, 5.0], [5.0, 0.0, 5.0]]), 12.0, 2.0, 0.5, torch.float32))
+    for name, coords, box, rc, skin, dt in cases:
+        torch.set_default_dtype(dt)
+        try:
+            mol = _reader(tmp, name, coords, "W", box, rc, skin, is_fs=True)
+            ei = mol.graph_data.edge_index
+            _save(name, pos=mol.coordinates, box=mol.box.H, cutoff=rc, skin=skin,
+                  i=ei[0], j=ei[1], dist=mol.graph_data.edge_attr)
+        finally:
+            torch.set_default_dtype(torch.float32)
+
+
+def lj_cases(tmp):
+    from core.force.lennard_jones_force import LennardJonesForce
+    torch.set_default_dtype(torch.float64)
+    try:
+        x, L = oin.fcc_lattice(3)
+        x = oin.jitter(x, 0.05, 0)
+        params = {"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}}
+        for mode in ("raw", "fs", "switch"):
+            mol = _reader(tmp, "ar108", x, "Ar", L, 7.0, 0.5, params=params)
+            mol.is_fs = mode == "fs"
+            mol.is_switch = mode == "switch"
+            out = LennardJonesForce(mol)()
+            ei = mol.graph_data.edge_index
+            _save(f"lj_ar108_{mode}_f64", pos=mol.coordinates, box=mol.box.H, i=ei[0], j=ei[1],
+                  eps=mol.pair_params[0], sigma=mol.pair_params[1], rc=7.0, rs=0.9 * 7.0,
+                  energy=out["energy"], forces=out["forces"], virial=out["virial"],
+                  virial_tensor=out["virial_tensor"])
+    finally:
+        torch.set_default_dtype(torch.float32)
+
+
+def eam_cases(tmp):
+    from io_utils.eam_parser import EAMParser
+    from core.force.eam_force_cu import EAMForceCUDAExt
+    pot = oin.write_fs_w_setfl(os.path.join(tmp, "W_synthetic.eam.fs"))
+    parser = EAMParser(pot, torch.device("cpu"))
+    x, L = oin.bcc_lattice(5)
+    for name, coords in (("eam_w250_jitter_f32", oin.jitter(x, 0.05, 5)), ("eam_w250_perfect_f32", x)):
+        mol = _reader(tmp, name, coords, "W", L, parser.cutoff, 0.5, is_fs=True)
+        ff = EAMForceCUDAExt(parser, mol, use_extension=False)
+        out = ff()
+        ei = mol.graph_data.edge_index
+        _save(name, pos=mol.coordinates, box=mol.box.H, i=ei[0], j=ei[1], dist=mol.graph_data.edge_attr,
+              energy=out["energy"], forces=out["forces"], virial=out["virial"],
+              virial_tensor=out["virial_tensor"], embedding_energy=out["embedding_energy"],
+              pair_potential=out["pair_potential"],
+              density_table=ff.density_table[0, 0], density_deriv_table=ff.density_deriv_table[0, 0],
+              pair_table=ff.pair_table[0, 0], pair_deriv_table=ff.pair_deriv_table[0, 0],
+              embed_table=ff.embed_table[0], embed_deriv_table=ff.embed_deriv_table[0])
+    xt, H = oin.bcc_triclinic(6)
+    mol = _reader(tmp, "eam_wtri432_f32", oin.jitter(xt, 0.05, 6), "W", H, parser.cutoff, 0.5, is_fs=True)
+    out = EAMForceCUDAExt(parser, mol, use_extension=False)()
+    ei = mol.graph_data.edge_index
+    _save("eam_wtri432_f32", pos=mol.coordinates, box=mol.box.H, i=ei[0], j=ei[1],
+          energy=out["energy"], forces=out["forces"], virial=out["virial"], virial_tensor=out["virial_tensor"])
+
+
+class _NoisePatch:
+    """Replace torch.randn_like with Philox normals so a run can be replayed."""
+
+    def __init__(self, seed):
+        self.seed, self.step, self.orig = seed, 0, None
+
+    def __enter__(self):
+        self.orig = torch.randn_like
+
+        def fake(t, *a, **k):
+            z = torch.as_tensor(langevin_normals(t.shape[0], self.step, self.seed)).to(t.dtype)
+            self.step += 1
+            return z
+        torch.randn_like = fake
+        return self
+
+    def __exit__(self, *exc):
+        torch.randn_like = self.orig
+
+
+def md_cases(tmp):
+    from core.force.lennard_jones_force import LennardJonesForce
+    from core.force.eam_force_cu import EAMForceCUDAExt
+    from core.integrator.integrator import VerletIntegrator
+    from core.md_model import BaseModel, SumBackboneInterface
+    from core.barostat import BerendsenBarostat
+    from io_utils.eam_parser import EAMParser
+
+    # LJ argon, FP64, NVE and Langevin NVT (config 1 inputs), 30 steps each.
+    torch.set_default_dtype(torch.float64)
+    try:
+        x, L = oin.fcc_lattice(3)
+        x = oin.jitter(x, 0.05, 0)
+        v0 = oin.maxwell_boltzmann(np.full(len(x), oin.AR_MASS), 94.4, 1)
+        params = {"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}}
+        for ens in ("NVE", "NVT"):
+            mol = _reader(tmp, "ar108md", x, "Ar", L, 7.0, 0.5, params=params)
+            integ = VerletIntegrator(mol, dt=0.002, ensemble=ens,
+                                     temperature=(94.4, 94.4) if ens == "NVT" else None,
+                                     gamma=10.0 if ens == "NVT" else None)
+            mol.atom_velocities = torch.tensor(v0)
+            model = BaseModel(SumBackboneInterface([LennardJonesForce(mol)], mol), integ, mol)
+            rec = {k: [] for k in ("energy", "kinetic_energy", "temperature")}
+            with _NoisePatch(seed=1234):
+                for _ in range(30):
+                    out = model()
+                    for k in rec:
+                        rec[k].append(float(out[k]))
+            _save(f"md_ar108_{ens.lower()}_f64", x0=x, v0=v0, box=L, dt=0.002, steps=30, noise_seed=1234,
+                  T=94.4, gamma=10.0, x=mol.coordinates, v=mol.atom_velocities, forces=out["forces"],
+                  rebuilds=mol.profile["neighbor_builds"],
+                  **{k: np.array(v) for k, v in rec.items()})
+    finally:
+        torch.set_default_dtype(torch.float32)
+
+    # EAM-W 250 FP32: NVE and Berendsen NPT (the reference EAM path is FP32 only).
+    pot = oin.write_fs_w_setfl(os.path.join(tmp, "W_synthetic.eam.fs"))
+    parser = EAMParser(pot, torch.device("cpu"))
+    x, L = oin.bcc_lattice(5)
+    x = oin.jitter(x, 0.02, 7)
+    v0 = oin.maxwell_boltzmann(np.full(len(x), oin.W_MASS), 300.0, 8)
+    for ens in ("NVE", "NPT"):
+        mol = _reader(tmp, "w250md", x, "W", L, parser.cutoff, 0.5, is_fs=True)
+        integ = VerletIntegrator(mol, dt=0.002, ensemble=ens,
+                                 temperature=(300.0, 300.0) if ens == "NPT" else None,
+                                 gamma=10.0 if ens == "NPT" else None)
+        mol.atom_velocities = torch.tensor(v0, dtype=torch.float32)
+        baro = BerendsenBarostat(mol, target_pressure=0.0, tau_p=0.5) if ens == "NPT" else None
+        model = BaseModel(SumBackboneInterface([EAMForceCUDAExt(parser, mol, use_extension=False)], mol),
+                          integ, mol, barostat=baro)
+        rec = {k: [] for k in ("energy", "kinetic_energy", "temperature", "pressure")}
+        with _NoisePatch(seed=99):
+            for _ in range(20):
+                out = model()
+                for k in rec:
+                    if k in out:
+                        rec[k].append(float(out[k]))
+        _save(f"md_w250_{ens.lower()}_f32", x0=x, v0=v0, box0=L, box=mol.box.H, dt=0.002, steps=20,
+              noise_seed=99, T=300.0, gamma=10.0, tau_p=0.5, x=mol.coordinates, v=mol.atom_velocities,
+              rebuilds=mol.profile["neighbor_builds"], **{k: np.array(v) for k, v in rec.items() if v})
+
+
+def main():
+    if not os.path.isdir(REF):
+        raise SystemExit(f"reference checkout not found at {REF}")
+    _stub_imports()
+    import builtins
+    quiet = builtins.print
+    with tempfile.TemporaryDirectory() as tmp:
+        builtins.print = lambda *a, **k: None if str(a[0] if a else "").startswith("[EAM") else quiet(*a, **k)
+        try:
+            neighbor_cases(tmp)
+            lj_cases(tmp)
+            eam_cases(tmp)
+            md_cases(tmp)
+        finally:
+            builtins.print = quiet
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,190 @@
+"""Pin the CPU oracle against golden vectors produced by the reference itself.
+
+The fixtures in tests/golden/ were written by tests/golden/make_golden.py,
+which runs the unmodified reference (core/, io_utils/) on seeded inputs.
+Tolerances:
+  * neighbor pair sets: bit-exact (same (i, j) set, same order);
+  * LJ FP64: 1e-12 relative (same arithmetic, scatter order may differ);
+  * EAM: the oracle in float32-table mode against the FP32 reference at
+    float32 round-off; the FP64 oracle against the FP32 reference at 2e-5;
+  * MD trajectories: 1e-9 (FP64 LJ) / 1e-4 relative energies (FP32 EAM).
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import eam as oeam
+from oracle import inputs as oin
+from oracle import neighbor as onb
+from oracle.box import OracleBox
+from oracle.integrator import OracleMD
+from oracle.lj import lj_forward
+from oracle.philox import langevin_normals, philox4x32_10
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLD, name + ".npz")))
+
+
+NBR_CASES = ["nbr_ar108_f64", "nbr_w250_f32", "nbr_wtri432_f32", "nbr_wtri432_f64",
+             "nbr_gas300_orth_f32", "nbr_pair2_f64", "nbr_far3_f32"]
+
+
+@pytest.mark.parametrize("name", NBR_CASES)
+@pytest.mark.parametrize("mode", ["brute", "auto"])
+def test_neighbor_pair_set_bit_exact(name, mode):
+    g = load(name)
+    box = OracleBox(g["box"])
+    pos = g["pos"]
+    rc2 = onb.rc2_like_reference(float(g["cutoff"]), float(g["skin"]), pos.dtype)
+    hl = onb.half_list(pos, box, rc2, mode=mode)
+    assert np.array_equal(hl["i"], g["i"]) and np.array_equal(hl["j"], g["j"])
+    if len(g["i"]):
+        d = onb.edge_distances(pos, hl["i"], hl["j"], box)
+        np.testing.assert_allclose(d, g["dist"], rtol=1e-6 if pos.dtype == np.float32 else 1e-14)
+        assert (hl["d2"] < rc2).all()
+
+
+def test_cell_mode_equals_brute_force_large():
+    x, L = oin.bcc_lattice(12)                     # 3456 atoms, 9 cells per axis
+    x = oin.jitter(x, 0.08, 11).astype(np.float32)
+    box = OracleBox(L)
+    rc2 = onb.rc2_like_reference(4.4, 0.5, np.float32)
+    a = onb.half_list(x, box, rc2, mode="brute")
+    b = onb.half_list(x, box, rc2, mode="cell")
+    assert np.array_equal(a["i"], b["i"]) and np.array_equal(a["j"], b["j"])
+    assert np.array_equal(a["image"], b["image"]) and np.array_equal(a["d2"], b["d2"])
+
+
+def test_cell_mode_equals_brute_force_triclinic():
+    x, H = oin.bcc_triclinic(10)
+    x = oin.jitter(x, 0.08, 12)
+    box = OracleBox(H)
+    rc2 = onb.rc2_like_reference(4.4, 0.5, np.float64)
+    a = onb.half_list(x, box, rc2, mode="brute")
+    b = onb.half_list(x, box, rc2, mode="cell")
+    assert np.array_equal(a["i"], b["i"]) and np.array_equal(a["j"], b["j"])
+
+
+@pytest.mark.parametrize("mode", ["raw", "fs", "switch"])
+def test_lj_fp64_matches_reference(mode):
+    g = load(f"lj_ar108_{mode}_f64")
+    box = OracleBox(g["box"])
+    out = lj_forward(torch.tensor(g["pos"]), g["i"], g["j"], g["eps"], g["sigma"], box,
+                     float(g["rc"]), mode, float(g["rs"]))
+    np.testing.assert_allclose(out["energy"].item(), g["energy"], rtol=1e-12)
+    np.testing.assert_allclose(out["forces"].numpy(), g["forces"], rtol=1e-10, atol=1e-13)
+    np.testing.assert_allclose(out["virial"].item(), g["virial"], rtol=1e-12)
+    np.testing.assert_allclose(out["virial_tensor"].numpy(), g["virial_tensor"], rtol=1e-11, atol=1e-14)
+
+
+@pytest.fixture(scope="module")
+def fsw(tmp_path_factory):
+    path = oin.write_fs_w_setfl(str(tmp_path_factory.mktemp("pot") / "W_synthetic.eam.fs"))
+    return oeam.parse_eam(path)
+
+
+def test_eam_tables_fp32_bit_exact(fsw):
+    g = load("eam_w250_jitter_f32")
+    t32 = oeam.EAMTables(fsw, dtype=torch.float32)
+    for key, tab in (("density_table", t32.density[0, 0]), ("density_deriv_table", t32.density_deriv[0, 0]),
+                     ("pair_table", t32.pair[0, 0]), ("pair_deriv_table", t32.pair_deriv[0, 0]),
+                     ("embed_table", t32.embed[0]), ("embed_deriv_table", t32.embed_deriv[0])):
+        assert np.array_equal(tab.numpy(), g[key]), key
+
+
+@pytest.mark.parametrize("name", ["eam_w250_jitter_f32", "eam_w250_perfect_f32", "eam_wtri432_f32"])
+def test_eam_oracle_matches_reference(fsw, name):
+    g = load(name)
+    box = OracleBox(g["box"])
+    types = np.zeros(len(g["pos"]), np.int64)
+    t32 = oeam.EAMTables(fsw, dtype=torch.float32)
+    o32 = oeam.eam_forward(torch.tensor(g["pos"]), g["i"], g["j"], types, box, t32)
+    np.testing.assert_allclose(o32["energy"].item(), g["energy"], rtol=2e-6)
+    np.testing.assert_allclose(o32["forces"].numpy(), g["forces"], atol=5e-5)
+    np.testing.assert_allclose(o32["virial_tensor"].numpy(), g["virial_tensor"], rtol=1e-4, atol=2e-2)
+    t64 = oeam.EAMTables(fsw, dtype=torch.float64)
+    o64 = oeam.eam_forward(torch.tensor(g["pos"]).double(), g["i"], g["j"], types, box, t64)
+    np.testing.assert_allclose(o64["energy"].item(), g["energy"], rtol=2e-5)
+    rmse = np.sqrt(((o64["forces"].numpy() - g["forces"]) ** 2).mean())
+    assert rmse < 1e-4, rmse
+
+
+def test_eam_perfect_lattice_known_answer(fsw):
+    rho, F, half_phi, e_atom = oin.perfect_bcc_known_answer()
+    assert abs(rho - 31.179650) < 1e-5 and abs(e_atom - (-8.900002)) < 1e-5
+    g = load("eam_w250_perfect_f32")
+    t64 = oeam.EAMTables(fsw, dtype=torch.float64)
+    out = oeam.eam_forward(torch.tensor(g["pos"]).double(), g["i"], g["j"], np.zeros(250, np.int64),
+                           OracleBox(g["box"]), t64)
+    assert abs(out["energy"].item() / 250 - e_atom) < 2e-5
+    assert float(g["energy"]) / 250 == pytest.approx(-8.9000010, abs=2e-6)
+    # positions are float32-rounded lattice sites, so forces vanish only to ~1e-5
+    assert np.abs(out["forces"].numpy()).max() < 2e-5
+
+
+def test_philox_known_answer():
+    # Random123 known-answer vector for philox4x32-10 with counter = key = 0.
+    out = philox4x32_10(0, 0, 0, 0, 0, 0)
+    assert [int(v) for v in out] == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    # and with all-ones counter/key
+    m = 0xFFFFFFFF
+    out = philox4x32_10(m, m, m, m, m, m)
+    assert [int(v) for v in out] == [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
+    z = langevin_normals(20000, 3, 77)
+    assert abs(z.mean()) < 0.02 and abs(z.std() - 1) < 0.02
+
+
+def _lj_force_fn(box, eps, sigma):
+    def fn(x, i, j):
+        # the reference keeps per-edge LJ parameters in float32 (reader.py:193-195)
+        return lj_forward(x, i, j, np.full(len(i), eps, np.float32), np.full(len(i), sigma, np.float32),
+                          box, 7.0, "raw")
+    return fn
+
+
+@pytest.mark.parametrize("ens", ["nve", "nvt"])
+def test_md_lj_fp64_matches_reference(ens):
+    g = load(f"md_ar108_{ens}_f64")
+    box = OracleBox(float(g["box"]))
+    eps, sigma = 0.0104, 3.405
+    md = OracleMD(g["x0"], g["v0"], np.full(108, oin.AR_MASS), box, _lj_force_fn(box, eps, sigma),
+                  cutoff=7.0, skin=0.5, dt=float(g["dt"]), ensemble=ens.upper(),
+                  temperature=float(g["T"]), gamma=float(g["gamma"]),
+                  noise_fn=lambda s: langevin_normals(108, s, int(g["noise_seed"])))
+    e = [md.step() for _ in range(int(g["steps"]))]
+    np.testing.assert_allclose([float(r["energy"]) for r in e], g["energy"], rtol=1e-9)
+    np.testing.assert_allclose([float(r["kinetic_energy"]) for r in e], g["kinetic_energy"], rtol=1e-9)
+    np.testing.assert_allclose(md.x.numpy(), g["x"], atol=1e-10)
+    np.testing.assert_allclose(md.v.numpy(), g["v"], atol=1e-9)
+    # the reference counts rebuilds from the first step on (the list built at
+    # construction, reader.py:83, precedes its profile counter, reader.py:87)
+    assert md.rebuilds - 1 == int(g["rebuilds"])
+
+
+@pytest.mark.parametrize("ens", ["nve", "npt"])
+def test_md_eam_fp32_matches_reference(fsw, ens):
+    g = load(f"md_w250_{ens}_f32")
+    box = OracleBox(float(g["box0"]))
+    t32 = oeam.EAMTables(fsw, dtype=torch.float32)
+    types = np.zeros(250, np.int64)
+
+    def ff(x, i, j):
+        return oeam.eam_forward(x, i, j, types, box, t32)
+    baro = dict(P0=0.0, tau=float(g["tau_p"])) if ens == "npt" else None
+    md = OracleMD(np.asarray(g["x0"], np.float32), np.asarray(g["v0"], np.float32), np.full(250, oin.W_MASS),
+                  box, ff, cutoff=fsw.cutoff, skin=0.5, dt=float(g["dt"]),
+                  ensemble="NPT" if ens == "npt" else "NVE", temperature=float(g["T"]), gamma=float(g["gamma"]),
+                  dtype=torch.float32, noise_fn=lambda s: langevin_normals(250, s, int(g["noise_seed"])),
+                  barostat=baro)
+    e = [md.step() for _ in range(int(g["steps"]))]
+    np.testing.assert_allclose([float(r["energy"]) for r in e], g["energy"], rtol=1e-5)
+    np.testing.assert_allclose([float(r["kinetic_energy"]) for r in e], g["kinetic_energy"], rtol=1e-3)
+    if ens == "npt":
+        np.testing.assert_allclose([r["pressure"] for r in e], g["pressure"], rtol=1e-3, atol=50.0)
+        np.testing.assert_allclose(box.H.numpy(), g["box"], rtol=1e-6)
+    np.testing.assert_allclose(md.x.numpy(), g["x"], atol=1e-4)
