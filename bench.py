@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Throughput of the EAM-W per-step force path on B200 (atom-steps/s).
+
+Workload (one step = one MD step through BaseModel: first half-kick + drift
+with the skin/2 trigger, conditional Verlet-list rebuild, two-pass EAM,
+second half-kick): BCC tungsten 2 n^3 atoms (n = 80 -> 1,024,000), a = 3.165 A,
+synthetic Finnis-Sinclair potential tabulated in eam/fs layout, skin 0.5 A,
+NVE from Maxwell-Boltzmann velocities at 300 K, dt = 2 fs; FP32 pair/EAM
+arithmetic, FP64 integration and reductions.  Inputs are seeded synthetic
+data.  The device state (~0.4 GB) exceeds the 126 MB L2, so no L2 flush is
+needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+With N > 1 (launched by torchrun) every rank runs an independent replica
+(weak scaling, no collective on the data path); the time is the max over
+ranks and the value is the total atom-steps of all ranks per second.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s (EAM-W, 1 B200): plain vs batched vs MLP at stated force RMSE"
+UNIT = "atom-steps/s"
+A_W, M_W = 3.165, 183.84
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=300)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--n", type=int, default=80, help="BCC cells per side (atoms = 2 n^3)")
+    p.add_argument("--graph-steps", type=int, default=20)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-extras", action="store_true", help="skip e2e / cpu baseline (profiling runs)")
+    return p.parse_args()
+
+
+def bcc(n):
+    g = np.arange(n)
+    cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0.5]])
+    return ((cells[:, None, :] + basis[None]).reshape(-1, 3) * A_W).astype(np.float64), n * A_W
+
+
+def write_potential(path, n=5000, d_rho=0.012, cutoff=4.4):
+    """Synthetic Finnis-Sinclair W in eam/fs layout: phi = (r-c)^2 (c0 + c1 r + c2 r^2),
+    rho = (r-d)^2, F = -A sqrt(rho); 5000-point r and rho grids; pair block holds r*phi."""
+    c, d, A, c0, c1, c2 = 3.25, 4.400224, 1.896373, 47.1346499, -33.7665655, 6.2541999
+    dr = cutoff / n
+    r = np.arange(n) * dr
+    rho = np.arange(n) * d_rho
+    F = -A * np.sqrt(rho)
+    f = np.where(r < d, (r - d) ** 2, 0.0)
+    phi = np.where(r < c, (r - c) ** 2 * (c0 + c1 * r + c2 * r * r), 0.0)
+    out = ["synthetic Finnis-Sinclair W", "eam/fs layout", "", "1 W", f"{n} {d_rho!r} {n} {dr!r} {cutoff!r}",
+           f"74 {M_W} {A_W} bcc"]
+    for blk in (F, f, r * phi):
+        out += [" ".join(f"{v:.16e}" for v in blk[k:k + 5]) for k in range(0, n, 5)]
+    with open(path, "w") as fh:
+        fh.write("\n".join(out) + "\n")
+    return path
+
+
+def mb_velocities(n_atoms, T, seed):
+    rng = np.random.default_rng(seed)
+    m = M_W * 1.036427e-4
+    v = rng.standard_normal((n_atoms, 3)) * np.sqrt(8.617333262e-5 * T / m)
+    return v - v.mean(0)
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks, power, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", self.gpu_id], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle port)
+def cpu_baseline(seconds: float, n_cells: int = 20):
+    """The oracle's restatement of the reference CPU path (FP32 EAM, as the
+    reference's EAM path; torch CPU ops, all host threads) on a bounded sample."""
+    import torch
+    from oracle import eam as oeam
+    from oracle import inputs as oin
+    from oracle.box import OracleBox
+    from oracle.integrator import OracleMD
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    with tempfile.TemporaryDirectory() as tmp:
+        pot = oin.write_fs_w_setfl(os.path.join(tmp, "W.eam.fs"))
+        tables = oeam.EAMTables(oeam.parse_eam(pot), dtype=torch.float32)
+    x, L = bcc(n_cells)
+    box = OracleBox(L)
+    types = np.zeros(len(x), np.int64)
+    md = OracleMD(x.astype(np.float32), mb_velocities(len(x), 300.0, 5).astype(np.float32), np.full(len(x), M_W),
+                  box, lambda xx, i, j: oeam.eam_forward(xx, i, j, types, box, tables), cutoff=4.4, skin=0.5,
+                  dt=0.002, ensemble="NVE", dtype=torch.float32)
+    md.step()                                   # warm-up
+    steps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds or steps < 3:
+        md.step()
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": len(x) * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"oracle FP32 restatement of the reference CPU path (torch CPU), BCC W {len(x)} atoms, "
+                      f"{steps} NVE steps incl. its own list rebuilds, {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    # each step: one MD step of the oracle port on a 16,000-atom sample of the same workload
+    per = max(1.0, 120.0 / max(1, args.steps + args.warmup))
+    base = cpu_baseline(seconds=per * args.steps, n_cells=20)
+    line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "EAM-W bulk BCC, synthetic FS potential, NVE 300 K, dt 2 fs, skin 0.5 A",
+                       "atoms": 16000},
+            "impl": "reference", "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    import simulon_b200 as sb
+    from simulon_b200 import _lib
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    x, L = bcc(args.n)
+    N = len(x)
+    v = mb_velocities(N, 300.0, 1000 + rank)
+    tmp = tempfile.mkdtemp()
+    pot = write_potential(os.path.join(tmp, "W_synthetic.eam.fs"))
+    parser = sb.EAMParser(pot)
+    mol = sb.AtomFileReader.from_arrays(["W"] * N, x, L, parser.cutoff, device=dev, skin_thickness=0.5, is_fs=True)
+    mol.atom_velocities = torch.tensor(v, device=dev)
+    ff = sb.EAMForceCUDAExt(parser, mol)
+    integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NVE")
+    model = sb.BaseModel(sb.SumBackboneInterface([ff], mol), integ, mol)
+    eng = mol.engine
+    G = args.graph_steps
+
+    # warm-up (captures the graph, runs W steps)
+    model.run(max(args.warmup, G), graph_steps=G)
+    torch.cuda.synchronize()
+    if eng.status():
+        raise RuntimeError(f"device status {eng.status():#x} after warm-up")
+    rb0 = int(eng.flags[3].item())
+
+    # timed region: K steps, events on the launching stream, barrier + sync both sides
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    gpu_id = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(gpu_id) as clocks:
+        e0.record(stream)
+        model.run(args.steps, graph_steps=G)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    status = eng.status()
+    rebuilds = int(eng.flags[3].item()) - rb0
+    value = world * N * args.steps / (ms / 1e3)
+    nbr = eng.neighbor_stats()
+    nbar = nbr["mean"]
+
+    # dominant kernel: EAM pass 2 (forces, pair energy, virial), timed alone with events
+    R = 50
+    ka, kb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    eng.eam_forces(ff.tables)
+    torch.cuda.synchronize()
+    ka.record(stream)
+    for _ in range(R):
+        _lib.call("sim_eam_force", eng.st_ref, ff.tables.ref, eng.stream)
+    kb.record(stream)
+    torch.cuda.synchronize()
+    k_ms = ka.elapsed_time(kb) / R
+    pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pa.record(stream)
+    for _ in range(R):
+        _lib.call("sim_eam_density", eng.st_ref, ff.tables.ref, eng.stream)
+    pb.record(stream)
+    torch.cuda.synchronize()
+    p1_ms = pa.elapsed_time(pb) / R
+    peak, peak_kind = measured_peaks()
+    bytes_pass2 = N * (16 + 4 * nbar + 4 + 16)           # posq, list, own F', force out
+    bytes_pass1 = N * (16 + 4 * nbar + 4)                # posq, list, F' out
+    achieved = bytes_pass2 / (k_ms / 1e3) / 1e9
+    # step-level algorithmic bytes per atom-step (EAM: pass1 + pass2 + integrator 152 + rebuild/K)
+    rebuild_bytes = 16 + 88 + 4 * nbar
+    K_rb = args.steps / max(rebuilds, 1)
+    B_step = (16 + 4 * nbar + 4) + (16 + 4 * nbar + 4 + 16) + 152 + rebuild_bytes / K_rb
+    step_achieved = value / world * B_step / 1e9
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+            "config": {"workload": f"EAM-W bulk BCC 2*{args.n}^3 = {N:,} atoms per GPU, synthetic FS W (eam/fs "
+                                   "tables 5000 pts), NVE from 300 K MB velocities, dt 2 fs, skin 0.5 A",
+                       "form": "plain", "atoms_per_gpu": N, "graph_steps": G,
+                       "l2": "state ~0.4 GB > 126 MB L2 (no flush needed)",
+                       "neighbors_mean": nbar, "neighbor_capacity": nbr["cap"], "rebuilds_in_timed": rebuilds,
+                       "parallelism": f"replicas x{world}"},
+            "status": status,
+            "roofline": {"bound": "hbm", "kernel": "k_eam_force (EAM pass 2)", "achieved": achieved,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "bytes_per_launch": bytes_pass2, "launch_ms": k_ms,
+                         "pass1_ms": p1_ms, "pass1_bytes": bytes_pass1},
+            "step_roofline": {"bytes_per_atom_step": B_step, "achieved": step_achieved, "peak": peak,
+                              "frac": step_achieved / peak, "unit": "GB/s"},
+            "clocks": clocks.summary(),
+            "gpu_launches": 15 * args.steps}
+
+    if not args.no_extras and rank == 0:
+        line["e2e"] = e2e(model, mol, x, v, args, dev)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        if not args.no_extras and world == 1:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+
+
+def e2e(model, mol, x, v, args, dev):
+    """Same metric through the public API with host buffers: pinned H2D of the
+    state, K steps, D2H of every step's scalars and of the final state."""
+    import torch
+    N = len(x)
+    xh = torch.tensor(x).pin_memory()
+    vh = torch.tensor(v).pin_memory()
+    K = args.steps
+    log_h = torch.empty(K, model.engine.log.shape[1], dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mol.update_coordinates(xh)          # H2D + cell sort + list build
+    mol.atom_velocities = vh            # H2D
+    done = 0
+    G = args.graph_steps
+    while done < K:
+        k = min(G * 5, K - done)
+        model.run(k, graph_steps=G)
+        log_h[done:done + k].copy_(model.step_log(model.steps_done - k, k), non_blocking=True)
+        done += k
+    x_out = mol.coordinates.cpu()
+    v_out = mol.atom_velocities.cpu()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    assert torch.isfinite(x_out).all() and torch.isfinite(log_h).all()
+    row_bytes = log_h.shape[1] * 8
+    return {"value": N * K / dt, "unit": UNIT, "h2d_bytes_per_step": 2 * N * 24 / K,
+            "d2h_bytes_per_step": row_bytes + 2 * N * 24 / K, "seconds": dt,
+            "path": "AtomFileReader.update_coordinates / atom_velocities -> BaseModel.run -> coordinates/velocities + step log"}
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)

@@ -1,0 +1,295 @@
+/*
+ * simb200.h -- C ABI of the B200-native Simulon force path (libsimb200.so).
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t
+ * (passed as void*), launches asynchronously on that stream and returns an
+ * int status (SIM_OK = 0).  Nothing is allocated inside the library and no
+ * device state is kept between calls: the caller (PyTorch on the Python side)
+ * owns every buffer.  Errors found on the device (neighbour-list overflow,
+ * non-finite values, box too small) are reported through a caller-owned
+ * device status word that the host reads when it chooses to synchronise.
+ *
+ * Two groups of entry points:
+ *
+ *  1. Drop-ins for the reference's native module `simulon_cuda`
+ *     (cuda source/ops.cpp:47-53), same argument meaning:
+ *       sim_legacy_density_pass   <- density_pass   (cuda source/eam_cuda_ext.cpp:30-42)
+ *       sim_legacy_force_pass     <- force_pass     (cuda source/eam_cuda_ext.cpp:44-60)
+ *       sim_legacy_lj_energy_force<- lj_energy_force_cuda (cuda source/lj_energy_force.cpp:10-20)
+ *                                    + configure_lj_smoothing (ops.cpp:43-45) folded into
+ *                                    the mode/rc/rs arguments (no device globals)
+ *       sim_half_list_*           <- neighbor_search_cuda (cuda source/neighbor_search_kernel.cu:73-138)
+ *                                    and find_neighbors_gpu_pbc (core/neighbor_search/gpu_kdtree.py:56-87):
+ *                                    half list i<j in the caller's dtype, bit-exact
+ *                                    with the reference's torch arithmetic, any box.
+ *
+ *  2. The device-resident engine (atoms kept in cell order, full Verlet list in
+ *     ELL layout, FP64 integration state), which replaces the per-step work of
+ *     BaseModel.forward (core/md_model.py:88-166):
+ *       sim_rebuild               <- AtomFileReader.update_neighbor_list (io_utils/reader.py:212-242)
+ *       sim_eam_forces            <- EAMForceCUDAExt.forward (core/force/eam_force_cu.py:461-579)
+ *       sim_lj_forces             <- LennardJonesForce.forward (core/force/lennard_jones_force.py:15-95)
+ *       sim_integrate_first       <- VerletIntegrator.first_half + update_coordinates' skin/2
+ *                                    trigger (core/integrator/integrator.py:91-99, io_utils/reader.py:136-163)
+ *       sim_integrate_second      <- VerletIntegrator.second_half (integrator.py:102-124)
+ *       sim_berendsen             <- BerendsenBarostat.step (core/barostat.py:36-68)
+ *       sim_gather_original       -- un-permute per-atom arrays to the caller's atom order
+ */
+#ifndef SIMB200_H
+#define SIMB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (return values and device status-word bits) ---------- */
+#define SIM_OK               0
+#define SIM_ERR_ARG          1   /* bad argument (null pointer, size, unsupported combination) */
+#define SIM_ERR_CUDA         2   /* a CUDA launch failed; see sim_last_cuda_error()            */
+#define SIM_ERR_BOX          4   /* box too small for the cutoff (needs L > 2 (rc+skin))       */
+#define SIM_STATUS_OVERFLOW  8   /* device: a neighbour row exceeded the ELL capacity          */
+#define SIM_STATUS_NONFINITE 16  /* device: NaN/Inf in forces, positions or velocities         */
+#define SIM_STATUS_CELLCAP   32  /* device: half-list export row capacity exceeded             */
+
+/* ---- simulation box (rows are lattice vectors, row-vector convention) -- */
+typedef struct SimBox {
+    double H[9];        /* H[3*r + c]                                          */
+    double Hinv[9];
+    float  Hf[9];       /* H rounded to float (used by the FP32 pair kernels)  */
+    int32_t orthogonal; /* off-diagonals all within 1e-8 of zero (core/box.py:54-57) */
+    int32_t pad[3];
+} SimBox;
+
+/* ---- engine description: caller-allocated device buffers ---------------- *
+ * n atoms live in "slots" 0..n-1 in cell order; per-atom arrays have stride
+ * n_pad (a multiple of 128).  SoA FP64 vectors are [3][n_pad].              */
+typedef struct SimEngine {
+    int64_t n, n_pad;
+    int32_t n_types, nbr_cap;        /* ELL capacity (neighbours per atom)      */
+    int32_t ncell[3], n_cells;       /* cell grid, fixed for the engine's life  */
+    double  x_rc;                    /* list cutoff rc + skin                   */
+    double  skin_half2;              /* (skin/2)^2 for the rebuild trigger      */
+    SimBox* box;                     /* device, updated in place by Berendsen  */
+    /* integration state, cell order */
+    double* x;        /* [3][n_pad] positions (unwrapped, as the reference)   */
+    double* v;        /* [3][n_pad] velocities                               */
+    float*  f32;      /* [n_pad][4] forces (FP32 pair path, float4; .w unused) */
+    double* f64;      /* [3][n_pad] forces (FP64 pair path) or NULL            */
+    int32_t* posq;    /* [n_pad][4] int4: fixed-point fractional coordinates
+                         u = frac(x H^-1) * 2^32 (uint32) in .xyz, type in .w;
+                         the int32 difference of two codes is the minimum-image
+                         fractional displacement (16-byte gathers)            */
+    int32_t* xref;    /* [3][n_pad] fixed-point positions at the last rebuild */
+    int32_t* orig;    /* [n_pad] original atom index of each slot             */
+    float*  fp;       /* [n_pad] F'(rho) (EAM)                                */
+    int32_t* nbr;     /* [nbr_cap][n_pad] neighbour slots (ELL, column-major) */
+    int32_t* nnbr;    /* [n_pad] neighbour counts                             */
+    /* rebuild scratch */
+    int32_t* cell_of;     /* [n_pad] */
+    int32_t* cell_count;  /* [n_cells + 1] */
+    int32_t* cell_start;  /* [n_cells + 1] */
+    int32_t* cell_rank;   /* [2*n_cells]: linear cell -> Morton rank, then rank -> linear */
+    int32_t* perm;        /* [n_pad] new slot -> old slot */
+    double*  x_alt;       /* [3][n_pad] */
+    double*  v_alt;       /* [3][n_pad] */
+    float*   f32_alt;     /* [n_pad][4] */
+    double*  f64_alt;     /* [3][n_pad] or NULL */
+    int32_t* orig_alt;    /* [n_pad] */
+    /* per-type constants */
+    double*  inv_mass;    /* [n_types] 1/m in ps^2 A^-2 eV^-1 ... see integrator */
+    double*  mass;        /* [n_types] m in eV ps^2 / A^2                        */
+    /* control and reductions */
+    int32_t* flags;       /* [8]: [0] rebuild requested, [1] status bits, [2] longest
+                             neighbour row seen on overflow, [3] rebuilds performed */
+    double*  partials;    /* [n_blocks_max * SIM_RED_SLOTS] */
+    uint32_t* red_counter;/* [4] last-block counters (self-resetting) */
+    double*  red_out;     /* [SIM_RED_SLOTS] final FP64 sums */
+    int32_t  n_blocks_max;
+    int32_t  pad0;
+} SimEngine;
+
+/* reduction slot layout (FP64 Kahan-compensated sums over all atoms) */
+#define SIM_RED_EPOT_EMBED 0
+#define SIM_RED_EPOT_PAIR  1
+#define SIM_RED_VIRIAL     2   /* scalar virial, force-field sign convention  */
+#define SIM_RED_W_XX 3
+#define SIM_RED_W_YY 4
+#define SIM_RED_W_ZZ 5
+#define SIM_RED_W_XY 6
+#define SIM_RED_W_XZ 7
+#define SIM_RED_W_YZ 8
+#define SIM_RED_KE   9
+#define SIM_RED_K_XX 10
+#define SIM_RED_K_YY 11
+#define SIM_RED_K_ZZ 12
+#define SIM_RED_K_XY 13
+#define SIM_RED_K_XZ 14
+#define SIM_RED_K_YZ 15
+#define SIM_RED_SLOTS 16
+
+/* ---- EAM tables (FP32, uniform grids; eam_force_cu.py:334-396) ---------- */
+typedef struct SimEAMTables {
+    const float* density;        /* [E][E][n_r]  host type, neighbour type  */
+    const float* density_deriv;  /* [E][E][n_r]                              */
+    const float* pair;           /* [E][E][n_r]                              */
+    const float* pair_deriv;     /* [E][E][n_r]                              */
+    const float* embed;          /* [E][n_rho]                               */
+    const float* embed_deriv;    /* [E][n_rho]                               */
+    const float* rho_min;        /* [E]  (device)                            */
+    const float* inv_drho;       /* [E]                                      */
+    const float* rho_clamp_hi;   /* [E]  rho_min + drho (n_rho-1)(1-1e-7)    */
+    int32_t n_types, n_r, n_rho, pad;
+    float cutoff, inv_dr, r_clamp_hi, pad2;   /* r_clamp_hi = r_max (1-1e-7) */
+} SimEAMTables;
+
+/* ---- LJ parameters (per type pair; lennard_jones_force.py:41-79) ------- */
+#define SIM_LJ_RAW    0
+#define SIM_LJ_SHIFT  1   /* force shift ("is_fs")                        */
+#define SIM_LJ_SWITCH 2   /* quintic switch on [rs, rc] ("is_switch")     */
+typedef struct SimLJParams {
+    const double* c4eps;    /* [E*E] 4*eps formed as the reference does (float32) */
+    const double* c24eps;   /* [E*E] 24*eps (float32 product)                      */
+    const double* sigma;    /* [E*E]                                               */
+    const double* u_rc;     /* [E*E] shift-mode energy at rc                       */
+    const double* f_rc;     /* [E*E] shift-mode force magnitude at rc              */
+    int32_t n_types, mode;
+    double rc, rs;
+} SimLJParams;
+
+/* ---- integrator parameters (integrator.py:45-124) ---------------------- */
+typedef struct SimIntegrator {
+    double dt;
+    double damp;            /* exp(-gamma dt); 1 when not Langevin          */
+    const double* rff;      /* [n_types] sqrt(kB T/m (1-exp(-2 gamma dt))) or NULL */
+    uint64_t seed;          /* Philox key                                   */
+    uint64_t* step_ctr;     /* device step counter: incremented by
+                               sim_integrate_first, read by sim_integrate_second
+                               (so a captured graph draws fresh noise each replay) */
+    int32_t langevin;
+    int32_t pad;
+} SimIntegrator;
+
+/* ---- Berendsen (barostat.py:21-68) -------------------------------------- */
+typedef struct SimBerendsen {
+    double target_bar, tau, kappa, mu_max, dt;
+    int32_t coordinate_scale_power;   /* 2 = the reference's behaviour (coordinates
+                                         and graph_data.pos alias, both scaled)     */
+    int32_t reset_reference;          /* 1 = last_positions reset after scaling    */
+} SimBerendsen;
+
+/* ==== group 1: drop-ins for the reference's native module ================ */
+
+/* density_pass (eam_cuda_ext.cpp:30-42): rho_out[row] += f_{t_row,t_col}(r),
+ * rho_out[col] += f_{t_col,t_row}(r) per half-list edge; accumulates in place. */
+int sim_legacy_density_pass(const float* distances, const int64_t* row, const int64_t* col,
+                            const int64_t* atom_types, int64_t n_edges,
+                            const float* density_table, int32_t n_types,
+                            double inv_dr, int64_t n_r, float* rho_out, void* stream);
+
+/* force_pass (eam_cuda_ext.cpp:44-60): forces_out[row] += -s rij/r, forces_out[col] -= ... */
+int sim_legacy_force_pass(const float* distances, const float* dist_vec, const int64_t* row,
+                          const int64_t* col, const int64_t* atom_types, int64_t n_edges,
+                          const float* density_deriv_table, const float* pair_deriv_table,
+                          const float* dF_drho, int32_t n_types, double inv_dr, int64_t n_r,
+                          float* forces_out, void* stream);
+
+/* lj_energy_force_cuda (lj_energy_force.cpp:10-20) with the smoothing mode of
+ * configure_lj_smoothing (ops.cpp:43-45) passed explicitly.  forces_out [N,3]
+ * and energy_out [1] must be zeroed by the caller (the reference allocates zeros). */
+int sim_legacy_lj_energy_force(const float* pos, const int64_t* edge_i, const int64_t* edge_j,
+                               int64_t n_edges, const float* sigma, const float* epsilon,
+                               float box_length, int32_t mode, float rc, float rs,
+                               float* forces_out, float* energy_out, void* stream);
+
+/* Half Verlet list in the caller's atom order and dtype (find_neighbors_gpu_pbc,
+ * gpu_kdtree.py:56-155 + reader.py:477-484).  Two phases:
+ *   sim_half_list_count: bins atoms, counts pairs j>i with d^2 < rc2 per atom,
+ *     writes row_ptr[n+1] (exclusive scan, int64) -- total = row_ptr[n];
+ *   sim_half_list_fill : writes edge_i/edge_j (int64, sorted by (i,j)),
+ *     image (int32 [E,3], optional) and dist (|min image|, optional).
+ * dtype_code: 0 = float32 positions, 1 = float64.  Scratch: see the Python
+ * wrapper (cell arrays of size n_cells+1 and n, one int64 per atom).       */
+int sim_half_list_count(const void* pos, int32_t dtype_code, int64_t n, const SimBox* box_host,
+                        double rc2, const int32_t* ncell, int32_t* cell_of, int32_t* cell_count,
+                        int32_t* cell_start, int32_t* sorted_idx, int64_t* row_ptr,
+                        void* stream);
+int sim_half_list_fill(const void* pos, int32_t dtype_code, int64_t n, const SimBox* box_host,
+                       double rc2, const int32_t* ncell, const int32_t* cell_start,
+                       const int32_t* sorted_idx, const int32_t* cell_of, const int64_t* row_ptr,
+                       int64_t* edge_i, int64_t* edge_j, int32_t* image, void* dist,
+                       void* stream);
+
+/* ==== group 2: the device-resident engine ================================ */
+
+/* Load atoms (original order, host-layout [N,3] FP64 device arrays) into slot
+ * order 0..n-1 and run the first full rebuild.  types: int32 [N]. */
+int sim_engine_load(const SimEngine* e, const double* x_rows, const double* v_rows,
+                    const int32_t* types, void* stream);
+
+/* Rebuild (cell binning, counting sort, deterministic in-cell order by original
+ * index, permutation of the state, ELL list).  With only_if_flagged = 1 the
+ * kernels read flags[0] and do nothing unless a rebuild was requested. */
+int sim_rebuild(const SimEngine* e, int32_t only_if_flagged, void* stream);
+
+/* EAM forces on the engine state.  Writes f32 (or f64), fp, and the
+ * reduction slots EPOT_*, VIRIAL, W_* (red_out).  Scalar virial follows the
+ * reference's EAM convention: sum over pairs of s*r (eam_force_cu.py:569). */
+int sim_eam_forces(const SimEngine* e, const SimEAMTables* t, void* stream);
+/* The two passes of sim_eam_forces as separate launches (pass 1 writes fp
+ * and EPOT_EMBED; pass 2 needs pass 1's fp of the same positions). */
+int sim_eam_density(const SimEngine* e, const SimEAMTables* t, void* stream);
+int sim_eam_force(const SimEngine* e, const SimEAMTables* t, void* stream);
+
+/* LJ forces; precision 0 = FP32 pair arithmetic, 1 = FP64 (positions read
+ * from e->x, forces to e->f64).  Scalar virial = sum F*r (lennard_jones_force.py:93). */
+int sim_lj_forces(const SimEngine* e, const SimLJParams* p, int32_t precision, void* stream);
+
+/* first_half: v += 0.5 a dt; x += v dt; refresh posq; skin/2 trigger -> flags[0].
+ * force_precision: 0 reads f32, 1 reads f64. */
+int sim_integrate_first(const SimEngine* e, const SimIntegrator* p, int32_t force_precision,
+                        void* stream);
+
+/* second_half: Langevin O-step (Philox noise by original index), half kick,
+ * kinetic energy and kinetic tensor sum m v(x)v into red_out. */
+int sim_integrate_second(const SimEngine* e, const SimIntegrator* p, int32_t force_precision,
+                         void* stream);
+
+/* Berendsen: reads red_out (K tensor, W tensor) and the device box, computes
+ * P (bar) and mu on the device in FP64, scales box, coordinates (mu^power),
+ * velocities; writes pressure_out[0] = P (bar), pressure_out[1] = mu. */
+int sim_berendsen(const SimEngine* e, const SimBerendsen* p, double* pressure_out, void* stream);
+
+/* Scatter caller rows into slots: dst_soa[c*n_pad + k] = rows[orig[k]*3 + c]. */
+int sim_scatter_original_f64(const SimEngine* e, const double* rows, double* dst_soa, void* stream);
+
+/* Append red_out (SIM_RED_SLOTS doubles), extra[0..n_extra) and the status
+ * word to log[(step_ctr % capacity) * row_width ...]; row_width = SIM_RED_SLOTS + n_extra + 1. */
+int sim_log_step(const SimEngine* e, const uint64_t* step_ctr, const double* extra, int32_t n_extra,
+                 double* log, int32_t capacity, void* stream);
+
+/* Un-permute: out_rows[orig[k]*3 + c] = src[c*n_pad + k] (FP64 or FP32 source). */
+int sim_gather_original_f64(const SimEngine* e, const double* src_soa, double* out_rows, void* stream);
+int sim_gather_original_f32(const SimEngine* e, const float* src_soa, double* out_rows, void* stream);
+
+/* Export the engine's list as the reference's half list (pairs i<j by
+ * original index, sorted by (i,j)) -- count then fill, like sim_half_list_*. */
+int sim_engine_half_count(const SimEngine* e, double rc2, int64_t* row_ptr, void* stream);
+int sim_engine_half_fill(const SimEngine* e, double rc2, const int64_t* row_ptr,
+                         int64_t* edge_i, int64_t* edge_j, double* dist, void* stream);
+
+/* Exclusive scan helper used by the wrappers: out[0]=0, out[k+1]=sum in[0..k]. */
+int sim_scan_i64(const int64_t* in, int64_t n, int64_t* out, void* stream);
+
+/* Message for the last CUDA error seen by this library (host string). */
+const char* sim_last_cuda_error(void);
+int sim_version(void);
+/* sizeof of SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator,
+ * SimBerendsen (host-only; lets bindings verify their struct layouts). */
+int sim_struct_sizes(int64_t* out, int32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SIMB200_H */

@@ -9,8 +9,10 @@ GPU's noise exactly (up to the last ulp of the float32 transcendentals).
 Counter layout for Langevin noise of atom ``a`` (original, unsorted index) at
 step ``s``:  ctr = (a, s & 0xffffffff, s >> 32, stream), key = (seed_lo, seed_hi).
 Normals: u_k = (x_k + 0.5) * 2^-32 in float32 arithmetic, then
-z0 = sqrt(-2 ln u0) cos(2 pi u1), z1 = sqrt(-2 ln u0) sin(2 pi u1),
-z2 = sqrt(-2 ln u2) cos(2 pi u3) -- three normals per atom.
+z0 = sqrt(-2 ln u0) cos(pi 2u1), z1 = sqrt(-2 ln u0) sin(pi 2u1),
+z2 = sqrt(-2 ln u2) cos(pi 2u3) -- three normals per atom.  The
+transcendentals are evaluated in float64 and rounded to float32 (the device
+uses float32 logf/sincospif, accurate to about one ulp).
 """
 from __future__ import annotations
 
@@ -50,8 +52,12 @@ def langevin_normals(n_atoms: int, step: int, seed: int, stream: int = 0, orig_i
                       np.full_like(a, np.uint32(stream)), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF)
     f = np.float32
     u = [(xk.astype(np.float32) + f(0.5)) * f(2.0 ** -32) for xk in x]
-    r0 = np.sqrt(f(-2.0) * np.log(u[0]))
-    r1 = np.sqrt(f(-2.0) * np.log(u[2]))
-    two_pi = f(2.0 * np.pi)
-    z = np.stack([r0 * np.cos(two_pi * u[1]), r0 * np.sin(two_pi * u[1]), r1 * np.cos(two_pi * u[3])], 1)
+    def lg(x):
+        return np.log(x.astype(np.float64)).astype(np.float32)
+
+    def cs(x, fn):
+        return fn(np.pi * (f(2.0) * x).astype(np.float64)).astype(np.float32)
+    r0 = np.sqrt(f(-2.0) * lg(u[0]))
+    r1 = np.sqrt(f(-2.0) * lg(u[2]))
+    z = np.stack([r0 * cs(u[1], np.cos), r0 * cs(u[1], np.sin), r1 * cs(u[3], np.cos)], 1)
     return z.astype(np.float64)

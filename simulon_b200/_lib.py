@@ -1,0 +1,163 @@
+"""ctypes binding of libsimb200.so (the C ABI declared in include/simb200.h).
+
+The library is built in-tree (``simulon_b200/lib/libsimb200.so``) by
+``simulon_b200.build``.  There is no CPU fallback: importing the engine on a
+machine without the built library, or calling it with CPU tensors, raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libsimb200.so")
+
+SIM_OK = 0
+SIM_ERR_ARG = 1
+SIM_ERR_CUDA = 2
+SIM_ERR_BOX = 4
+SIM_STATUS_OVERFLOW = 8
+SIM_STATUS_NONFINITE = 16
+
+RED_EPOT_EMBED, RED_EPOT_PAIR, RED_VIRIAL = 0, 1, 2
+RED_W = slice(3, 9)          # xx yy zz xy xz yz
+RED_KE = 9
+RED_K = slice(10, 16)
+RED_SLOTS = 16
+
+c_p = ctypes.c_void_p
+
+
+class SimBox(ctypes.Structure):
+    _fields_ = [("H", ctypes.c_double * 9), ("Hinv", ctypes.c_double * 9), ("Hf", ctypes.c_float * 9),
+                ("orthogonal", ctypes.c_int32), ("pad", ctypes.c_int32 * 3)]
+
+
+class SimEngine(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("n_pad", ctypes.c_int64),
+                ("n_types", ctypes.c_int32), ("nbr_cap", ctypes.c_int32),
+                ("ncell", ctypes.c_int32 * 3), ("n_cells", ctypes.c_int32),
+                ("x_rc", ctypes.c_double), ("skin_half2", ctypes.c_double),
+                ("box", c_p),
+                ("x", c_p), ("v", c_p), ("f32", c_p), ("f64", c_p), ("posq", c_p), ("xref", c_p),
+                ("orig", c_p), ("fp", c_p), ("nbr", c_p), ("nnbr", c_p),
+                ("cell_of", c_p), ("cell_count", c_p), ("cell_start", c_p), ("cell_rank", c_p),
+                ("perm", c_p), ("x_alt", c_p), ("v_alt", c_p), ("f32_alt", c_p), ("f64_alt", c_p),
+                ("orig_alt", c_p),
+                ("inv_mass", c_p), ("mass", c_p),
+                ("flags", c_p), ("partials", c_p), ("red_counter", c_p), ("red_out", c_p),
+                ("n_blocks_max", ctypes.c_int32), ("pad0", ctypes.c_int32)]
+
+
+class SimEAMTables(ctypes.Structure):
+    _fields_ = [("density", c_p), ("density_deriv", c_p), ("pair", c_p), ("pair_deriv", c_p),
+                ("embed", c_p), ("embed_deriv", c_p), ("rho_min", c_p), ("inv_drho", c_p),
+                ("rho_clamp_hi", c_p),
+                ("n_types", ctypes.c_int32), ("n_r", ctypes.c_int32), ("n_rho", ctypes.c_int32),
+                ("pad", ctypes.c_int32),
+                ("cutoff", ctypes.c_float), ("inv_dr", ctypes.c_float), ("r_clamp_hi", ctypes.c_float),
+                ("pad2", ctypes.c_float)]
+
+
+class SimLJParams(ctypes.Structure):
+    _fields_ = [("c4eps", c_p), ("c24eps", c_p), ("sigma", c_p), ("u_rc", c_p), ("f_rc", c_p),
+                ("n_types", ctypes.c_int32), ("mode", ctypes.c_int32),
+                ("rc", ctypes.c_double), ("rs", ctypes.c_double)]
+
+
+class SimIntegrator(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("damp", ctypes.c_double), ("rff", c_p),
+                ("seed", ctypes.c_uint64), ("step_ctr", c_p),
+                ("langevin", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+class SimBerendsen(ctypes.Structure):
+    _fields_ = [("target_bar", ctypes.c_double), ("tau", ctypes.c_double), ("kappa", ctypes.c_double),
+                ("mu_max", ctypes.c_double), ("dt", ctypes.c_double),
+                ("coordinate_scale_power", ctypes.c_int32), ("reset_reference", ctypes.c_int32)]
+
+
+_P = ctypes.POINTER
+# name -> argtypes (restype int unless listed in _RESTYPES)
+SIGNATURES = {
+    "sim_legacy_density_pass": [c_p, c_p, c_p, c_p, ctypes.c_int64, c_p, ctypes.c_int32, ctypes.c_double,
+                                ctypes.c_int64, c_p, c_p],
+    "sim_legacy_force_pass": [c_p, c_p, c_p, c_p, c_p, ctypes.c_int64, c_p, c_p, c_p, ctypes.c_int32,
+                              ctypes.c_double, ctypes.c_int64, c_p, c_p],
+    "sim_legacy_lj_energy_force": [c_p, c_p, c_p, ctypes.c_int64, c_p, c_p, ctypes.c_float, ctypes.c_int32,
+                                   ctypes.c_float, ctypes.c_float, c_p, c_p, c_p],
+    "sim_half_list_count": [c_p, ctypes.c_int32, ctypes.c_int64, _P(SimBox), ctypes.c_double, c_p, c_p, c_p,
+                            c_p, c_p, c_p, c_p],
+    "sim_half_list_fill": [c_p, ctypes.c_int32, ctypes.c_int64, _P(SimBox), ctypes.c_double, c_p, c_p, c_p,
+                           c_p, c_p, c_p, c_p, c_p, c_p, c_p],
+    "sim_engine_load": [_P(SimEngine), c_p, c_p, c_p, c_p],
+    "sim_rebuild": [_P(SimEngine), ctypes.c_int32, c_p],
+    "sim_eam_forces": [_P(SimEngine), _P(SimEAMTables), c_p],
+    "sim_eam_density": [_P(SimEngine), _P(SimEAMTables), c_p],
+    "sim_eam_force": [_P(SimEngine), _P(SimEAMTables), c_p],
+    "sim_lj_forces": [_P(SimEngine), _P(SimLJParams), ctypes.c_int32, c_p],
+    "sim_integrate_first": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
+    "sim_integrate_second": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
+    "sim_berendsen": [_P(SimEngine), _P(SimBerendsen), c_p, c_p],
+    "sim_gather_original_f64": [_P(SimEngine), c_p, c_p, c_p],
+    "sim_gather_original_f32": [_P(SimEngine), c_p, c_p, c_p],
+    "sim_scatter_original_f64": [_P(SimEngine), c_p, c_p, c_p],
+    "sim_log_step": [_P(SimEngine), c_p, c_p, ctypes.c_int32, c_p, ctypes.c_int32, c_p],
+    "sim_engine_half_count": [_P(SimEngine), ctypes.c_double, c_p, c_p],
+    "sim_engine_half_fill": [_P(SimEngine), ctypes.c_double, c_p, c_p, c_p, c_p, c_p],
+    "sim_scan_i64": [c_p, ctypes.c_int64, c_p, c_p],
+    "sim_last_cuda_error": [],
+    "sim_version": [],
+    "sim_struct_sizes": [c_p, ctypes.c_int32],
+}
+STRUCTS = (SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator, SimBerendsen)
+_RESTYPES = {"sim_last_cuda_error": ctypes.c_char_p}
+
+_lib = None
+
+
+class SimError(RuntimeError):
+    pass
+
+
+def load(path: str = LIB_PATH):
+    """Load the shared library and declare every exported entry point."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libsimb200.so not built ({path}); run `python -m simulon_b200.build`")
+    lib = ctypes.CDLL(path)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = _RESTYPES.get(name, ctypes.c_int)
+    _lib = lib
+    return lib
+
+
+def check(rc: int, what: str):
+    if rc == SIM_OK:
+        return
+    msg = {SIM_ERR_ARG: "invalid argument", SIM_ERR_CUDA: "CUDA error", SIM_ERR_BOX: "box too small"}.get(rc, str(rc))
+    detail = ""
+    if rc == SIM_ERR_CUDA:
+        detail = ": " + load().sim_last_cuda_error().decode()
+    raise SimError(f"{what} failed ({msg}){detail}")
+
+
+def call(name: str, *args):
+    """Call an entry point and raise SimError on a non-zero status."""
+    check(getattr(load(), name)(*args), name)
+
+
+def ptr(t) -> int:
+    """Device pointer of a tensor (None -> NULL)."""
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def stream_of(device=None) -> int:
+    import torch
+    return torch.cuda.current_stream(device).cuda_stream

@@ -1,0 +1,163 @@
+// Shared device helpers for libsimb200 (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/simb200.h"
+
+#define SIM_THREADS 256
+
+namespace simb200 {
+
+// ---- error plumbing --------------------------------------------------------
+void set_cuda_error(cudaError_t err, const char* where);
+int  launch_status(const char* where);   // checks cudaGetLastError after a launch
+
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// ---- fixed-point fractional coordinates -----------------------------------
+// u = frac(s) * 2^32 stored as uint32; the difference of two codes read as
+// int32 is the minimum-image fractional displacement in [-1/2, 1/2).
+__device__ __forceinline__ uint32_t to_fixed(double s) {
+    return (uint32_t)(unsigned long long)__double2ll_rn(s * 4294967296.0);
+}
+__device__ __forceinline__ float fixed_delta(int32_t a, int32_t b) {
+    return __int2float_rn((int32_t)((uint32_t)a - (uint32_t)b)) * 2.3283064365386963e-10f;
+}
+
+// fractional coordinate of a Cartesian row vector x: s_k = sum_r x_r Hinv[r][k]
+__device__ __forceinline__ void cart_to_frac(const SimBox& b, double x0, double x1, double x2,
+                                             double* s) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        s[k] = fma(x2, b.Hinv[6 + k], fma(x1, b.Hinv[3 + k], x0 * b.Hinv[k]));
+}
+
+// Cartesian displacement (FP32) of a fractional displacement t: r = t H
+__device__ __forceinline__ void frac_to_cart_f(const SimBox& b, float t0, float t1, float t2,
+                                               float& r0, float& r1, float& r2) {
+    if (b.orthogonal) {
+        r0 = t0 * b.Hf[0];
+        r1 = t1 * b.Hf[4];
+        r2 = t2 * b.Hf[8];
+    } else {
+        r0 = fmaf(t2, b.Hf[6], fmaf(t1, b.Hf[3], t0 * b.Hf[0]));
+        r1 = fmaf(t2, b.Hf[7], fmaf(t1, b.Hf[4], t0 * b.Hf[1]));
+        r2 = fmaf(t2, b.Hf[8], fmaf(t1, b.Hf[5], t0 * b.Hf[2]));
+    }
+}
+
+// Minimum image in FP64 following core/box.py:109-130 with torch's CPU op order
+// (orthogonal: r - d*rint(r/d); triclinic: fma-chained row-vector products).
+__device__ __forceinline__ void min_image_f64(const SimBox& b, double& r0, double& r1, double& r2) {
+    if (b.orthogonal) {
+        double d0 = b.H[0], d1 = b.H[4], d2 = b.H[8];
+        r0 = __dsub_rn(r0, __dmul_rn(d0, rint(__ddiv_rn(r0, d0))));
+        r1 = __dsub_rn(r1, __dmul_rn(d1, rint(__ddiv_rn(r1, d1))));
+        r2 = __dsub_rn(r2, __dmul_rn(d2, rint(__ddiv_rn(r2, d2))));
+    } else {
+        double s[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            s[k] = __fma_rn(r2, b.Hinv[6 + k], __fma_rn(r1, b.Hinv[3 + k], __dmul_rn(r0, b.Hinv[k])));
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s[k] = __dsub_rn(s[k], rint(s[k]));
+        r0 = __fma_rn(s[2], b.H[6], __fma_rn(s[1], b.H[3], __dmul_rn(s[0], b.H[0])));
+        r1 = __fma_rn(s[2], b.H[7], __fma_rn(s[1], b.H[4], __dmul_rn(s[0], b.H[1])));
+        r2 = __fma_rn(s[2], b.H[8], __fma_rn(s[1], b.H[5], __dmul_rn(s[0], b.H[2])));
+    }
+}
+
+__device__ __forceinline__ double norm2_f64(double a, double b, double c) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c));
+}
+
+// ---- reductions -------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-reduce `vals[0..NV)` (FP64) and store one row of `partials` per block.
+// Deterministic: fixed shuffle tree, fixed warp order.
+template <int NV>
+__device__ __forceinline__ void block_partials(double (&vals)[NV], double* partials, int slot0) {
+    __shared__ double red[NV][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double s = warp_sum(vals[k]);
+        if (lane == 0) red[k][warp] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
+        partials[(size_t)blockIdx.x * SIM_RED_SLOTS + slot0 + threadIdx.x] = s;
+    }
+}
+
+// The last block to finish sums all partial rows for slots [slot0, slot0+NV)
+// with Kahan compensation in block order and resets the counter (so a
+// captured graph can replay).  Must be called by every thread of every block.
+template <int NV>
+__device__ __forceinline__ void last_block_finalize(double* partials, uint32_t* counter,
+                                                    double* out, int slot0) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t done = atomicAdd(counter, 1u);
+        is_last = (done == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    if (threadIdx.x < NV) {
+        double s = 0.0, c = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) {
+            double y = __ldcg(&partials[(size_t)b * SIM_RED_SLOTS + slot0 + threadIdx.x]) - c;
+            double t = s + y;
+            c = (t - s) - y;
+            s = t;
+        }
+        out[slot0 + threadIdx.x] = s;
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+}
+
+// ---- Philox4x32-10 (Salmon et al., SC'11) ------------------------------------
+struct U4 { uint32_t x, y, z, w; };
+__device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// Three standard normals for atom `a` at `step` (float32 Box-Muller).
+__device__ __forceinline__ void langevin_normals(uint32_t a, uint64_t step, uint64_t seed,
+                                                 float& z0, float& z1, float& z2) {
+    U4 c{a, (uint32_t)step, (uint32_t)(step >> 32), 0u};
+    U4 x = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const float sc = 2.3283064365386963e-10f;
+    float u0 = __fmul_rn(__fadd_rn(__uint2float_rn(x.x), 0.5f), sc);
+    float u1 = __fmul_rn(__fadd_rn(__uint2float_rn(x.y), 0.5f), sc);
+    float u2 = __fmul_rn(__fadd_rn(__uint2float_rn(x.z), 0.5f), sc);
+    float u3 = __fmul_rn(__fadd_rn(__uint2float_rn(x.w), 0.5f), sc);
+    float r0 = sqrtf(__fmul_rn(-2.0f, logf(u0)));
+    float r1 = sqrtf(__fmul_rn(-2.0f, logf(u2)));
+    float s0, c0, s1, c1;
+    sincospif(__fmul_rn(2.0f, u1), &s0, &c0);
+    sincospif(__fmul_rn(2.0f, u3), &s1, &c1);
+    z0 = __fmul_rn(r0, c0);
+    z1 = __fmul_rn(r0, s0);
+    z2 = __fmul_rn(r1, c1);
+}
+
+}  // namespace simb200

@@ -1,0 +1,327 @@
+// Velocity Verlet / Langevin / Berendsen on the device, FP64 state (sm_100a).
+//
+// first_half  (core/integrator/integrator.py:91-99):
+//     a = F/m;  v_half = v + (0.5 a) dt;  x = x + v_half dt
+//   fused with the skin/2 rebuild trigger of AtomFileReader.update_coordinates
+//   (io_utils/reader.py:136-163): |min_image(x - x_last)| > skin/2 for any
+//   atom sets flags[0]; the fixed-point positions used by the pair kernels
+//   are refreshed in the same pass.
+// second_half (integrator.py:102-124):
+//     v = v_half damp + xi rff (Langevin);  v = v + (0.5 a') dt;
+//     K = sum 0.5 m v^2,  K_ab = sum m v_a v_b (md_model.py:83-86)
+//   Langevin noise xi comes from Philox4x32-10 keyed by (seed, original atom
+//   index, step), so it does not depend on the cell order.
+// Berendsen (core/barostat.py:36-68): P, mu and the box update are computed on
+// the device in FP64; no host round trip.
+// The arithmetic order matches the reference (explicit _rn intrinsics keep
+// nvcc from contracting into FMAs).
+#include <cstdio>
+#include <cstring>
+#include "common.cuh"
+
+namespace simb200 {
+
+static char g_err[512] = "";
+
+void set_cuda_error(cudaError_t err, const char* where) {
+    snprintf(g_err, sizeof(g_err), "%s: %s (%s)", where, cudaGetErrorString(err), cudaGetErrorName(err));
+}
+
+int launch_status(const char* where) {
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) {
+        set_cuda_error(err, where);
+        return SIM_ERR_CUDA;
+    }
+    return SIM_OK;
+}
+
+__device__ __forceinline__ double load_force(const SimEngine& e, int prec, int64_t i, int c) {
+    if (prec == 1) return e.f64[c * e.n_pad + i];
+    return (double)e.f32[4 * i + c];
+}
+
+__global__ void __launch_bounds__(SIM_THREADS) k_first_half(SimEngine e, SimIntegrator p, int prec) {
+    const int64_t P = e.n_pad;
+    const SimBox& b = *e.box;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool trigger = false, bad = false;
+    if (i == 0 && p.step_ctr) *p.step_ctr += 1;   // the step index sim_integrate_second reads
+    if (i < e.n) {
+        int4* posq = reinterpret_cast<int4*>(e.posq);
+        int4 q = posq[i];
+        const double m = e.mass[q.w];
+        double xn[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double a = __ddiv_rn(load_force(e, prec, i, c), m);
+            const double vh = __dadd_rn(e.v[c * P + i], __dmul_rn(__dmul_rn(0.5, a), p.dt));
+            xn[c] = __dadd_rn(e.x[c * P + i], __dmul_rn(vh, p.dt));
+            e.v[c * P + i] = vh;
+            e.x[c * P + i] = xn[c];
+            bad |= !isfinite(xn[c]) || !isfinite(vh);
+        }
+        double s[3];
+        cart_to_frac(b, xn[0], xn[1], xn[2], s);
+        q.x = (int32_t)to_fixed(s[0]);
+        q.y = (int32_t)to_fixed(s[1]);
+        q.z = (int32_t)to_fixed(s[2]);
+        posq[i] = q;
+        // displacement since the last rebuild, minimum image in fractional space
+        const double t0 = (double)(int32_t)((uint32_t)q.x - (uint32_t)e.xref[i]) * 2.3283064365386963e-10;
+        const double t1 = (double)(int32_t)((uint32_t)q.y - (uint32_t)e.xref[P + i]) * 2.3283064365386963e-10;
+        const double t2 = (double)(int32_t)((uint32_t)q.z - (uint32_t)e.xref[2 * P + i]) * 2.3283064365386963e-10;
+        const double d0 = t0 * b.H[0] + t1 * b.H[3] + t2 * b.H[6];
+        const double d1 = t0 * b.H[1] + t1 * b.H[4] + t2 * b.H[7];
+        const double d2 = t0 * b.H[2] + t1 * b.H[5] + t2 * b.H[8];
+        trigger = d0 * d0 + d1 * d1 + d2 * d2 > e.skin_half2;
+    }
+    if (__any_sync(0xffffffffu, trigger) && (threadIdx.x & 31) == 0) e.flags[0] = 1;
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+}
+
+__global__ void __launch_bounds__(SIM_THREADS) k_second_half(SimEngine e, SimIntegrator p, int prec) {
+    const int64_t P = e.n_pad;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double vals[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (i < e.n) {
+        const int type = e.posq[4 * i + 3];
+        const double m = e.mass[type];
+        double z[3] = {0.0, 0.0, 0.0};
+        double rff = 0.0;
+        if (p.langevin) {
+            float z0, z1, z2;
+            langevin_normals((uint32_t)e.orig[i], *p.step_ctr, p.seed, z0, z1, z2);
+            z[0] = z0; z[1] = z1; z[2] = z2;
+            rff = p.rff[type];
+        }
+        double v[3];
+        bool bad = false;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double vel = e.v[c * P + i];
+            if (p.langevin) vel = __dadd_rn(__dmul_rn(vel, p.damp), __dmul_rn(z[c], rff));
+            const double a = __ddiv_rn(load_force(e, prec, i, c), m);
+            vel = __dadd_rn(vel, __dmul_rn(__dmul_rn(0.5, a), p.dt));
+            e.v[c * P + i] = vel;
+            v[c] = vel;
+            bad |= !isfinite(vel);
+        }
+        const double hm = 0.5 * m;
+        vals[0] = hm * v[0] * v[0] + hm * v[1] * v[1] + hm * v[2] * v[2];
+        vals[1] = m * v[0] * v[0];
+        vals[2] = m * v[1] * v[1];
+        vals[3] = m * v[2] * v[2];
+        vals[4] = m * v[0] * v[1];
+        vals[5] = m * v[0] * v[2];
+        vals[6] = m * v[1] * v[2];
+        if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+    }
+    block_partials<7>(vals, e.partials, SIM_RED_KE);
+    last_block_finalize<7>(e.partials, e.red_counter + 2, e.red_out, SIM_RED_KE);
+}
+
+// ---- Berendsen -------------------------------------------------------------
+__device__ double det3(const double* H) {
+    return H[0] * (H[4] * H[8] - H[5] * H[7]) - H[1] * (H[3] * H[8] - H[5] * H[6]) +
+           H[2] * (H[3] * H[7] - H[4] * H[6]);
+}
+
+__global__ void k_berendsen_mu(SimEngine e, SimBerendsen p, double* out) {
+    SimBox& b = *e.box;
+    const double V = fabs(det3(b.H));
+    const double* r = e.red_out;
+    // stress = (K + W)/V; P = trace/3 (eV/A^3) -> bar
+    const double sxx = (r[SIM_RED_K_XX] + r[SIM_RED_W_XX]) / V;
+    const double syy = (r[SIM_RED_K_YY] + r[SIM_RED_W_YY]) / V;
+    const double szz = (r[SIM_RED_K_ZZ] + r[SIM_RED_W_ZZ]) / V;
+    const double P = ((sxx + syy) + szz) / 3.0 * 1602176.6208;
+    double mu3 = 1.0 + p.kappa * (p.dt / p.tau) * (P - p.target_bar);
+    const double lo = (1.0 - p.mu_max) * (1.0 - p.mu_max) * (1.0 - p.mu_max);
+    const double hi = (1.0 + p.mu_max) * (1.0 + p.mu_max) * (1.0 + p.mu_max);
+    mu3 = fmax(mu3, lo);
+    mu3 = fmin(mu3, hi);
+    const double mu = pow(mu3, 1.0 / 3.0);
+    for (int k = 0; k < 9; ++k) {
+        b.H[k] *= mu;
+        b.Hinv[k] /= mu;
+        b.Hf[k] = (float)b.H[k];
+    }
+    out[0] = P;
+    out[1] = mu;
+}
+
+__global__ void __launch_bounds__(SIM_THREADS) k_berendsen_scale(SimEngine e, SimBerendsen p, const double* mu_p) {
+    const int64_t P = e.n_pad;
+    const SimBox& b = *e.box;
+    const double mu = mu_p[1];
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= e.n) return;
+    double x[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double xc = e.x[c * P + i];
+        for (int k = 0; k < p.coordinate_scale_power; ++k) xc = __dmul_rn(xc, mu);
+        e.x[c * P + i] = xc;
+        x[c] = xc;
+        e.v[c * P + i] = __dmul_rn(e.v[c * P + i], mu);
+    }
+    double s[3];
+    cart_to_frac(b, x[0], x[1], x[2], s);
+    int4* posq = reinterpret_cast<int4*>(e.posq);
+    int4 q = posq[i];
+    q.x = (int32_t)to_fixed(s[0]);
+    q.y = (int32_t)to_fixed(s[1]);
+    q.z = (int32_t)to_fixed(s[2]);
+    posq[i] = q;
+    if (p.reset_reference) {
+        e.xref[i] = q.x;
+        e.xref[P + i] = q.y;
+        e.xref[2 * P + i] = q.z;
+    }
+}
+
+// ---- load / gather ------------------------------------------------------------
+__global__ void k_load(SimEngine e, const double* __restrict__ xr, const double* __restrict__ vr,
+                       const int32_t* __restrict__ types) {
+    const int64_t P = e.n_pad;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P; i += (int64_t)gridDim.x * blockDim.x) {
+        const bool live = i < e.n;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            e.x[c * P + i] = live ? xr[3 * i + c] : 0.0;
+            e.v[c * P + i] = live && vr ? vr[3 * i + c] : 0.0;
+            if (e.f64) e.f64[c * P + i] = 0.0;
+        }
+        reinterpret_cast<float4*>(e.f32)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        e.orig[i] = live ? (int32_t)i : -1;
+        reinterpret_cast<int4*>(e.posq)[i] = make_int4(0, 0, 0, live ? types[i] : 0);
+        e.nnbr[i] = 0;
+    }
+}
+
+__global__ void k_zero_i32(int32_t* p, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = 0;
+}
+
+__global__ void k_gather_f64(SimEngine e, const double* __restrict__ src, double* __restrict__ out) {
+    const int64_t P = e.n_pad;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < e.n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = e.orig[k];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) out[3 * o + c] = src[c * P + k];
+    }
+}
+
+__global__ void k_scatter_f64(SimEngine e, const double* __restrict__ rows, double* __restrict__ dst) {
+    const int64_t P = e.n_pad;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < e.n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = e.orig[k];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dst[c * P + k] = rows[3 * o + c];
+    }
+}
+
+__global__ void k_log_step(SimEngine e, const uint64_t* ctr, const double* extra, int n_extra, double* log, int cap) {
+    const int w = SIM_RED_SLOTS + n_extra + 1;
+    const uint64_t s = ctr ? *ctr : 0;
+    double* row = log + (size_t)(s % (uint64_t)cap) * w;
+    const int t = threadIdx.x;
+    if (t < SIM_RED_SLOTS) row[t] = e.red_out[t];
+    else if (t < SIM_RED_SLOTS + n_extra) row[t] = extra[t - SIM_RED_SLOTS];
+    else if (t == SIM_RED_SLOTS + n_extra) row[t] = (double)e.flags[1];
+}
+
+__global__ void k_gather_f32(SimEngine e, const float* __restrict__ src, double* __restrict__ out) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < e.n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = e.orig[k];
+        const float4 f = reinterpret_cast<const float4*>(src)[k];
+        out[3 * o] = f.x;
+        out[3 * o + 1] = f.y;
+        out[3 * o + 2] = f.z;
+    }
+}
+
+static int grid_atoms(int64_t n) {
+    int64_t g = ceil_div(n, SIM_THREADS);
+    return (int)(g < 1 ? 1 : (g > 148 * 32 ? 148 * 32 : g));
+}
+
+}  // namespace simb200
+
+using namespace simb200;
+
+extern "C" int sim_integrate_first(const SimEngine* ep, const SimIntegrator* p, int32_t force_precision, void* stream) {
+    if (!ep || !p || ep->n <= 0 || (force_precision == 1 && !ep->f64)) return SIM_ERR_ARG;
+    k_first_half<<<(int)ceil_div(ep->n, SIM_THREADS), SIM_THREADS, 0, (cudaStream_t)stream>>>(*ep, *p, force_precision);
+    return launch_status("sim_integrate_first");
+}
+
+extern "C" int sim_integrate_second(const SimEngine* ep, const SimIntegrator* p, int32_t force_precision, void* stream) {
+    if (!ep || !p || ep->n <= 0 || (force_precision == 1 && !ep->f64)) return SIM_ERR_ARG;
+    if (p->langevin && !p->rff) return SIM_ERR_ARG;
+    const int blocks = (int)ceil_div(ep->n, SIM_THREADS);
+    if (blocks > ep->n_blocks_max) return SIM_ERR_ARG;
+    k_second_half<<<blocks, SIM_THREADS, 0, (cudaStream_t)stream>>>(*ep, *p, force_precision);
+    return launch_status("sim_integrate_second");
+}
+
+extern "C" int sim_berendsen(const SimEngine* ep, const SimBerendsen* p, double* pressure_out, void* stream) {
+    if (!ep || !p || !pressure_out || p->tau <= 0.0) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    k_berendsen_mu<<<1, 1, 0, st>>>(*ep, *p, pressure_out);
+    k_berendsen_scale<<<(int)ceil_div(ep->n, SIM_THREADS), SIM_THREADS, 0, st>>>(*ep, *p, pressure_out);
+    return launch_status("sim_berendsen");
+}
+
+extern "C" int sim_engine_load(const SimEngine* ep, const double* x_rows, const double* v_rows, const int32_t* types,
+                               void* stream) {
+    if (!ep || !x_rows || !types || ep->n <= 0 || ep->n_pad < ep->n || (ep->n_pad % 128) != 0) return SIM_ERR_ARG;
+    if (ep->nbr_cap <= 0 || ep->n_cells <= 0) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const SimEngine& e = *ep;
+    k_load<<<grid_atoms(e.n_pad), SIM_THREADS, 0, st>>>(e, x_rows, v_rows, types);
+    k_zero_i32<<<grid_atoms(e.n_cells + 1), SIM_THREADS, 0, st>>>(e.cell_count, e.n_cells + 1);
+    k_zero_i32<<<1, 32, 0, st>>>(e.flags, 8);
+    k_zero_i32<<<1, 32, 0, st>>>((int32_t*)e.red_counter, 4);
+    int rc = launch_status("sim_engine_load");
+    if (rc != SIM_OK) return rc;
+    return sim_rebuild(ep, 0, stream);
+}
+
+extern "C" int sim_gather_original_f64(const SimEngine* ep, const double* src_soa, double* out_rows, void* stream) {
+    if (!ep || !src_soa || !out_rows) return SIM_ERR_ARG;
+    k_gather_f64<<<grid_atoms(ep->n), SIM_THREADS, 0, (cudaStream_t)stream>>>(*ep, src_soa, out_rows);
+    return launch_status("sim_gather_original_f64");
+}
+
+extern "C" int sim_scatter_original_f64(const SimEngine* ep, const double* rows, double* dst_soa, void* stream) {
+    if (!ep || !rows || !dst_soa) return SIM_ERR_ARG;
+    k_scatter_f64<<<grid_atoms(ep->n), SIM_THREADS, 0, (cudaStream_t)stream>>>(*ep, rows, dst_soa);
+    return launch_status("sim_scatter_original_f64");
+}
+
+extern "C" int sim_log_step(const SimEngine* ep, const uint64_t* step_ctr, const double* extra, int32_t n_extra,
+                            double* log, int32_t capacity, void* stream) {
+    if (!ep || !log || capacity <= 0 || n_extra < 0 || n_extra > 32 || (n_extra > 0 && !extra)) return SIM_ERR_ARG;
+    k_log_step<<<1, 64, 0, (cudaStream_t)stream>>>(*ep, step_ctr, extra, n_extra, log, capacity);
+    return launch_status("sim_log_step");
+}
+
+extern "C" int sim_gather_original_f32(const SimEngine* ep, const float* src_soa, double* out_rows, void* stream) {
+    if (!ep || !src_soa || !out_rows) return SIM_ERR_ARG;
+    k_gather_f32<<<grid_atoms(ep->n), SIM_THREADS, 0, (cudaStream_t)stream>>>(*ep, src_soa, out_rows);
+    return launch_status("sim_gather_original_f32");
+}
+
+extern "C" const char* sim_last_cuda_error(void) { return g_err; }
+extern "C" int sim_version(void) { return 1; }
+
+extern "C" int sim_struct_sizes(int64_t* out, int32_t n) {
+    const int64_t sizes[6] = {(int64_t)sizeof(SimBox), (int64_t)sizeof(SimEngine), (int64_t)sizeof(SimEAMTables),
+                              (int64_t)sizeof(SimLJParams), (int64_t)sizeof(SimIntegrator),
+                              (int64_t)sizeof(SimBerendsen)};
+    if (!out || n < 6) return SIM_ERR_ARG;
+    for (int k = 0; k < 6; ++k) out[k] = sizes[k];
+    return SIM_OK;
+}

@@ -1,0 +1,559 @@
+// Verlet neighbour lists on the device (sm_100a).
+//
+// Engine rebuild (replaces AtomFileReader.update_neighbor_list, io_utils/reader.py:212-242,
+// and the O(N^2) search it calls, core/neighbor_search/gpu_kdtree.py:90-155):
+//   bin atoms into cells at least rc+skin wide (fractional coordinates, any
+//   triclinic box) -> counting sort with cells visited in Morton order ->
+//   deterministic in-cell order (by original index) -> permute the state ->
+//   full list in ELL layout nbr[k*n_pad + i] so that a warp's loads of
+//   neighbour k coalesce.  Capacity overflow sets a status bit; nothing is
+//   silently truncated (the reference truncates at 500, neighbor_search_kernel.cu:35).
+//
+// Half-list export (drop-in for find_neighbors_gpu_pbc / neighbor_search_cuda):
+//   same binning on the caller's positions, then each pair i<j tested with
+//   the exact floating-point operation sequence of the reference's torch
+//   code (core/box.py:109-130; gpu_kdtree.py:130-138) in the caller's dtype,
+//   so the (i, j, image) set is bit-identical.  Rows are emitted sorted by j.
+#include "common.cuh"
+
+namespace simb200 {
+
+// ---------------------------------------------------------------------------
+// single-block exclusive scan (cell counts, row counts); out has n+1 entries
+template <typename T>
+__global__ void k_scan_exclusive(const T* __restrict__ in, int64_t n, T* __restrict__ out,
+                                 T* zero_after, const int32_t* gate) {
+    if (gate && __ldg(gate) == 0) return;
+    __shared__ T warp_tot[32];
+    __shared__ T carry_s;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nthreads = blockDim.x;
+    if (tid == 0) carry_s = 0;
+    __syncthreads();
+    const int64_t tile = (int64_t)nthreads * 8;
+    for (int64_t base = 0; base < n; base += tile) {
+        T v[8];
+        T local = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            int64_t idx = base + (int64_t)tid * 8 + k;
+            v[k] = idx < n ? in[idx] : (T)0;
+            local += v[k];
+        }
+        T incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            T w = lane < (nthreads >> 5) ? warp_tot[lane] : (T)0;
+            T wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                T y = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += y;
+            }
+            warp_tot[lane] = wi - w;   // exclusive warp offsets
+        }
+        __syncthreads();
+        T run = carry_s + warp_tot[warp] + (incl - local);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            int64_t idx = base + (int64_t)tid * 8 + k;
+            if (idx < n) {
+                out[idx] = run;
+                if (zero_after) zero_after[idx] = 0;
+            }
+            run += v[k];
+        }
+        __syncthreads();
+        if (tid == nthreads - 1) carry_s = run;
+        __syncthreads();
+    }
+    if (tid == 0) out[n] = carry_s;
+}
+
+// ---------------------------------------------------------------------------
+// engine rebuild kernels (gate = flags, kernel returns unless flags[0] != 0)
+
+__device__ __forceinline__ int cell_coord(double s, int n) {
+    s -= floor(s);
+    int c = (int)(s * (double)n);
+    return c < 0 ? 0 : (c >= n ? n - 1 : c);
+}
+
+__global__ void k_bin(SimEngine e, const int32_t* gate) {
+    if (gate && __ldg(gate) == 0) return;
+    const SimBox& b = *e.box;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < e.n; k += (int64_t)gridDim.x * blockDim.x) {
+        double s[3];
+        cart_to_frac(b, e.x[k], e.x[e.n_pad + k], e.x[2 * e.n_pad + k], s);
+        int cx = cell_coord(s[0], e.ncell[0]);
+        int cy = cell_coord(s[1], e.ncell[1]);
+        int cz = cell_coord(s[2], e.ncell[2]);
+        int lin = cx + e.ncell[0] * (cy + e.ncell[1] * cz);
+        int rank = e.cell_rank[lin];
+        e.cell_of[k] = rank;
+        atomicAdd(&e.cell_count[rank], 1);
+    }
+}
+
+__global__ void k_scatter(SimEngine e, const int32_t* gate) {
+    if (gate && __ldg(gate) == 0) return;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < e.n; k += (int64_t)gridDim.x * blockDim.x) {
+        int c = e.cell_of[k];
+        int p = e.cell_start[c] + atomicAdd(&e.cell_count[c], 1);
+        e.perm[p] = (int32_t)k;
+    }
+}
+
+// In-cell order by original index: reruns are bitwise reproducible.
+__global__ void k_sort_cells(SimEngine e, const int32_t* gate) {
+    if (gate && __ldg(gate) == 0) return;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < e.n_cells; c += gridDim.x * blockDim.x) {
+        int b0 = e.cell_start[c], b1 = e.cell_start[c + 1];
+        for (int a = b0 + 1; a < b1; ++a) {
+            int key = e.perm[a];
+            int ko = e.orig[key];
+            int p = a - 1;
+            while (p >= b0 && e.orig[e.perm[p]] > ko) {
+                e.perm[p + 1] = e.perm[p];
+                --p;
+            }
+            e.perm[p + 1] = key;
+        }
+    }
+}
+
+__global__ void k_permute(SimEngine e, const int32_t* gate) {
+    if (gate && __ldg(gate) == 0) return;
+    const int64_t P = e.n_pad;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < e.n; m += (int64_t)gridDim.x * blockDim.x) {
+        int64_t o = e.perm[m];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            e.x_alt[c * P + m] = e.x[c * P + o];
+            e.v_alt[c * P + m] = e.v[c * P + o];
+            if (e.f64_alt) e.f64_alt[c * P + m] = e.f64[c * P + o];
+        }
+        reinterpret_cast<float4*>(e.f32_alt)[m] = reinterpret_cast<const float4*>(e.f32)[o];
+        e.orig_alt[m] = e.orig[o];
+        e.cell_of[m] = e.posq[4 * o + 3];   // stash the type; posq is rewritten by k_commit
+    }
+}
+
+// Copy the permuted state back, refresh fixed-point positions, the skin
+// reference, and the per-slot cell rank.
+__global__ void k_commit(SimEngine e, const int32_t* gate) {
+    if (gate && __ldg(gate) == 0) return;
+    const int64_t P = e.n_pad;
+    const SimBox& b = *e.box;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < e.n; m += (int64_t)gridDim.x * blockDim.x) {
+        double x0 = e.x_alt[m], x1 = e.x_alt[P + m], x2 = e.x_alt[2 * P + m];
+        e.x[m] = x0; e.x[P + m] = x1; e.x[2 * P + m] = x2;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            e.v[c * P + m] = e.v_alt[c * P + m];
+            if (e.f64) e.f64[c * P + m] = e.f64_alt[c * P + m];
+        }
+        reinterpret_cast<float4*>(e.f32)[m] = reinterpret_cast<const float4*>(e.f32_alt)[m];
+        e.orig[m] = e.orig_alt[m];
+        int type = e.cell_of[m];
+        double s[3];
+        cart_to_frac(b, x0, x1, x2, s);
+        uint32_t u0 = to_fixed(s[0]), u1 = to_fixed(s[1]), u2 = to_fixed(s[2]);
+        reinterpret_cast<int4*>(e.posq)[m] = make_int4((int32_t)u0, (int32_t)u1, (int32_t)u2, type);
+        e.xref[m] = (int32_t)u0; e.xref[P + m] = (int32_t)u1; e.xref[2 * P + m] = (int32_t)u2;
+    }
+}
+
+// slot -> cell rank after the sort (binary search over cell_start)
+__global__ void k_slot_cells(SimEngine e, const int32_t* gate) {
+    if (gate && __ldg(gate) == 0) return;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < e.n; m += (int64_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = e.n_cells;          // find c with start[c] <= m < start[c+1]
+        while (hi - lo > 1) {
+            int mid = (lo + hi) >> 1;
+            if (e.cell_start[mid] <= m) lo = mid; else hi = mid;
+        }
+        e.cell_of[m] = lo;
+    }
+}
+
+// unique stencil offsets along one axis: n>=3 -> {-1,0,1}; n==2 -> {0,1}; n==1 -> {0}
+__device__ __forceinline__ int stencil_count(int n) { return n >= 3 ? 3 : n; }
+__device__ __forceinline__ int stencil_cell(int c, int k, int n) {
+    if (n >= 3) { int v = c + k - 1; return v < 0 ? v + n : (v >= n ? v - n : v); }
+    return k;   // n <= 2: enumerate every cell once
+}
+
+// Full list in ELL layout.  Test in FP32 on fixed-point displacements; the
+// radius carries a 2e-6 relative margin so that an exact FP64/FP32 filter
+// applied later (half-list export, force cutoffs) always sees a superset.
+__global__ void __launch_bounds__(SIM_THREADS) k_build_ell(SimEngine e, const int32_t* cell_lin,
+                                                          float rc2_list, const int32_t* gate) {
+    if (gate && __ldg(gate) == 0) return;
+    const int64_t P = e.n_pad;
+    const SimBox& b = *e.box;
+    const int nx = e.ncell[0], ny = e.ncell[1], nz = e.ncell[2];
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= e.n) return;
+    const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
+    const int4 qi = posq[i];
+    const int lin = cell_lin[e.cell_of[i]];
+    const int cx = lin % nx, cy = (lin / nx) % ny, cz = lin / (nx * ny);
+    int cnt = 0;
+    const int sx = stencil_count(nx), sy = stencil_count(ny), sz = stencil_count(nz);
+    for (int kz = 0; kz < sz; ++kz) {
+        int z = stencil_cell(cz, kz, nz);
+        for (int ky = 0; ky < sy; ++ky) {
+            int y = stencil_cell(cy, ky, ny);
+            for (int kx = 0; kx < sx; ++kx) {
+                int xx = stencil_cell(cx, kx, nx);
+                int r = e.cell_rank[xx + nx * (y + ny * z)];
+                int j0 = e.cell_start[r], j1 = e.cell_start[r + 1];
+                for (int j = j0; j < j1; ++j) {
+                    if (j == i) continue;
+                    const int4 qj = posq[j];
+                    float t0 = fixed_delta(qi.x, qj.x);
+                    float t1 = fixed_delta(qi.y, qj.y);
+                    float t2 = fixed_delta(qi.z, qj.z);
+                    float r0, r1, r2;
+                    frac_to_cart_f(b, t0, t1, t2, r0, r1, r2);
+                    float d2 = __fadd_rn(__fadd_rn(__fmul_rn(r0, r0), __fmul_rn(r1, r1)), __fmul_rn(r2, r2));
+                    if (d2 < rc2_list) {
+                        if (cnt < e.nbr_cap) e.nbr[(int64_t)cnt * P + i] = j;
+                        ++cnt;
+                    }
+                }
+            }
+        }
+    }
+    e.nnbr[i] = cnt < e.nbr_cap ? cnt : e.nbr_cap;
+    if (cnt > e.nbr_cap) {
+        atomicOr(&e.flags[1], SIM_STATUS_OVERFLOW);
+        atomicMax(&e.flags[2], cnt);
+    }
+}
+
+// Count the rebuild (flags[3]) when it ran and clear the request.
+__global__ void k_finish_rebuild(int32_t* flags, int gated) {
+    if (!gated || flags[0] != 0) flags[3] += 1;
+    flags[0] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// exact half-list export in the caller's dtype
+
+template <typename T> struct Exact;
+template <> struct Exact<float> {
+    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    static __device__ __forceinline__ float rnd(float a) { return rintf(a); }
+    static __device__ __forceinline__ float sqr(float a) { return __fsqrt_rn(a); }
+};
+template <> struct Exact<double> {
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+    static __device__ __forceinline__ double rnd(double a) { return rint(a); }
+    static __device__ __forceinline__ double sqr(double a) { return __dsqrt_rn(a); }
+};
+
+template <typename T>
+struct BoxT {
+    T H[9], Hi[9];
+    int orth;
+};
+
+// d^2 of the minimum image of pos_i - pos_j with the reference's op order.
+template <typename T>
+__device__ __forceinline__ T exact_d2(const BoxT<T>& b, const T* pi, const T* pj, int32_t* img) {
+    using X = Exact<T>;
+    T r[3], o[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r[k] = X::sub(pi[k], pj[k]);
+    if (b.orth) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            T d = b.H[4 * k];
+            T n = X::rnd(X::div(r[k], d));
+            o[k] = X::sub(r[k], X::mul(d, n));
+            img[k] = (int32_t)n;
+        }
+    } else {
+        T s[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            s[k] = X::fma(r[2], b.Hi[6 + k], X::fma(r[1], b.Hi[3 + k], X::mul(r[0], b.Hi[k])));
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            T n = X::rnd(s[k]);
+            img[k] = (int32_t)n;
+            s[k] = X::sub(s[k], n);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            o[k] = X::fma(s[2], b.H[6 + k], X::fma(s[1], b.H[3 + k], X::mul(s[0], b.H[k])));
+    }
+    return X::add(X::add(X::mul(o[0], o[0]), X::mul(o[1], o[1])), X::mul(o[2], o[2]));
+}
+
+template <typename T>
+__global__ void k_hl_bin(const T* __restrict__ pos, int64_t n, SimBox box, int3 nc,
+                         int32_t* cell_of, int32_t* cell_count) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double s[3];
+        cart_to_frac(box, (double)pos[3 * i], (double)pos[3 * i + 1], (double)pos[3 * i + 2], s);
+        int cx = cell_coord(s[0], nc.x), cy = cell_coord(s[1], nc.y), cz = cell_coord(s[2], nc.z);
+        int lin = cx + nc.x * (cy + nc.y * cz);
+        cell_of[i] = lin;
+        atomicAdd(&cell_count[lin], 1);
+    }
+}
+
+__global__ void k_hl_scatter(int64_t n, const int32_t* cell_of, const int32_t* cell_start,
+                             int32_t* cell_fill, int32_t* sorted_idx) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int c = cell_of[i];
+        sorted_idx[cell_start[c] + atomicAdd(&cell_fill[c], 1)] = (int32_t)i;
+    }
+}
+
+__global__ void k_hl_sort_cells(int n_cells, const int32_t* cell_start, int32_t* sorted_idx) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cells; c += gridDim.x * blockDim.x) {
+        int b0 = cell_start[c], b1 = cell_start[c + 1];
+        for (int a = b0 + 1; a < b1; ++a) {
+            int key = sorted_idx[a];
+            int p = a - 1;
+            while (p >= b0 && sorted_idx[p] > key) { sorted_idx[p + 1] = sorted_idx[p]; --p; }
+            sorted_idx[p + 1] = key;
+        }
+    }
+}
+
+template <typename T, bool FILL>
+__global__ void __launch_bounds__(SIM_THREADS) k_hl_pairs(const T* __restrict__ pos, int64_t n, BoxT<T> b,
+                                                          T rc2, int3 nc, const int32_t* __restrict__ cell_of,
+                                                          const int32_t* __restrict__ cell_start,
+                                                          const int32_t* __restrict__ sorted_idx,
+                                                          int64_t* row_cnt, const int64_t* __restrict__ row_ptr,
+                                                          int64_t* edge_i, int64_t* edge_j, int32_t* image,
+                                                          T* dist) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    T pi[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    const int lin = cell_of[i];
+    const int cx = lin % nc.x, cy = (lin / nc.x) % nc.y, cz = lin / (nc.x * nc.y);
+    int64_t cnt = 0;
+    int64_t base = FILL ? row_ptr[i] : 0;
+    const int sx = stencil_count(nc.x), sy = stencil_count(nc.y), sz = stencil_count(nc.z);
+    for (int kz = 0; kz < sz; ++kz) {
+        int z = stencil_cell(cz, kz, nc.z);
+        for (int ky = 0; ky < sy; ++ky) {
+            int y = stencil_cell(cy, ky, nc.y);
+            for (int kx = 0; kx < sx; ++kx) {
+                int c = stencil_cell(cx, kx, nc.x) + nc.x * (y + nc.y * z);
+                for (int a = cell_start[c]; a < cell_start[c + 1]; ++a) {
+                    int64_t j = sorted_idx[a];
+                    if (j <= i) continue;
+                    T pj[3] = {pos[3 * j], pos[3 * j + 1], pos[3 * j + 2]};
+                    int32_t img[3];
+                    T d2 = exact_d2<T>(b, pi, pj, img);
+                    if (d2 < rc2) {
+                        if (FILL) {
+                            int64_t e = base + cnt;
+                            edge_j[e] = j;
+                            if (image) { image[3 * e] = img[0]; image[3 * e + 1] = img[1]; image[3 * e + 2] = img[2]; }
+                            if (dist) dist[e] = Exact<T>::sqr(d2);
+                        }
+                        ++cnt;
+                    }
+                }
+            }
+        }
+    }
+    if (!FILL) { row_cnt[i] = cnt; return; }
+    // sort the row by j (insertion sort; rows are short), carrying image and dist
+    for (int64_t a = base + 1; a < base + cnt; ++a) {
+        int64_t kj = edge_j[a];
+        int32_t k0 = 0, k1 = 0, k2 = 0;
+        if (image) { k0 = image[3 * a]; k1 = image[3 * a + 1]; k2 = image[3 * a + 2]; }
+        T kd = dist ? dist[a] : (T)0;
+        int64_t p = a - 1;
+        while (p >= base && edge_j[p] > kj) {
+            edge_j[p + 1] = edge_j[p];
+            if (image) { image[3 * (p + 1)] = image[3 * p]; image[3 * (p + 1) + 1] = image[3 * p + 1]; image[3 * (p + 1) + 2] = image[3 * p + 2]; }
+            if (dist) dist[p + 1] = dist[p];
+            --p;
+        }
+        edge_j[p + 1] = kj;
+        if (image) { image[3 * (p + 1)] = k0; image[3 * (p + 1) + 1] = k1; image[3 * (p + 1) + 2] = k2; }
+        if (dist) dist[p + 1] = kd;
+    }
+    for (int64_t a = base; a < base + cnt; ++a) edge_i[a] = i;
+}
+
+template <typename T>
+BoxT<T> make_boxt(const SimBox& h) {
+    BoxT<T> b;
+    for (int k = 0; k < 9; ++k) { b.H[k] = (T)h.H[k]; b.Hi[k] = (T)h.Hinv[k]; }
+    b.orth = h.orthogonal;
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// engine list -> reference half list (pairs by original index, exact FP64 filter)
+
+template <bool FILL>
+__global__ void __launch_bounds__(SIM_THREADS) k_engine_half(SimEngine e, double rc2, int64_t* row_cnt,
+                                                             const int64_t* row_ptr, int64_t* edge_i,
+                                                             int64_t* edge_j, double* dist) {
+    int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= e.n) return;
+    const int64_t P = e.n_pad;
+    const SimBox& b = *e.box;
+    const int32_t oi = e.orig[s];
+    const double xi0 = e.x[s], xi1 = e.x[P + s], xi2 = e.x[2 * P + s];
+    const int nn = e.nnbr[s];
+    int64_t cnt = 0, base = FILL ? row_ptr[oi] : 0;
+    for (int k = 0; k < nn; ++k) {
+        int j = e.nbr[(int64_t)k * P + s];
+        int32_t oj = e.orig[j];
+        if (oj <= oi) continue;
+        double r0 = __dsub_rn(xi0, e.x[j]), r1 = __dsub_rn(xi1, e.x[P + j]), r2 = __dsub_rn(xi2, e.x[2 * P + j]);
+        min_image_f64(b, r0, r1, r2);
+        double d2 = norm2_f64(r0, r1, r2);
+        if (d2 < rc2) {
+            if (FILL) {
+                edge_j[base + cnt] = oj;
+                if (dist) dist[base + cnt] = __dsqrt_rn(d2);
+            }
+            ++cnt;
+        }
+    }
+    if (!FILL) { row_cnt[oi] = cnt; return; }
+    for (int64_t a = base + 1; a < base + cnt; ++a) {
+        int64_t kj = edge_j[a];
+        double kd = dist ? dist[a] : 0.0;
+        int64_t p = a - 1;
+        while (p >= base && edge_j[p] > kj) { edge_j[p + 1] = edge_j[p]; if (dist) dist[p + 1] = dist[p]; --p; }
+        edge_j[p + 1] = kj;
+        if (dist) dist[p + 1] = kd;
+    }
+    for (int64_t a = base; a < base + cnt; ++a) edge_i[a] = oi;
+}
+
+static int grid_for(int64_t n) {
+    int64_t g = ceil_div(n, SIM_THREADS);
+    return (int)(g < 1 ? 1 : (g > 148 * 32 ? 148 * 32 : g));
+}
+
+}  // namespace simb200
+
+using namespace simb200;
+
+extern "C" int sim_rebuild(const SimEngine* ep, int32_t only_if_flagged, void* stream) {
+    if (!ep || !ep->box || ep->n <= 0) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const SimEngine& e = *ep;
+    const int32_t* gate = only_if_flagged ? e.flags : nullptr;
+    const int g = grid_for(e.n);
+    // cell_count must be zero here: the scan of the previous rebuild leaves it zeroed,
+    // and sim_engine_load zeroes it before the first rebuild.
+    k_bin<<<g, SIM_THREADS, 0, st>>>(e, gate);
+    k_scan_exclusive<int32_t><<<1, 1024, 0, st>>>(e.cell_count, e.n_cells, e.cell_start, e.cell_count, gate);
+    k_scatter<<<g, SIM_THREADS, 0, st>>>(e, gate);
+    k_sort_cells<<<grid_for(e.n_cells), SIM_THREADS, 0, st>>>(e, gate);
+    k_permute<<<g, SIM_THREADS, 0, st>>>(e, gate);
+    k_commit<<<g, SIM_THREADS, 0, st>>>(e, gate);
+    // the scatter left cell_count == counts; zero them for the next rebuild
+    k_scan_exclusive<int32_t><<<1, 1024, 0, st>>>(e.cell_count, e.n_cells, e.cell_start, e.cell_count, gate);
+    k_slot_cells<<<g, SIM_THREADS, 0, st>>>(e, gate);
+    const float rc2_list = (float)(e.x_rc * e.x_rc * (1.0 + 4e-6));
+    // cell_lin (rank -> linear index) is stored right after cell_rank
+    k_build_ell<<<(int)ceil_div(e.n, SIM_THREADS), SIM_THREADS, 0, st>>>(e, e.cell_rank + e.n_cells, rc2_list, gate);
+    k_finish_rebuild<<<1, 1, 0, st>>>(e.flags, only_if_flagged ? 1 : 0);
+    return launch_status("sim_rebuild");
+}
+
+extern "C" int sim_half_list_count(const void* pos, int32_t dtype_code, int64_t n, const SimBox* box_host,
+                                   double rc2, const int32_t* ncell, int32_t* cell_of, int32_t* cell_count,
+                                   int32_t* cell_start, int32_t* sorted_idx, int64_t* row_ptr, void* stream) {
+    if (!pos || !box_host || !ncell || n < 0 || (dtype_code != 0 && dtype_code != 1)) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    int3 nc = make_int3(ncell[0], ncell[1], ncell[2]);
+    int n_cells = nc.x * nc.y * nc.z;
+    if (n == 0) {
+        cudaMemsetAsync(row_ptr, 0, sizeof(int64_t), st);
+        return launch_status("sim_half_list_count");
+    }
+    cudaMemsetAsync(cell_count, 0, sizeof(int32_t) * (n_cells + 1), st);
+    const int g = grid_for(n);
+    if (dtype_code == 0) k_hl_bin<float><<<g, SIM_THREADS, 0, st>>>((const float*)pos, n, *box_host, nc, cell_of, cell_count);
+    else k_hl_bin<double><<<g, SIM_THREADS, 0, st>>>((const double*)pos, n, *box_host, nc, cell_of, cell_count);
+    k_scan_exclusive<int32_t><<<1, 1024, 0, st>>>(cell_count, n_cells, cell_start, cell_count, nullptr);
+    k_hl_scatter<<<g, SIM_THREADS, 0, st>>>(n, cell_of, cell_start, cell_count, sorted_idx);
+    k_hl_sort_cells<<<grid_for(n_cells), SIM_THREADS, 0, st>>>(n_cells, cell_start, sorted_idx);
+    // row counts go to row_ptr[1..n] then an exclusive scan in place via a shifted copy
+    int64_t* cnt = row_ptr + 1;
+    const int gb = (int)ceil_div(n, SIM_THREADS);
+    if (dtype_code == 0)
+        k_hl_pairs<float, false><<<gb, SIM_THREADS, 0, st>>>((const float*)pos, n, make_boxt<float>(*box_host), (float)rc2, nc,
+                                                             cell_of, cell_start, sorted_idx, cnt, nullptr, nullptr, nullptr, nullptr, nullptr);
+    else
+        k_hl_pairs<double, false><<<gb, SIM_THREADS, 0, st>>>((const double*)pos, n, make_boxt<double>(*box_host), rc2, nc,
+                                                              cell_of, cell_start, sorted_idx, cnt, nullptr, nullptr, nullptr, nullptr, nullptr);
+    k_scan_exclusive<int64_t><<<1, 1024, 0, st>>>(cnt, n, row_ptr, nullptr, nullptr);
+    return launch_status("sim_half_list_count");
+}
+
+extern "C" int sim_half_list_fill(const void* pos, int32_t dtype_code, int64_t n, const SimBox* box_host,
+                                  double rc2, const int32_t* ncell, const int32_t* cell_start,
+                                  const int32_t* sorted_idx, const int32_t* cell_of, const int64_t* row_ptr,
+                                  int64_t* edge_i, int64_t* edge_j, int32_t* image, void* dist, void* stream) {
+    if (!pos || !box_host || !ncell || n < 0 || (dtype_code != 0 && dtype_code != 1)) return SIM_ERR_ARG;
+    if (n == 0) return SIM_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    int3 nc = make_int3(ncell[0], ncell[1], ncell[2]);
+    const int gb = (int)ceil_div(n, SIM_THREADS);
+    if (dtype_code == 0)
+        k_hl_pairs<float, true><<<gb, SIM_THREADS, 0, st>>>((const float*)pos, n, make_boxt<float>(*box_host), (float)rc2, nc,
+                                                            cell_of, cell_start, sorted_idx, nullptr, row_ptr, edge_i, edge_j, image, (float*)dist);
+    else
+        k_hl_pairs<double, true><<<gb, SIM_THREADS, 0, st>>>((const double*)pos, n, make_boxt<double>(*box_host), rc2, nc,
+                                                             cell_of, cell_start, sorted_idx, nullptr, row_ptr, edge_i, edge_j, image, (double*)dist);
+    return launch_status("sim_half_list_fill");
+}
+
+extern "C" int sim_engine_half_count(const SimEngine* ep, double rc2, int64_t* row_ptr, void* stream) {
+    if (!ep || !row_ptr) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const SimEngine& e = *ep;
+    k_engine_half<false><<<(int)ceil_div(e.n, SIM_THREADS), SIM_THREADS, 0, st>>>(e, rc2, row_ptr + 1, nullptr, nullptr, nullptr, nullptr);
+    k_scan_exclusive<int64_t><<<1, 1024, 0, st>>>(row_ptr + 1, e.n, row_ptr, nullptr, nullptr);
+    return launch_status("sim_engine_half_count");
+}
+
+extern "C" int sim_engine_half_fill(const SimEngine* ep, double rc2, const int64_t* row_ptr, int64_t* edge_i,
+                                    int64_t* edge_j, double* dist, void* stream) {
+    if (!ep || !row_ptr || !edge_i || !edge_j) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const SimEngine& e = *ep;
+    k_engine_half<true><<<(int)ceil_div(e.n, SIM_THREADS), SIM_THREADS, 0, st>>>(e, rc2, nullptr, row_ptr, edge_i, edge_j, dist);
+    return launch_status("sim_engine_half_fill");
+}
+
+extern "C" int sim_scan_i64(const int64_t* in, int64_t n, int64_t* out, void* stream) {
+    if (!in || !out || n < 0) return SIM_ERR_ARG;
+    k_scan_exclusive<int64_t><<<1, 1024, 0, (cudaStream_t)stream>>>(in, n, out, nullptr, nullptr);
+    return launch_status("sim_scan_i64");
+}

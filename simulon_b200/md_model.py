@@ -1,0 +1,141 @@
+"""Step model with the interface of core/md_model.py (SumBackboneInterface, BaseModel).
+
+``BaseModel.forward`` keeps the reference's order (md_model.py:88-166):
+first call computes forces; then first_half (with the skin/2 trigger and a
+conditional list rebuild) -> forces -> second_half -> optional Berendsen.
+Unlike the reference it makes no host synchronisation: every quantity stays
+on the device and the returned mapping materialises values when read.
+
+``BaseModel.run(n)`` executes n such steps through captured CUDA graphs
+(``graph_steps`` steps per graph), logging energy, kinetic energy, virial,
+pressure and the status word of every step into a device ring buffer.
+"""
+from __future__ import annotations
+
+import torch
+import torch.nn as nn
+
+from . import _lib
+from .forces import BackboneInterface, LazyOutputs
+from .integrator import IntegratorInterface
+
+__all__ = ["BackboneInterface", "IntegratorInterface", "SumBackboneInterface", "BaseModel"]
+
+
+class SumBackboneInterface(nn.Module):
+    """Sum of force-field backbones (md_model.py:19-52).  One device
+    backbone per system is supported (its outputs are returned as they are)."""
+
+    def __init__(self, backbones, molecular):
+        super().__init__()
+        self.backbones = nn.ModuleList(backbones)
+        self.molecular = molecular
+        self.device = molecular.device
+        self.atom_num = molecular.atom_count
+        if len(self.backbones) != 1:
+            raise NotImplementedError("exactly one device force field per system is supported")
+        self.force_precision = getattr(self.backbones[0], "force_precision", 0)
+
+    def compute(self):
+        self.backbones[0].compute()
+
+    def forward(self):
+        return self.backbones[0]()
+
+
+class BaseModel(nn.Module):
+    def __init__(self, sum_bone, integrator, molecular, barostat=None):
+        super().__init__()
+        self.sum_bone = sum_bone
+        self.Integrator = integrator
+        self.molecular = molecular
+        self.barostat = barostat
+        self.engine = molecular.engine
+        integrator.force_precision = sum_bone.force_precision
+        self._first_call = True
+        self.steps_done = 0
+        self.profile = {"pair_time": 0.0, "integrate_time": 0.0, "pair_calls": 0, "integrate_calls": 0}
+        self._graphs = {}
+
+    # one step, launches only (no host sync)
+    def _step_launches(self):
+        self.Integrator.first_half()
+        self.sum_bone.compute()
+        self.Integrator.second_half()
+        if self.barostat is not None:
+            self.barostat.step(self.Integrator.dt)
+        self.engine.log_step()
+
+    def _outputs(self):
+        eng, mol = self.engine, self.molecular
+        dt = mol.dtype
+        red = eng.red_out
+        n = mol.atom_count
+        kB = self.Integrator.BOLTZMAN
+        ke = lambda: red[_lib.RED_KE].to(dt)
+        prod = dict(forces=lambda: eng.gather("f").to(dt),
+                    energy=lambda: eng.potential_energy().to(dt),
+                    virial=lambda: red[_lib.RED_VIRIAL].to(dt),
+                    virial_tensor=lambda: eng.virial_tensor().to(dt),
+                    updated_coordinates=lambda: mol.coordinates,
+                    kinetic_energy=ke,
+                    temperature=lambda: (2.0 / 3.0) * ke() / (n * kB))
+        if self.barostat is not None:
+            prod["pressure"] = lambda: eng.extra[0]
+        return LazyOutputs(**prod)
+
+    def _prime(self):
+        # forces of the current positions are needed by the first half step:
+        # on the first call (md_model.py:91-102) and after coordinates were replaced
+        if self._first_call or not self.engine.forces_valid:
+            self.sum_bone.compute()
+            self._first_call = False
+
+    def forward(self):
+        self._prime()
+        self._step_launches()
+        self.steps_done += 1
+        self.profile["pair_calls"] += 1
+        self.profile["integrate_calls"] += 1
+        return self._outputs()
+
+    # ---- graph-captured multi-step execution ------------------------------
+    def _graph(self, k: int):
+        if k not in self._graphs:
+            s = torch.cuda.Stream(self.engine.device)
+            s.wait_stream(torch.cuda.current_stream(self.engine.device))
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                for _ in range(k):
+                    self._step_launches()
+            torch.cuda.current_stream(self.engine.device).wait_stream(s)
+            self._graphs[k] = g
+        return self._graphs[k]
+
+    def run(self, n_steps: int, graph_steps: int = 20):
+        """Advance n_steps with CUDA graphs (no host sync); returns the last outputs.
+
+        Capturing records launches without executing them, so the device state
+        is unchanged by the capture itself.
+        """
+        self._prime()
+        full, rest = divmod(int(n_steps), int(graph_steps))
+        if full:
+            g = self._graph(int(graph_steps))
+            for _ in range(full):
+                g.replay()
+        for _ in range(rest):
+            self._step_launches()
+        self.steps_done += int(n_steps)
+        self.profile["pair_calls"] += int(n_steps)
+        self.profile["integrate_calls"] += int(n_steps)
+        return self._outputs()
+
+    def step_log(self, first_step: int, count: int) -> torch.Tensor:
+        """Rows of the per-step device log for steps [first_step, first_step+count)
+        (columns: reduction slots, pressure, mu, status)."""
+        cap = self.engine.log_capacity
+        if count > cap:
+            raise ValueError("log window exceeds the ring buffer")
+        idx = torch.arange(first_step, first_step + count, device=self.engine.device) % cap
+        return self.engine.log[idx]

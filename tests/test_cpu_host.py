@@ -1,0 +1,145 @@
+"""CPU-only checks: the C-ABI library loads and exports every declared entry
+point, the ctypes struct layouts match the C ones, and the host-side logic
+(cell grid, Morton order, rc^2 formation, EAM file parsing and table
+construction, LJ constants) agrees with the oracle.  No GPU compute calls."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import eam as oeam
+from oracle import inputs as oin
+from oracle import neighbor as onb
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from simulon_b200 import build, _lib
+    build.build()
+    return _lib.load()
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "simb200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(sim_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol(lib):
+    from simulon_b200 import _lib
+    names = declared_symbols()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, f"{name} not bound in simulon_b200._lib"
+
+
+def test_struct_layouts_match(lib):
+    from simulon_b200 import _lib
+    out = np.zeros(6, np.int64)
+    assert lib.sim_struct_sizes(out.ctypes.data, 6) == 0
+    assert list(out) == [ctypes.sizeof(s) for s in _lib.STRUCTS]
+    assert lib.sim_version() == 1
+
+
+def test_argument_errors_are_reported_without_gpu(lib):
+    from simulon_b200 import _lib
+    assert lib.sim_rebuild(None, 0, None) == _lib.SIM_ERR_ARG
+    assert lib.sim_legacy_density_pass(None, None, None, None, 0, None, 1, 1.0, 1, None, None) == _lib.SIM_ERR_ARG
+    assert lib.sim_legacy_density_pass(None, None, None, None, 0, None, 1, 1.0, 8, None, None) == _lib.SIM_OK
+    with pytest.raises(_lib.SimError):
+        _lib.check(_lib.SIM_ERR_ARG, "probe")
+
+
+def test_cell_grid_and_morton_order():
+    from simulon_b200.engine import cell_grid, morton_rank, estimate_capacity, perpendicular_widths
+    L = 80 * 3.165
+    nc = cell_grid(np.diag([L] * 3), 4.9, 1_024_000)
+    assert list(nc) == [51, 51, 51]
+    H = oin.triclinic_box(L)
+    w = perpendicular_widths(H)
+    assert np.all(w / cell_grid(H, 4.9, 1_024_000) >= 4.9)
+    r, lin = morton_rank(np.array([5, 6, 7]))
+    assert sorted(r.tolist()) == list(range(210)) and np.array_equal(r[lin], np.arange(210))
+    # consecutive ranks are spatial neighbours most of the time
+    cx, cy, cz = lin % 5, (lin // 5) % 6, lin // 30
+    steps = np.abs(np.diff(cx)) + np.abs(np.diff(cy)) + np.abs(np.diff(cz))
+    assert np.mean(steps == 1) > 0.5
+    assert estimate_capacity(16000, np.diag([63.3] * 3), 4.9) >= 32
+    assert list(cell_grid(np.diag([15.78] * 3), 7.5, 108)) == [2, 2, 2]
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_reference_rc2(dtype):
+    from simulon_b200.neighbor import reference_rc2
+    cut = torch.tensor(4.4, dtype=dtype) + torch.tensor(0.5, dtype=dtype)
+    npd = np.float32 if dtype == torch.float32 else np.float64
+    assert reference_rc2(cut, dtype) == onb.rc2_like_reference(4.4, 0.5, npd)
+
+
+@pytest.fixture(scope="module")
+def pot(tmp_path_factory):
+    return oin.write_fs_w_setfl(str(tmp_path_factory.mktemp("pot") / "W_synthetic.eam.fs"))
+
+
+def test_eam_parser_matches_oracle(pot):
+    from simulon_b200 import EAMParser
+    a, b = EAMParser(pot), oeam.parse_eam(pot)
+    assert a.elements == b.elements and a.is_fs_format == b.is_fs_format and a.cutoff == b.cutoff
+    for name in ("embedding_splines", "density_splines", "density_deriv_splines"):
+        assert np.array_equal(getattr(a, name)[0].c, getattr(b, name)[0].c)
+    assert np.array_equal(a.pair_potential_splines[0][0].c, b.pair_potential_splines[0][0].c)
+
+
+def test_device_tables_match_oracle_fp64(pot):
+    from simulon_b200 import EAMParser, EAMDeviceTables
+    t = EAMDeviceTables(EAMParser(pot), "cpu")
+    o = oeam.EAMTables(oeam.parse_eam(pot), dtype=torch.float64)
+    for mine, theirs in (("density", o.density), ("density_deriv", o.density_deriv), ("pair", o.pair),
+                         ("pair_deriv", o.pair_deriv), ("embed", o.embed), ("embed_deriv", o.embed_deriv)):
+        np.testing.assert_allclose(t.host64[mine], theirs.numpy(), rtol=1e-13, atol=1e-12)
+    assert abs(t.inv_dr - o.inv_dr) < 1e-9 and t.rho_min64[0] == o.rho_min[0]
+
+
+def test_alloy_and_setfl_formats(tmp_path):
+    """Two-element eam/alloy and single-element setfl files parse like the oracle."""
+    from simulon_b200 import EAMParser
+    nr, nrho = 200, 150
+    r = np.arange(nr) * 0.03
+    rho = np.arange(nrho) * 0.2
+    lines = ["c1", "c2", "c3", "2 Ni Al", f"{nrho} 0.2 {nr} 0.03 5.97", "28 58.69 3.52 fcc"]
+    blocks = [-np.sqrt(rho), np.exp(-r), "13 26.98 4.05 fcc", -0.8 * np.sqrt(rho), 0.7 * np.exp(-r),
+              r * np.exp(-2 * r), r * 0.5 * np.exp(-2 * r), r * 0.25 * np.exp(-2 * r)]
+    for b in blocks:
+        if isinstance(b, str):
+            lines.append(b)
+        else:
+            lines += [" ".join(repr(float(v)) for v in b[k:k + 4]) for k in range(0, len(b), 4)]
+    path = tmp_path / "NiAl.eam.alloy"
+    path.write_text("\n".join(lines) + "\n")
+    a, b = EAMParser(str(path)), oeam.parse_eam(str(path))
+    assert a.elements == ["Ni", "Al"] and not a.is_fs_format and not b.is_fs_format
+    assert np.array_equal(a.pair_potential_splines[0][1].c, b.pair_potential_splines[0][1].c)
+    assert np.array_equal(a.density_splines_by_pair[0][1].c, b.density_splines_by_pair[0][1].c)
+
+
+def test_lj_constants_follow_reference_float32():
+    from simulon_b200.forces import lj_type_pair_params
+    p = lj_type_pair_params({"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}}, 1, 7.0, "cpu")
+    eps = torch.tensor([0.0104], dtype=torch.float32)
+    assert float(p["c24eps"]) == float(24.0 * eps)            # formed in float32, as the reference
+    assert float(p["sigma"]) == float(np.float32(3.405))
+    sr = torch.tensor([3.405], dtype=torch.float32) / 7.0
+    assert float(p["f_rc"]) == float(24.0 * eps * (1.0 / 7.0) * (2.0 * (sr ** 6) ** 2 - sr ** 6))
+
+
+def test_product_path_refuses_cpu():
+    import simulon_b200 as sb
+    x, L = oin.bcc_lattice(3)
+    with pytest.raises(RuntimeError):
+        sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], np.diag([L] * 3), 4.4, 0.5, device="cpu")

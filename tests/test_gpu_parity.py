@@ -1,0 +1,308 @@
+"""GPU parity: the CUDA path (through libsimb200's C ABI) against the oracle
+and against golden vectors produced by the reference itself.
+
+Tolerances (stated per test):
+  * neighbour pair sets: bit-exact, including the integer image of each pair;
+  * EAM forces vs the FP64 oracle: RMSE <= 1e-5 eV/A (the plain-path target),
+    energy per atom within 2e-6 eV;
+  * LJ FP64 vs the reference's FP64 path: 1e-10 relative;
+  * MD trajectories: FP64 LJ NVE/NVT within 1e-8 A after 30 steps (NVT uses
+    the same Philox noise as the replayed reference run).
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import eam as oeam
+from oracle import inputs as oin
+from oracle import neighbor as onb
+from oracle.box import OracleBox
+from oracle.philox import langevin_normals
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+DEV = torch.device("cuda")
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLD, name + ".npz")))
+
+
+@pytest.fixture(scope="module")
+def sb():
+    import simulon_b200
+    simulon_b200._lib.load()
+    return simulon_b200
+
+
+@pytest.fixture(scope="module")
+def fsw_path(tmp_path_factory):
+    return oin.write_fs_w_setfl(str(tmp_path_factory.mktemp("pot") / "W_synthetic.eam.fs"))
+
+
+# ---------------------------------------------------------------- neighbours
+NBR = ["nbr_ar108_f64", "nbr_w250_f32", "nbr_wtri432_f32", "nbr_wtri432_f64", "nbr_gas300_orth_f32",
+       "nbr_pair2_f64", "nbr_far3_f32"]
+
+
+@pytest.mark.parametrize("name", NBR)
+def test_half_list_matches_reference_bit_exact(sb, name):
+    g = load(name)
+    pos = torch.tensor(g["pos"], device=DEV)
+    dt = pos.dtype
+    cutoff = torch.tensor(float(g["cutoff"]), dtype=dt) + torch.tensor(float(g["skin"]), dtype=dt)
+    ei, dist, img = sb.find_neighbors_gpu_pbc(pos, cutoff, OracleBox(g["box"]), return_image=True)
+    assert np.array_equal(ei[0].cpu().numpy(), g["i"]) and np.array_equal(ei[1].cpu().numpy(), g["j"])
+    o = onb.half_list(g["pos"], OracleBox(g["box"]), onb.rc2_like_reference(float(g["cutoff"]), float(g["skin"]),
+                                                                           g["pos"].dtype))
+    assert np.array_equal(img.cpu().numpy(), o["image"])
+    if len(g["i"]):
+        np.testing.assert_allclose(dist.cpu().numpy(), g["dist"], rtol=1e-6 if dt == torch.float32 else 1e-14)
+
+
+@pytest.mark.parametrize("dtype,tri", [(np.float32, False), (np.float64, True), (np.float32, True)])
+def test_half_list_large_matches_oracle(sb, dtype, tri):
+    if tri:
+        x, H = oin.bcc_triclinic(16)
+    else:
+        x, L = oin.bcc_lattice(20)
+        H = np.diag([L, L, L])
+    x = oin.jitter(x, 0.08, 21).astype(dtype)
+    rc2 = onb.rc2_like_reference(4.4, 0.5, dtype)
+    o = onb.half_list(x, OracleBox(H), rc2, mode="cell")
+    ei, _, img = sb.neighbor.half_list(torch.tensor(x, device=DEV), rc2, H, return_image=True)
+    assert np.array_equal(ei[0].cpu().numpy(), o["i"]) and np.array_equal(ei[1].cpu().numpy(), o["j"])
+    assert np.array_equal(img.cpu().numpy(), o["image"])
+
+
+def test_engine_list_export_matches_oracle(sb):
+    x, L = oin.bcc_lattice(12)
+    x = oin.jitter(x, 0.1, 22)
+    eng = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], np.diag([L] * 3), 4.4, 0.5, device=DEV)
+    ei, dist = eng.half_list(4.9 ** 2)
+    o = onb.half_list(x, OracleBox(L), 4.9 ** 2)
+    assert np.array_equal(ei[0].cpu().numpy(), o["i"]) and np.array_equal(ei[1].cpu().numpy(), o["j"])
+    assert eng.status() == 0
+    # slots are a permutation of the atoms and positions round-trip exactly
+    assert torch.equal(eng.gather("x").cpu(), torch.tensor(x))
+
+
+# ---------------------------------------------------------------- EAM
+def _eam_engine(sb, fsw_path, x, H, v=None):
+    parser = sb.EAMParser(fsw_path)
+    tables = sb.EAMDeviceTables(parser, DEV)
+    eng = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], H, parser.cutoff, 0.5, velocities=v, device=DEV)
+    return eng, tables, parser
+
+
+def _oracle_eam64(fsw_path, x, H):
+    p = oeam.parse_eam(fsw_path)
+    t64 = oeam.EAMTables(p, dtype=torch.float64)
+    box = OracleBox(H)
+    hl = onb.half_list(np.asarray(x, np.float64), box, 4.9 ** 2)
+    return oeam.eam_forward(torch.tensor(x, dtype=torch.float64), hl["i"], hl["j"], np.zeros(len(x), np.int64),
+                            box, t64)
+
+
+@pytest.mark.parametrize("n,tri", [(5, False), (20, False), (8, True)])
+def test_eam_forces_vs_fp64_oracle(sb, fsw_path, n, tri):
+    if tri:
+        x, H = oin.bcc_triclinic(n)
+    else:
+        x, L = oin.bcc_lattice(n)
+        H = np.diag([L] * 3)
+    x = oin.jitter(x, 0.06, 30 + n)
+    eng, tables, _ = _eam_engine(sb, fsw_path, x, H)
+    eng.eam_forces(tables)
+    f = eng.gather("f").cpu().numpy()
+    e = float(eng.potential_energy())
+    o = _oracle_eam64(fsw_path, x, H)
+    rmse = float(np.sqrt(((f - o["forces"].numpy()) ** 2).mean()))
+    assert rmse <= 1e-5, rmse
+    assert abs(e - float(o["energy"])) / len(x) < 2e-6
+    red = eng.red_out.cpu().numpy()
+    W = o["virial_tensor"].numpy()
+    np.testing.assert_allclose(red[3:6], np.diag(W), rtol=2e-5, atol=1e-3)
+    np.testing.assert_allclose(red[6:9], [W[0, 1], W[0, 2], W[1, 2]], atol=1e-3)
+    np.testing.assert_allclose(red[2], float(o["virial"]), rtol=2e-5, atol=1e-3)
+    np.testing.assert_allclose(red[0], float(o["embedding_energy"]), rtol=1e-6)
+    assert eng.status() == 0
+
+
+def test_eam_vs_reference_golden(sb, fsw_path):
+    for name in ("eam_w250_jitter_f32", "eam_wtri432_f32"):
+        g = load(name)
+        eng, tables, _ = _eam_engine(sb, fsw_path, g["pos"].astype(np.float64), g["box"])
+        eng.eam_forces(tables)
+        f = eng.gather("f").cpu().numpy()
+        # the reference path is FP32 throughout; agreement at its round-off
+        assert np.sqrt(((f - g["forces"]) ** 2).mean()) < 5e-5
+        assert abs(float(eng.potential_energy()) - float(g["energy"])) / len(f) < 5e-6
+
+
+def test_eam_perfect_lattice_known_answer(sb, fsw_path):
+    x, L = oin.bcc_lattice(10)
+    eng, tables, _ = _eam_engine(sb, fsw_path, x, np.diag([L] * 3))
+    eng.eam_forces(tables)
+    _, _, _, e_atom = oin.perfect_bcc_known_answer()
+    assert abs(float(eng.potential_energy()) / len(x) - e_atom) < 1e-5
+    assert float(eng.gather("f").abs().max()) < 1e-5
+
+
+def test_eam_reruns_bitwise_identical(sb, fsw_path):
+    x, L = oin.bcc_lattice(16)
+    x = oin.jitter(x, 0.07, 40)
+    outs = []
+    for _ in range(2):
+        eng, tables, _ = _eam_engine(sb, fsw_path, x, np.diag([L] * 3))
+        eng.eam_forces(tables)
+        outs.append((eng.gather("f").cpu(), eng.red_out.cpu()))
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+
+
+# ---------------------------------------------------------------- LJ
+def _lj_system(sb, tmp_path, x, L, mode, dtype):
+    torch.set_default_dtype(dtype)
+    try:
+        path = oin.write_xyz(str(tmp_path / "ar.xyz"), x, "Ar")
+        mol = sb.AtomFileReader(path, L, 7.0, device=DEV, parameter={"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}},
+                                skin_thickness=0.5, is_fs=mode == "fs", is_switch=mode == "switch")
+        return mol, sb.LennardJonesForce(mol)
+    finally:
+        torch.set_default_dtype(torch.float32)
+
+
+@pytest.mark.parametrize("mode", ["raw", "fs", "switch"])
+def test_lj_fp64_matches_reference(sb, tmp_path, mode):
+    g = load(f"lj_ar108_{mode}_f64")
+    mol, ff = _lj_system(sb, tmp_path, g["pos"], float(g["box"][0, 0]), mode, torch.float64)
+    out = ff()
+    np.testing.assert_allclose(float(out["energy"]), float(g["energy"]), rtol=1e-11)
+    np.testing.assert_allclose(out["forces"].cpu().numpy(), g["forces"], rtol=1e-9, atol=1e-13)
+    np.testing.assert_allclose(float(out["virial"]), float(g["virial"]), rtol=1e-11)
+    np.testing.assert_allclose(out["virial_tensor"].cpu().numpy(), g["virial_tensor"], rtol=1e-10, atol=1e-13)
+
+
+@pytest.mark.parametrize("mode", ["raw", "fs", "switch"])
+def test_lj_fp32_pairs_match_reference(sb, tmp_path, mode):
+    g = load(f"lj_ar108_{mode}_f64")
+    mol, ff = _lj_system(sb, tmp_path, g["pos"], float(g["box"][0, 0]), mode, torch.float32)
+    out = ff()
+    assert abs(float(out["energy"]) - float(g["energy"])) < 2e-6 * abs(float(g["energy"])) + 1e-6
+    f = out["forces"].double().cpu().numpy()
+    assert np.sqrt(((f - g["forces"]) ** 2).mean()) < 2e-6
+
+
+# ---------------------------------------------------------------- MD
+@pytest.mark.parametrize("ens", ["nve", "nvt"])
+def test_md_lj_fp64_matches_reference_trajectory(sb, tmp_path, ens):
+    g = load(f"md_ar108_{ens}_f64")
+    torch.set_default_dtype(torch.float64)
+    try:
+        path = oin.write_xyz(str(tmp_path / "ar.xyz"), g["x0"], "Ar")
+        mol = sb.AtomFileReader(path, float(g["box"]), 7.0, device=DEV,
+                                parameter={"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}}, skin_thickness=0.5)
+        integ = sb.VerletIntegrator(mol, dt=float(g["dt"]), ensemble=ens.upper(),
+                                    temperature=(94.4, 94.4) if ens == "nvt" else None,
+                                    gamma=10.0 if ens == "nvt" else None, seed=int(g["noise_seed"]))
+        mol.atom_velocities = torch.tensor(g["v0"], device=DEV)
+        model = sb.BaseModel(sb.SumBackboneInterface([sb.LennardJonesForce(mol)], mol), integ, mol)
+        e, k = [], []
+        for _ in range(int(g["steps"])):
+            out = model()
+            e.append(float(out["energy"]))
+            k.append(float(out["kinetic_energy"]))
+        np.testing.assert_allclose(e, g["energy"], rtol=1e-9)
+        np.testing.assert_allclose(k, g["kinetic_energy"], rtol=1e-7 if ens == "nvt" else 1e-9)
+        np.testing.assert_allclose(mol.coordinates.cpu().numpy(), g["x"], atol=1e-8)
+        np.testing.assert_allclose(mol.atom_velocities.cpu().numpy(), g["v"], atol=1e-7)
+    finally:
+        torch.set_default_dtype(torch.float32)
+
+
+@pytest.mark.parametrize("ens", ["nve", "npt"])
+def test_md_eam_matches_reference_trajectory(sb, fsw_path, tmp_path, ens):
+    g = load(f"md_w250_{ens}_f32")
+    path = oin.write_xyz(str(tmp_path / "w.xyz"), g["x0"], "W")
+    parser = sb.EAMParser(fsw_path)
+    mol = sb.AtomFileReader(path, float(g["box0"]), parser.cutoff, device=DEV, skin_thickness=0.5, is_fs=True)
+    integ = sb.VerletIntegrator(mol, dt=float(g["dt"]), ensemble="NPT" if ens == "npt" else "NVE",
+                                temperature=(300.0, 300.0) if ens == "npt" else None,
+                                gamma=10.0 if ens == "npt" else None, seed=int(g["noise_seed"]))
+    mol.atom_velocities = torch.tensor(g["v0"].astype(np.float32), device=DEV)
+    baro = sb.BerendsenBarostat(mol, 0.0, float(g["tau_p"])) if ens == "npt" else None
+    model = sb.BaseModel(sb.SumBackboneInterface([sb.EAMForceCUDAExt(parser, mol)], mol), integ, mol, barostat=baro)
+    e, p = [], []
+    for _ in range(int(g["steps"])):
+        out = model()
+        e.append(float(out["energy"]))
+        if baro is not None:
+            p.append(float(out["pressure"]))
+    # the reference integrates in FP32 here; the device keeps FP64 state
+    np.testing.assert_allclose(e, g["energy"], rtol=2e-5)
+    if baro is not None:
+        np.testing.assert_allclose(p, g["pressure"], rtol=2e-3, atol=100.0)
+        np.testing.assert_allclose(mol.engine.box_matrix(), g["box"], rtol=2e-6)
+    np.testing.assert_allclose(mol.coordinates.cpu().numpy(), g["x"], atol=5e-4)
+
+
+def test_graph_run_matches_eager_steps(sb, fsw_path):
+    x, L = oin.bcc_lattice(10)
+    x = oin.jitter(x, 0.05, 50)
+    v = oin.maxwell_boltzmann(np.full(len(x), oin.W_MASS), 600.0, 51)
+    res = []
+    for use_graph in (False, True):
+        eng, tables, parser = _eam_engine(sb, fsw_path, x, np.diag([L] * 3), v)
+        # drive the engine with an NVT integrator (exercises noise + conditional rebuilds)
+        from simulon_b200.engine import integrator_params
+        integ = integrator_params(eng, 0.002, langevin=True, temperature=600.0, gamma=10.0, seed=7)
+        eng.eam_forces(tables)
+        steps = 60
+        if use_graph:
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                for _ in range(20):
+                    eng.integrate_first(integ, 0)
+                    eng.rebuild(True)
+                    eng.eam_forces(tables)
+                    eng.integrate_second(integ, 0)
+            torch.cuda.current_stream().wait_stream(s)
+            for _ in range(steps // 20):
+                g.replay()
+        else:
+            for _ in range(steps):
+                eng.integrate_first(integ, 0)
+                eng.rebuild(True)
+                eng.eam_forces(tables)
+                eng.integrate_second(integ, 0)
+        torch.cuda.synchronize()
+        res.append((eng.gather("x").cpu(), eng.gather("v").cpu(), int(eng.flags[3].item())))
+    assert torch.equal(res[0][0], res[1][0]) and torch.equal(res[0][1], res[1][1])
+    assert res[0][2] == res[1][2] and res[0][2] >= 2      # the load rebuild plus at least one triggered
+
+
+def test_langevin_noise_matches_oracle_philox(sb, fsw_path):
+    """One NVT step from rest with zero forces isolates the noise: v = xi * rff."""
+    x, L = oin.bcc_lattice(6)
+    eng, tables, parser = _eam_engine(sb, fsw_path, x, np.diag([L] * 3))
+    from simulon_b200.engine import integrator_params
+    integ = integrator_params(eng, 0.002, langevin=True, temperature=300.0, gamma=10.0, seed=123456789)
+    eng.f32.zero_()
+    eng.integrate_first(integ, 0)
+    eng.integrate_second(integ, 0)
+    v = eng.gather("v").cpu().numpy()
+    z = langevin_normals(len(x), 0, 123456789)
+    rff = integ.keep[0].cpu().numpy()[0]
+    np.testing.assert_allclose(v, z * rff, rtol=1e-6, atol=1e-12)
+
+
+def test_neighbor_overflow_is_detected_and_grown(sb, fsw_path):
+    x, L = oin.bcc_lattice(8)
+    eng = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], np.diag([L] * 3), 4.4, 0.5, device=DEV, nbr_cap=8)
+    assert eng.nbr_cap >= 26 and eng.status() & sb._lib.SIM_STATUS_OVERFLOW == 0
+    assert eng.neighbor_stats()["max"] == 26
