@@ -306,7 +306,9 @@ def run_b200(args):
             "step_roofline": {"bytes_per_atom_step": B_step, "achieved": step_achieved, "peak": peak,
                               "frac": step_achieved / peak, "unit": "GB/s"},
             "clocks": clocks.summary(),
-            "gpu_launches": 15 * args.steps}
+            # per step: first half, IF-node condition, EAM pass 1, pass 2 + second half, step log;
+            # each triggered rebuild adds its 10 kernels (the IF body)
+            "gpu_launches": 5 * args.steps + 10 * rebuilds}
 
     if not args.no_extras and rank == 0:
         line["e2e"] = e2e(model, mol, x, v, args, dev)

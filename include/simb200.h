@@ -233,6 +233,12 @@ int sim_engine_load(const SimEngine* e, const double* x_rows, const double* v_ro
  * kernels read flags[0] and do nothing unless a rebuild was requested. */
 int sim_rebuild(const SimEngine* e, int32_t only_if_flagged, void* stream);
 
+/* Rebuild only if flags[0] is set.  While `stream` is being captured into a
+ * CUDA graph this adds a one-thread kernel and an IF conditional node whose
+ * body is the rebuild (so a step without a rebuild launches one tiny kernel);
+ * otherwise it is sim_rebuild(e, 1, stream). */
+int sim_rebuild_if_needed(const SimEngine* e, void* stream);
+
 /* EAM forces on the engine state.  Writes f32 (or f64), fp, and the
  * reduction slots EPOT_*, VIRIAL, W_* (red_out).  Scalar virial follows the
  * reference's EAM convention: sum over pairs of s*r (eam_force_cu.py:569). */
@@ -241,6 +247,10 @@ int sim_eam_forces(const SimEngine* e, const SimEAMTables* t, void* stream);
  * and EPOT_EMBED; pass 2 needs pass 1's fp of the same positions). */
 int sim_eam_density(const SimEngine* e, const SimEAMTables* t, void* stream);
 int sim_eam_force(const SimEngine* e, const SimEAMTables* t, void* stream);
+/* Pass 2 with the second half of the velocity-Verlet step (Langevin O-step,
+ * half kick, K and K tensor) fused into its epilogue; equivalent to
+ * sim_eam_force followed by sim_integrate_second with FP32 forces. */
+int sim_eam_force_integrate(const SimEngine* e, const SimEAMTables* t, const SimIntegrator* p, void* stream);
 
 /* LJ forces; precision 0 = FP32 pair arithmetic, 1 = FP64 (positions read
  * from e->x, forces to e->f64).  Scalar virial = sum F*r (lennard_jones_force.py:93). */

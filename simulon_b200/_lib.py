@@ -92,9 +92,11 @@ SIGNATURES = {
                            c_p, c_p, c_p, c_p, c_p, c_p, c_p],
     "sim_engine_load": [_P(SimEngine), c_p, c_p, c_p, c_p],
     "sim_rebuild": [_P(SimEngine), ctypes.c_int32, c_p],
+    "sim_rebuild_if_needed": [_P(SimEngine), c_p],
     "sim_eam_forces": [_P(SimEngine), _P(SimEAMTables), c_p],
     "sim_eam_density": [_P(SimEngine), _P(SimEAMTables), c_p],
     "sim_eam_force": [_P(SimEngine), _P(SimEAMTables), c_p],
+    "sim_eam_force_integrate": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), c_p],
     "sim_lj_forces": [_P(SimEngine), _P(SimLJParams), ctypes.c_int32, c_p],
     "sim_integrate_first": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_integrate_second": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],

@@ -11,6 +11,7 @@ namespace simb200 {
 // ---- error plumbing --------------------------------------------------------
 void set_cuda_error(cudaError_t err, const char* where);
 int  launch_status(const char* where);   // checks cudaGetLastError after a launch
+void prepare_capture_stream();           // side stream used to capture IF-node bodies
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
@@ -158,6 +159,36 @@ __device__ __forceinline__ void langevin_normals(uint32_t a, uint64_t step, uint
     z0 = __fmul_rn(r0, c0);
     z1 = __fmul_rn(r0, s0);
     z2 = __fmul_rn(r1, c1);
+}
+
+// Second half of velocity Verlet for slot i (integrator.py:102-124):
+//   v = v_half * damp + xi * rff   (Langevin, noise by original index and step)
+//   v = v + (0.5 * F/m) * dt
+// Writes e.v and returns the new velocity in v_out.
+__device__ __forceinline__ void second_half_atom(const SimEngine& e, const SimIntegrator& p, int64_t i, int type,
+                                                 uint64_t step, double f0, double f1, double f2, double* v_out,
+                                                 bool& bad) {
+    const int64_t P = e.n_pad;
+    const double m = e.mass[type];
+    double z[3] = {0.0, 0.0, 0.0};
+    double rff = 0.0;
+    if (p.langevin) {
+        float z0, z1, z2;
+        langevin_normals((uint32_t)e.orig[i], step, p.seed, z0, z1, z2);
+        z[0] = z0; z[1] = z1; z[2] = z2;
+        rff = p.rff[type];
+    }
+    const double f[3] = {f0, f1, f2};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double vel = e.v[c * P + i];
+        if (p.langevin) vel = __dadd_rn(__dmul_rn(vel, p.damp), __dmul_rn(z[c], rff));
+        const double a = __ddiv_rn(f[c], m);
+        vel = __dadd_rn(vel, __dmul_rn(__dmul_rn(0.5, a), p.dt));
+        e.v[c * P + i] = vel;
+        v_out[c] = vel;
+        bad |= !isfinite(vel);
+    }
 }
 
 }  // namespace simb200

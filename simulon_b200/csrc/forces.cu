@@ -59,7 +59,9 @@ __device__ __forceinline__ void pair_vector(const SimBox& b, const int4& qi, con
 }
 
 // ---------------------------------------------------------------------------
-// EAM pass 1: density, embedding, F'(rho)
+// EAM pass 1: density, embedding, F'(rho).
+// Persistent grid (a few blocks per SM): each block stages the density table
+// in shared memory once and then walks atom tiles with a grid stride.
 template <bool SMEM>
 __global__ void __launch_bounds__(SIM_THREADS) k_eam_density(SimEngine e, SimEAMTables t) {
     extern __shared__ float s_tab[];
@@ -73,18 +75,18 @@ __global__ void __launch_bounds__(SIM_THREADS) k_eam_density(SimEngine e, SimEAM
     }
     const SimBox& b = *e.box;
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
+    const int32_t* __restrict__ nbr = e.nbr;
     const int64_t P = e.n_pad;
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const float rc2 = __fmul_rn(t.cutoff, t.cutoff);
-    double vals[1] = {0.0};
-    if (i < e.n) {
+    double acc = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
         const int4 qi = posq[i];
         const int ti = qi.w;
         const int nn = e.nnbr[i];
         float rho = 0.0f;
         for (int k = 0; k < nn; ++k) {
-            const int j = __ldg(&e.nbr[(int64_t)k * P + i]);
-            const int4 qj = posq[j];
+            const int j = __ldg(&nbr[(int64_t)k * P + i]);
+            const int4 qj = __ldg(&posq[j]);
             float r0, r1, r2;
             pair_vector(b, qi, qj, r0, r1, r2);
             const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
@@ -99,84 +101,118 @@ __global__ void __launch_bounds__(SIM_THREADS) k_eam_density(SimEngine e, SimEAM
         float F, Fp;
         embed_lookup(t, ti, rho, F, Fp);
         e.fp[i] = Fp;
-        vals[0] = (double)F;
+        acc += (double)F;
     }
+    double vals[1] = {acc};
     block_partials<1>(vals, e.partials, SIM_RED_EPOT_EMBED);
     last_block_finalize<1>(e.partials, e.red_counter + 0, e.red_out, SIM_RED_EPOT_EMBED);
 }
 
-// EAM pass 2: forces, pair energy, virial
-#define EAM_FORCE_THREADS 512
-template <bool SMEM>
-__global__ void __launch_bounds__(EAM_FORCE_THREADS) k_eam_force(SimEngine e, SimEAMTables t) {
-    extern __shared__ float s_tab[];
+// EAM pass 2: forces, pair energy, virial.
+// SINGLE (one element type): the three r-tables are interleaved in shared
+// memory as float4 {f', phi, phi', 0} per grid point, so one pair costs two
+// 16-byte shared loads; f'_{ti,tj} = f'_{tj,ti}.  Otherwise the tables are
+// read through L1 from global memory.
+#define EAM_FORCE_THREADS 1024
+struct EamPairAcc {
+    float fx = 0.f, fy = 0.f, fz = 0.f, ep = 0.f, vir = 0.f;
+    float wxx = 0.f, wyy = 0.f, wzz = 0.f, wxy = 0.f, wxz = 0.f, wyz = 0.f;
+    __device__ __forceinline__ void add(float s, float phi, float r, float r0, float r1, float r2) {
+        const float c = -s / r;            // force on i: c * rij
+        const float ax = c * r0, ay = c * r1, az = c * r2;
+        fx += ax; fy += ay; fz += az;
+        ep += phi;
+        vir = fmaf(s, r, vir);
+        wxx = fmaf(ax, r0, wxx); wyy = fmaf(ay, r1, wyy); wzz = fmaf(az, r2, wzz);
+        wxy = fmaf(ax, r1, wxy); wxz = fmaf(ax, r2, wxz); wyz = fmaf(ay, r2, wyz);
+    }
+};
+
+// INTEG: the epilogue also finishes the step for atom i -- the second half
+// of velocity Verlet with the Langevin O-step (integrator.py:102-124) -- and
+// accumulates K and sum m v(x)v, so forces never make a second trip through
+// HBM for the half kick.
+template <bool SINGLE, bool INTEG>
+__global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e, SimEAMTables t, SimIntegrator ip) {
+    extern __shared__ float4 s_tab4[];
     const int nt = t.n_types;
-    const size_t tsz = (size_t)nt * nt * t.n_r;
-    const float* dd = t.density_deriv;
-    const float* ph = t.pair;
-    const float* pd = t.pair_deriv;
-    if (SMEM) {
-        for (size_t k = threadIdx.x; k < tsz; k += blockDim.x) {
-            s_tab[k] = __ldg(&t.density_deriv[k]);
-            s_tab[tsz + k] = __ldg(&t.pair[k]);
-            s_tab[2 * tsz + k] = __ldg(&t.pair_deriv[k]);
-        }
+    if (SINGLE) {
+        for (int k = threadIdx.x; k < t.n_r; k += blockDim.x)
+            s_tab4[k] = make_float4(__ldg(&t.density_deriv[k]), __ldg(&t.pair[k]), __ldg(&t.pair_deriv[k]), 0.f);
         __syncthreads();
-        dd = s_tab;
-        ph = s_tab + tsz;
-        pd = s_tab + 2 * tsz;
     }
     const SimBox& b = *e.box;
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
+    const int32_t* __restrict__ nbr = e.nbr;
+    const float* __restrict__ fp = e.fp;
     const int64_t P = e.n_pad;
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const float rc2 = __fmul_rn(t.cutoff, t.cutoff);
-    double vals[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (i < e.n) {
+    float acc[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    bool bad = false;
+    const uint64_t step = INTEG && ip.step_ctr ? *ip.step_ctr : 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
         const int4 qi = posq[i];
         const int ti = qi.w;
-        const float fpi = e.fp[i];
+        const float fpi = fp[i];
         const int nn = e.nnbr[i];
-        float fx = 0.f, fy = 0.f, fz = 0.f, ep = 0.f, vir = 0.f;
-        float wxx = 0.f, wyy = 0.f, wzz = 0.f, wxy = 0.f, wxz = 0.f, wyz = 0.f;
+        EamPairAcc a;
         for (int k = 0; k < nn; ++k) {
-            const int j = __ldg(&e.nbr[(int64_t)k * P + i]);
-            const int4 qj = posq[j];
+            const int j = __ldg(&nbr[(int64_t)k * P + i]);
+            const int4 qj = __ldg(&posq[j]);
             float r0, r1, r2;
             pair_vector(b, qi, qj, r0, r1, r2);
             const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
             if (d2 < rc2) {
                 const float r = sqrtf(d2);
                 if (r < t.cutoff) {
-                    const int tj = qj.w;
-                    const float fpj = __ldg(&e.fp[j]);
+                    const float fpj = __ldg(&fp[j]);
                     Lerp l = lerp_r(r, t.r_clamp_hi, t.inv_dr, t.n_r);
-                    const size_t oij = (size_t)(ti * nt + tj) * t.n_r;
-                    const size_t oji = (size_t)(tj * nt + ti) * t.n_r;
-                    const float d_col = lerp_at(dd + oij, l);   // f'_{ti,tj}: density i receives from j
-                    const float d_row = lerp_at(dd + oji, l);   // f'_{tj,ti}
-                    const float phi = lerp_at(ph + oij, l);
-                    const float dphi = lerp_at(pd + oij, l);
-                    const float s = fmaf(fpi, d_col, fmaf(fpj, d_row, dphi));
-                    const float c = -s / r;            // f = c * rij
-                    const float ax = c * r0, ay = c * r1, az = c * r2;
-                    fx += ax; fy += ay; fz += az;
-                    ep += phi;
-                    vir = fmaf(s, r, vir);
-                    wxx = fmaf(ax, r0, wxx); wyy = fmaf(ay, r1, wyy); wzz = fmaf(az, r2, wzz);
-                    wxy = fmaf(ax, r1, wxy); wxz = fmaf(ax, r2, wxz); wyz = fmaf(ay, r2, wyz);
+                    if (SINGLE) {
+                        const float4 v0 = s_tab4[l.i0], v1 = s_tab4[l.i1];
+                        const float dd = __fadd_rn(v0.x, __fmul_rn(l.frac, __fsub_rn(v1.x, v0.x)));
+                        const float phi = __fadd_rn(v0.y, __fmul_rn(l.frac, __fsub_rn(v1.y, v0.y)));
+                        const float dphi = __fadd_rn(v0.z, __fmul_rn(l.frac, __fsub_rn(v1.z, v0.z)));
+                        a.add(fmaf(fpi, dd, fmaf(fpj, dd, dphi)), phi, r, r0, r1, r2);
+                    } else {
+                        const int tj = qj.w;
+                        const size_t oij = (size_t)(ti * nt + tj) * t.n_r;
+                        const size_t oji = (size_t)(tj * nt + ti) * t.n_r;
+                        const float d_col = lerp_at(t.density_deriv + oij, l);   // f'_{ti,tj}
+                        const float d_row = lerp_at(t.density_deriv + oji, l);   // f'_{tj,ti}
+                        const float phi = lerp_at(t.pair + oij, l);
+                        const float dphi = lerp_at(t.pair_deriv + oij, l);
+                        a.add(fmaf(fpi, d_col, fmaf(fpj, d_row, dphi)), phi, r, r0, r1, r2);
+                    }
                 }
             }
         }
-        reinterpret_cast<float4*>(e.f32)[i] = make_float4(fx, fy, fz, 0.0f);
-        vals[0] = 0.5 * (double)ep;
-        vals[1] = 0.5 * (double)vir;
-        vals[2] = 0.5 * (double)wxx; vals[3] = 0.5 * (double)wyy; vals[4] = 0.5 * (double)wzz;
-        vals[5] = 0.5 * (double)wxy; vals[6] = 0.5 * (double)wxz; vals[7] = 0.5 * (double)wyz;
-        if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+        reinterpret_cast<float4*>(e.f32)[i] = make_float4(a.fx, a.fy, a.fz, 0.0f);
+        acc[0] += a.ep; acc[1] += a.vir;
+        acc[2] += a.wxx; acc[3] += a.wyy; acc[4] += a.wzz; acc[5] += a.wxy; acc[6] += a.wxz; acc[7] += a.wyz;
+        bad |= !(isfinite(a.fx) && isfinite(a.fy) && isfinite(a.fz));
+        if (INTEG) {
+            double v[3];
+            second_half_atom(e, ip, i, ti, step, (double)a.fx, (double)a.fy, (double)a.fz, v, bad);
+            const double m = e.mass[ti];
+            acc[8] += (float)(0.5 * m * v[0] * v[0] + 0.5 * m * v[1] * v[1] + 0.5 * m * v[2] * v[2]);
+            acc[9] += (float)(m * v[0] * v[0]); acc[10] += (float)(m * v[1] * v[1]); acc[11] += (float)(m * v[2] * v[2]);
+            acc[12] += (float)(m * v[0] * v[1]); acc[13] += (float)(m * v[0] * v[2]); acc[14] += (float)(m * v[1] * v[2]);
+        }
     }
-    block_partials<8>(vals, e.partials, SIM_RED_EPOT_PAIR);
-    last_block_finalize<8>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+    if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+    if (INTEG) {
+        double vals[15];
+#pragma unroll
+        for (int k = 0; k < 15; ++k) vals[k] = k < 8 ? 0.5 * (double)acc[k] : (double)acc[k];
+        block_partials<15>(vals, e.partials, SIM_RED_EPOT_PAIR);
+        last_block_finalize<15>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+    } else {
+        double vals[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) vals[k] = 0.5 * (double)acc[k];
+        block_partials<8>(vals, e.partials, SIM_RED_EPOT_PAIR);
+        last_block_finalize<8>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -403,15 +439,43 @@ static int grid_edges(int64_t n) {
 using namespace simb200;
 
 static size_t eam_smem_pass1(const SimEAMTables& t) { return (size_t)t.n_types * t.n_types * t.n_r * sizeof(float); }
-static size_t eam_smem_pass2(const SimEAMTables& t) { return 3 * eam_smem_pass1(t); }
 
 static const size_t kSmemLimit = 200 * 1024;
+
+// Persistent grid size: resident blocks per SM (occupancy query, once per
+// configuration) times the SM count, never more than the atom tiles.
+static int persistent_grid(const void* fn, int threads, size_t smem, int64_t n) {
+    // occupancy queries are cached per (kernel, block, smem) so that calls made
+    // while a stream is being captured only read the cache
+    struct Entry { const void* fn; int threads; size_t smem; int per_sm; };
+    static Entry cache[32];
+    static int n_cache = 0;
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    int per_sm = 0;
+    for (int k = 0; k < n_cache; ++k)
+        if (cache[k].fn == fn && cache[k].threads == threads && cache[k].smem == smem) per_sm = cache[k].per_sm;
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        if (n_cache < 32) cache[n_cache++] = Entry{fn, threads, smem, per_sm};
+    }
+    const int64_t tiles = ceil_div(n, threads);
+    const int64_t g = (int64_t)per_sm * sms;
+    return (int)(g < tiles ? g : (tiles < 1 ? 1 : tiles));
+}
 
 static void eam_set_attributes() {
     static bool done = false;   // first call happens before any stream capture
     if (!done) {
         cudaFuncSetAttribute(k_eam_density<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit);
-        cudaFuncSetAttribute(k_eam_force<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit);
+        cudaFuncSetAttribute(k_eam_force<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit);
+        cudaFuncSetAttribute(k_eam_force<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit);
         done = true;
     }
 }
@@ -420,26 +484,51 @@ extern "C" int sim_eam_density(const SimEngine* ep, const SimEAMTables* tp, void
     if (!ep || !tp || ep->n <= 0) return SIM_ERR_ARG;
     const SimEngine& e = *ep;
     const SimEAMTables& t = *tp;
-    const int blocks = (int)ceil_div(e.n, SIM_THREADS);
-    if (blocks > e.n_blocks_max) return SIM_ERR_ARG;
     eam_set_attributes();
     const size_t s1 = eam_smem_pass1(t);
-    if (s1 <= kSmemLimit) k_eam_density<true><<<blocks, SIM_THREADS, s1, (cudaStream_t)stream>>>(e, t);
-    else k_eam_density<false><<<blocks, SIM_THREADS, 0, (cudaStream_t)stream>>>(e, t);
+    if (s1 <= kSmemLimit) {
+        const int g = persistent_grid((const void*)k_eam_density<true>, SIM_THREADS, s1, e.n);
+        if (g > e.n_blocks_max) return SIM_ERR_ARG;
+        k_eam_density<true><<<g, SIM_THREADS, s1, (cudaStream_t)stream>>>(e, t);
+    } else {
+        const int g = persistent_grid((const void*)k_eam_density<false>, SIM_THREADS, 0, e.n);
+        if (g > e.n_blocks_max) return SIM_ERR_ARG;
+        k_eam_density<false><<<g, SIM_THREADS, 0, (cudaStream_t)stream>>>(e, t);
+    }
     return launch_status("sim_eam_density");
 }
 
-extern "C" int sim_eam_force(const SimEngine* ep, const SimEAMTables* tp, void* stream) {
+template <bool INTEG>
+static int launch_eam_force(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip, void* stream) {
     if (!ep || !tp || ep->n <= 0) return SIM_ERR_ARG;
     const SimEngine& e = *ep;
     const SimEAMTables& t = *tp;
-    const int blocks = (int)ceil_div(e.n, EAM_FORCE_THREADS);
-    if (blocks > e.n_blocks_max) return SIM_ERR_ARG;
+    SimIntegrator integ{};
+    if (INTEG) {
+        if (!ip || !ip->step_ctr || (ip->langevin && !ip->rff)) return SIM_ERR_ARG;
+        integ = *ip;
+    }
     eam_set_attributes();
-    const size_t s2 = eam_smem_pass2(t);
-    if (s2 <= kSmemLimit) k_eam_force<true><<<blocks, EAM_FORCE_THREADS, s2, (cudaStream_t)stream>>>(e, t);
-    else k_eam_force<false><<<blocks, EAM_FORCE_THREADS, 0, (cudaStream_t)stream>>>(e, t);
-    return launch_status("sim_eam_force");
+    const size_t s2 = (size_t)t.n_r * sizeof(float4);
+    if (t.n_types == 1 && s2 <= kSmemLimit) {
+        const int g = persistent_grid((const void*)k_eam_force<true, INTEG>, EAM_FORCE_THREADS, s2, e.n);
+        if (g > e.n_blocks_max) return SIM_ERR_ARG;
+        k_eam_force<true, INTEG><<<g, EAM_FORCE_THREADS, s2, (cudaStream_t)stream>>>(e, t, integ);
+    } else {
+        const int g = persistent_grid((const void*)k_eam_force<false, INTEG>, EAM_FORCE_THREADS, 0, e.n);
+        if (g > e.n_blocks_max) return SIM_ERR_ARG;
+        k_eam_force<false, INTEG><<<g, EAM_FORCE_THREADS, 0, (cudaStream_t)stream>>>(e, t, integ);
+    }
+    return launch_status(INTEG ? "sim_eam_force_integrate" : "sim_eam_force");
+}
+
+extern "C" int sim_eam_force(const SimEngine* ep, const SimEAMTables* tp, void* stream) {
+    return launch_eam_force<false>(ep, tp, nullptr, stream);
+}
+
+extern "C" int sim_eam_force_integrate(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip,
+                                       void* stream) {
+    return launch_eam_force<true>(ep, tp, ip, stream);
 }
 
 extern "C" int sim_eam_forces(const SimEngine* ep, const SimEAMTables* tp, void* stream) {

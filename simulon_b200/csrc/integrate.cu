@@ -81,32 +81,15 @@ __global__ void __launch_bounds__(SIM_THREADS) k_first_half(SimEngine e, SimInte
 }
 
 __global__ void __launch_bounds__(SIM_THREADS) k_second_half(SimEngine e, SimIntegrator p, int prec) {
-    const int64_t P = e.n_pad;
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     double vals[7] = {0, 0, 0, 0, 0, 0, 0};
     if (i < e.n) {
         const int type = e.posq[4 * i + 3];
         const double m = e.mass[type];
-        double z[3] = {0.0, 0.0, 0.0};
-        double rff = 0.0;
-        if (p.langevin) {
-            float z0, z1, z2;
-            langevin_normals((uint32_t)e.orig[i], *p.step_ctr, p.seed, z0, z1, z2);
-            z[0] = z0; z[1] = z1; z[2] = z2;
-            rff = p.rff[type];
-        }
         double v[3];
         bool bad = false;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            double vel = e.v[c * P + i];
-            if (p.langevin) vel = __dadd_rn(__dmul_rn(vel, p.damp), __dmul_rn(z[c], rff));
-            const double a = __ddiv_rn(load_force(e, prec, i, c), m);
-            vel = __dadd_rn(vel, __dmul_rn(__dmul_rn(0.5, a), p.dt));
-            e.v[c * P + i] = vel;
-            v[c] = vel;
-            bad |= !isfinite(vel);
-        }
+        second_half_atom(e, p, i, type, *p.step_ctr, load_force(e, prec, i, 0), load_force(e, prec, i, 1),
+                         load_force(e, prec, i, 2), v, bad);
         const double hm = 0.5 * m;
         vals[0] = hm * v[0] * v[0] + hm * v[1] * v[1] + hm * v[2] * v[2];
         vals[1] = m * v[0] * v[0];
@@ -280,6 +263,7 @@ extern "C" int sim_engine_load(const SimEngine* ep, const double* x_rows, const 
     if (ep->nbr_cap <= 0 || ep->n_cells <= 0) return SIM_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     const SimEngine& e = *ep;
+    prepare_capture_stream();   // outside any capture: create the IF-body capture stream once
     k_load<<<grid_atoms(e.n_pad), SIM_THREADS, 0, st>>>(e, x_rows, v_rows, types);
     k_zero_i32<<<grid_atoms(e.n_cells + 1), SIM_THREADS, 0, st>>>(e.cell_count, e.n_cells + 1);
     k_zero_i32<<<1, 32, 0, st>>>(e.flags, 8);

@@ -199,9 +199,8 @@ __global__ void __launch_bounds__(SIM_THREADS) k_build_ell(SimEngine e, const in
     const int64_t P = e.n_pad;
     const SimBox& b = *e.box;
     const int nx = e.ncell[0], ny = e.ncell[1], nz = e.ncell[2];
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= e.n) return;
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
     const int4 qi = posq[i];
     const int lin = cell_lin[e.cell_of[i]];
     const int cx = lin % nx, cy = (lin / nx) % ny, cz = lin / (nx * ny);
@@ -236,6 +235,7 @@ __global__ void __launch_bounds__(SIM_THREADS) k_build_ell(SimEngine e, const in
     if (cnt > e.nbr_cap) {
         atomicOr(&e.flags[1], SIM_STATUS_OVERFLOW);
         atomicMax(&e.flags[2], cnt);
+    }
     }
 }
 
@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(SIM_THREADS) k_engine_half(SimEngine e, double
 
 static int grid_for(int64_t n) {
     int64_t g = ceil_div(n, SIM_THREADS);
-    return (int)(g < 1 ? 1 : (g > 148 * 32 ? 148 * 32 : g));
+    return (int)(g < 1 ? 1 : (g > 148 * 8 ? 148 * 8 : g));
 }
 
 }  // namespace simb200
@@ -480,9 +480,61 @@ extern "C" int sim_rebuild(const SimEngine* ep, int32_t only_if_flagged, void* s
     k_slot_cells<<<g, SIM_THREADS, 0, st>>>(e, gate);
     const float rc2_list = (float)(e.x_rc * e.x_rc * (1.0 + 4e-6));
     // cell_lin (rank -> linear index) is stored right after cell_rank
-    k_build_ell<<<(int)ceil_div(e.n, SIM_THREADS), SIM_THREADS, 0, st>>>(e, e.cell_rank + e.n_cells, rc2_list, gate);
+    k_build_ell<<<g, SIM_THREADS, 0, st>>>(e, e.cell_rank + e.n_cells, rc2_list, gate);
     k_finish_rebuild<<<1, 1, 0, st>>>(e.flags, only_if_flagged ? 1 : 0);
     return launch_status("sim_rebuild");
+}
+
+// ---------------------------------------------------------------------------
+// Conditional rebuild inside a captured CUDA graph: a one-thread kernel turns
+// flags[0] (set by the skin/2 trigger) into the value of an IF node whose body
+// holds the ungated rebuild kernels, so a step without a rebuild pays one tiny
+// launch instead of the whole rebuild sequence.
+
+__global__ void k_set_rebuild_condition(cudaGraphConditionalHandle h, const int32_t* flags) {
+    cudaGraphSetConditional(h, flags[0] != 0 ? 1u : 0u);
+}
+
+static cudaStream_t g_body_stream = nullptr;
+
+void simb200::prepare_capture_stream() {
+    if (!g_body_stream) cudaStreamCreateWithFlags(&g_body_stream, cudaStreamNonBlocking);
+}
+
+extern "C" int sim_rebuild_if_needed(const SimEngine* ep, void* stream) {
+    if (!ep || !ep->box || ep->n <= 0) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: capture info"); return SIM_ERR_CUDA; }
+    if (cs != cudaStreamCaptureStatusActive || !g_body_stream) return sim_rebuild(ep, 1, stream);
+    cudaGraphConditionalHandle h;
+    err = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: handle"); return SIM_ERR_CUDA; }
+    k_set_rebuild_condition<<<1, 1, 0, st>>>(h, ep->flags);
+    err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: capture info 2"); return SIM_ERR_CUDA; }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    err = cudaGraphAddNode(&node, graph, deps, ndeps, &cp);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: add node"); return SIM_ERR_CUDA; }
+    err = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: deps"); return SIM_ERR_CUDA; }
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    err = cudaStreamBeginCaptureToGraph(g_body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: body capture"); return SIM_ERR_CUDA; }
+    int rc = sim_rebuild(ep, 0, g_body_stream);
+    cudaGraph_t captured = nullptr;
+    err = cudaStreamEndCapture(g_body_stream, &captured);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: end body capture"); return SIM_ERR_CUDA; }
+    return rc;
 }
 
 extern "C" int sim_half_list_count(const void* pos, int32_t dtype_code, int64_t n, const SimBox* box_host,

@@ -255,6 +255,17 @@ class MDEngine:
     def rebuild(self, only_if_flagged: bool = True):
         _lib.call("sim_rebuild", self.st_ref, int(only_if_flagged), self.stream)
 
+    def rebuild_if_needed(self):
+        """Conditional rebuild (an IF node when captured in a CUDA graph)."""
+        _lib.call("sim_rebuild_if_needed", self.st_ref, self.stream)
+
+    def eam_forces_integrate(self, tables, integ):
+        """EAM pass 1, then pass 2 with the second half-step fused into it."""
+        _lib.call("sim_eam_density", self.st_ref, tables.ref, self.stream)
+        _lib.call("sim_eam_force_integrate", self.st_ref, tables.ref, integ.ref, self.stream)
+        self._last_force_precision = 0
+        self.forces_valid = True
+
     def eam_forces(self, tables):
         _lib.call("sim_eam_forces", self.st_ref, tables.ref, self.stream)
         self._last_force_precision = 0

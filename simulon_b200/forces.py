@@ -87,6 +87,10 @@ class EAMForceCUDAExt(BackboneInterface):
     def compute(self):
         self.molecular.engine.eam_forces(self.tables)
 
+    def compute_and_finish(self, integrator):
+        """Forces plus the integrator's second half in one pass over the atoms."""
+        self.molecular.engine.eam_forces_integrate(self.tables, integrator.params)
+
     def forward(self):
         self.compute()
         red = self.molecular.engine.red_out

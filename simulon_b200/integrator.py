@@ -60,7 +60,7 @@ class VerletIntegrator(IntegratorInterface):
         """v += 0.5 F/m dt; x += v dt; skin/2 trigger; conditional list rebuild."""
         eng = self.molecular.engine
         eng.integrate_first(self.params, self.force_precision)
-        eng.rebuild(only_if_flagged=True)
+        eng.rebuild_if_needed()
 
     def second_half(self, forces_new=None):
         eng = self.molecular.engine

@@ -60,8 +60,12 @@ class BaseModel(nn.Module):
     # one step, launches only (no host sync)
     def _step_launches(self):
         self.Integrator.first_half()
-        self.sum_bone.compute()
-        self.Integrator.second_half()
+        fused = getattr(self.sum_bone.backbones[0], "compute_and_finish", None)
+        if fused is not None and hasattr(self.Integrator, "params"):
+            fused(self.Integrator)        # EAM: second half fused into pass 2
+        else:
+            self.sum_bone.compute()
+            self.Integrator.second_half()
         if self.barostat is not None:
             self.barostat.step(self.Integrator.dt)
         self.engine.log_step()

@@ -254,12 +254,26 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
     x = oin.jitter(x, 0.05, 50)
     v = oin.maxwell_boltzmann(np.full(len(x), oin.W_MASS), 600.0, 51)
     res = []
-    for use_graph in (False, True):
+    from simulon_b200.engine import integrator_params
+    # (graph?, conditional IF-node rebuild?, second half fused into EAM pass 2?)
+    modes = [(False, False, False), (True, False, False), (True, True, False), (True, True, True), (False, True, True)]
+    for use_graph, cond, fused in modes:
         eng, tables, parser = _eam_engine(sb, fsw_path, x, np.diag([L] * 3), v)
-        # drive the engine with an NVT integrator (exercises noise + conditional rebuilds)
-        from simulon_b200.engine import integrator_params
+        # an NVT integrator exercises the noise and triggers rebuilds
         integ = integrator_params(eng, 0.002, langevin=True, temperature=600.0, gamma=10.0, seed=7)
         eng.eam_forces(tables)
+
+        def step():
+            eng.integrate_first(integ, 0)
+            if cond:
+                eng.rebuild_if_needed()
+            else:
+                eng.rebuild(True)
+            if fused:
+                eng.eam_forces_integrate(tables, integ)
+            else:
+                eng.eam_forces(tables)
+                eng.integrate_second(integ, 0)
         steps = 60
         if use_graph:
             s = torch.cuda.Stream()
@@ -267,23 +281,21 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=s):
                 for _ in range(20):
-                    eng.integrate_first(integ, 0)
-                    eng.rebuild(True)
-                    eng.eam_forces(tables)
-                    eng.integrate_second(integ, 0)
+                    step()
             torch.cuda.current_stream().wait_stream(s)
             for _ in range(steps // 20):
                 g.replay()
         else:
             for _ in range(steps):
-                eng.integrate_first(integ, 0)
-                eng.rebuild(True)
-                eng.eam_forces(tables)
-                eng.integrate_second(integ, 0)
+                step()
         torch.cuda.synchronize()
-        res.append((eng.gather("x").cpu(), eng.gather("v").cpu(), int(eng.flags[3].item())))
-    assert torch.equal(res[0][0], res[1][0]) and torch.equal(res[0][1], res[1][1])
-    assert res[0][2] == res[1][2] and res[0][2] >= 2      # the load rebuild plus at least one triggered
+        res.append((eng.gather("x").cpu(), eng.gather("v").cpu(), int(eng.flags[3].item()),
+                    eng.red_out.cpu().numpy()))
+    for r in res[1:]:
+        assert torch.equal(res[0][0], r[0]) and torch.equal(res[0][1], r[1])
+        assert r[2] == res[0][2]
+        np.testing.assert_allclose(r[3][9], res[0][3][9], rtol=1e-6)   # kinetic energy (FP32 per-thread partials)
+    assert res[0][2] >= 2      # the load rebuild plus at least one triggered
 
 
 def test_langevin_noise_matches_oracle_philox(sb, fsw_path):
