@@ -261,14 +261,15 @@ def run_b200(args):
     nbr = eng.neighbor_stats()
     nbar = nbr["mean"]
 
-    # dominant kernel: EAM pass 2 (forces, pair energy, virial), timed alone with events
+    # dominant kernel: EAM pass 2 with the fused second half-step (forces, pair
+    # energy, virial, half kick, kinetic tensor), timed alone with events
     R = 50
     ka, kb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     eng.eam_forces(ff.tables)
     torch.cuda.synchronize()
     ka.record(stream)
     for _ in range(R):
-        _lib.call("sim_eam_force", eng.st_ref, ff.tables.ref, eng.stream)
+        _lib.call("sim_eam_force_integrate", eng.st_ref, ff.tables.ref, integ.params.ref, eng.stream)
     kb.record(stream)
     torch.cuda.synchronize()
     k_ms = ka.elapsed_time(kb) / R
@@ -280,7 +281,7 @@ def run_b200(args):
     torch.cuda.synchronize()
     p1_ms = pa.elapsed_time(pb) / R
     peak, peak_kind = measured_peaks()
-    bytes_pass2 = N * (16 + 4 * nbar + 4 + 16)           # posq, list, own F', force out
+    bytes_pass2 = N * (16 + 4 * nbar + 4 + 16 + 48)      # posq, list, own F', force out, v read+write
     bytes_pass1 = N * (16 + 4 * nbar + 4)                # posq, list, F' out
     achieved = bytes_pass2 / (k_ms / 1e3) / 1e9
     # step-level algorithmic bytes per atom-step (EAM: pass1 + pass2 + integrator 152 + rebuild/K)
@@ -299,7 +300,8 @@ def run_b200(args):
                        "neighbors_mean": nbar, "neighbor_capacity": nbr["cap"], "rebuilds_in_timed": rebuilds,
                        "parallelism": f"replicas x{world}"},
             "status": status,
-            "roofline": {"bound": "hbm", "kernel": "k_eam_force (EAM pass 2)", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "k_eam_force<single,integ,ortho> (EAM pass 2 + second half-step)",
+                         "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "bytes_per_launch": bytes_pass2, "launch_ms": k_ms,
                          "pass1_ms": p1_ms, "pass1_bytes": bytes_pass1},

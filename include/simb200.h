@@ -83,7 +83,8 @@ typedef struct SimEngine {
                          fractional displacement (16-byte gathers)            */
     int32_t* xref;    /* [3][n_pad] fixed-point positions at the last rebuild */
     int32_t* orig;    /* [n_pad] original atom index of each slot             */
-    float*  fp;       /* [n_pad] F'(rho) (EAM)                                */
+    int32_t* posfp;   /* [n_pad][4] int4 {posq.x, posq.y, posq.z, F'(rho) bits}
+                         written by EAM pass 1, gathered by pass 2            */
     int32_t* nbr;     /* [nbr_cap][n_pad] neighbour slots (ELL, column-major) */
     int32_t* nnbr;    /* [n_pad] neighbour counts                             */
     /* rebuild scratch */
@@ -107,7 +108,8 @@ typedef struct SimEngine {
     uint32_t* red_counter;/* [4] last-block counters (self-resetting) */
     double*  red_out;     /* [SIM_RED_SLOTS] final FP64 sums */
     int32_t  n_blocks_max;
-    int32_t  pad0;
+    int32_t  box_orthogonal;  /* 1 if the box is (and stays) orthogonal: selects the
+                                 kernels specialised for a diagonal H */
 } SimEngine;
 
 /* reduction slot layout (FP64 Kahan-compensated sums over all atoms) */

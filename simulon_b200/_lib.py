@@ -40,13 +40,13 @@ class SimEngine(ctypes.Structure):
                 ("x_rc", ctypes.c_double), ("skin_half2", ctypes.c_double),
                 ("box", c_p),
                 ("x", c_p), ("v", c_p), ("f32", c_p), ("f64", c_p), ("posq", c_p), ("xref", c_p),
-                ("orig", c_p), ("fp", c_p), ("nbr", c_p), ("nnbr", c_p),
+                ("orig", c_p), ("posfp", c_p), ("nbr", c_p), ("nnbr", c_p),
                 ("cell_of", c_p), ("cell_count", c_p), ("cell_start", c_p), ("cell_rank", c_p),
                 ("perm", c_p), ("x_alt", c_p), ("v_alt", c_p), ("f32_alt", c_p), ("f64_alt", c_p),
                 ("orig_alt", c_p),
                 ("inv_mass", c_p), ("mass", c_p),
                 ("flags", c_p), ("partials", c_p), ("red_counter", c_p), ("red_out", c_p),
-                ("n_blocks_max", ctypes.c_int32), ("pad0", ctypes.c_int32)]
+                ("n_blocks_max", ctypes.c_int32), ("box_orthogonal", ctypes.c_int32)]
 
 
 class SimEAMTables(ctypes.Structure):

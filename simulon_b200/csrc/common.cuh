@@ -12,6 +12,9 @@ namespace simb200 {
 void set_cuda_error(cudaError_t err, const char* where);
 int  launch_status(const char* where);   // checks cudaGetLastError after a launch
 void prepare_capture_stream();           // side stream used to capture IF-node bodies
+// Persistent grid: resident blocks per SM (cached occupancy query) x SM count,
+// capped by the number of atom tiles.
+int persistent_grid(const void* fn, int threads, size_t smem, int64_t n);
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
@@ -45,6 +48,12 @@ __device__ __forceinline__ void frac_to_cart_f(const SimBox& b, float t0, float 
         r1 = fmaf(t2, b.Hf[7], fmaf(t1, b.Hf[4], t0 * b.Hf[1]));
         r2 = fmaf(t2, b.Hf[8], fmaf(t1, b.Hf[5], t0 * b.Hf[2]));
     }
+}
+
+// Minimum-image Cartesian displacement x_i - x_j (FP32) of two fixed-point positions.
+__device__ __forceinline__ void pair_vector(const SimBox& b, const int4& qi, const int4& qj,
+                                            float& r0, float& r1, float& r2) {
+    frac_to_cart_f(b, fixed_delta(qi.x, qj.x), fixed_delta(qi.y, qj.y), fixed_delta(qi.z, qj.z), r0, r1, r2);
 }
 
 // Minimum image in FP64 following core/box.py:109-130 with torch's CPU op order

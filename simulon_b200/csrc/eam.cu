@@ -1,0 +1,368 @@
+// Two-pass EAM on the engine state (sm_100a).
+//
+// Follows EAMForceCUDAExt.forward (core/force/eam_force_cu.py:461-579):
+//   pass 1: rho_i = sum_j f_{ti,tj}(r_ij) over r < rc; F(rho_i), F'(rho_i)
+//   pass 2: s_ij = F'_i f'_{ti,tj}(r) + F'_j f'_{tj,ti}(r) + phi'_{ti,tj}(r);
+//           f_i += -s_ij r_ij/r;  E_pair = 1/2 sum phi;  W = 1/2 sum s r;
+//           W_ab = 1/2 sum f_a r_b        (scalar virial sign of eam_force_cu.py:569)
+// with linear interpolation on the uniform tables of eam_force_cu.py:437-459
+// (clamp r to r_max(1-1e-7), idx = trunc(r/dr), next = min(idx+1, n-1)).
+//
+// Design: one thread per atom over the full ELL list (no atomics, bitwise
+// reproducible); persistent grids so each block stages its lookup tables in
+// shared memory once; the neighbour loop is unrolled with the index and
+// position loads issued before the arithmetic, so each thread keeps several
+// independent gathers in flight.  Pass 1 writes one 16-byte record
+// {fixed-point x, y, z, F'} per atom, so pass 2 fetches a neighbour's position
+// and its F'(rho) with a single 16-byte gather.  Kernels are specialised for
+// orthogonal boxes (three box terms instead of nine in registers).
+#include "common.cuh"
+
+namespace simb200 {
+
+#define EAM_DENSITY_THREADS 256
+#define EAM_FORCE_THREADS 1024
+#define EAM_UNROLL1 4
+#define EAM_UNROLL2 2
+
+struct Lerp {
+    int i0, i1;
+    float frac;
+};
+// _interp_r: clamp, scale, truncate
+__device__ __forceinline__ Lerp lerp_r(float r, float r_hi, float inv_dr, int n_r) {
+    const float rc = fminf(fmaxf(r, 0.0f), r_hi);
+    const float idx_f = rc * inv_dr;
+    const int i = (int)idx_f;
+    return Lerp{i, min(i + 1, n_r - 1), idx_f - (float)i};
+}
+__device__ __forceinline__ float lerp_at(const float* tab, const Lerp& l) {
+    const float v0 = tab[l.i0];
+    return fmaf(l.frac, tab[l.i1] - v0, v0);
+}
+// _interp_rho for F and F' of type ti
+__device__ __forceinline__ void embed_lookup(const SimEAMTables& t, int ti, float rho, float& F, float& Fp) {
+    const float lo = t.rho_min[ti];
+    const float rc = fminf(fmaxf(rho, lo), t.rho_clamp_hi[ti]);
+    const float idx_f = (rc - lo) * t.inv_drho[ti];
+    const int i = (int)idx_f;
+    const int i1 = min(i + 1, t.n_rho - 1);
+    const float frac = idx_f - (float)i;
+    const float* e = t.embed + (size_t)ti * t.n_rho;
+    const float* d = t.embed_deriv + (size_t)ti * t.n_rho;
+    F = fmaf(frac, e[i1] - e[i], e[i]);
+    Fp = fmaf(frac, d[i1] - d[i], d[i]);
+}
+
+// Box rows in registers; ORTHO uses only the diagonal.
+struct BoxF {
+    float h[9];
+    __device__ __forceinline__ explicit BoxF(const SimBox& b) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) h[k] = b.Hf[k];
+    }
+};
+template <bool ORTHO>
+__device__ __forceinline__ void rvec(const BoxF& b, const int4& qi, const int4& qj, float& r0, float& r1, float& r2) {
+    const float t0 = fixed_delta(qi.x, qj.x), t1 = fixed_delta(qi.y, qj.y), t2 = fixed_delta(qi.z, qj.z);
+    if (ORTHO) {
+        r0 = t0 * b.h[0];
+        r1 = t1 * b.h[4];
+        r2 = t2 * b.h[8];
+    } else {
+        r0 = fmaf(t2, b.h[6], fmaf(t1, b.h[3], t0 * b.h[0]));
+        r1 = fmaf(t2, b.h[7], fmaf(t1, b.h[4], t0 * b.h[1]));
+        r2 = fmaf(t2, b.h[8], fmaf(t1, b.h[5], t0 * b.h[2]));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pass 1
+template <bool SMEM, bool ORTHO>
+__device__ __forceinline__ float density_term(const BoxF& b, const int4& qi, const int4& qj, float rc2,
+                                              const float* tab_i, const SimEAMTables& t) {
+    float r0, r1, r2;
+    rvec<ORTHO>(b, qi, qj, r0, r1, r2);
+    const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
+    if (!(d2 < rc2)) return 0.0f;
+    const float r = d2 * rsqrtf(d2);
+    return lerp_at(tab_i + (size_t)qj.w * t.n_r, lerp_r(r, t.r_clamp_hi, t.inv_dr, t.n_r));
+}
+
+template <bool SMEM, bool ORTHO>
+__global__ void __launch_bounds__(EAM_DENSITY_THREADS) k_eam_density(SimEngine e, SimEAMTables t) {
+    extern __shared__ float s_dens[];
+    const float* dens = t.density;
+    const int nt = t.n_types;
+    if (SMEM) {
+        const int total = nt * nt * t.n_r;
+        for (int k = threadIdx.x; k < total; k += blockDim.x) s_dens[k] = __ldg(&t.density[k]);
+        __syncthreads();
+        dens = s_dens;
+    }
+    const BoxF b(*e.box);
+    const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
+    int4* __restrict__ posfp = reinterpret_cast<int4*>(e.posfp);
+    const int32_t* __restrict__ nbr = e.nbr;
+    const int64_t P = e.n_pad;
+    const float rc2 = t.cutoff * t.cutoff;
+    double acc = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int4 qi = posq[i];
+        const int ti = qi.w;
+        const int nn = e.nnbr[i];
+        const float* tab_i = dens + (size_t)ti * nt * t.n_r;
+        float rho = 0.0f;
+        int k = 0;
+        for (; k + EAM_UNROLL1 <= nn; k += EAM_UNROLL1) {
+            int j[EAM_UNROLL1];
+            int4 q[EAM_UNROLL1];
+#pragma unroll
+            for (int u = 0; u < EAM_UNROLL1; ++u) j[u] = __ldg(&nbr[(int64_t)(k + u) * P + i]);
+#pragma unroll
+            for (int u = 0; u < EAM_UNROLL1; ++u) q[u] = __ldg(&posq[j[u]]);
+#pragma unroll
+            for (int u = 0; u < EAM_UNROLL1; ++u) rho += density_term<SMEM, ORTHO>(b, qi, q[u], rc2, tab_i, t);
+        }
+        for (; k < nn; ++k)
+            rho += density_term<SMEM, ORTHO>(b, qi, __ldg(&posq[__ldg(&nbr[(int64_t)k * P + i])]), rc2, tab_i, t);
+        float F, Fp;
+        embed_lookup(t, ti, rho, F, Fp);
+        posfp[i] = make_int4(qi.x, qi.y, qi.z, __float_as_int(Fp));
+        acc += (double)F;
+    }
+    double vals[1] = {acc};
+    block_partials<1>(vals, e.partials, SIM_RED_EPOT_EMBED);
+    last_block_finalize<1>(e.partials, e.red_counter + 0, e.red_out, SIM_RED_EPOT_EMBED);
+}
+
+// ---------------------------------------------------------------------------
+// pass 2.  Per-thread accumulators: acc[0] pair energy, acc[1] scalar virial,
+// acc[2..7] virial tensor (xx yy zz xy xz yz), acc[8] K, acc[9..14] K tensor;
+// only the three force components are per atom.
+__device__ __forceinline__ void pair_force(float s, float phi, float r, float inv_r, float r0, float r1, float r2,
+                                           float& fx, float& fy, float& fz, float (&acc)[15]) {
+    const float c = -s * inv_r;            // force on i = c * r_ij
+    const float ax = c * r0, ay = c * r1, az = c * r2;
+    fx += ax; fy += ay; fz += az;
+    acc[0] += phi;
+    acc[1] = fmaf(s, r, acc[1]);
+    acc[2] = fmaf(ax, r0, acc[2]); acc[3] = fmaf(ay, r1, acc[3]); acc[4] = fmaf(az, r2, acc[4]);
+    acc[5] = fmaf(ax, r1, acc[5]); acc[6] = fmaf(ax, r2, acc[6]); acc[7] = fmaf(ay, r2, acc[7]);
+}
+
+// One element type: the r-tables are interleaved in shared memory as float4
+// {f', phi, phi', 0}; f'_{ti,tj} = f'_{tj,ti}.
+template <bool ORTHO>
+__device__ __forceinline__ void pair_single(const BoxF& b, const int4& pi, const int4& qj, float rc2, float fpi,
+                                            const float4* tab, const SimEAMTables& t, float& fx, float& fy,
+                                            float& fz, float (&acc)[15]) {
+    float r0, r1, r2;
+    rvec<ORTHO>(b, pi, qj, r0, r1, r2);
+    const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
+    if (!(d2 < rc2)) return;
+    const float inv_r = rsqrtf(d2);
+    const float r = d2 * inv_r;
+    const Lerp l = lerp_r(r, t.r_clamp_hi, t.inv_dr, t.n_r);
+    const float4 v0 = tab[l.i0], v1 = tab[l.i1];
+    const float dd = fmaf(l.frac, v1.x - v0.x, v0.x);
+    const float phi = fmaf(l.frac, v1.y - v0.y, v0.y);
+    const float dphi = fmaf(l.frac, v1.z - v0.z, v0.z);
+    pair_force(fmaf(fpi + __int_as_float(qj.w), dd, dphi), phi, r, inv_r, r0, r1, r2, fx, fy, fz, acc);
+}
+
+// INTEG: the epilogue also finishes the step for atom i -- the second half of
+// velocity Verlet with the Langevin O-step (integrator.py:102-124) -- and
+// accumulates K and sum m v(x)v, so the half kick needs no extra pass.
+template <bool SINGLE, bool INTEG, bool ORTHO>
+__global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e, SimEAMTables t, SimIntegrator ip) {
+    extern __shared__ float4 s_tab4[];
+    if (SINGLE) {
+        for (int k = threadIdx.x; k < t.n_r; k += blockDim.x)
+            s_tab4[k] = make_float4(__ldg(&t.density_deriv[k]), __ldg(&t.pair[k]), __ldg(&t.pair_deriv[k]), 0.f);
+        __syncthreads();
+    }
+    const BoxF b(*e.box);
+    const int4* __restrict__ posfp = reinterpret_cast<const int4*>(e.posfp);
+    const int32_t* __restrict__ nbr = e.nbr;
+    const int64_t P = e.n_pad;
+    const float rc2 = t.cutoff * t.cutoff;
+    float acc[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    bool bad = false;
+    const uint64_t step = INTEG && ip.step_ctr ? *ip.step_ctr : 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int4 pi = posfp[i];
+        const float fpi = __int_as_float(pi.w);
+        const int nn = e.nnbr[i];
+        float fx = 0.f, fy = 0.f, fz = 0.f;
+        int ti = 0;
+        if (SINGLE) {
+            int k = 0;
+            for (; k + EAM_UNROLL2 <= nn; k += EAM_UNROLL2) {
+                int j[EAM_UNROLL2];
+                int4 q[EAM_UNROLL2];
+#pragma unroll
+                for (int u = 0; u < EAM_UNROLL2; ++u) j[u] = __ldg(&nbr[(int64_t)(k + u) * P + i]);
+#pragma unroll
+                for (int u = 0; u < EAM_UNROLL2; ++u) q[u] = __ldg(&posfp[j[u]]);
+#pragma unroll
+                for (int u = 0; u < EAM_UNROLL2; ++u) pair_single<ORTHO>(b, pi, q[u], rc2, fpi, s_tab4, t, fx, fy, fz, acc);
+            }
+            for (; k < nn; ++k)
+                pair_single<ORTHO>(b, pi, __ldg(&posfp[__ldg(&nbr[(int64_t)k * P + i])]), rc2, fpi, s_tab4, t,
+                                   fx, fy, fz, acc);
+        } else {
+            const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
+            const int nt = t.n_types;
+            ti = posq[i].w;
+            for (int k = 0; k < nn; ++k) {
+                const int j = __ldg(&nbr[(int64_t)k * P + i]);
+                const int4 qj = __ldg(&posfp[j]);
+                float r0, r1, r2;
+                rvec<ORTHO>(b, pi, qj, r0, r1, r2);
+                const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
+                if (!(d2 < rc2)) continue;
+                const float inv_r = rsqrtf(d2);
+                const float r = d2 * inv_r;
+                const int tj = __ldg(&posq[j]).w;
+                const Lerp l = lerp_r(r, t.r_clamp_hi, t.inv_dr, t.n_r);
+                const size_t oij = (size_t)(ti * nt + tj) * t.n_r;
+                const size_t oji = (size_t)(tj * nt + ti) * t.n_r;
+                const float d_col = lerp_at(t.density_deriv + oij, l);   // f'_{ti,tj}
+                const float d_row = lerp_at(t.density_deriv + oji, l);   // f'_{tj,ti}
+                const float phi = lerp_at(t.pair + oij, l);
+                const float dphi = lerp_at(t.pair_deriv + oij, l);
+                pair_force(fmaf(fpi, d_col, fmaf(__int_as_float(qj.w), d_row, dphi)), phi, r, inv_r, r0, r1, r2,
+                           fx, fy, fz, acc);
+            }
+        }
+        reinterpret_cast<float4*>(e.f32)[i] = make_float4(fx, fy, fz, 0.0f);
+        bad |= !(isfinite(fx) && isfinite(fy) && isfinite(fz));
+        if (INTEG) {
+            double v[3];
+            second_half_atom(e, ip, i, ti, step, (double)fx, (double)fy, (double)fz, v, bad);
+            const double m = e.mass[ti];
+            acc[8] += (float)(0.5 * m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+            acc[9] += (float)(m * v[0] * v[0]); acc[10] += (float)(m * v[1] * v[1]); acc[11] += (float)(m * v[2] * v[2]);
+            acc[12] += (float)(m * v[0] * v[1]); acc[13] += (float)(m * v[0] * v[2]); acc[14] += (float)(m * v[1] * v[2]);
+        }
+    }
+    if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+    if (INTEG) {
+        double vals[15];
+#pragma unroll
+        for (int k = 0; k < 15; ++k) vals[k] = k < 8 ? 0.5 * (double)acc[k] : (double)acc[k];
+        block_partials<15>(vals, e.partials, SIM_RED_EPOT_PAIR);
+        last_block_finalize<15>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+    } else {
+        double vals[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) vals[k] = 0.5 * (double)acc[k];
+        block_partials<8>(vals, e.partials, SIM_RED_EPOT_PAIR);
+        last_block_finalize<8>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+    }
+}
+
+}  // namespace simb200
+
+using namespace simb200;
+
+static const size_t kSmemLimit = 200 * 1024;
+
+static size_t smem_pass1(const SimEAMTables& t) { return (size_t)t.n_types * t.n_types * t.n_r * sizeof(float); }
+static size_t smem_pass2(const SimEAMTables& t) { return (size_t)t.n_r * sizeof(float4); }
+
+template <typename K>
+static void allow_smem(K kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit);
+}
+
+static void eam_set_attributes() {
+    static bool done = false;   // the first call happens before any stream capture
+    if (!done) {
+        allow_smem(k_eam_density<true, true>);
+        allow_smem(k_eam_density<true, false>);
+        allow_smem(k_eam_force<true, false, true>);
+        allow_smem(k_eam_force<true, true, true>);
+        allow_smem(k_eam_force<true, false, false>);
+        allow_smem(k_eam_force<true, true, false>);
+        done = true;
+    }
+}
+
+static bool valid_tables(const SimEAMTables& t) {
+    return t.n_types >= 1 && t.n_r >= 2 && t.n_rho >= 2 && t.density && t.density_deriv && t.pair &&
+           t.pair_deriv && t.embed && t.embed_deriv && t.rho_min && t.inv_drho && t.rho_clamp_hi;
+}
+
+template <bool SMEM, bool ORTHO>
+static int launch_density(const SimEngine& e, const SimEAMTables& t, size_t smem, cudaStream_t st) {
+    const int g = persistent_grid((const void*)k_eam_density<SMEM, ORTHO>, EAM_DENSITY_THREADS, smem, e.n);
+    if (g > e.n_blocks_max) return SIM_ERR_ARG;
+    k_eam_density<SMEM, ORTHO><<<g, EAM_DENSITY_THREADS, smem, st>>>(e, t);
+    return SIM_OK;
+}
+
+extern "C" int sim_eam_density(const SimEngine* ep, const SimEAMTables* tp, void* stream) {
+    if (!ep || !tp || ep->n <= 0 || !ep->posfp || !valid_tables(*tp) || tp->n_types > ep->n_types) return SIM_ERR_ARG;
+    const SimEngine& e = *ep;
+    const SimEAMTables& t = *tp;
+    eam_set_attributes();
+    const size_t s1 = smem_pass1(t);
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if (s1 <= kSmemLimit)
+        rc = e.box_orthogonal ? launch_density<true, true>(e, t, s1, st) : launch_density<true, false>(e, t, s1, st);
+    else
+        rc = e.box_orthogonal ? launch_density<false, true>(e, t, 0, st) : launch_density<false, false>(e, t, 0, st);
+    if (rc != SIM_OK) return rc;
+    return launch_status("sim_eam_density");
+}
+
+template <bool SINGLE, bool INTEG, bool ORTHO>
+static int launch_force(const SimEngine& e, const SimEAMTables& t, const SimIntegrator& ip, cudaStream_t st) {
+    const size_t smem = SINGLE ? smem_pass2(t) : 0;
+    const int g = persistent_grid((const void*)k_eam_force<SINGLE, INTEG, ORTHO>, EAM_FORCE_THREADS, smem, e.n);
+    if (g > e.n_blocks_max) return SIM_ERR_ARG;
+    k_eam_force<SINGLE, INTEG, ORTHO><<<g, EAM_FORCE_THREADS, smem, st>>>(e, t, ip);
+    return SIM_OK;
+}
+
+template <bool INTEG>
+static int launch_eam_force(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip, void* stream) {
+    if (!ep || !tp || ep->n <= 0 || !ep->posfp || !valid_tables(*tp)) return SIM_ERR_ARG;
+    const SimEngine& e = *ep;
+    const SimEAMTables& t = *tp;
+    SimIntegrator integ{};
+    if (INTEG) {
+        if (!ip || !ip->step_ctr || (ip->langevin && !ip->rff)) return SIM_ERR_ARG;
+        integ = *ip;
+    }
+    eam_set_attributes();
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool single = t.n_types == 1 && smem_pass2(t) <= kSmemLimit;
+    int rc;
+    if (single)
+        rc = e.box_orthogonal ? launch_force<true, INTEG, true>(e, t, integ, st)
+                              : launch_force<true, INTEG, false>(e, t, integ, st);
+    else
+        rc = e.box_orthogonal ? launch_force<false, INTEG, true>(e, t, integ, st)
+                              : launch_force<false, INTEG, false>(e, t, integ, st);
+    if (rc != SIM_OK) return rc;
+    return launch_status(INTEG ? "sim_eam_force_integrate" : "sim_eam_force");
+}
+
+extern "C" int sim_eam_force(const SimEngine* ep, const SimEAMTables* tp, void* stream) {
+    return launch_eam_force<false>(ep, tp, nullptr, stream);
+}
+
+extern "C" int sim_eam_force_integrate(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip,
+                                       void* stream) {
+    return launch_eam_force<true>(ep, tp, ip, stream);
+}
+
+extern "C" int sim_eam_forces(const SimEngine* ep, const SimEAMTables* tp, void* stream) {
+    int rc = sim_eam_density(ep, tp, stream);
+    if (rc != SIM_OK) return rc;
+    return sim_eam_force(ep, tp, stream);
+}

@@ -27,6 +27,32 @@ void set_cuda_error(cudaError_t err, const char* where) {
     snprintf(g_err, sizeof(g_err), "%s: %s (%s)", where, cudaGetErrorString(err), cudaGetErrorName(err));
 }
 
+int persistent_grid(const void* fn, int threads, size_t smem, int64_t n) {
+    // cached per (kernel, block, smem) so calls made while a stream is being
+    // captured only read the cache
+    struct Entry { const void* fn; int threads; size_t smem; int per_sm; };
+    static Entry cache[32];
+    static int n_cache = 0;
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    int per_sm = 0;
+    for (int k = 0; k < n_cache; ++k)
+        if (cache[k].fn == fn && cache[k].threads == threads && cache[k].smem == smem) per_sm = cache[k].per_sm;
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        if (n_cache < 32) cache[n_cache++] = Entry{fn, threads, smem, per_sm};
+    }
+    const int64_t tiles = ceil_div(n, threads);
+    const int64_t g = (int64_t)per_sm * sms;
+    return (int)(g < tiles ? g : (tiles < 1 ? 1 : tiles));
+}
+
 int launch_status(const char* where) {
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) {

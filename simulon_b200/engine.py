@@ -130,7 +130,7 @@ class MDEngine:
         self.posq = torch.zeros(P, 4, **i32)
         self.xref = torch.zeros(3, P, **i32)
         self.orig = torch.zeros(P, **i32)
-        self.fp = torch.zeros(P, device=dev, dtype=torch.float32)
+        self.posfp = torch.zeros(P, 4, **i32)
         self.nbr = torch.zeros(self.nbr_cap, P, **i32)
         self.nnbr = torch.zeros(P, **i32)
         self.cell_of = torch.zeros(P, **i32)
@@ -177,11 +177,12 @@ class MDEngine:
         s.skin_half2 = (self.skin / 2.0) ** 2
         p = _lib.ptr
         s.box = p(self.box_dev)
-        for name in ("x", "v", "f32", "f64", "posq", "xref", "orig", "fp", "nbr", "nnbr", "cell_of",
+        for name in ("x", "v", "f32", "f64", "posq", "xref", "orig", "posfp", "nbr", "nnbr", "cell_of",
                      "cell_count", "cell_start", "cell_rank", "perm", "x_alt", "v_alt", "f32_alt", "f64_alt",
                      "orig_alt", "inv_mass", "mass", "flags", "partials", "red_counter", "red_out"):
             setattr(s, name, p(getattr(self, name)))
         s.n_blocks_max = self.n_blocks_max
+        s.box_orthogonal = int(self.box.orthogonal)
         self.st = s
         self.st_ref = ctypes.byref(s)
 
@@ -250,6 +251,7 @@ class MDEngine:
     def set_box(self, H):
         self.box = make_box(H)
         self.box_dev.copy_(torch.frombuffer(bytearray(bytes(self.box)), dtype=torch.uint8))
+        self.st.box_orthogonal = int(self.box.orthogonal)
 
     # ---- step primitives ---------------------------------------------------
     def rebuild(self, only_if_flagged: bool = True):
