@@ -142,6 +142,11 @@ typedef struct SimEAMTables {
     const float* rho_min;        /* [E]  (device)                            */
     const float* inv_drho;       /* [E]                                      */
     const float* rho_clamp_hi;   /* [E]  rho_min + drho (n_rho-1)(1-1e-7)    */
+    /* the same r-tables as value + forward difference, so v(k + frac) =
+     * fma(frac, d_k, v_k) with d_k = v_{min(k+1,n-1)} - v_k (float32):       */
+    const float* dens_vd;        /* [E][E][n_r] float2 {f_k, df_k}                 */
+    const float* deriv_vd;       /* [E][E][n_r] float4 {f'_k, phi'_k, df'_k, dphi'_k} */
+    const float* pair_vd;        /* [E][E][n_r] float2 {phi_k, dphi_k}             */
     int32_t n_types, n_r, n_rho, pad;
     float cutoff, inv_dr, r_clamp_hi, pad2;   /* r_clamp_hi = r_max (1-1e-7) */
 } SimEAMTables;

@@ -52,7 +52,7 @@ class SimEngine(ctypes.Structure):
 class SimEAMTables(ctypes.Structure):
     _fields_ = [("density", c_p), ("density_deriv", c_p), ("pair", c_p), ("pair_deriv", c_p),
                 ("embed", c_p), ("embed_deriv", c_p), ("rho_min", c_p), ("inv_drho", c_p),
-                ("rho_clamp_hi", c_p),
+                ("rho_clamp_hi", c_p), ("dens_vd", c_p), ("deriv_vd", c_p), ("pair_vd", c_p),
                 ("n_types", ctypes.c_int32), ("n_r", ctypes.c_int32), ("n_rho", ctypes.c_int32),
                 ("pad", ctypes.c_int32),
                 ("cutoff", ctypes.c_float), ("inv_dr", ctypes.c_float), ("r_clamp_hi", ctypes.c_float),

@@ -9,37 +9,28 @@
 // (clamp r to r_max(1-1e-7), idx = trunc(r/dr), next = min(idx+1, n-1)).
 //
 // Design: one thread per atom over the full ELL list (no atomics, bitwise
-// reproducible); persistent grids so each block stages its lookup tables in
-// shared memory once; the neighbour loop is unrolled with the index and
-// position loads issued before the arithmetic, so each thread keeps several
-// independent gathers in flight.  Pass 1 writes one 16-byte record
-// {fixed-point x, y, z, F'} per atom, so pass 2 fetches a neighbour's position
-// and its F'(rho) with a single 16-byte gather.  Kernels are specialised for
-// orthogonal boxes (three box terms instead of nine in registers).
+// reproducible).  Persistent grids: each block stages its tables in shared
+// memory once.  Tables are stored as value + forward difference so each
+// interpolation is one FMA, and pass 2 fetches {f', phi', df', dphi'} with one
+// 16-byte load and interpolates f' and phi' with one packed FP32x2 FMA.
+// Pass 1 writes a 16-byte record {fixed-point x, y, z, F'} per atom so pass 2
+// gathers a neighbour's position and F'(rho) together.  Rows of the list are
+// sorted by distance at rebuild, so a warp's lanes reach the in-cutoff and
+// out-of-cutoff neighbours at the same k and rarely diverge.  Kernels are
+// specialised for orthogonal boxes (three box terms in registers).
 #include "common.cuh"
 
 namespace simb200 {
 
-#define EAM_DENSITY_THREADS 256
+#define EAM_DENSITY_THREADS 512
 #define EAM_FORCE_THREADS 1024
-#define EAM_UNROLL1 4
-#define EAM_UNROLL2 2
 
-struct Lerp {
-    int i0, i1;
-    float frac;
-};
-// _interp_r: clamp, scale, truncate
-__device__ __forceinline__ Lerp lerp_r(float r, float r_hi, float inv_dr, int n_r) {
-    const float rc = fminf(fmaxf(r, 0.0f), r_hi);
-    const float idx_f = rc * inv_dr;
-    const int i = (int)idx_f;
-    return Lerp{i, min(i + 1, n_r - 1), idx_f - (float)i};
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
-__device__ __forceinline__ float lerp_at(const float* tab, const Lerp& l) {
-    const float v0 = tab[l.i0];
-    return fmaf(l.frac, tab[l.i1] - v0, v0);
-}
+
 // _interp_rho for F and F' of type ti
 __device__ __forceinline__ void embed_lookup(const SimEAMTables& t, int ti, float rho, float& F, float& Fp) {
     const float lo = t.rho_min[ti];
@@ -54,17 +45,19 @@ __device__ __forceinline__ void embed_lookup(const SimEAMTables& t, int ti, floa
     Fp = fmaf(frac, d[i1] - d[i], d[i]);
 }
 
-// Box rows in registers; ORTHO uses only the diagonal.
+// Box terms in registers, with the 2^-32 of the fixed-point code folded in.
 struct BoxF {
     float h[9];
     __device__ __forceinline__ explicit BoxF(const SimBox& b) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) h[k] = b.Hf[k];
+        for (int k = 0; k < 9; ++k) h[k] = b.Hf[k] * 2.3283064365386963e-10f;
     }
 };
 template <bool ORTHO>
 __device__ __forceinline__ void rvec(const BoxF& b, const int4& qi, const int4& qj, float& r0, float& r1, float& r2) {
-    const float t0 = fixed_delta(qi.x, qj.x), t1 = fixed_delta(qi.y, qj.y), t2 = fixed_delta(qi.z, qj.z);
+    const float t0 = __int2float_rn((int32_t)((uint32_t)qi.x - (uint32_t)qj.x));
+    const float t1 = __int2float_rn((int32_t)((uint32_t)qi.y - (uint32_t)qj.y));
+    const float t2 = __int2float_rn((int32_t)((uint32_t)qi.z - (uint32_t)qj.z));
     if (ORTHO) {
         r0 = t0 * b.h[0];
         r1 = t1 * b.h[4];
@@ -76,27 +69,39 @@ __device__ __forceinline__ void rvec(const BoxF& b, const int4& qi, const int4& 
     }
 }
 
+// r inside the cutoff -> table row and fraction (_interp_r)
+struct Lerp {
+    int k;
+    float frac;
+};
+__device__ __forceinline__ Lerp lerp_r(float r, const SimEAMTables& t) {
+    const float idx_f = fminf(r, t.r_clamp_hi) * t.inv_dr;
+    const int k = (int)idx_f;
+    return Lerp{k, idx_f - (float)k};
+}
+
 // ---------------------------------------------------------------------------
 // pass 1
-template <bool SMEM, bool ORTHO>
+template <bool ORTHO>
 __device__ __forceinline__ float density_term(const BoxF& b, const int4& qi, const int4& qj, float rc2,
-                                              const float* tab_i, const SimEAMTables& t) {
+                                              const float2* tab_i, const SimEAMTables& t) {
     float r0, r1, r2;
     rvec<ORTHO>(b, qi, qj, r0, r1, r2);
     const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
     if (!(d2 < rc2)) return 0.0f;
-    const float r = d2 * rsqrtf(d2);
-    return lerp_at(tab_i + (size_t)qj.w * t.n_r, lerp_r(r, t.r_clamp_hi, t.inv_dr, t.n_r));
+    const Lerp l = lerp_r(d2 * rsqrt_approx(d2), t);
+    const float2 v = tab_i[(size_t)qj.w * t.n_r + l.k];
+    return fmaf(l.frac, v.y, v.x);
 }
 
 template <bool SMEM, bool ORTHO>
 __global__ void __launch_bounds__(EAM_DENSITY_THREADS) k_eam_density(SimEngine e, SimEAMTables t) {
-    extern __shared__ float s_dens[];
-    const float* dens = t.density;
+    extern __shared__ float2 s_dens[];
+    const float2* dens = reinterpret_cast<const float2*>(t.dens_vd);
     const int nt = t.n_types;
     if (SMEM) {
         const int total = nt * nt * t.n_r;
-        for (int k = threadIdx.x; k < total; k += blockDim.x) s_dens[k] = __ldg(&t.density[k]);
+        for (int k = threadIdx.x; k < total; k += blockDim.x) s_dens[k] = __ldg(&dens[k]);
         __syncthreads();
         dens = s_dens;
     }
@@ -111,21 +116,21 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS) k_eam_density(SimEngine e
         const int4 qi = posq[i];
         const int ti = qi.w;
         const int nn = e.nnbr[i];
-        const float* tab_i = dens + (size_t)ti * nt * t.n_r;
+        const float2* tab_i = dens + (size_t)ti * nt * t.n_r;
         float rho = 0.0f;
         int k = 0;
-        for (; k + EAM_UNROLL1 <= nn; k += EAM_UNROLL1) {
-            int j[EAM_UNROLL1];
-            int4 q[EAM_UNROLL1];
+        for (; k + 4 <= nn; k += 4) {
+            int j[4];
+            int4 q[4];
 #pragma unroll
-            for (int u = 0; u < EAM_UNROLL1; ++u) j[u] = __ldg(&nbr[(int64_t)(k + u) * P + i]);
+            for (int u = 0; u < 4; ++u) j[u] = __ldg(&nbr[(int64_t)(k + u) * P + i]);
 #pragma unroll
-            for (int u = 0; u < EAM_UNROLL1; ++u) q[u] = __ldg(&posq[j[u]]);
+            for (int u = 0; u < 4; ++u) q[u] = __ldg(&posq[j[u]]);
 #pragma unroll
-            for (int u = 0; u < EAM_UNROLL1; ++u) rho += density_term<SMEM, ORTHO>(b, qi, q[u], rc2, tab_i, t);
+            for (int u = 0; u < 4; ++u) rho += density_term<ORTHO>(b, qi, q[u], rc2, tab_i, t);
         }
         for (; k < nn; ++k)
-            rho += density_term<SMEM, ORTHO>(b, qi, __ldg(&posq[__ldg(&nbr[(int64_t)k * P + i])]), rc2, tab_i, t);
+            rho += density_term<ORTHO>(b, qi, __ldg(&posq[__ldg(&nbr[(int64_t)k * P + i])]), rc2, tab_i, t);
         float F, Fp;
         embed_lookup(t, ti, rho, F, Fp);
         posfp[i] = make_int4(qi.x, qi.y, qi.z, __float_as_int(Fp));
@@ -151,24 +156,24 @@ __device__ __forceinline__ void pair_force(float s, float phi, float r, float in
     acc[5] = fmaf(ax, r1, acc[5]); acc[6] = fmaf(ax, r2, acc[6]); acc[7] = fmaf(ay, r2, acc[7]);
 }
 
-// One element type: the r-tables are interleaved in shared memory as float4
-// {f', phi, phi', 0}; f'_{ti,tj} = f'_{tj,ti}.
+// One element type: f'_{ti,tj} = f'_{tj,ti}; tables {f', phi', df', dphi'} and
+// {phi, dphi} staged in shared memory.
 template <bool ORTHO>
 __device__ __forceinline__ void pair_single(const BoxF& b, const int4& pi, const int4& qj, float rc2, float fpi,
-                                            const float4* tab, const SimEAMTables& t, float& fx, float& fy,
-                                            float& fz, float (&acc)[15]) {
+                                            const float4* tab_d, const float2* tab_p, const SimEAMTables& t,
+                                            float& fx, float& fy, float& fz, float (&acc)[15]) {
     float r0, r1, r2;
     rvec<ORTHO>(b, pi, qj, r0, r1, r2);
     const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
     if (!(d2 < rc2)) return;
-    const float inv_r = rsqrtf(d2);
+    const float inv_r = rsqrt_approx(d2);
     const float r = d2 * inv_r;
-    const Lerp l = lerp_r(r, t.r_clamp_hi, t.inv_dr, t.n_r);
-    const float4 v0 = tab[l.i0], v1 = tab[l.i1];
-    const float dd = fmaf(l.frac, v1.x - v0.x, v0.x);
-    const float phi = fmaf(l.frac, v1.y - v0.y, v0.y);
-    const float dphi = fmaf(l.frac, v1.z - v0.z, v0.z);
-    pair_force(fmaf(fpi + __int_as_float(qj.w), dd, dphi), phi, r, inv_r, r0, r1, r2, fx, fy, fz, acc);
+    const Lerp l = lerp_r(r, t);
+    const float4 d = tab_d[l.k];
+    const float2 p = tab_p[l.k];
+    const float2 dd_dp = __ffma2_rn(make_float2(l.frac, l.frac), make_float2(d.z, d.w), make_float2(d.x, d.y));
+    const float phi = fmaf(l.frac, p.y, p.x);
+    pair_force(fmaf(fpi + __int_as_float(qj.w), dd_dp.x, dd_dp.y), phi, r, inv_r, r0, r1, r2, fx, fy, fz, acc);
 }
 
 // INTEG: the epilogue also finishes the step for atom i -- the second half of
@@ -177,9 +182,15 @@ __device__ __forceinline__ void pair_single(const BoxF& b, const int4& pi, const
 template <bool SINGLE, bool INTEG, bool ORTHO>
 __global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e, SimEAMTables t, SimIntegrator ip) {
     extern __shared__ float4 s_tab4[];
+    float4* tab_d = s_tab4;
+    float2* tab_p = reinterpret_cast<float2*>(s_tab4 + t.n_r);
     if (SINGLE) {
-        for (int k = threadIdx.x; k < t.n_r; k += blockDim.x)
-            s_tab4[k] = make_float4(__ldg(&t.density_deriv[k]), __ldg(&t.pair[k]), __ldg(&t.pair_deriv[k]), 0.f);
+        const float4* gd = reinterpret_cast<const float4*>(t.deriv_vd);
+        const float2* gp = reinterpret_cast<const float2*>(t.pair_vd);
+        for (int k = threadIdx.x; k < t.n_r; k += blockDim.x) {
+            tab_d[k] = __ldg(&gd[k]);
+            tab_p[k] = __ldg(&gp[k]);
+        }
         __syncthreads();
     }
     const BoxF b(*e.box);
@@ -198,22 +209,22 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e,
         int ti = 0;
         if (SINGLE) {
             int k = 0;
-            for (; k + EAM_UNROLL2 <= nn; k += EAM_UNROLL2) {
-                int j[EAM_UNROLL2];
-                int4 q[EAM_UNROLL2];
-#pragma unroll
-                for (int u = 0; u < EAM_UNROLL2; ++u) j[u] = __ldg(&nbr[(int64_t)(k + u) * P + i]);
-#pragma unroll
-                for (int u = 0; u < EAM_UNROLL2; ++u) q[u] = __ldg(&posfp[j[u]]);
-#pragma unroll
-                for (int u = 0; u < EAM_UNROLL2; ++u) pair_single<ORTHO>(b, pi, q[u], rc2, fpi, s_tab4, t, fx, fy, fz, acc);
+            for (; k + 2 <= nn; k += 2) {
+                const int j0 = __ldg(&nbr[(int64_t)k * P + i]);
+                const int j1 = __ldg(&nbr[(int64_t)(k + 1) * P + i]);
+                const int4 q0 = __ldg(&posfp[j0]);
+                const int4 q1 = __ldg(&posfp[j1]);
+                pair_single<ORTHO>(b, pi, q0, rc2, fpi, tab_d, tab_p, t, fx, fy, fz, acc);
+                pair_single<ORTHO>(b, pi, q1, rc2, fpi, tab_d, tab_p, t, fx, fy, fz, acc);
             }
-            for (; k < nn; ++k)
-                pair_single<ORTHO>(b, pi, __ldg(&posfp[__ldg(&nbr[(int64_t)k * P + i])]), rc2, fpi, s_tab4, t,
+            if (k < nn)
+                pair_single<ORTHO>(b, pi, __ldg(&posfp[__ldg(&nbr[(int64_t)k * P + i])]), rc2, fpi, tab_d, tab_p, t,
                                    fx, fy, fz, acc);
         } else {
             const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
             const int nt = t.n_types;
+            const float4* gd = reinterpret_cast<const float4*>(t.deriv_vd);
+            const float2* gp = reinterpret_cast<const float2*>(t.pair_vd);
             ti = posq[i].w;
             for (int k = 0; k < nn; ++k) {
                 const int j = __ldg(&nbr[(int64_t)k * P + i]);
@@ -222,16 +233,17 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e,
                 rvec<ORTHO>(b, pi, qj, r0, r1, r2);
                 const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
                 if (!(d2 < rc2)) continue;
-                const float inv_r = rsqrtf(d2);
+                const float inv_r = rsqrt_approx(d2);
                 const float r = d2 * inv_r;
                 const int tj = __ldg(&posq[j]).w;
-                const Lerp l = lerp_r(r, t.r_clamp_hi, t.inv_dr, t.n_r);
-                const size_t oij = (size_t)(ti * nt + tj) * t.n_r;
-                const size_t oji = (size_t)(tj * nt + ti) * t.n_r;
-                const float d_col = lerp_at(t.density_deriv + oij, l);   // f'_{ti,tj}
-                const float d_row = lerp_at(t.density_deriv + oji, l);   // f'_{tj,ti}
-                const float phi = lerp_at(t.pair + oij, l);
-                const float dphi = lerp_at(t.pair_deriv + oij, l);
+                const Lerp l = lerp_r(r, t);
+                const float4 dij = __ldg(&gd[(size_t)(ti * nt + tj) * t.n_r + l.k]);   // f'_{ti,tj}, phi'_{ti,tj}
+                const float4 dji = __ldg(&gd[(size_t)(tj * nt + ti) * t.n_r + l.k]);   // f'_{tj,ti}
+                const float2 p = __ldg(&gp[(size_t)(ti * nt + tj) * t.n_r + l.k]);
+                const float d_col = fmaf(l.frac, dij.z, dij.x);
+                const float d_row = fmaf(l.frac, dji.z, dji.x);
+                const float dphi = fmaf(l.frac, dij.w, dij.y);
+                const float phi = fmaf(l.frac, p.y, p.x);
                 pair_force(fmaf(fpi, d_col, fmaf(__int_as_float(qj.w), d_row, dphi)), phi, r, inv_r, r0, r1, r2,
                            fx, fy, fz, acc);
             }
@@ -269,8 +281,8 @@ using namespace simb200;
 
 static const size_t kSmemLimit = 200 * 1024;
 
-static size_t smem_pass1(const SimEAMTables& t) { return (size_t)t.n_types * t.n_types * t.n_r * sizeof(float); }
-static size_t smem_pass2(const SimEAMTables& t) { return (size_t)t.n_r * sizeof(float4); }
+static size_t smem_pass1(const SimEAMTables& t) { return (size_t)t.n_types * t.n_types * t.n_r * sizeof(float2); }
+static size_t smem_pass2(const SimEAMTables& t) { return (size_t)t.n_r * (sizeof(float4) + sizeof(float2)); }
 
 template <typename K>
 static void allow_smem(K kernel) {
@@ -291,8 +303,8 @@ static void eam_set_attributes() {
 }
 
 static bool valid_tables(const SimEAMTables& t) {
-    return t.n_types >= 1 && t.n_r >= 2 && t.n_rho >= 2 && t.density && t.density_deriv && t.pair &&
-           t.pair_deriv && t.embed && t.embed_deriv && t.rho_min && t.inv_drho && t.rho_clamp_hi;
+    return t.n_types >= 1 && t.n_r >= 2 && t.n_rho >= 2 && t.embed && t.embed_deriv && t.rho_min && t.inv_drho &&
+           t.rho_clamp_hi && t.dens_vd && t.deriv_vd && t.pair_vd;
 }
 
 template <bool SMEM, bool ORTHO>

@@ -190,6 +190,8 @@ __device__ __forceinline__ int stencil_cell(int c, int k, int n) {
     return k;   // n <= 2: enumerate every cell once
 }
 
+#define ELL_SORT_MAX 128   // rows up to this length are sorted by distance
+
 // Full list in ELL layout.  Test in FP32 on fixed-point displacements; the
 // radius carries a 2e-6 relative margin so that an exact FP64/FP32 filter
 // applied later (half-list export, force cutoffs) always sees a superset.
@@ -200,6 +202,8 @@ __global__ void __launch_bounds__(SIM_THREADS) k_build_ell(SimEngine e, const in
     const SimBox& b = *e.box;
     const int nx = e.ncell[0], ny = e.ncell[1], nz = e.ncell[2];
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
+    float key_d2[ELL_SORT_MAX];
+    int key_j[ELL_SORT_MAX];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
     const int4 qi = posq[i];
     const int lin = cell_lin[e.cell_of[i]];
@@ -224,14 +228,36 @@ __global__ void __launch_bounds__(SIM_THREADS) k_build_ell(SimEngine e, const in
                     frac_to_cart_f(b, t0, t1, t2, r0, r1, r2);
                     float d2 = __fadd_rn(__fadd_rn(__fmul_rn(r0, r0), __fmul_rn(r1, r1)), __fmul_rn(r2, r2));
                     if (d2 < rc2_list) {
-                        if (cnt < e.nbr_cap) e.nbr[(int64_t)cnt * P + i] = j;
+                        if (cnt < e.nbr_cap) {
+                            if (cnt < ELL_SORT_MAX) { key_d2[cnt] = d2; key_j[cnt] = j; }
+                            e.nbr[(int64_t)cnt * P + i] = j;
+                        }
                         ++cnt;
                     }
                 }
             }
         }
     }
-    e.nnbr[i] = cnt < e.nbr_cap ? cnt : e.nbr_cap;
+    const int kept = cnt < e.nbr_cap ? cnt : e.nbr_cap;
+    if (kept <= ELL_SORT_MAX) {
+        // nearest first (ties by slot): in a crystal every row then lists the
+        // same shells in the same order, so a warp's lanes agree on which
+        // neighbours fall inside the force cutoff
+        for (int a = 1; a < kept; ++a) {
+            const float kd = key_d2[a];
+            const int kj = key_j[a];
+            int p = a - 1;
+            while (p >= 0 && (key_d2[p] > kd || (key_d2[p] == kd && key_j[p] > kj))) {
+                key_d2[p + 1] = key_d2[p];
+                key_j[p + 1] = key_j[p];
+                --p;
+            }
+            key_d2[p + 1] = kd;
+            key_j[p + 1] = kj;
+        }
+        for (int a = 0; a < kept; ++a) e.nbr[(int64_t)a * P + i] = key_j[a];
+    }
+    e.nnbr[i] = kept;
     if (cnt > e.nbr_cap) {
         atomicOr(&e.flags[1], SIM_STATUS_OVERFLOW);
         atomicMax(&e.flags[2], cnt);

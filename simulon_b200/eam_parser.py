@@ -196,9 +196,18 @@ class EAMDeviceTables:
         self.tensors["rho_min"] = torch.tensor(lo, **to)
         self.tensors["inv_drho"] = torch.tensor(inv, **to)
         self.tensors["rho_clamp_hi"] = torch.tensor(hi, **to)
+
+        def vd(*tabs):
+            # value and forward difference, interleaved: (..., n_r, 2*len(tabs))
+            vals = [t.astype(np.float32) for t in tabs]
+            diffs = [np.concatenate([v[..., 1:] - v[..., :-1], np.zeros_like(v[..., :1])], -1) for v in vals]
+            return np.ascontiguousarray(np.stack(vals + diffs, -1))
+        self.tensors["dens_vd"] = torch.as_tensor(vd(host["density"])).to(device)
+        self.tensors["deriv_vd"] = torch.as_tensor(vd(host["density_deriv"], host["pair_deriv"])).to(device)
+        self.tensors["pair_vd"] = torch.as_tensor(vd(host["pair"])).to(device)
         s = _lib.SimEAMTables()
         for k in ("density", "density_deriv", "pair", "pair_deriv", "embed", "embed_deriv", "rho_min",
-                  "inv_drho", "rho_clamp_hi"):
+                  "inv_drho", "rho_clamp_hi", "dens_vd", "deriv_vd", "pair_vd"):
             setattr(s, k, _lib.ptr(self.tensors[k]))
         s.n_types, s.n_r, s.n_rho = E, self.n_r, self.n_rho
         s.cutoff = self.cutoff
