@@ -82,28 +82,37 @@ __device__ __forceinline__ Lerp lerp_r(float r, const SimEAMTables& t) {
 
 // ---------------------------------------------------------------------------
 // pass 1
-template <bool ORTHO>
+// Shared-memory window of the r-tables: rows k in [k_lo, n_r) (r >= k_lo dr);
+// the rare shorter distances read the global table.
+struct Window {
+    int k_lo, n_win;
+};
+
+template <bool SMEM, bool ORTHO>
 __device__ __forceinline__ float density_term(const BoxF& b, const int4& qi, const int4& qj, float rc2,
-                                              const float2* tab_i, const SimEAMTables& t) {
+                                              const float2* g_i, const float2* s_i, Window w,
+                                              const SimEAMTables& t) {
     float r0, r1, r2;
     rvec<ORTHO>(b, qi, qj, r0, r1, r2);
     const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
     if (!(d2 < rc2)) return 0.0f;
     const Lerp l = lerp_r(d2 * rsqrt_approx(d2), t);
-    const float2 v = tab_i[(size_t)qj.w * t.n_r + l.k];
+    float2 v;
+    if (SMEM && l.k >= w.k_lo) v = s_i[qj.w * w.n_win + (l.k - w.k_lo)];
+    else v = __ldg(&g_i[(size_t)qj.w * t.n_r + l.k]);
     return fmaf(l.frac, v.y, v.x);
 }
 
 template <bool SMEM, bool ORTHO>
-__global__ void __launch_bounds__(EAM_DENSITY_THREADS) k_eam_density(SimEngine e, SimEAMTables t) {
+__global__ void __launch_bounds__(EAM_DENSITY_THREADS) k_eam_density(SimEngine e, SimEAMTables t, Window w) {
     extern __shared__ float2 s_dens[];
     const float2* dens = reinterpret_cast<const float2*>(t.dens_vd);
     const int nt = t.n_types;
     if (SMEM) {
-        const int total = nt * nt * t.n_r;
-        for (int k = threadIdx.x; k < total; k += blockDim.x) s_dens[k] = __ldg(&dens[k]);
+        for (int tt = 0; tt < nt * nt; ++tt)
+            for (int k = threadIdx.x; k < w.n_win; k += blockDim.x)
+                s_dens[tt * w.n_win + k] = __ldg(&dens[(size_t)tt * t.n_r + w.k_lo + k]);
         __syncthreads();
-        dens = s_dens;
     }
     const BoxF b(*e.box);
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
@@ -116,7 +125,8 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS) k_eam_density(SimEngine e
         const int4 qi = posq[i];
         const int ti = qi.w;
         const int nn = e.nnbr[i];
-        const float2* tab_i = dens + (size_t)ti * nt * t.n_r;
+        const float2* g_i = dens + (size_t)ti * nt * t.n_r;
+        const float2* s_i = s_dens + (size_t)ti * nt * w.n_win;
         float rho = 0.0f;
         int k = 0;
         for (; k + 4 <= nn; k += 4) {
@@ -127,10 +137,11 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS) k_eam_density(SimEngine e
 #pragma unroll
             for (int u = 0; u < 4; ++u) q[u] = __ldg(&posq[j[u]]);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) rho += density_term<ORTHO>(b, qi, q[u], rc2, tab_i, t);
+            for (int u = 0; u < 4; ++u) rho += density_term<SMEM, ORTHO>(b, qi, q[u], rc2, g_i, s_i, w, t);
         }
         for (; k < nn; ++k)
-            rho += density_term<ORTHO>(b, qi, __ldg(&posq[__ldg(&nbr[(int64_t)k * P + i])]), rc2, tab_i, t);
+            rho += density_term<SMEM, ORTHO>(b, qi, __ldg(&posq[__ldg(&nbr[(int64_t)k * P + i])]), rc2, g_i, s_i,
+                                             w, t);
         float F, Fp;
         embed_lookup(t, ti, rho, F, Fp);
         posfp[i] = make_int4(qi.x, qi.y, qi.z, __float_as_int(Fp));
@@ -160,8 +171,9 @@ __device__ __forceinline__ void pair_force(float s, float phi, float r, float in
 // {phi, dphi} staged in shared memory.
 template <bool ORTHO>
 __device__ __forceinline__ void pair_single(const BoxF& b, const int4& pi, const int4& qj, float rc2, float fpi,
-                                            const float4* tab_d, const float2* tab_p, const SimEAMTables& t,
-                                            float& fx, float& fy, float& fz, float (&acc)[15]) {
+                                            const float4* tab_d, const float2* tab_p, Window w,
+                                            const SimEAMTables& t, float& fx, float& fy, float& fz,
+                                            float (&acc)[15]) {
     float r0, r1, r2;
     rvec<ORTHO>(b, pi, qj, r0, r1, r2);
     const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
@@ -169,8 +181,15 @@ __device__ __forceinline__ void pair_single(const BoxF& b, const int4& pi, const
     const float inv_r = rsqrt_approx(d2);
     const float r = d2 * inv_r;
     const Lerp l = lerp_r(r, t);
-    const float4 d = tab_d[l.k];
-    const float2 p = tab_p[l.k];
+    float4 d;
+    float2 p;
+    if (l.k >= w.k_lo) {
+        d = tab_d[l.k - w.k_lo];
+        p = tab_p[l.k - w.k_lo];
+    } else {
+        d = __ldg(reinterpret_cast<const float4*>(t.deriv_vd) + l.k);
+        p = __ldg(reinterpret_cast<const float2*>(t.pair_vd) + l.k);
+    }
     const float2 dd_dp = __ffma2_rn(make_float2(l.frac, l.frac), make_float2(d.z, d.w), make_float2(d.x, d.y));
     const float phi = fmaf(l.frac, p.y, p.x);
     pair_force(fmaf(fpi + __int_as_float(qj.w), dd_dp.x, dd_dp.y), phi, r, inv_r, r0, r1, r2, fx, fy, fz, acc);
@@ -180,14 +199,15 @@ __device__ __forceinline__ void pair_single(const BoxF& b, const int4& pi, const
 // velocity Verlet with the Langevin O-step (integrator.py:102-124) -- and
 // accumulates K and sum m v(x)v, so the half kick needs no extra pass.
 template <bool SINGLE, bool INTEG, bool ORTHO>
-__global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e, SimEAMTables t, SimIntegrator ip) {
+__global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e, SimEAMTables t, SimIntegrator ip,
+                                                                    Window w) {
     extern __shared__ float4 s_tab4[];
     float4* tab_d = s_tab4;
-    float2* tab_p = reinterpret_cast<float2*>(s_tab4 + t.n_r);
+    float2* tab_p = reinterpret_cast<float2*>(s_tab4 + w.n_win);
     if (SINGLE) {
-        const float4* gd = reinterpret_cast<const float4*>(t.deriv_vd);
-        const float2* gp = reinterpret_cast<const float2*>(t.pair_vd);
-        for (int k = threadIdx.x; k < t.n_r; k += blockDim.x) {
+        const float4* gd = reinterpret_cast<const float4*>(t.deriv_vd) + w.k_lo;
+        const float2* gp = reinterpret_cast<const float2*>(t.pair_vd) + w.k_lo;
+        for (int k = threadIdx.x; k < w.n_win; k += blockDim.x) {
             tab_d[k] = __ldg(&gd[k]);
             tab_p[k] = __ldg(&gp[k]);
         }
@@ -208,18 +228,22 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e,
         float fx = 0.f, fy = 0.f, fz = 0.f;
         int ti = 0;
         if (SINGLE) {
+            // the next two list entries are fetched while the current pair is
+            // gathered and evaluated, so the list's DRAM latency overlaps work
+            int jn0 = nn > 0 ? __ldg(&nbr[i]) : 0;
+            int jn1 = nn > 1 ? __ldg(&nbr[P + i]) : 0;
             int k = 0;
             for (; k + 2 <= nn; k += 2) {
-                const int j0 = __ldg(&nbr[(int64_t)k * P + i]);
-                const int j1 = __ldg(&nbr[(int64_t)(k + 1) * P + i]);
+                const int j0 = jn0, j1 = jn1;
+                if (k + 2 < nn) jn0 = __ldg(&nbr[(int64_t)(k + 2) * P + i]);
+                if (k + 3 < nn) jn1 = __ldg(&nbr[(int64_t)(k + 3) * P + i]);
                 const int4 q0 = __ldg(&posfp[j0]);
                 const int4 q1 = __ldg(&posfp[j1]);
-                pair_single<ORTHO>(b, pi, q0, rc2, fpi, tab_d, tab_p, t, fx, fy, fz, acc);
-                pair_single<ORTHO>(b, pi, q1, rc2, fpi, tab_d, tab_p, t, fx, fy, fz, acc);
+                pair_single<ORTHO>(b, pi, q0, rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
+                pair_single<ORTHO>(b, pi, q1, rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
             }
             if (k < nn)
-                pair_single<ORTHO>(b, pi, __ldg(&posfp[__ldg(&nbr[(int64_t)k * P + i])]), rc2, fpi, tab_d, tab_p, t,
-                                   fx, fy, fz, acc);
+                pair_single<ORTHO>(b, pi, __ldg(&posfp[jn0]), rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
         } else {
             const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
             const int nt = t.n_types;
@@ -281,8 +305,18 @@ using namespace simb200;
 
 static const size_t kSmemLimit = 200 * 1024;
 
-static size_t smem_pass1(const SimEAMTables& t) { return (size_t)t.n_types * t.n_types * t.n_r * sizeof(float2); }
-static size_t smem_pass2(const SimEAMTables& t) { return (size_t)t.n_r * (sizeof(float4) + sizeof(float2)); }
+// Rows of the r-tables kept in shared memory: the top kWindowRows (r from
+// (n_r - kWindowRows) dr up to the cutoff; 2.2 A for an 8192-row table on
+// [0, 4.4 A]).  A smaller footprint leaves L1 capacity for neighbour gathers.
+static const int kWindowRows = 4096;
+static Window table_window(const SimEAMTables& t) {
+    const int n_win = t.n_r < kWindowRows ? t.n_r : kWindowRows;
+    return Window{t.n_r - n_win, n_win};
+}
+static size_t smem_pass1(const SimEAMTables& t) {
+    return (size_t)t.n_types * t.n_types * table_window(t).n_win * sizeof(float2);
+}
+static size_t smem_pass2(const SimEAMTables& t) { return (size_t)table_window(t).n_win * (sizeof(float4) + sizeof(float2)); }
 
 template <typename K>
 static void allow_smem(K kernel) {
@@ -311,7 +345,7 @@ template <bool SMEM, bool ORTHO>
 static int launch_density(const SimEngine& e, const SimEAMTables& t, size_t smem, cudaStream_t st) {
     const int g = persistent_grid((const void*)k_eam_density<SMEM, ORTHO>, EAM_DENSITY_THREADS, smem, e.n);
     if (g > e.n_blocks_max) return SIM_ERR_ARG;
-    k_eam_density<SMEM, ORTHO><<<g, EAM_DENSITY_THREADS, smem, st>>>(e, t);
+    k_eam_density<SMEM, ORTHO><<<g, EAM_DENSITY_THREADS, smem, st>>>(e, t, table_window(t));
     return SIM_OK;
 }
 
@@ -336,7 +370,7 @@ static int launch_force(const SimEngine& e, const SimEAMTables& t, const SimInte
     const size_t smem = SINGLE ? smem_pass2(t) : 0;
     const int g = persistent_grid((const void*)k_eam_force<SINGLE, INTEG, ORTHO>, EAM_FORCE_THREADS, smem, e.n);
     if (g > e.n_blocks_max) return SIM_ERR_ARG;
-    k_eam_force<SINGLE, INTEG, ORTHO><<<g, EAM_FORCE_THREADS, smem, st>>>(e, t, ip);
+    k_eam_force<SINGLE, INTEG, ORTHO><<<g, EAM_FORCE_THREADS, smem, st>>>(e, t, ip, table_window(t));
     return SIM_OK;
 }
 
