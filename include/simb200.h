@@ -52,6 +52,9 @@ extern "C" {
 #define SIM_STATUS_OVERFLOW  8   /* device: a neighbour row exceeded the ELL capacity          */
 #define SIM_STATUS_NONFINITE 16  /* device: NaN/Inf in forces, positions or velocities         */
 #define SIM_STATUS_CELLCAP   32  /* device: half-list export row capacity exceeded             */
+#define SIM_STATUS_HALO      64  /* device: a tile's halo exceeded halo_cap (flags[4] = size)  */
+
+#define SIM_TILE 1024            /* atoms per neighbour tile (= threads of a tiled block)      */
 
 /* ---- simulation box (rows are lattice vectors, row-vector convention) -- */
 typedef struct SimBox {
@@ -110,6 +113,14 @@ typedef struct SimEngine {
     int32_t  n_blocks_max;
     int32_t  box_orthogonal;  /* 1 if the box is (and stays) orthogonal: selects the
                                  kernels specialised for a diagonal H */
+    /* neighbour tiles: SIM_TILE consecutive slots per tile; the tile's halo is the
+     * sorted set of out-of-tile neighbour slots; nbr16 holds the list as tile-local
+     * indices (< SIM_TILE: own slot tile*SIM_TILE + idx; else halo[idx - SIM_TILE]).
+     * NULL nbr16 disables the tiled kernels.                                     */
+    int32_t  n_tiles, halo_cap;
+    int32_t* halo;        /* [n_tiles][halo_cap] */
+    int32_t* halo_n;      /* [n_tiles] */
+    uint16_t* nbr16;      /* [nbr_cap][n_pad] */
 } SimEngine;
 
 /* reduction slot layout (FP64 Kahan-compensated sums over all atoms) */

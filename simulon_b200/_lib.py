@@ -46,7 +46,9 @@ class SimEngine(ctypes.Structure):
                 ("orig_alt", c_p),
                 ("inv_mass", c_p), ("mass", c_p),
                 ("flags", c_p), ("partials", c_p), ("red_counter", c_p), ("red_out", c_p),
-                ("n_blocks_max", ctypes.c_int32), ("box_orthogonal", ctypes.c_int32)]
+                ("n_blocks_max", ctypes.c_int32), ("box_orthogonal", ctypes.c_int32),
+                ("n_tiles", ctypes.c_int32), ("halo_cap", ctypes.c_int32),
+                ("halo", c_p), ("halo_n", c_p), ("nbr16", c_p)]
 
 
 class SimEAMTables(ctypes.Structure):

@@ -15,6 +15,11 @@ void prepare_capture_stream();           // side stream used to capture IF-node 
 // Persistent grid: resident blocks per SM (cached occupancy query) x SM count,
 // capped by the number of atom tiles.
 int persistent_grid(const void* fn, int threads, size_t smem, int64_t n);
+// neighbour tiles (tiles.cu)
+void launch_build_halo(const SimEngine& e, const int32_t* gate, cudaStream_t st);
+bool tiled_eam_usable(const SimEngine& e, const SimEAMTables& t);
+int launch_eam_density_tiled(const SimEngine& e, const SimEAMTables& t, cudaStream_t st);
+int launch_eam_force_tiled(const SimEngine& e, const SimEAMTables& t, const SimIntegrator* ip, cudaStream_t st);
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 

@@ -357,7 +357,9 @@ extern "C" int sim_eam_density(const SimEngine* ep, const SimEAMTables* tp, void
     const size_t s1 = smem_pass1(t);
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
-    if (s1 <= kSmemLimit)
+    if (tiled_eam_usable(e, t))
+        rc = launch_eam_density_tiled(e, t, st);
+    else if (s1 <= kSmemLimit)
         rc = e.box_orthogonal ? launch_density<true, true>(e, t, s1, st) : launch_density<true, false>(e, t, s1, st);
     else
         rc = e.box_orthogonal ? launch_density<false, true>(e, t, 0, st) : launch_density<false, false>(e, t, 0, st);
@@ -388,7 +390,9 @@ static int launch_eam_force(const SimEngine* ep, const SimEAMTables* tp, const S
     cudaStream_t st = (cudaStream_t)stream;
     const bool single = t.n_types == 1 && smem_pass2(t) <= kSmemLimit;
     int rc;
-    if (single)
+    if (tiled_eam_usable(e, t))
+        rc = launch_eam_force_tiled(e, t, INTEG ? &integ : nullptr, st);
+    else if (single)
         rc = e.box_orthogonal ? launch_force<true, INTEG, true>(e, t, integ, st)
                               : launch_force<true, INTEG, false>(e, t, integ, st);
     else

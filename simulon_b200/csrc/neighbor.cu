@@ -507,6 +507,7 @@ extern "C" int sim_rebuild(const SimEngine* ep, int32_t only_if_flagged, void* s
     const float rc2_list = (float)(e.x_rc * e.x_rc * (1.0 + 4e-6));
     // cell_lin (rank -> linear index) is stored right after cell_rank
     k_build_ell<<<g, SIM_THREADS, 0, st>>>(e, e.cell_rank + e.n_cells, rc2_list, gate);
+    launch_build_halo(e, gate, st);
     k_finish_rebuild<<<1, 1, 0, st>>>(e.flags, only_if_flagged ? 1 : 0);
     return launch_status("sim_rebuild");
 }

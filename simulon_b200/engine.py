@@ -24,6 +24,8 @@ from . import _lib
 MASS_TO_INTERNAL = 10.0 / (6.02214076e23 * 1.60218e-19)   # amu -> eV ps^2 / A^2 (integrator.py:61-64)
 KB_EV = 8.617333262e-5                                      # integrator.py:41
 LOG_EXTRA = 2                                               # pressure (bar), mu
+TILE = 1024                 # atoms per neighbour tile (SIM_TILE)
+HALO_CAP_MAX = 4096         # largest halo the tiled kernels accept
 
 
 def make_box(H) -> _lib.SimBox:
@@ -97,7 +99,8 @@ class MDEngine:
     """
 
     def __init__(self, positions, types, masses_amu, H, cutoff: float, skin: float, *, velocities=None,
-                 device=None, nbr_cap: int | None = None, fp64_forces: bool = False, log_capacity: int = 4096):
+                 device=None, nbr_cap: int | None = None, fp64_forces: bool = False, log_capacity: int = 4096,
+                 use_tiles: bool = True, halo_cap: int = 3072):
         self.lib = _lib.load()
         self.device = torch.device(device or "cuda")
         if self.device.type != "cuda":
@@ -131,7 +134,10 @@ class MDEngine:
         self.xref = torch.zeros(3, P, **i32)
         self.orig = torch.zeros(P, **i32)
         self.posfp = torch.zeros(P, 4, **i32)
-        self.nbr = torch.zeros(self.nbr_cap, P, **i32)
+        self.n_tiles = (n + TILE - 1) // TILE
+        self.halo_cap = int(halo_cap)
+        self.use_tiles = bool(use_tiles)
+        self._alloc_lists()
         self.nnbr = torch.zeros(P, **i32)
         self.cell_of = torch.zeros(P, **i32)
         self.cell_count = torch.zeros(self.n_cells + 1, **i32)
@@ -183,6 +189,8 @@ class MDEngine:
             setattr(s, name, p(getattr(self, name)))
         s.n_blocks_max = self.n_blocks_max
         s.box_orthogonal = int(self.box.orthogonal)
+        s.n_tiles, s.halo_cap = self.n_tiles, self.halo_cap
+        s.halo, s.halo_n, s.nbr16 = _lib.ptr(self.halo), _lib.ptr(self.halo_n), _lib.ptr(self.nbr16)
         self.st = s
         self.st_ref = ctypes.byref(s)
 
@@ -200,20 +208,39 @@ class MDEngine:
         self.forces_valid = False
         self.ensure_capacity()
 
+    def _alloc_lists(self):
+        dev, P = self.device, self.n_pad
+        self.nbr = torch.zeros(self.nbr_cap, P, device=dev, dtype=torch.int32)
+        if self.use_tiles:
+            self.nbr16 = torch.zeros(self.nbr_cap, P, device=dev, dtype=torch.int16)
+            self.halo = torch.zeros(self.n_tiles, self.halo_cap, device=dev, dtype=torch.int32)
+            self.halo_n = torch.zeros(self.n_tiles, device=dev, dtype=torch.int32)
+        else:
+            self.nbr16 = self.halo = self.halo_n = None
+
     def ensure_capacity(self) -> bool:
-        """Grow the ELL list if the last rebuild overflowed (synchronises).  True if it grew."""
-        flags = self.flags.cpu()
-        if not int(flags[1]) & _lib.SIM_STATUS_OVERFLOW:
-            return False
-        need = int(flags[2])
-        self.nbr_cap = int(math.ceil((need * 1.15 + 8) / 8.0) * 8)
-        self.nbr = torch.zeros(self.nbr_cap, self.n_pad, device=self.device, dtype=torch.int32)
-        self.flags.zero_()
-        self._make_struct()
-        _lib.call("sim_rebuild", self.st_ref, 0, self.stream)
-        if int(self.flags[1].item()) & _lib.SIM_STATUS_OVERFLOW:
-            raise _lib.SimError("neighbour list overflow persists after growing the capacity")
-        return True
+        """Grow the neighbour list or the tile halos if the last rebuild overflowed
+        them (synchronises).  True if anything grew."""
+        grew = False
+        for _ in range(3):
+            flags = self.flags.cpu()
+            bits = int(flags[1])
+            if not bits & (_lib.SIM_STATUS_OVERFLOW | _lib.SIM_STATUS_HALO):
+                return grew
+            if bits & _lib.SIM_STATUS_OVERFLOW:
+                self.nbr_cap = int(math.ceil((int(flags[2]) * 1.15 + 8) / 8.0) * 8)
+            if bits & _lib.SIM_STATUS_HALO:
+                want = int(math.ceil(int(flags[4]) * 1.2 / 256.0) * 256)
+                if want <= HALO_CAP_MAX:
+                    self.halo_cap = max(self.halo_cap, want)
+                else:
+                    self.use_tiles = False          # fall back to the untiled kernels
+            self._alloc_lists()
+            self.flags.zero_()
+            self._make_struct()
+            _lib.call("sim_rebuild", self.st_ref, 0, self.stream)
+            grew = True
+        raise _lib.SimError("neighbour list / halo overflow persists after growing the capacity")
 
     def gather(self, which: str) -> torch.Tensor:
         """[N,3] float64 in the original atom order: 'x', 'v', 'f' (forces)."""

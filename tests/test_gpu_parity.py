@@ -152,6 +152,29 @@ def test_eam_perfect_lattice_known_answer(sb, fsw_path):
     assert float(eng.gather("f").abs().max()) < 1e-5
 
 
+@pytest.mark.parametrize("tri", [False, True])
+def test_eam_tiled_equals_untiled(sb, fsw_path, tri):
+    """Shared-memory neighbour tiles (16-bit tile-local lists) reproduce the
+    untiled kernels' forces bit for bit; sums agree to float32 round-off."""
+    if tri:
+        x, H = oin.bcc_triclinic(14)
+    else:
+        x, L = oin.bcc_lattice(16)
+        H = np.diag([L] * 3)
+    x = oin.jitter(x, 0.07, 41)
+    parser = sb.EAMParser(fsw_path)
+    tables = sb.EAMDeviceTables(parser, DEV)
+    out = []
+    for tiles in (False, True):
+        eng = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], H, parser.cutoff, 0.5, device=DEV,
+                          use_tiles=tiles)
+        assert eng.n_tiles > 1 and eng.status() == 0
+        eng.eam_forces(tables)
+        out.append((eng.gather("f").cpu(), eng.red_out.cpu().numpy()))
+    assert torch.equal(out[0][0], out[1][0])
+    np.testing.assert_allclose(out[1][1][:9], out[0][1][:9], rtol=1e-6, atol=1e-6)
+
+
 def test_eam_reruns_bitwise_identical(sb, fsw_path):
     x, L = oin.bcc_lattice(16)
     x = oin.jitter(x, 0.07, 40)
