@@ -18,6 +18,7 @@ SIM_ERR_CUDA = 2
 SIM_ERR_BOX = 4
 SIM_STATUS_OVERFLOW = 8
 SIM_STATUS_NONFINITE = 16
+SIM_STATUS_HALO = 64
 
 RED_EPOT_EMBED, RED_EPOT_PAIR, RED_VIRIAL = 0, 1, 2
 RED_W = slice(3, 9)          # xx yy zz xy xz yz

@@ -143,3 +143,27 @@ def test_product_path_refuses_cpu():
     x, L = oin.bcc_lattice(3)
     with pytest.raises(RuntimeError):
         sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], np.diag([L] * 3), 4.4, 0.5, device="cpu")
+
+
+def test_package_references_resolve():
+    """Every `_lib.<name>` / `engine.<name>` attribute the package uses exists
+    (these modules cannot be exercised end to end without a GPU)."""
+    import ast
+    import glob
+    from simulon_b200 import _lib, engine
+    mods = {"_lib": _lib}
+    missing = []
+    for path in glob.glob(os.path.join(ROOT, "simulon_b200", "*.py")) + [os.path.join(ROOT, "bench.py")]:
+        tree = ast.parse(open(path).read())
+        for node in ast.walk(tree):
+            if isinstance(node, ast.Attribute) and isinstance(node.value, ast.Name) and node.value.id in mods:
+                if not hasattr(mods[node.value.id], node.attr):
+                    missing.append(f"{os.path.basename(path)}: {node.value.id}.{node.attr}")
+    assert not missing, missing
+    # status bits mirror the header
+    hdr = open(os.path.join(ROOT, "include", "simb200.h")).read()
+    for name in ("SIM_OK", "SIM_ERR_ARG", "SIM_ERR_CUDA", "SIM_STATUS_OVERFLOW", "SIM_STATUS_NONFINITE",
+                 "SIM_STATUS_HALO"):
+        val = int(re.search(rf"#define {name}\s+(\d+)", hdr).group(1))
+        assert getattr(_lib, name) == val, name
+    assert engine.TILE == int(re.search(r"#define SIM_TILE\s+(\d+)", hdr).group(1))
