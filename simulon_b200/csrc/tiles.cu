@@ -383,32 +383,41 @@ static int tiled_grid(const SimEngine& e) {
     return e.n_tiles < sms ? e.n_tiles : sms;
 }
 
+// Opt in to the largest dynamic shared memory the kernel can use: the device's
+// per-block opt-in limit minus the kernel's static shared memory.
 template <typename K>
-static void allow_smem_tiled(K kernel) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmemLimit);
+static bool allow_smem_tiled(K kernel) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return false;
+    const int dyn = optin - (int)fa.sharedSizeBytes;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess) return false;
+    if (dyn < (int)kTileSmemLimit) kTileSmemLimit = (size_t)dyn;
+    return true;
 }
 
-static void tiled_set_attributes() {
-    static bool done = false;   // the first call happens before any stream capture
-    if (!done) {
-        allow_smem_tiled(k_eam_density_tiled<true>);
-        allow_smem_tiled(k_eam_density_tiled<false>);
-        allow_smem_tiled(k_eam_force_tiled<true, true>);
-        allow_smem_tiled(k_eam_force_tiled<true, false>);
-        allow_smem_tiled(k_eam_force_tiled<false, true>);
-        allow_smem_tiled(k_eam_force_tiled<false, false>);
-        done = true;
+static bool tiled_set_attributes() {
+    static int state = 0;   // 0 unset, 1 ok, -1 failed; the first call precedes any stream capture
+    if (state == 0) {
+        bool ok = allow_smem_tiled(k_eam_density_tiled<true>) && allow_smem_tiled(k_eam_density_tiled<false>) &&
+                  allow_smem_tiled(k_eam_force_tiled<true, true>) && allow_smem_tiled(k_eam_force_tiled<true, false>) &&
+                  allow_smem_tiled(k_eam_force_tiled<false, true>) &&
+                  allow_smem_tiled(k_eam_force_tiled<false, false>);
+        state = ok ? 1 : -1;
+        cudaGetLastError();   // a failed attribute call must not surface at the next launch check
     }
+    return state == 1;
 }
 
 bool tiled_eam_usable(const SimEngine& e, const SimEAMTables& t) {
     return e.nbr16 && e.halo && e.halo_n && e.n_tiles > 0 && e.halo_cap > 0 && e.halo_cap <= HALO_SORT_MAX &&
-           t.n_types == 1 && tiled_smem_pass1(e, t) <= kTileSmemLimit - 8 * 1024 &&
-           tiled_smem_pass2(e, t) <= kTileSmemLimit - 8 * 1024;
+           t.n_types == 1 && tiled_set_attributes() && tiled_smem_pass1(e, t) <= kTileSmemLimit &&
+           tiled_smem_pass2(e, t) <= kTileSmemLimit;
 }
 
 int launch_eam_density_tiled(const SimEngine& e, const SimEAMTables& t, cudaStream_t st) {
-    tiled_set_attributes();
     const int g = tiled_grid(e);
     if (g > e.n_blocks_max) return SIM_ERR_ARG;
     const size_t smem = tiled_smem_pass1(e, t);
@@ -418,7 +427,6 @@ int launch_eam_density_tiled(const SimEngine& e, const SimEAMTables& t, cudaStre
 }
 
 int launch_eam_force_tiled(const SimEngine& e, const SimEAMTables& t, const SimIntegrator* ip, cudaStream_t st) {
-    tiled_set_attributes();
     const int g = tiled_grid(e);
     if (g > e.n_blocks_max) return SIM_ERR_ARG;
     const size_t smem = tiled_smem_pass2(e, t);
