@@ -100,7 +100,7 @@ class MDEngine:
 
     def __init__(self, positions, types, masses_amu, H, cutoff: float, skin: float, *, velocities=None,
                  device=None, nbr_cap: int | None = None, fp64_forces: bool = False, log_capacity: int = 4096,
-                 use_tiles: bool = True, halo_cap: int = 3072):
+                 use_tiles: bool = False, halo_cap: int = 3072):
         self.lib = _lib.load()
         self.device = torch.device(device or "cuda")
         if self.device.type != "cuda":
