@@ -270,6 +270,30 @@ int sim_eam_force(const SimEngine* e, const SimEAMTables* t, void* stream);
  * sim_eam_force followed by sim_integrate_second with FP32 forces. */
 int sim_eam_force_integrate(const SimEngine* e, const SimEAMTables* t, const SimIntegrator* p, void* stream);
 
+/* sim_eam_forces without caller-allocated scratch.  No counterpart in the
+ * reference (which allocates through PyTorch on every call); it exists for
+ * callers that cannot allocate device memory for the call -- a host code
+ * whose device memory is all handed out up front by its own pool, or one that
+ * binds this library over a plain C FFI with no device allocator.
+ *   Scratch: the per-atom {x, y, z, F'} records passed from the density pass
+ *   to the force pass, the reduction partials and the last-block counters come
+ *   from one fixed 4,456,704-byte array inside the library; e->posfp,
+ *   e->partials, e->red_counter and e->n_blocks_max are ignored (may be NULL /
+ *   0).  Every other SimEngine buffer and the outputs (f32 or f64, red_out,
+ *   flags) are the caller's, as for sim_eam_forces.
+ *   Limit: e->n_pad <= SIM_STATIC_MAX_ATOMS; a larger system returns
+ *   SIM_ERR_ARG before any CUDA call, with the reason in sim_last_cuda_error().
+ *   Set-up: the first call on each device looks up the array's device address
+ *   (cudaGetSymbolAddress, that device current); make it before any stream
+ *   capture.  Each call zeroes the counters itself (cudaMemsetAsync on
+ *   `stream`); nothing else has to start at zero.
+ *   Concurrency: one array per device, shared by all calls -- calls that can
+ *   overlap (other streams or host threads on the same device) race on it;
+ *   serialise them.
+ *   Allocates nothing: no cudaMalloc / cudaFree, no allocating library call. */
+#define SIM_STATIC_MAX_ATOMS 262144
+int sim_eam_forces_static(const SimEngine* e, const SimEAMTables* t, void* stream);
+
 /* LJ forces; precision 0 = FP32 pair arithmetic, 1 = FP64 (positions read
  * from e->x, forces to e->f64).  Scalar virial = sum F*r (lennard_jones_force.py:93). */
 int sim_lj_forces(const SimEngine* e, const SimLJParams* p, int32_t precision, void* stream);

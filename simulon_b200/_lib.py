@@ -19,6 +19,7 @@ SIM_ERR_BOX = 4
 SIM_STATUS_OVERFLOW = 8
 SIM_STATUS_NONFINITE = 16
 SIM_STATUS_HALO = 64
+SIM_STATIC_MAX_ATOMS = 262144   # atom-slot limit of sim_eam_forces_static
 
 RED_EPOT_EMBED, RED_EPOT_PAIR, RED_VIRIAL = 0, 1, 2
 RED_W = slice(3, 9)          # xx yy zz xy xz yz
@@ -97,6 +98,7 @@ SIGNATURES = {
     "sim_rebuild": [_P(SimEngine), ctypes.c_int32, c_p],
     "sim_rebuild_if_needed": [_P(SimEngine), c_p],
     "sim_eam_forces": [_P(SimEngine), _P(SimEAMTables), c_p],
+    "sim_eam_forces_static": [_P(SimEngine), _P(SimEAMTables), c_p],
     "sim_eam_density": [_P(SimEngine), _P(SimEAMTables), c_p],
     "sim_eam_force": [_P(SimEngine), _P(SimEAMTables), c_p],
     "sim_eam_force_integrate": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), c_p],

@@ -10,6 +10,7 @@ namespace simb200 {
 
 // ---- error plumbing --------------------------------------------------------
 void set_cuda_error(cudaError_t err, const char* where);
+void set_error_text(const char* msg);        // message returned by sim_last_cuda_error()
 int  launch_status(const char* where);   // checks cudaGetLastError after a launch
 void prepare_capture_stream();           // side stream used to capture IF-node bodies
 // Persistent grid: resident blocks per SM (cached occupancy query) x SM count,

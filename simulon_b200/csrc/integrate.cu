@@ -27,6 +27,8 @@ void set_cuda_error(cudaError_t err, const char* where) {
     snprintf(g_err, sizeof(g_err), "%s: %s (%s)", where, cudaGetErrorString(err), cudaGetErrorName(err));
 }
 
+void set_error_text(const char* msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
+
 int persistent_grid(const void* fn, int threads, size_t smem, int64_t n) {
     // cached per (kernel, block, smem) so calls made while a stream is being
     // captured only read the cache
