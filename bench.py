@@ -35,6 +35,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "atom-steps/s (EAM-W, 1 B200): plain vs batched vs MLP at stated force RMSE"
 UNIT = "atom-steps/s"
+PASS2_DRAM_BYTES_PER_ATOM = (78706432 + 6443776) / 524288   # k_eam_force<1,1,1>, ncu --set full
 A_W, M_W = 3.165, 183.84
 
 
@@ -284,6 +285,10 @@ def run_b200(args):
     bytes_pass2 = N * (16 + 4 * nbar + 4 + 16 + 48)      # posq, list, own F', force out, v read+write
     bytes_pass1 = N * (16 + 4 * nbar + 4)                # posq, list, F' out
     achieved = bytes_pass2 / (k_ms / 1e3) / 1e9
+    # measured DRAM bytes per atom of this kernel: dram__bytes_read.sum +
+    # dram__bytes_write.sum of one ncu capture on BCC W 2*64^3 = 524,288 atoms,
+    # scaled by the atom count (traffic grows with the atoms processed)
+    traffic = N * PASS2_DRAM_BYTES_PER_ATOM
     # step-level algorithmic bytes per atom-step (EAM: pass1 + pass2 + integrator 152 + rebuild/K)
     rebuild_bytes = 16 + 88 + 4 * nbar
     K_rb = args.steps / max(rebuilds, 1)
@@ -303,7 +308,8 @@ def run_b200(args):
             "roofline": {"bound": "hbm", "kernel": "k_eam_force<single,integ,ortho> (EAM pass 2 + second half-step)",
                          "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "bytes_per_launch": bytes_pass2, "launch_ms": k_ms,
+                         "traffic": traffic, "traffic_source": "ncu capture at 524,288 atoms, scaled per atom",
+                         "bytes_per_launch": bytes_pass2, "launch_ms": k_ms,
                          "pass1_ms": p1_ms, "pass1_bytes": bytes_pass1},
             "step_roofline": {"bytes_per_atom_step": B_step, "achieved": step_achieved, "peak": peak,
                               "frac": step_achieved / peak, "unit": "GB/s"},
