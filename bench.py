@@ -199,6 +199,18 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ GPU arm
+def launches_for(steps: int, graph_steps: int) -> int:
+    """Kernels of ours launched by BaseModel.run(steps): per run of k > 1 steps,
+    the first half-step and its IF-node condition, then per step EAM pass 1,
+    pass 2 (fused with the second half and the next first half) and the step
+    log, plus the IF-node condition between steps (4k + 1); a single step is
+    first half, condition, pass 1, pass 2 + second half, log (5).  Each
+    triggered rebuild adds the 10 kernels of the IF body."""
+    full, rest = divmod(int(steps), int(graph_steps))
+    per = lambda k: 0 if k == 0 else (5 if k == 1 else 4 * k + 1)
+    return full * per(int(graph_steps)) + per(rest)
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -314,9 +326,7 @@ def run_b200(args):
             "step_roofline": {"bytes_per_atom_step": B_step, "achieved": step_achieved, "peak": peak,
                               "frac": step_achieved / peak, "unit": "GB/s"},
             "clocks": clocks.summary(),
-            # per step: first half, IF-node condition, EAM pass 1, pass 2 + second half, step log;
-            # each triggered rebuild adds its 10 kernels (the IF body)
-            "gpu_launches": 5 * args.steps + 10 * rebuilds}
+            "gpu_launches": launches_for(args.steps, G) + 10 * rebuilds}
 
     if not args.no_extras and rank == 0:
         line["e2e"] = e2e(model, mol, x, v, args, dev)

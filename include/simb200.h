@@ -5,7 +5,8 @@
  * (passed as void*), launches asynchronously on that stream and returns an
  * int status (SIM_OK = 0).  Nothing is allocated inside the library and no
  * device state is kept between calls: the caller (PyTorch on the Python side)
- * owns every buffer.  Errors found on the device (neighbour-list overflow,
+ * owns every buffer (one exception: the fixed scratch array used by
+ * sim_eam_forces_static).  Errors found on the device (neighbour-list overflow,
  * non-finite values, box too small) are reported through a caller-owned
  * device status word that the host reads when it chooses to synchronise.
  *
@@ -121,6 +122,10 @@ typedef struct SimEngine {
     int32_t* halo;        /* [n_tiles][halo_cap] */
     int32_t* halo_n;      /* [n_tiles] */
     uint16_t* nbr16;      /* [nbr_cap][n_pad] */
+    /* EAM pass 1 records which list slots lie inside the cutoff (bit k of
+     * cut_mask[i] for slot k of atom i) and pass 2 visits only those; needs
+     * nbr_cap <= 64.  NULL: pass 2 tests every slot itself.                      */
+    uint64_t* cut_mask;   /* [n_pad] or NULL */
 } SimEngine;
 
 /* reduction slot layout (FP64 Kahan-compensated sums over all atoms) */
@@ -269,6 +274,16 @@ int sim_eam_force(const SimEngine* e, const SimEAMTables* t, void* stream);
  * half kick, K and K tensor) fused into its epilogue; equivalent to
  * sim_eam_force followed by sim_integrate_second with FP32 forces. */
 int sim_eam_force_integrate(const SimEngine* e, const SimEAMTables* t, const SimIntegrator* p, void* stream);
+/* sim_eam_force_integrate plus the first half of the NEXT step in the same
+ * pass (kick with the new forces, drift, posq refresh, skin/2 trigger into
+ * flags[0]): bit for bit sim_eam_force_integrate followed by
+ * sim_integrate_first(force_precision 0).  p->step_ctr must point to two
+ * words: [0] is advanced to the next step, [1] receives this step's index
+ * (pass &step_ctr[1] to sim_log_step for this step).  The state between such
+ * calls holds half-step velocities; end a run with sim_eam_force_integrate.
+ * Not available with neighbour tiles (nbr16 set): SIM_ERR_ARG. */
+int sim_eam_force_integrate_drift(const SimEngine* e, const SimEAMTables* t, const SimIntegrator* p,
+                                  void* stream);
 
 /* sim_eam_forces without caller-allocated scratch.  No counterpart in the
  * reference (which allocates through PyTorch on every call); it exists for

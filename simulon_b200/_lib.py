@@ -50,7 +50,7 @@ class SimEngine(ctypes.Structure):
                 ("flags", c_p), ("partials", c_p), ("red_counter", c_p), ("red_out", c_p),
                 ("n_blocks_max", ctypes.c_int32), ("box_orthogonal", ctypes.c_int32),
                 ("n_tiles", ctypes.c_int32), ("halo_cap", ctypes.c_int32),
-                ("halo", c_p), ("halo_n", c_p), ("nbr16", c_p)]
+                ("halo", c_p), ("halo_n", c_p), ("nbr16", c_p), ("cut_mask", c_p)]
 
 
 class SimEAMTables(ctypes.Structure):
@@ -102,6 +102,7 @@ SIGNATURES = {
     "sim_eam_density": [_P(SimEngine), _P(SimEAMTables), c_p],
     "sim_eam_force": [_P(SimEngine), _P(SimEAMTables), c_p],
     "sim_eam_force_integrate": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), c_p],
+    "sim_eam_force_integrate_drift": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), c_p],
     "sim_lj_forces": [_P(SimEngine), _P(SimLJParams), ctypes.c_int32, c_p],
     "sim_integrate_first": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_integrate_second": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],

@@ -117,7 +117,7 @@ __device__ __forceinline__ void block_partials(double (&vals)[NV], double* parti
 // with Kahan compensation in block order and resets the counter (so a
 // captured graph can replay).  Must be called by every thread of every block.
 template <int NV>
-__device__ __forceinline__ void last_block_finalize(double* partials, uint32_t* counter,
+__device__ __forceinline__ bool last_block_finalize(double* partials, uint32_t* counter,
                                                     double* out, int slot0) {
     __shared__ bool is_last;
     __threadfence();
@@ -127,7 +127,7 @@ __device__ __forceinline__ void last_block_finalize(double* partials, uint32_t* 
         is_last = (done == gridDim.x - 1);
     }
     __syncthreads();
-    if (!is_last) return;
+    if (!is_last) return false;
     __threadfence();
     if (threadIdx.x < NV) {
         double s = 0.0, c = 0.0;
@@ -140,6 +140,7 @@ __device__ __forceinline__ void last_block_finalize(double* partials, uint32_t* 
         out[slot0 + threadIdx.x] = s;
     }
     if (threadIdx.x == 0) *counter = 0u;
+    return true;
 }
 
 // ---- Philox4x32-10 (Salmon et al., SC'11) ------------------------------------
@@ -182,7 +183,7 @@ __device__ __forceinline__ void langevin_normals(uint32_t a, uint64_t step, uint
 // Writes e.v and returns the new velocity in v_out.
 __device__ __forceinline__ void second_half_atom(const SimEngine& e, const SimIntegrator& p, int64_t i, int type,
                                                  uint64_t step, double f0, double f1, double f2, double* v_out,
-                                                 bool& bad) {
+                                                 bool& bad, bool store = true) {
     const int64_t P = e.n_pad;
     const double m = e.mass[type];
     double z[3] = {0.0, 0.0, 0.0};
@@ -200,10 +201,48 @@ __device__ __forceinline__ void second_half_atom(const SimEngine& e, const SimIn
         if (p.langevin) vel = __dadd_rn(__dmul_rn(vel, p.damp), __dmul_rn(z[c], rff));
         const double a = __ddiv_rn(f[c], m);
         vel = __dadd_rn(vel, __dmul_rn(__dmul_rn(0.5, a), p.dt));
-        e.v[c * P + i] = vel;
+        if (store) e.v[c * P + i] = vel;
         v_out[c] = vel;
         bad |= !isfinite(vel);
     }
+}
+
+// First half of velocity Verlet for atom i (integrator.py:91-99): v += F/m dt/2,
+// x += v dt, refresh the fixed-point code in posq, and report whether the atom
+// moved more than skin/2 from its position at the last rebuild
+// (reader.py:136-163).  v_in: the velocity to kick (read from e.v when NULL).
+__device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimIntegrator& p, int64_t i, int type,
+                                                const double* f, const double* v_in, bool& bad) {
+    const int64_t P = e.n_pad;
+    const SimBox& b = *e.box;
+    const double m = e.mass[type];
+    double xn[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const double a = __ddiv_rn(f[c], m);
+        const double v0 = v_in ? v_in[c] : e.v[c * P + i];
+        const double vh = __dadd_rn(v0, __dmul_rn(__dmul_rn(0.5, a), p.dt));
+        xn[c] = __dadd_rn(e.x[c * P + i], __dmul_rn(vh, p.dt));
+        e.v[c * P + i] = vh;
+        e.x[c * P + i] = xn[c];
+        bad |= !isfinite(xn[c]) || !isfinite(vh);
+    }
+    double s[3];
+    cart_to_frac(b, xn[0], xn[1], xn[2], s);
+    int4 q;
+    q.x = (int32_t)to_fixed(s[0]);
+    q.y = (int32_t)to_fixed(s[1]);
+    q.z = (int32_t)to_fixed(s[2]);
+    q.w = type;
+    reinterpret_cast<int4*>(e.posq)[i] = q;
+    // displacement since the last rebuild, minimum image in fractional space
+    const double t0 = (double)(int32_t)((uint32_t)q.x - (uint32_t)e.xref[i]) * 2.3283064365386963e-10;
+    const double t1 = (double)(int32_t)((uint32_t)q.y - (uint32_t)e.xref[P + i]) * 2.3283064365386963e-10;
+    const double t2 = (double)(int32_t)((uint32_t)q.z - (uint32_t)e.xref[2 * P + i]) * 2.3283064365386963e-10;
+    const double d0 = t0 * b.H[0] + t1 * b.H[3] + t2 * b.H[6];
+    const double d1 = t0 * b.H[1] + t1 * b.H[4] + t2 * b.H[7];
+    const double d2 = t0 * b.H[2] + t1 * b.H[5] + t2 * b.H[8];
+    return d0 * d0 + d1 * d1 + d2 * d2 > e.skin_half2;
 }
 
 }  // namespace simb200

@@ -22,8 +22,28 @@
 
 namespace simb200 {
 
+// Launch shapes (tuned on B200; overridable at compile time for sweeps)
+#ifndef EAM_DENSITY_THREADS
 #define EAM_DENSITY_THREADS 512
+#endif
+#ifndef EAM_DENSITY_MIN_BLOCKS
+#define EAM_DENSITY_MIN_BLOCKS 3  // 3 x 512 threads per SM (<= 40 registers)
+#endif
+#ifndef EAM_CARVEOUT_PCT
+#define EAM_CARVEOUT_PCT -1       // shared-memory carveout hint in percent (-1: driver default)
+#endif
+#ifndef EAM_DENSITY_UNROLL
+#define EAM_DENSITY_UNROLL 4      // list entries gathered together in pass 1 (divides 32)
+#endif
+#ifndef EAM_FORCE_THREADS
 #define EAM_FORCE_THREADS 1024
+#endif
+#ifndef EAM_FORCE_MIN_BLOCKS
+#define EAM_FORCE_MIN_BLOCKS 1
+#endif
+#ifndef EAM_WINDOW_ROWS
+#define EAM_WINDOW_ROWS 4096
+#endif
 
 __device__ __forceinline__ float rsqrt_approx(float x) {
     float y;
@@ -91,11 +111,12 @@ struct Window {
 template <bool SMEM, bool ORTHO>
 __device__ __forceinline__ float density_term(const BoxF& b, const int4& qi, const int4& qj, float rc2,
                                               const float2* g_i, const float2* s_i, Window w,
-                                              const SimEAMTables& t) {
+                                              const SimEAMTables& t, bool& inside) {
     float r0, r1, r2;
     rvec<ORTHO>(b, qi, qj, r0, r1, r2);
     const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
-    if (!(d2 < rc2)) return 0.0f;
+    inside = d2 < rc2;
+    if (!inside) return 0.0f;
     const Lerp l = lerp_r(d2 * rsqrt_approx(d2), t);
     float2 v;
     if (SMEM && l.k >= w.k_lo) v = s_i[qj.w * w.n_win + (l.k - w.k_lo)];
@@ -104,7 +125,7 @@ __device__ __forceinline__ float density_term(const BoxF& b, const int4& qi, con
 }
 
 template <bool SMEM, bool ORTHO>
-__global__ void __launch_bounds__(EAM_DENSITY_THREADS) k_eam_density(SimEngine e, SimEAMTables t, Window w) {
+__global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k_eam_density(SimEngine e, SimEAMTables t, Window w) {
     extern __shared__ float2 s_dens[];
     const float2* dens = reinterpret_cast<const float2*>(t.dens_vd);
     const int nt = t.n_types;
@@ -120,6 +141,7 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS) k_eam_density(SimEngine e
     const int32_t* __restrict__ nbr = e.nbr;
     const int64_t P = e.n_pad;
     const float rc2 = t.cutoff * t.cutoff;
+    const bool use_mask = e.cut_mask != nullptr && e.nbr_cap <= 64;
     double acc = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
         const int4 qi = posq[i];
@@ -128,28 +150,50 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS) k_eam_density(SimEngine e
         const float2* g_i = dens + (size_t)ti * nt * t.n_r;
         const float2* s_i = s_dens + (size_t)ti * nt * w.n_win;
         float rho = 0.0f;
+        uint32_t in_lo = 0, in_hi = 0;     // bit k: slot k inside the cutoff
         int k = 0;
-        for (; k + 4 <= nn; k += 4) {
-            int j[4];
-            int4 q[4];
+        constexpr int U = EAM_DENSITY_UNROLL;
+        for (; k + U <= nn; k += U) {
+            int j[U];
+            int4 q[U];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) j[u] = __ldg(&nbr[(int64_t)(k + u) * P + i]);
+            for (int u = 0; u < U; ++u) j[u] = __ldg(&nbr[(int64_t)(k + u) * P + i]);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) q[u] = __ldg(&posq[j[u]]);
+            for (int u = 0; u < U; ++u) q[u] = __ldg(&posq[j[u]]);
+            uint32_t bits = 0;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) rho += density_term<SMEM, ORTHO>(b, qi, q[u], rc2, g_i, s_i, w, t);
+            for (int u = 0; u < U; ++u) {
+                bool in;
+                rho += density_term<SMEM, ORTHO>(b, qi, q[u], rc2, g_i, s_i, w, t, in);
+                bits |= (uint32_t)in << u;
+            }
+            if (k < 32) in_lo |= bits << k;
+            else in_hi |= bits << (k - 32);
         }
-        for (; k < nn; ++k)
+        for (; k < nn; ++k) {
+            bool in;
             rho += density_term<SMEM, ORTHO>(b, qi, __ldg(&posq[__ldg(&nbr[(int64_t)k * P + i])]), rc2, g_i, s_i,
-                                             w, t);
+                                             w, t, in);
+            if (k < 32) in_lo |= (uint32_t)in << k;
+            else in_hi |= (uint32_t)in << (k - 32);
+        }
         float F, Fp;
         embed_lookup(t, ti, rho, F, Fp);
         posfp[i] = make_int4(qi.x, qi.y, qi.z, __float_as_int(Fp));
+        if (use_mask) e.cut_mask[i] = ((uint64_t)in_hi << 32) | in_lo;
         acc += (double)F;
     }
     double vals[1] = {acc};
     block_partials<1>(vals, e.partials, SIM_RED_EPOT_EMBED);
     last_block_finalize<1>(e.partials, e.red_counter + 0, e.red_out, SIM_RED_EPOT_EMBED);
+}
+
+// Lowest set bit of m as a list slot (clearing it), or -1 when m is empty.
+__device__ __forceinline__ int pop_slot(uint64_t& m) {
+    if (m == 0) return -1;
+    const int k = __ffsll((long long)m) - 1;
+    m &= m - 1;
+    return k;
 }
 
 // ---------------------------------------------------------------------------
@@ -195,11 +239,16 @@ __device__ __forceinline__ void pair_single(const BoxF& b, const int4& pi, const
     pair_force(fmaf(fpi + __int_as_float(qj.w), dd_dp.x, dd_dp.y), phi, r, inv_r, r0, r1, r2, fx, fy, fz, acc);
 }
 
-// INTEG: the epilogue also finishes the step for atom i -- the second half of
+// INTEG 1: the epilogue also finishes the step for atom i -- the second half of
 // velocity Verlet with the Langevin O-step (integrator.py:102-124) -- and
 // accumulates K and sum m v(x)v, so the half kick needs no extra pass.
-template <bool SINGLE, bool INTEG, bool ORTHO>
-__global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e, SimEAMTables t, SimIntegrator ip,
+// INTEG 2: in addition the first half of the next step (kick with the same
+// forces, drift, posq refresh, skin/2 trigger); the last block advances the
+// step counter (step_ctr[0] = step + 1, step_ctr[1] = step for the step log).
+// Pass 2 reads only posfp (pass 1's copy of the positions), so atoms can move
+// while other threads still gather their neighbours.
+template <bool SINGLE, int INTEG, bool ORTHO>
+__global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam_force(SimEngine e, SimEAMTables t, SimIntegrator ip,
                                                                     Window w) {
     extern __shared__ float4 s_tab4[];
     float4* tab_d = s_tab4;
@@ -218,8 +267,9 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e,
     const int32_t* __restrict__ nbr = e.nbr;
     const int64_t P = e.n_pad;
     const float rc2 = t.cutoff * t.cutoff;
+    const bool use_mask = e.cut_mask != nullptr && e.nbr_cap <= 64;
     float acc[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    bool bad = false;
+    bool bad = false, trig = false;
     const uint64_t step = INTEG && ip.step_ctr ? *ip.step_ctr : 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
         const int4 pi = posfp[i];
@@ -227,7 +277,27 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e,
         const int nn = e.nnbr[i];
         float fx = 0.f, fy = 0.f, fz = 0.f;
         int ti = 0;
-        if (SINGLE) {
+        if (SINGLE && use_mask) {
+            // only the slots pass 1 found inside the cutoff; the next two list
+            // entries are fetched while the current pair is gathered and evaluated
+            uint64_t m = e.cut_mask[i];
+            int ka = pop_slot(m), kb = pop_slot(m);
+            int ja = ka >= 0 ? __ldg(&nbr[(int64_t)ka * P + i]) : 0;
+            int jb = kb >= 0 ? __ldg(&nbr[(int64_t)kb * P + i]) : 0;
+            while (kb >= 0) {
+                const int j0 = ja, j1 = jb;
+                ka = pop_slot(m);
+                kb = pop_slot(m);
+                if (ka >= 0) ja = __ldg(&nbr[(int64_t)ka * P + i]);
+                if (kb >= 0) jb = __ldg(&nbr[(int64_t)kb * P + i]);
+                const int4 q0 = __ldg(&posfp[j0]);
+                const int4 q1 = __ldg(&posfp[j1]);
+                pair_single<ORTHO>(b, pi, q0, rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
+                pair_single<ORTHO>(b, pi, q1, rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
+            }
+            if (ka >= 0)
+                pair_single<ORTHO>(b, pi, __ldg(&posfp[ja]), rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
+        } else if (SINGLE) {
             // the next two list entries are fetched while the current pair is
             // gathered and evaluated, so the list's DRAM latency overlaps work
             int jn0 = nn > 0 ? __ldg(&nbr[i]) : 0;
@@ -250,7 +320,8 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e,
             const float4* gd = reinterpret_cast<const float4*>(t.deriv_vd);
             const float2* gp = reinterpret_cast<const float2*>(t.pair_vd);
             ti = posq[i].w;
-            for (int k = 0; k < nn; ++k) {
+            uint64_t m = use_mask ? e.cut_mask[i] : 0;
+            for (int k = use_mask ? pop_slot(m) : 0; use_mask ? k >= 0 : k < nn; k = use_mask ? pop_slot(m) : k + 1) {
                 const int j = __ldg(&nbr[(int64_t)k * P + i]);
                 const int4 qj = __ldg(&posfp[j]);
                 float r0, r1, r2;
@@ -276,20 +347,29 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, 1) k_eam_force(SimEngine e,
         bad |= !(isfinite(fx) && isfinite(fy) && isfinite(fz));
         if (INTEG) {
             double v[3];
-            second_half_atom(e, ip, i, ti, step, (double)fx, (double)fy, (double)fz, v, bad);
+            second_half_atom(e, ip, i, ti, step, (double)fx, (double)fy, (double)fz, v, bad, INTEG == 1);
             const double m = e.mass[ti];
             acc[8] += (float)(0.5 * m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
             acc[9] += (float)(m * v[0] * v[0]); acc[10] += (float)(m * v[1] * v[1]); acc[11] += (float)(m * v[2] * v[2]);
             acc[12] += (float)(m * v[0] * v[1]); acc[13] += (float)(m * v[0] * v[2]); acc[14] += (float)(m * v[1] * v[2]);
+            if (INTEG == 2) {
+                const double f[3] = {(double)fx, (double)fy, (double)fz};
+                trig |= first_half_atom(e, ip, i, ti, f, v, bad);
+            }
         }
     }
+    if (INTEG == 2 && __any_sync(0xffffffffu, trig) && (threadIdx.x & 31) == 0) e.flags[0] = 1;
     if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
     if (INTEG) {
         double vals[15];
 #pragma unroll
         for (int k = 0; k < 15; ++k) vals[k] = k < 8 ? 0.5 * (double)acc[k] : (double)acc[k];
         block_partials<15>(vals, e.partials, SIM_RED_EPOT_PAIR);
-        last_block_finalize<15>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+        const bool last = last_block_finalize<15>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+        if (INTEG == 2 && last && threadIdx.x == 0) {
+            ip.step_ctr[1] = step;
+            ip.step_ctr[0] = step + 1;
+        }
     } else {
         double vals[8];
 #pragma unroll
@@ -308,7 +388,7 @@ static const size_t kSmemLimit = 200 * 1024;
 // Rows of the r-tables kept in shared memory: the top kWindowRows (r from
 // (n_r - kWindowRows) dr up to the cutoff; 2.2 A for an 8192-row table on
 // [0, 4.4 A]).  A smaller footprint leaves L1 capacity for neighbour gathers.
-static const int kWindowRows = 4096;
+static const int kWindowRows = EAM_WINDOW_ROWS;
 static Window table_window(const SimEAMTables& t) {
     const int n_win = t.n_r < kWindowRows ? t.n_r : kWindowRows;
     return Window{t.n_r - n_win, n_win};
@@ -321,6 +401,8 @@ static size_t smem_pass2(const SimEAMTables& t) { return (size_t)table_window(t)
 template <typename K>
 static void allow_smem(K kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit);
+    if (EAM_CARVEOUT_PCT >= 0)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, EAM_CARVEOUT_PCT);
 }
 
 static void eam_set_attributes() {
@@ -328,10 +410,12 @@ static void eam_set_attributes() {
     if (!done) {
         allow_smem(k_eam_density<true, true>);
         allow_smem(k_eam_density<true, false>);
-        allow_smem(k_eam_force<true, false, true>);
-        allow_smem(k_eam_force<true, true, true>);
-        allow_smem(k_eam_force<true, false, false>);
-        allow_smem(k_eam_force<true, true, false>);
+        allow_smem(k_eam_force<true, 0, true>);
+        allow_smem(k_eam_force<true, 1, true>);
+        allow_smem(k_eam_force<true, 2, true>);
+        allow_smem(k_eam_force<true, 0, false>);
+        allow_smem(k_eam_force<true, 1, false>);
+        allow_smem(k_eam_force<true, 2, false>);
         done = true;
     }
 }
@@ -367,7 +451,7 @@ extern "C" int sim_eam_density(const SimEngine* ep, const SimEAMTables* tp, void
     return launch_status("sim_eam_density");
 }
 
-template <bool SINGLE, bool INTEG, bool ORTHO>
+template <bool SINGLE, int INTEG, bool ORTHO>
 static int launch_force(const SimEngine& e, const SimEAMTables& t, const SimIntegrator& ip, cudaStream_t st) {
     const size_t smem = SINGLE ? smem_pass2(t) : 0;
     const int g = persistent_grid((const void*)k_eam_force<SINGLE, INTEG, ORTHO>, EAM_FORCE_THREADS, smem, e.n);
@@ -376,7 +460,7 @@ static int launch_force(const SimEngine& e, const SimEAMTables& t, const SimInte
     return SIM_OK;
 }
 
-template <bool INTEG>
+template <int INTEG>
 static int launch_eam_force(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip, void* stream) {
     if (!ep || !tp || ep->n <= 0 || !ep->posfp || !valid_tables(*tp)) return SIM_ERR_ARG;
     const SimEngine& e = *ep;
@@ -390,7 +474,12 @@ static int launch_eam_force(const SimEngine* ep, const SimEAMTables* tp, const S
     cudaStream_t st = (cudaStream_t)stream;
     const bool single = t.n_types == 1 && smem_pass2(t) <= kSmemLimit;
     int rc;
-    if (tiled_eam_usable(e, t))
+    const bool tiled = tiled_eam_usable(e, t);
+    if (INTEG == 2 && tiled) {
+        set_error_text("sim_eam_force_integrate_drift: not available with neighbour tiles (nbr16 set)");
+        return SIM_ERR_ARG;
+    }
+    if (tiled)
         rc = launch_eam_force_tiled(e, t, INTEG ? &integ : nullptr, st);
     else if (single)
         rc = e.box_orthogonal ? launch_force<true, INTEG, true>(e, t, integ, st)
@@ -399,7 +488,8 @@ static int launch_eam_force(const SimEngine* ep, const SimEAMTables* tp, const S
         rc = e.box_orthogonal ? launch_force<false, INTEG, true>(e, t, integ, st)
                               : launch_force<false, INTEG, false>(e, t, integ, st);
     if (rc != SIM_OK) return rc;
-    return launch_status(INTEG ? "sim_eam_force_integrate" : "sim_eam_force");
+    return launch_status(INTEG == 2 ? "sim_eam_force_integrate_drift"
+                                    : (INTEG ? "sim_eam_force_integrate" : "sim_eam_force"));
 }
 
 extern "C" int sim_eam_force(const SimEngine* ep, const SimEAMTables* tp, void* stream) {
@@ -409,6 +499,11 @@ extern "C" int sim_eam_force(const SimEngine* ep, const SimEAMTables* tp, void* 
 extern "C" int sim_eam_force_integrate(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip,
                                        void* stream) {
     return launch_eam_force<true>(ep, tp, ip, stream);
+}
+
+extern "C" int sim_eam_force_integrate_drift(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip,
+                                             void* stream) {
+    return launch_eam_force<2>(ep, tp, ip, stream);
 }
 
 extern "C" int sim_eam_forces(const SimEngine* ep, const SimEAMTables* tp, void* stream) {

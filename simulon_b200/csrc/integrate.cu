@@ -70,39 +70,12 @@ __device__ __forceinline__ double load_force(const SimEngine& e, int prec, int64
 }
 
 __global__ void __launch_bounds__(SIM_THREADS) k_first_half(SimEngine e, SimIntegrator p, int prec) {
-    const int64_t P = e.n_pad;
-    const SimBox& b = *e.box;
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     bool trigger = false, bad = false;
     if (i == 0 && p.step_ctr) *p.step_ctr += 1;   // the step index sim_integrate_second reads
     if (i < e.n) {
-        int4* posq = reinterpret_cast<int4*>(e.posq);
-        int4 q = posq[i];
-        const double m = e.mass[q.w];
-        double xn[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const double a = __ddiv_rn(load_force(e, prec, i, c), m);
-            const double vh = __dadd_rn(e.v[c * P + i], __dmul_rn(__dmul_rn(0.5, a), p.dt));
-            xn[c] = __dadd_rn(e.x[c * P + i], __dmul_rn(vh, p.dt));
-            e.v[c * P + i] = vh;
-            e.x[c * P + i] = xn[c];
-            bad |= !isfinite(xn[c]) || !isfinite(vh);
-        }
-        double s[3];
-        cart_to_frac(b, xn[0], xn[1], xn[2], s);
-        q.x = (int32_t)to_fixed(s[0]);
-        q.y = (int32_t)to_fixed(s[1]);
-        q.z = (int32_t)to_fixed(s[2]);
-        posq[i] = q;
-        // displacement since the last rebuild, minimum image in fractional space
-        const double t0 = (double)(int32_t)((uint32_t)q.x - (uint32_t)e.xref[i]) * 2.3283064365386963e-10;
-        const double t1 = (double)(int32_t)((uint32_t)q.y - (uint32_t)e.xref[P + i]) * 2.3283064365386963e-10;
-        const double t2 = (double)(int32_t)((uint32_t)q.z - (uint32_t)e.xref[2 * P + i]) * 2.3283064365386963e-10;
-        const double d0 = t0 * b.H[0] + t1 * b.H[3] + t2 * b.H[6];
-        const double d1 = t0 * b.H[1] + t1 * b.H[4] + t2 * b.H[7];
-        const double d2 = t0 * b.H[2] + t1 * b.H[5] + t2 * b.H[8];
-        trigger = d0 * d0 + d1 * d1 + d2 * d2 > e.skin_half2;
+        const double f[3] = {load_force(e, prec, i, 0), load_force(e, prec, i, 1), load_force(e, prec, i, 2)};
+        trigger = first_half_atom(e, p, i, e.posq[4 * i + 3], f, nullptr, bad);
     }
     if (__any_sync(0xffffffffu, trigger) && (threadIdx.x & 31) == 0) e.flags[0] = 1;
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);

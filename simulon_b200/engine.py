@@ -159,7 +159,9 @@ class MDEngine:
         self.partials = torch.zeros(self.n_blocks_max, _lib.RED_SLOTS, **f64)
         self.red_counter = torch.zeros(4, **i32)
         self.red_out = torch.zeros(_lib.RED_SLOTS, **f64)
-        self.step_ctr = torch.full((1,), -1, device=dev, dtype=torch.int64)
+        # [0] current step index (advanced by the first half-step), [1] index of
+        # the step whose second half ran in a drift-fused force pass (step log)
+        self.step_ctr = torch.full((2,), -1, device=dev, dtype=torch.int64)
         self.log_capacity = int(log_capacity)
         self.log = torch.zeros(self.log_capacity, _lib.RED_SLOTS + LOG_EXTRA + 1, **f64)
         self.extra = torch.zeros(LOG_EXTRA, **f64)
@@ -191,6 +193,7 @@ class MDEngine:
         s.box_orthogonal = int(self.box.orthogonal)
         s.n_tiles, s.halo_cap = self.n_tiles, self.halo_cap
         s.halo, s.halo_n, s.nbr16 = _lib.ptr(self.halo), _lib.ptr(self.halo_n), _lib.ptr(self.nbr16)
+        s.cut_mask = _lib.ptr(self.cut_mask)
         self.st = s
         self.st_ref = ctypes.byref(s)
 
@@ -211,6 +214,8 @@ class MDEngine:
     def _alloc_lists(self):
         dev, P = self.device, self.n_pad
         self.nbr = torch.zeros(self.nbr_cap, P, device=dev, dtype=torch.int32)
+        # in-cutoff slot mask written by EAM pass 1 (one 64-bit word per atom)
+        self.cut_mask = torch.zeros(P, device=dev, dtype=torch.int64) if self.nbr_cap <= 64 else None
         if self.use_tiles:
             self.nbr16 = torch.zeros(self.nbr_cap, P, device=dev, dtype=torch.int16)
             self.halo = torch.zeros(self.n_tiles, self.halo_cap, device=dev, dtype=torch.int32)
@@ -295,6 +300,14 @@ class MDEngine:
         self._last_force_precision = 0
         self.forces_valid = True
 
+    def eam_forces_integrate_drift(self, tables, integ):
+        """EAM pass 1, then pass 2 with this step's second half and the next
+        step's first half fused into it (needs the untiled kernels)."""
+        _lib.call("sim_eam_density", self.st_ref, tables.ref, self.stream)
+        _lib.call("sim_eam_force_integrate_drift", self.st_ref, tables.ref, integ.ref, self.stream)
+        self._last_force_precision = 0
+        self.forces_valid = True
+
     def eam_forces(self, tables):
         _lib.call("sim_eam_forces", self.st_ref, tables.ref, self.stream)
         self._last_force_precision = 0
@@ -314,8 +327,11 @@ class MDEngine:
     def berendsen(self, params):
         _lib.call("sim_berendsen", self.st_ref, params.ref, _lib.ptr(self.extra), self.stream)
 
-    def log_step(self):
-        _lib.call("sim_log_step", self.st_ref, _lib.ptr(self.step_ctr), _lib.ptr(self.extra), LOG_EXTRA,
+    def log_step(self, after_drift: bool = False):
+        """Record this step's reductions in the device log (after_drift: the step
+        was finished by eam_forces_integrate_drift, whose index is step_ctr[1])."""
+        ctr = self.step_ctr[1:] if after_drift else self.step_ctr
+        _lib.call("sim_log_step", self.st_ref, _lib.ptr(ctr), _lib.ptr(self.extra), LOG_EXTRA,
                   _lib.ptr(self.log), self.log_capacity, self.stream)
 
     # ---- reductions (device tensors, no sync) ----------------------------

@@ -91,6 +91,11 @@ class EAMForceCUDAExt(BackboneInterface):
         """Forces plus the integrator's second half in one pass over the atoms."""
         self.molecular.engine.eam_forces_integrate(self.tables, integrator.params)
 
+    def compute_finish_and_drift(self, integrator):
+        """Forces, the integrator's second half and the next step's first half
+        in one pass over the atoms."""
+        self.molecular.engine.eam_forces_integrate_drift(self.tables, integrator.params)
+
     def forward(self):
         self.compute()
         red = self.molecular.engine.red_out

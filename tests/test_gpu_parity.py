@@ -175,6 +175,28 @@ def test_eam_tiled_equals_untiled(sb, fsw_path, tri):
     np.testing.assert_allclose(out[1][1][:9], out[0][1][:9], rtol=1e-6, atol=1e-6)
 
 
+@pytest.mark.parametrize("tri", [False, True])
+def test_eam_cutoff_mask_equals_full_scan(sb, fsw_path, tri):
+    """Pass 2 over the in-cutoff slots recorded by pass 1 gives the same forces,
+    energies and virial, bit for bit, as pass 2 testing every list slot."""
+    if tri:
+        x, H = oin.bcc_triclinic(12)
+    else:
+        x, L = oin.bcc_lattice(14)
+        H = np.diag([L] * 3)
+    x = oin.jitter(x, 0.09, 43)
+    eng, tables, _ = _eam_engine(sb, fsw_path, x, H)
+    assert eng.cut_mask is not None
+    out = []
+    for masked in (True, False):
+        if not masked:
+            eng.cut_mask = None
+            eng._make_struct()
+        eng.eam_forces(tables)
+        out.append((eng.gather("f").cpu(), eng.red_out.cpu()))
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+
+
 def test_eam_reruns_bitwise_identical(sb, fsw_path):
     x, L = oin.bcc_lattice(16)
     x = oin.jitter(x, 0.07, 40)
@@ -272,19 +294,38 @@ def test_md_eam_matches_reference_trajectory(sb, fsw_path, tmp_path, ens):
     np.testing.assert_allclose(mol.coordinates.cpu().numpy(), g["x"], atol=5e-4)
 
 
+def _lib_red_slots():
+    from simulon_b200 import _lib
+    return _lib.RED_SLOTS
+
+
 def test_graph_run_matches_eager_steps(sb, fsw_path):
     x, L = oin.bcc_lattice(10)
     x = oin.jitter(x, 0.05, 50)
     v = oin.maxwell_boltzmann(np.full(len(x), oin.W_MASS), 600.0, 51)
     res = []
     from simulon_b200.engine import integrator_params
-    # (graph?, conditional IF-node rebuild?, second half fused into EAM pass 2?)
-    modes = [(False, False, False), (True, False, False), (True, True, False), (True, True, True), (False, True, True)]
+    # (graph?, conditional IF-node rebuild?, second half fused into EAM pass 2?);
+    # fused == "drift": the next step's first half is fused in as well
+    modes = [(False, False, False), (True, False, False), (True, True, False), (True, True, True), (False, True, True),
+             (False, True, "drift"), (True, True, "drift")]
     for use_graph, cond, fused in modes:
         eng, tables, parser = _eam_engine(sb, fsw_path, x, np.diag([L] * 3), v)
         # an NVT integrator exercises the noise and triggers rebuilds
         integ = integrator_params(eng, 0.002, langevin=True, temperature=600.0, gamma=10.0, seed=7)
         eng.eam_forces(tables)
+
+        def drift_steps(k):
+            eng.integrate_first(integ, 0)
+            eng.rebuild_if_needed()
+            for s in range(k):
+                if s < k - 1:
+                    eng.eam_forces_integrate_drift(tables, integ)
+                    eng.log_step(after_drift=True)
+                    eng.rebuild_if_needed()
+                else:
+                    eng.eam_forces_integrate(tables, integ)
+                    eng.log_step()
 
         def step():
             eng.integrate_first(integ, 0)
@@ -303,20 +344,32 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
             s.wait_stream(torch.cuda.current_stream())
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=s):
-                for _ in range(20):
-                    step()
+                if fused == "drift":
+                    drift_steps(20)
+                else:
+                    for _ in range(20):
+                        step()
+                        eng.log_step()
             torch.cuda.current_stream().wait_stream(s)
             for _ in range(steps // 20):
                 g.replay()
+        elif fused == "drift":
+            for _ in range(steps // 20):
+                drift_steps(20)
         else:
             for _ in range(steps):
                 step()
+                eng.log_step()
         torch.cuda.synchronize()
         res.append((eng.gather("x").cpu(), eng.gather("v").cpu(), int(eng.flags[3].item()),
-                    eng.red_out.cpu().numpy()))
+                    eng.red_out.cpu().numpy(), eng.log[:steps, :_lib_red_slots()].cpu().numpy(),
+                    eng.step_ctr.cpu().numpy()))
     for r in res[1:]:
         assert torch.equal(res[0][0], r[0]) and torch.equal(res[0][1], r[1])
         assert r[2] == res[0][2]
+        assert r[5][0] == res[0][5][0] == steps - 1
+        # per-step log rows: energies and virial agree to FP32 partial-sum order
+        np.testing.assert_allclose(r[4][:, :9], res[0][4][:, :9], rtol=1e-6, atol=1e-9)
         np.testing.assert_allclose(r[3][9], res[0][3][9], rtol=1e-6)   # kinetic energy (FP32 per-thread partials)
     assert res[0][2] >= 2      # the load rebuild plus at least one triggered
 
