@@ -10,7 +10,8 @@
  * non-finite values, box too small) are reported through a caller-owned
  * device status word that the host reads when it chooses to synchronise.
  *
- * Two groups of entry points:
+ * Three groups of entry points (the third, batched replicas, is described
+ * at its declarations below):
  *
  *  1. Drop-ins for the reference's native module `simulon_cuda`
  *     (cuda source/ops.cpp:47-53), same argument meaning:
@@ -349,11 +350,93 @@ int sim_engine_half_fill(const SimEngine* e, double rc2, const int64_t* row_ptr,
 /* Exclusive scan helper used by the wrappers: out[0]=0, out[k+1]=sum in[0..k]. */
 int sim_scan_i64(const int64_t* in, int64_t n, int64_t* out, void* stream);
 
+/* ==== group 3: batched replicas ========================================== *
+ * Many independent systems (replicas) of uneven size -- a temperature scan or
+ * a sweep of crack slabs, each run by the reference as its own BaseModel loop
+ * (run_scripts/w_crack.py:433-440) -- advance together: one launch of each
+ * kernel covers every replica.  Replica k owns the slots [off, off + n_slots)
+ * of the SimEngine arrays, with off and n_slots multiples of 32 so that every
+ * warp's 32 slots belong to one replica; its n atoms fill the first n slots,
+ * the remaining slots are padding that no kernel reads or writes.  Each
+ * replica has its own periodic box, cell grid, rebuild flag (only replicas
+ * whose atoms moved more than skin/2 are rebuilt) and Langevin temperature,
+ * and may hold atoms in grips that open at a fixed rate per step
+ * (w_crack.py:384-392: grip atoms keep their reference positions shifted by
+ * half the opening, with zero velocity).  One element type (n_types == 1). */
+typedef struct SimRep {
+    SimBox  box;
+    int64_t off;            /* first slot                                          */
+    int64_t first;          /* original index of the replica's first atom          */
+    int32_t n, n_slots;     /* atoms; slots reserved (n rounded up to 32)           */
+    int32_t ncell[3], n_cells;
+    int32_t cell_off;       /* first entry of this replica in the batch cell arrays:
+                               cell_count / cell_start hold n_cells + 1 entries from
+                               cell_off, cell_rank 2 * n_cells entries from 2 * cell_off
+                               (linear cell -> visiting rank, then rank -> linear)   */
+    int32_t grip_axis;      /* box row along which the grips open; -1: no grips     */
+    double  grip_rate;      /* opening per step (A): at step s the lower grip sits
+                               0.5 * rate * (s + 1) below its reference position,
+                               the upper grip as far above it                       */
+} SimRep;
+
+typedef struct SimBatch {
+    SimEngine e;            /* slot arrays; e.n = slots in use (sum of n_slots),
+                               e.n_pad >= e.n, a multiple of 128.  e.box, e.ncell,
+                               e.n_cells are not used (per replica); e.cell_count,
+                               e.cell_start index batch cell entries; e.flags[0] is
+                               set when some replica asks for a rebuild, [1] status
+                               bits, [2] longest row on overflow, [3] rebuild events */
+    SimRep*  rep;           /* [n_rep] device                                        */
+    int32_t  n_rep;
+    int32_t  n_cell_entries;/* sum over replicas of n_cells + 1                       */
+    int32_t* slot_rep;      /* [e.n_pad] replica k of each slot; -1 - k for padding    */
+    int32_t* cell_rep;      /* [n_cell_entries] replica of each cell entry             */
+    int32_t* rep_flags;     /* [n_rep] 1: rebuild this replica                         */
+    int32_t* rep_rebuilds;  /* [n_rep] rebuilds performed                              */
+    int8_t*  grip;          /* [atoms, original order] 0 free, 1 lower grip, 2 upper   */
+    double*  gref;          /* [3][e.n_pad] grip reference positions, by original index */
+    double*  rep_rff;       /* [n_rep] Langevin noise amplitude sqrt(kB T (1-damp^2)/m) */
+    double*  chunk_red;     /* [e.n_pad / 32][SIM_RED_SLOTS] per-warp partial sums      */
+    double*  rep_red;       /* [n_rep][SIM_RED_SLOTS] per-replica FP64 sums            */
+} SimBatch;
+
+/* Load atoms x_rows/v_rows [atoms][3] FP64 and types [atoms] (original order,
+ * replica after replica) into their slots and build every replica's list. */
+int sim_batch_load(const SimBatch* b, const double* x_rows, const double* v_rows, const int32_t* types,
+                   void* stream);
+/* Rebuild the replicas whose rep_flags are set (all with only_flagged = 0). */
+int sim_batch_rebuild(const SimBatch* b, int32_t only_flagged, void* stream);
+/* As sim_rebuild_if_needed: an IF node on flags[0] while capturing. */
+int sim_batch_rebuild_if_needed(const SimBatch* b, void* stream);
+/* EAM pass 1 over all replicas (writes posfp, cut_mask, EPOT_EMBED partials). */
+int sim_batch_eam_density(const SimBatch* b, const SimEAMTables* t, void* stream);
+/* EAM pass 2 over all replicas.  mode 0: forces and pair reductions; 1: plus
+ * the second half-step (Langevin with rep_rff, grips held); 2: plus the first
+ * half of the next step (as sim_eam_force_integrate_drift).  p->rff is not
+ * used (rep_rff is); p->step_ctr[0] is this step's index. */
+int sim_batch_eam_force(const SimBatch* b, const SimEAMTables* t, const SimIntegrator* p, int32_t mode,
+                        void* stream);
+/* First half-step of every replica (advances step_ctr[0]; grips placed). */
+int sim_batch_first_half(const SimBatch* b, const SimIntegrator* p, void* stream);
+/* Per-replica FP64 sums of the partials into rep_red; when log != NULL also
+ * into log row (*step % log_cap), laid out [log_cap][n_rep][SIM_RED_SLOTS]. */
+int sim_batch_reduce(const SimBatch* b, const uint64_t* step, double* log, int32_t log_cap, void* stream);
+/* One whole step of every replica: pass 1, pass 2 (mode 2, or mode 1 when
+ * last != 0), the per-replica sums and log row, and (unless last) the advance
+ * of step_ctr[0] and the conditional rebuild.  A run of k steps is
+ * sim_batch_first_half followed by k calls, the last one with last = 1. */
+int sim_batched_step(const SimBatch* b, const SimEAMTables* t, const SimIntegrator* p, int32_t last,
+                     double* log, int32_t log_cap, void* stream);
+/* Slot arrays -> rows in original order (padding skipped). */
+int sim_batch_gather_f64(const SimBatch* b, const double* src_soa, double* out_rows, void* stream);
+int sim_batch_gather_f32(const SimBatch* b, const float* src_aos4, double* out_rows, void* stream);
+
 /* Message for the last CUDA error seen by this library (host string). */
 const char* sim_last_cuda_error(void);
 int sim_version(void);
 /* sizeof of SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator,
- * SimBerendsen (host-only; lets bindings verify their struct layouts). */
+ * SimBerendsen, SimRep, SimBatch (host-only; lets bindings verify their
+ * struct layouts; n >= 8). */
 int sim_struct_sizes(int64_t* out, int32_t n);
 
 #ifdef __cplusplus

@@ -13,6 +13,7 @@ import sys
 
 from . import _lib
 from .barostat import BerendsenBarostat
+from .batch import BatchedEngine, Replica, crack_slab, crack_sweep, partition_replicas
 from .box import Box
 from .eam_parser import EAMDeviceTables, EAMParser
 from .engine import MDEngine
@@ -36,4 +37,5 @@ def install_simulon_cuda():
 __all__ = ["AtomFileReader", "Box", "EAMParser", "EAMDeviceTables", "EAMForce", "EAMForceCUDA", "EAMForceCUDAExt",
            "LennardJonesForce", "BackboneInterface", "IntegratorInterface", "VerletIntegrator",
            "BerendsenBarostat", "SumBackboneInterface", "BaseModel", "MDSimulator", "MDEngine",
-           "find_neighbors_gpu_pbc", "install_simulon_cuda"]
+           "find_neighbors_gpu_pbc", "install_simulon_cuda", "BatchedEngine", "Replica", "crack_slab",
+           "crack_sweep", "partition_replicas"]

@@ -81,6 +81,19 @@ class SimBerendsen(ctypes.Structure):
                 ("coordinate_scale_power", ctypes.c_int32), ("reset_reference", ctypes.c_int32)]
 
 
+class SimRep(ctypes.Structure):
+    _fields_ = [("box", SimBox), ("off", ctypes.c_int64), ("first", ctypes.c_int64),
+                ("n", ctypes.c_int32), ("n_slots", ctypes.c_int32), ("ncell", ctypes.c_int32 * 3),
+                ("n_cells", ctypes.c_int32), ("cell_off", ctypes.c_int32), ("grip_axis", ctypes.c_int32),
+                ("grip_rate", ctypes.c_double)]
+
+
+class SimBatch(ctypes.Structure):
+    _fields_ = [("e", SimEngine), ("rep", c_p), ("n_rep", ctypes.c_int32), ("n_cell_entries", ctypes.c_int32),
+                ("slot_rep", c_p), ("cell_rep", c_p), ("rep_flags", c_p), ("rep_rebuilds", c_p), ("grip", c_p),
+                ("gref", c_p), ("rep_rff", c_p), ("chunk_red", c_p), ("rep_red", c_p)]
+
+
 _P = ctypes.POINTER
 # name -> argtypes (restype int unless listed in _RESTYPES)
 SIGNATURES = {
@@ -114,11 +127,22 @@ SIGNATURES = {
     "sim_engine_half_count": [_P(SimEngine), ctypes.c_double, c_p, c_p],
     "sim_engine_half_fill": [_P(SimEngine), ctypes.c_double, c_p, c_p, c_p, c_p, c_p],
     "sim_scan_i64": [c_p, ctypes.c_int64, c_p, c_p],
+    "sim_batch_load": [_P(SimBatch), c_p, c_p, c_p, c_p],
+    "sim_batch_rebuild": [_P(SimBatch), ctypes.c_int32, c_p],
+    "sim_batch_rebuild_if_needed": [_P(SimBatch), c_p],
+    "sim_batch_eam_density": [_P(SimBatch), _P(SimEAMTables), c_p],
+    "sim_batch_eam_force": [_P(SimBatch), _P(SimEAMTables), _P(SimIntegrator), ctypes.c_int32, c_p],
+    "sim_batch_first_half": [_P(SimBatch), _P(SimIntegrator), c_p],
+    "sim_batch_reduce": [_P(SimBatch), c_p, c_p, ctypes.c_int32, c_p],
+    "sim_batched_step": [_P(SimBatch), _P(SimEAMTables), _P(SimIntegrator), ctypes.c_int32, c_p, ctypes.c_int32,
+                         c_p],
+    "sim_batch_gather_f64": [_P(SimBatch), c_p, c_p, c_p],
+    "sim_batch_gather_f32": [_P(SimBatch), c_p, c_p, c_p],
     "sim_last_cuda_error": [],
     "sim_version": [],
     "sim_struct_sizes": [c_p, ctypes.c_int32],
 }
-STRUCTS = (SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator, SimBerendsen)
+STRUCTS = (SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator, SimBerendsen, SimRep, SimBatch)
 _RESTYPES = {"sim_last_cuda_error": ctypes.c_char_p}
 
 _lib = None

@@ -1,0 +1,706 @@
+// Batched replicas (sm_100a): many independent EAM systems of uneven size in
+// one launch per kernel.
+//
+// Layout: replica k owns slots [off, off + n_slots) of the shared SimEngine
+// arrays, off and n_slots multiples of 32, so a warp's 32 slots always belong
+// to one replica and per-replica data (box, cell grid, temperature, grip
+// rate) is warp-uniform.  Positions carry the replica's own fixed-point
+// fractional code, so the minimum image of every pair is the int32 difference
+// as in the single-system engine; only the conversion to Cartesian uses the
+// replica's box.  Neighbour rows hold batch slot indices.
+//
+// Rebuilds are per replica: the skin/2 trigger sets rep_flags[k], and every
+// rebuild kernel skips the slots and cells of replicas that are not flagged,
+// so a hot replica can rebuild every few steps without touching the others.
+//
+// Reductions: each warp writes the sums of its 32 slots to chunk_red; one
+// block per replica then adds its chunks in a fixed order in FP64 with Kahan
+// compensation (deterministic, no atomics).
+//
+// Pair arithmetic, table interpolation and integration are the single-system
+// engine's (eam_device.cuh, grid.cuh, common.cuh), so a replica advanced in a
+// batch matches the same system advanced alone.
+#include <cstdio>
+#include "common.cuh"
+#include "grid.cuh"
+#include "eam_device.cuh"
+
+namespace simb200 {
+
+#define BATCH_DENSITY_THREADS 512
+#define BATCH_FORCE_THREADS 1024
+#define BATCH_WINDOW_ROWS 4096
+
+__device__ __forceinline__ int slot_replica(const SimBatch& B, int64_t i, bool& real) {
+    const int r = B.slot_rep[i];
+    real = r >= 0;
+    return r >= 0 ? r : -1 - r;
+}
+
+// ---------------------------------------------------------------------------
+// rebuild (gated per replica by rep_flags)
+
+__global__ void k_bb_bin(SimBatch B, int only_flagged) {
+    const SimEngine& e = B.e;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+        bool real;
+        const int k = slot_replica(B, i, real);
+        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+        const SimRep& R = B.rep[k];
+        double s[3];
+        cart_to_frac(R.box, e.x[i], e.x[e.n_pad + i], e.x[2 * e.n_pad + i], s);
+        const int cx = cell_coord(s[0], R.ncell[0]);
+        const int cy = cell_coord(s[1], R.ncell[1]);
+        const int cz = cell_coord(s[2], R.ncell[2]);
+        const int lin = cx + R.ncell[0] * (cy + R.ncell[1] * cz);
+        const int c = R.cell_off + e.cell_rank[2 * R.cell_off + lin];
+        e.cell_of[i] = c;
+        atomicAdd(&e.cell_count[c], 1);
+    }
+}
+
+// One block per replica: exclusive scan of its cell counts, based at its first
+// slot; counts are zeroed for the scatter.
+__global__ void __launch_bounds__(1024) k_bb_scan(SimBatch B, int only_flagged) {
+    const int k = blockIdx.x;
+    if (only_flagged && B.rep_flags[k] == 0) return;
+    const SimRep& R = B.rep[k];
+    int32_t* cnt = B.e.cell_count + R.cell_off;
+    int32_t* start = B.e.cell_start + R.cell_off;
+    const int n = R.n_cells;
+    __shared__ int32_t warp_tot[32];
+    __shared__ int32_t carry_s;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) carry_s = (int32_t)R.off;
+    __syncthreads();
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int idx = base + tid;
+        const int32_t v = idx < n ? cnt[idx] : 0;
+        int32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const int32_t w = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+            int32_t wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += y;
+            }
+            warp_tot[lane] = wi - w;
+        }
+        __syncthreads();
+        const int32_t run = carry_s + warp_tot[warp] + (incl - v);
+        if (idx < n) {
+            start[idx] = run;
+            cnt[idx] = 0;
+        }
+        __syncthreads();
+        if (tid == blockDim.x - 1) carry_s = run + v;
+        __syncthreads();
+    }
+    if (tid == 0) start[n] = carry_s;
+}
+
+__global__ void k_bb_scatter(SimBatch B, int only_flagged) {
+    const SimEngine& e = B.e;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+        bool real;
+        const int k = slot_replica(B, i, real);
+        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+        const int c = e.cell_of[i];
+        e.perm[e.cell_start[c] + atomicAdd(&e.cell_count[c], 1)] = (int32_t)i;
+    }
+}
+
+// In-cell order by original index (reruns are bitwise reproducible); counts
+// are cleared for the next rebuild.
+__global__ void k_bb_sort_cells(SimBatch B, int only_flagged) {
+    const SimEngine& e = B.e;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < B.n_cell_entries; c += gridDim.x * blockDim.x) {
+        const int k = B.cell_rep[c];
+        if (only_flagged && B.rep_flags[k] == 0) continue;
+        if (c - B.rep[k].cell_off >= B.rep[k].n_cells) continue;   // the closing entry
+        e.cell_count[c] = 0;
+        const int b0 = e.cell_start[c], b1 = e.cell_start[c + 1];
+        for (int a = b0 + 1; a < b1; ++a) {
+            const int key = e.perm[a];
+            const int ko = e.orig[key];
+            int p = a - 1;
+            while (p >= b0 && e.orig[e.perm[p]] > ko) {
+                e.perm[p + 1] = e.perm[p];
+                --p;
+            }
+            e.perm[p + 1] = key;
+        }
+    }
+}
+
+__global__ void k_bb_permute(SimBatch B, int only_flagged) {
+    const SimEngine& e = B.e;
+    const int64_t P = e.n_pad;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < e.n; m += (int64_t)gridDim.x * blockDim.x) {
+        bool real;
+        const int k = slot_replica(B, m, real);
+        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+        const int64_t o = e.perm[m];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            e.x_alt[c * P + m] = e.x[c * P + o];
+            e.v_alt[c * P + m] = e.v[c * P + o];
+        }
+        reinterpret_cast<float4*>(e.f32_alt)[m] = reinterpret_cast<const float4*>(e.f32)[o];
+        e.orig_alt[m] = e.orig[o];
+        e.cell_of[m] = e.posq[4 * o + 3];   // the type; posq is rewritten by k_bb_commit
+    }
+}
+
+__global__ void k_bb_commit(SimBatch B, int only_flagged) {
+    const SimEngine& e = B.e;
+    const int64_t P = e.n_pad;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < e.n; m += (int64_t)gridDim.x * blockDim.x) {
+        bool real;
+        const int k = slot_replica(B, m, real);
+        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+        const double x0 = e.x_alt[m], x1 = e.x_alt[P + m], x2 = e.x_alt[2 * P + m];
+        e.x[m] = x0; e.x[P + m] = x1; e.x[2 * P + m] = x2;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) e.v[c * P + m] = e.v_alt[c * P + m];
+        reinterpret_cast<float4*>(e.f32)[m] = reinterpret_cast<const float4*>(e.f32_alt)[m];
+        e.orig[m] = e.orig_alt[m];
+        const int type = e.cell_of[m];
+        double s[3];
+        cart_to_frac(B.rep[k].box, x0, x1, x2, s);
+        const uint32_t u0 = to_fixed(s[0]), u1 = to_fixed(s[1]), u2 = to_fixed(s[2]);
+        reinterpret_cast<int4*>(e.posq)[m] = make_int4((int32_t)u0, (int32_t)u1, (int32_t)u2, type);
+        e.xref[m] = (int32_t)u0; e.xref[P + m] = (int32_t)u1; e.xref[2 * P + m] = (int32_t)u2;
+    }
+}
+
+// slot -> cell entry after the sort (binary search over the replica's starts)
+__global__ void k_bb_slot_cells(SimBatch B, int only_flagged) {
+    const SimEngine& e = B.e;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < e.n; m += (int64_t)gridDim.x * blockDim.x) {
+        bool real;
+        const int k = slot_replica(B, m, real);
+        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+        const SimRep& R = B.rep[k];
+        int lo = R.cell_off, hi = R.cell_off + R.n_cells;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (e.cell_start[mid] <= m) lo = mid; else hi = mid;
+        }
+        e.cell_of[m] = lo;
+    }
+}
+
+__global__ void __launch_bounds__(SIM_THREADS) k_bb_build_ell(SimBatch B, float rc2_list, int only_flagged) {
+    const SimEngine& e = B.e;
+    const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
+    uint32_t key_d2[ELL_SORT_MAX];
+    int key_j[ELL_SORT_MAX];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+        bool real;
+        const int k = slot_replica(B, i, real);
+        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+        const SimRep& R = B.rep[k];
+        const int32_t* rank = e.cell_rank + 2 * R.cell_off;
+        const CellGrid g{&R.box, R.ncell[0], R.ncell[1], R.ncell[2], rank, e.cell_start + R.cell_off};
+        const int lin = rank[R.n_cells + (e.cell_of[i] - R.cell_off)];
+        ell_row(posq, i, lin, g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags, key_d2, key_j);
+    }
+}
+
+__global__ void k_bb_finish(SimBatch B, int only_flagged) {
+    bool any = false;
+    for (int k = threadIdx.x; k < B.n_rep; k += blockDim.x) {
+        if (!only_flagged || B.rep_flags[k] != 0) {
+            B.rep_rebuilds[k] += 1;
+            any = true;
+        }
+        B.rep_flags[k] = 0;
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
+        if (any) B.e.flags[3] += 1;
+        B.e.flags[0] = 0;
+    }
+}
+
+static int grid_slots(int64_t n) {
+    const int64_t g = ceil_div(n, SIM_THREADS);
+    return (int)(g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g));
+}
+
+static int batch_rebuild(const SimBatch& B, int only_flagged, cudaStream_t st) {
+    const int g = grid_slots(B.e.n);
+    k_bb_bin<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
+    k_bb_scan<<<B.n_rep, 1024, 0, st>>>(B, only_flagged);
+    k_bb_scatter<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
+    k_bb_sort_cells<<<grid_slots(B.n_cell_entries), SIM_THREADS, 0, st>>>(B, only_flagged);
+    k_bb_permute<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
+    k_bb_commit<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
+    k_bb_slot_cells<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
+    const float rc2_list = (float)(B.e.x_rc * B.e.x_rc * (1.0 + 4e-6));
+    k_bb_build_ell<<<g, SIM_THREADS, 0, st>>>(B, rc2_list, only_flagged);
+    k_bb_finish<<<1, 256, 0, st>>>(B, only_flagged);
+    return launch_status("sim_batch_rebuild");
+}
+
+// ---------------------------------------------------------------------------
+// load: rows in original order (replica after replica) -> slots
+
+__global__ void k_bb_load(SimBatch B, const double* __restrict__ x_rows, const double* __restrict__ v_rows,
+                          const int32_t* __restrict__ types) {
+    const SimEngine& e = B.e;
+    const int64_t P = e.n_pad;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < P; m += (int64_t)gridDim.x * blockDim.x) {
+        bool real = false;
+        int k = 0;
+        if (m < e.n) k = slot_replica(B, m, real);
+        e.nnbr[m] = 0;
+        reinterpret_cast<float4*>(e.f32)[m] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!real) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) { e.x[c * P + m] = 0.0; e.v[c * P + m] = 0.0; e.xref[c * P + m] = 0; }
+            reinterpret_cast<int4*>(e.posq)[m] = make_int4(0, 0, 0, 0);
+            reinterpret_cast<int4*>(e.posfp)[m] = make_int4(0, 0, 0, 0);
+            e.orig[m] = -1;
+            continue;
+        }
+        const SimRep& R = B.rep[k];
+        const int64_t a = R.first + (m - R.off);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            e.x[c * P + m] = x_rows[3 * a + c];
+            e.v[c * P + m] = v_rows ? v_rows[3 * a + c] : 0.0;
+        }
+        e.orig[m] = (int32_t)a;
+        reinterpret_cast<int4*>(e.posq)[m] = make_int4(0, 0, 0, types[a]);
+    }
+}
+
+__global__ void k_bb_flag_all(SimBatch B) {
+    for (int k = threadIdx.x; k < B.n_rep; k += blockDim.x) B.rep_flags[k] = 1;
+    if (threadIdx.x == 0) B.e.flags[0] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// EAM pass 1: as k_eam_density, with the replica's box per warp and per-warp
+// embedding-energy sums
+
+template <bool ORTHO>
+__global__ void __launch_bounds__(BATCH_DENSITY_THREADS, 3) k_bb_density(SimBatch B, SimEAMTables t, Window w) {
+    extern __shared__ float2 s_dens[];
+    const SimEngine& e = B.e;
+    const float2* dens = reinterpret_cast<const float2*>(t.dens_vd);
+    for (int k = threadIdx.x; k < w.n_win; k += blockDim.x) s_dens[k] = __ldg(&dens[w.k_lo + k]);
+    __syncthreads();
+    const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
+    int4* __restrict__ posfp = reinterpret_cast<int4*>(e.posfp);
+    const int32_t* __restrict__ nbr = e.nbr;
+    const int64_t P = e.n_pad;
+    const float rc2 = t.cutoff * t.cutoff;
+    const bool use_mask = e.cut_mask != nullptr && e.nbr_cap <= 64;
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+        bool real;
+        const int k = slot_replica(B, i, real);
+        const BoxF b(B.rep[k].box);
+        float F = 0.0f;
+        if (real) {
+            const int4 qi = posq[i];
+            const int nn = e.nnbr[i];
+            float rho = 0.0f;
+            uint32_t in_lo = 0, in_hi = 0;
+            int kk = 0;
+            for (; kk + 4 <= nn; kk += 4) {
+                int j[4];
+                int4 q[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) j[u] = __ldg(&nbr[(int64_t)(kk + u) * P + i]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) q[u] = __ldg(&posq[j[u]]);
+                uint32_t bits = 0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    bool in;
+                    rho += density_term<true, ORTHO>(b, qi, q[u], rc2, dens, s_dens, w, t, in);
+                    bits |= (uint32_t)in << u;
+                }
+                if (kk < 32) in_lo |= bits << kk;
+                else in_hi |= bits << (kk - 32);
+            }
+            for (; kk < nn; ++kk) {
+                bool in;
+                rho += density_term<true, ORTHO>(b, qi, __ldg(&posq[__ldg(&nbr[(int64_t)kk * P + i])]), rc2, dens,
+                                                 s_dens, w, t, in);
+                if (kk < 32) in_lo |= (uint32_t)in << kk;
+                else in_hi |= (uint32_t)in << (kk - 32);
+            }
+            float Fp;
+            embed_lookup(t, 0, rho, F, Fp);
+            posfp[i] = make_int4(qi.x, qi.y, qi.z, __float_as_int(Fp));
+            if (use_mask) e.cut_mask[i] = ((uint64_t)in_hi << 32) | in_lo;
+        }
+        const float sum = warp_sum_f(F);
+        if (lane == 0) B.chunk_red[(i >> 5) * SIM_RED_SLOTS + SIM_RED_EPOT_EMBED] = (double)sum;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// EAM pass 2 (+ integration): as k_eam_force<SINGLE>, with per-replica box,
+// Langevin amplitude and grips, and per-warp sums of the 15 reduction slots.
+
+// Grip atom at step `step`: its reference position moved along the grip axis
+// by half the opening (lower grip -, upper grip +).
+__device__ __forceinline__ void grip_position(const SimBatch& B, const SimRep& R, int code, int64_t a, uint64_t step,
+                                              double* xn) {
+    const double* h = R.box.H + 3 * R.grip_axis;
+    const double len = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+    const double d = (code == 2 ? 1.0 : -1.0) * (0.5 * R.grip_rate * (double)(step + 1)) / len;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) xn[c] = B.gref[c * B.e.n_pad + a] + d * h[c];
+}
+
+template <int MODE, bool ORTHO>
+__global__ void __launch_bounds__(BATCH_FORCE_THREADS, 1) k_bb_force(SimBatch B, SimEAMTables t, SimIntegrator ip,
+                                                                     Window w) {
+    extern __shared__ float4 s_tab4[];
+    const SimEngine& e = B.e;
+    float4* tab_d = s_tab4;
+    float2* tab_p = reinterpret_cast<float2*>(s_tab4 + w.n_win);
+    {
+        const float4* gd = reinterpret_cast<const float4*>(t.deriv_vd) + w.k_lo;
+        const float2* gp = reinterpret_cast<const float2*>(t.pair_vd) + w.k_lo;
+        for (int k = threadIdx.x; k < w.n_win; k += blockDim.x) {
+            tab_d[k] = __ldg(&gd[k]);
+            tab_p[k] = __ldg(&gp[k]);
+        }
+        __syncthreads();
+    }
+    const int4* __restrict__ posfp = reinterpret_cast<const int4*>(e.posfp);
+    const int32_t* __restrict__ nbr = e.nbr;
+    const int64_t P = e.n_pad;
+    const float rc2 = t.cutoff * t.cutoff;
+    const bool use_mask = e.cut_mask != nullptr && e.nbr_cap <= 64;
+    const int lane = threadIdx.x & 31;
+    bool bad = false;
+    const uint64_t step = MODE && ip.step_ctr ? *ip.step_ctr : 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+        bool real;
+        const int k = slot_replica(B, i, real);
+        const SimRep& R = B.rep[k];
+        const BoxF b(R.box);
+        float acc[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        bool trig = false;
+        if (real) {
+            const int4 pi = posfp[i];
+            const float fpi = __int_as_float(pi.w);
+            float fx = 0.f, fy = 0.f, fz = 0.f;
+            if (use_mask) {
+                uint64_t m = e.cut_mask[i];
+                for (int kk = pop_slot(m); kk >= 0; kk = pop_slot(m))
+                    pair_single<ORTHO>(b, pi, __ldg(&posfp[__ldg(&nbr[(int64_t)kk * P + i])]), rc2, fpi, tab_d,
+                                       tab_p, w, t, fx, fy, fz, acc);
+            } else {
+                const int nn = e.nnbr[i];
+                for (int kk = 0; kk < nn; ++kk)
+                    pair_single<ORTHO>(b, pi, __ldg(&posfp[__ldg(&nbr[(int64_t)kk * P + i])]), rc2, fpi, tab_d,
+                                       tab_p, w, t, fx, fy, fz, acc);
+            }
+            reinterpret_cast<float4*>(e.f32)[i] = make_float4(fx, fy, fz, 0.0f);
+            bad |= !(isfinite(fx) && isfinite(fy) && isfinite(fz));
+            if (MODE) {
+                const int64_t a = e.orig[i];
+                const int code = B.grip[a];
+                const double m = e.mass[0];
+                double v[3] = {0.0, 0.0, 0.0};
+                if (code == 0) {
+                    SimIntegrator ipk = ip;
+                    ipk.rff = B.rep_rff + k;          // one element type: rff[0] of this replica
+                    second_half_atom(e, ipk, i, 0, step, (double)fx, (double)fy, (double)fz, v, bad, MODE == 1);
+                } else if (MODE == 1) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) e.v[c * P + i] = 0.0;
+                }
+                acc[8] += (float)(0.5 * m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+                acc[9] += (float)(m * v[0] * v[0]); acc[10] += (float)(m * v[1] * v[1]); acc[11] += (float)(m * v[2] * v[2]);
+                acc[12] += (float)(m * v[0] * v[1]); acc[13] += (float)(m * v[0] * v[2]); acc[14] += (float)(m * v[1] * v[2]);
+                if (MODE == 2) {
+                    if (code == 0) {
+                        const double f[3] = {(double)fx, (double)fy, (double)fz};
+                        trig = first_half_atom(e, R.box, ip, i, 0, f, v, bad);
+                    } else {
+                        double xn[3];
+                        grip_position(B, R, code, a, step + 1, xn);
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) e.v[c * P + i] = 0.0;
+                        trig = place_atom(e, R.box, i, 0, xn);
+                    }
+                }
+            }
+        }
+        if (MODE == 2 && __any_sync(0xffffffffu, trig) && lane == 0) {
+            B.rep_flags[k] = 1;
+            e.flags[0] = 1;
+        }
+        double* out = B.chunk_red + (i >> 5) * SIM_RED_SLOTS;
+#pragma unroll
+        for (int s = 0; s < 15; ++s) {
+            if (!MODE && s >= 8) break;
+            const float v = warp_sum_f(acc[s]);
+            if (lane == 0) out[SIM_RED_EPOT_PAIR + s] = s < 8 ? 0.5 * (double)v : (double)v;
+        }
+    }
+    if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+}
+
+// First half-step of every replica at the start of a run (step = *ctr + 1;
+// the counter itself is advanced by k_bb_advance_step afterwards).
+__global__ void k_bb_first_half(SimBatch B, SimIntegrator p) {
+    const SimEngine& e = B.e;
+    const int64_t P = e.n_pad;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool trig = false, bad = false;
+    const uint64_t step = *p.step_ctr + 1;
+    int k = 0;
+    if (i < e.n) {
+        bool real;
+        k = slot_replica(B, i, real);
+        if (real) {
+            const SimRep& R = B.rep[k];
+            const int64_t a = e.orig[i];
+            const int code = B.grip[a];
+            if (code == 0) {
+                const float4 f4 = reinterpret_cast<const float4*>(e.f32)[i];
+                const double f[3] = {(double)f4.x, (double)f4.y, (double)f4.z};
+                trig = first_half_atom(e, R.box, p, i, 0, f, nullptr, bad);
+            } else {
+                double xn[3];
+                grip_position(B, R, code, a, step, xn);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) e.v[c * P + i] = 0.0;
+                trig = place_atom(e, R.box, i, 0, xn);
+            }
+        }
+    }
+    if (__any_sync(0xffffffffu, trig) && (threadIdx.x & 31) == 0) {
+        B.rep_flags[k] = 1;
+        e.flags[0] = 1;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+}
+
+__global__ void k_bb_advance_step(uint64_t* ctr) { *ctr += 1; }
+
+// One block per replica: FP64 Kahan sums of its warps' partials in a fixed
+// order; with a log, also into row (*step % cap).
+__global__ void __launch_bounds__(256) k_bb_reduce(SimBatch B, const uint64_t* step, double* log, int cap) {
+    const int k = blockIdx.x;
+    const SimRep& R = B.rep[k];
+    const int64_t c0 = R.off >> 5, c1 = (R.off + R.n_slots) >> 5;
+    __shared__ double part[256][SIM_RED_SLOTS + 1];
+    double s[SIM_RED_SLOTS], comp[SIM_RED_SLOTS];
+#pragma unroll
+    for (int q = 0; q < SIM_RED_SLOTS; ++q) { s[q] = 0.0; comp[q] = 0.0; }
+    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+        const double* src = B.chunk_red + c * SIM_RED_SLOTS;
+#pragma unroll
+        for (int q = 0; q < SIM_RED_SLOTS; ++q) {
+            const double y = src[q] - comp[q];
+            const double tt = s[q] + y;
+            comp[q] = (tt - s[q]) - y;
+            s[q] = tt;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < SIM_RED_SLOTS; ++q) part[threadIdx.x][q] = s[q];
+    __syncthreads();
+    if (threadIdx.x < SIM_RED_SLOTS) {
+        const int q = threadIdx.x;
+        double acc = 0.0, cc = 0.0;
+        for (int t = 0; t < (int)blockDim.x; ++t) {
+            const double y = part[t][q] - cc;
+            const double tt = acc + y;
+            cc = (tt - acc) - y;
+            acc = tt;
+        }
+        B.rep_red[k * SIM_RED_SLOTS + q] = acc;
+        if (log) log[((*step % (uint64_t)cap) * B.n_rep + k) * SIM_RED_SLOTS + q] = acc;
+    }
+}
+
+__global__ void k_bb_gather_f64(SimBatch B, const double* __restrict__ src, double* __restrict__ out) {
+    const SimEngine& e = B.e;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < e.n; m += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = e.orig[m];
+        if (B.slot_rep[m] < 0 || o < 0) continue;
+        out[3 * o] = src[m];
+        out[3 * o + 1] = src[e.n_pad + m];
+        out[3 * o + 2] = src[2 * e.n_pad + m];
+    }
+}
+
+__global__ void k_bb_gather_f32(SimBatch B, const float* __restrict__ src, double* __restrict__ out) {
+    const SimEngine& e = B.e;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < e.n; m += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = e.orig[m];
+        if (B.slot_rep[m] < 0 || o < 0) continue;
+        const float4 f = reinterpret_cast<const float4*>(src)[m];
+        out[3 * o] = f.x;
+        out[3 * o + 1] = f.y;
+        out[3 * o + 2] = f.z;
+    }
+}
+
+}  // namespace simb200
+
+using namespace simb200;
+
+static bool batch_ok(const SimBatch* b) {
+    return b && b->rep && b->n_rep > 0 && b->e.n > 0 && b->e.n % 32 == 0 && b->e.n_pad >= b->e.n &&
+           b->e.n_pad % 128 == 0 && b->slot_rep && b->cell_rep && b->rep_flags && b->rep_rebuilds && b->grip &&
+           b->gref && b->rep_rff && b->chunk_red && b->rep_red && b->e.n_types == 1 && b->e.nbr_cap > 0;
+}
+
+static Window batch_window(const SimEAMTables& t) {
+    const int n_win = t.n_r < BATCH_WINDOW_ROWS ? t.n_r : BATCH_WINDOW_ROWS;
+    return Window{t.n_r - n_win, n_win};
+}
+
+static bool batch_tables_ok(const SimEAMTables* t) {
+    return t && t->n_types == 1 && t->n_r >= 2 && t->n_rho >= 2 && t->dens_vd && t->deriv_vd && t->pair_vd &&
+           t->embed && t->embed_deriv && t->rho_min && t->inv_drho && t->rho_clamp_hi;
+}
+
+static void batch_set_attributes() {
+    static bool done = false;   // the first call happens before any stream capture
+    if (done) return;
+    const int lim = 200 * 1024;
+    cudaFuncSetAttribute(k_bb_density<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_bb_density<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_bb_force<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_bb_force<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_bb_force<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_bb_force<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_bb_force<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_bb_force<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaGetLastError();
+    done = true;
+}
+
+extern "C" int sim_batch_load(const SimBatch* b, const double* x_rows, const double* v_rows, const int32_t* types,
+                              void* stream) {
+    if (!batch_ok(b) || !x_rows || !types) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    prepare_capture_stream();
+    batch_set_attributes();
+    k_bb_load<<<grid_slots(b->e.n_pad), SIM_THREADS, 0, st>>>(*b, x_rows, v_rows, types);
+    k_bb_flag_all<<<1, 256, 0, st>>>(*b);
+    return batch_rebuild(*b, 1, st);
+}
+
+extern "C" int sim_batch_rebuild(const SimBatch* b, int32_t only_flagged, void* stream) {
+    if (!batch_ok(b)) return SIM_ERR_ARG;
+    return batch_rebuild(*b, only_flagged ? 1 : 0, (cudaStream_t)stream);
+}
+
+static int batch_rebuild_body(const void* ctx, cudaStream_t s) { return batch_rebuild(*(const SimBatch*)ctx, 1, s); }
+
+extern "C" int sim_batch_rebuild_if_needed(const SimBatch* b, void* stream) {
+    if (!batch_ok(b)) return SIM_ERR_ARG;
+    // the replica flags gate every kernel, so the eager path is the same body
+    return launch_if_flag((cudaStream_t)stream, b->e.flags, batch_rebuild_body, batch_rebuild_body, b,
+                          "sim_batch_rebuild_if_needed");
+}
+
+extern "C" int sim_batch_eam_density(const SimBatch* b, const SimEAMTables* t, void* stream) {
+    if (!batch_ok(b) || !batch_tables_ok(t)) return SIM_ERR_ARG;
+    batch_set_attributes();
+    const Window w = batch_window(*t);
+    const size_t smem = (size_t)w.n_win * sizeof(float2);
+    const bool ortho = b->e.box_orthogonal != 0;
+    const void* fn = ortho ? (const void*)k_bb_density<true> : (const void*)k_bb_density<false>;
+    const int g = persistent_grid(fn, BATCH_DENSITY_THREADS, smem, b->e.n);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (ortho) k_bb_density<true><<<g, BATCH_DENSITY_THREADS, smem, st>>>(*b, *t, w);
+    else k_bb_density<false><<<g, BATCH_DENSITY_THREADS, smem, st>>>(*b, *t, w);
+    return launch_status("sim_batch_eam_density");
+}
+
+template <int MODE>
+static void launch_bb_force(const SimBatch& b, const SimEAMTables& t, const SimIntegrator& ip, bool ortho,
+                            cudaStream_t st) {
+    const Window w = batch_window(t);
+    const size_t smem = (size_t)w.n_win * (sizeof(float4) + sizeof(float2));
+    const void* fn = ortho ? (const void*)k_bb_force<MODE, true> : (const void*)k_bb_force<MODE, false>;
+    const int g = persistent_grid(fn, BATCH_FORCE_THREADS, smem, b.e.n);
+    if (ortho) k_bb_force<MODE, true><<<g, BATCH_FORCE_THREADS, smem, st>>>(b, t, ip, w);
+    else k_bb_force<MODE, false><<<g, BATCH_FORCE_THREADS, smem, st>>>(b, t, ip, w);
+}
+
+extern "C" int sim_batch_eam_force(const SimBatch* b, const SimEAMTables* t, const SimIntegrator* p, int32_t mode,
+                                   void* stream) {
+    if (!batch_ok(b) || !batch_tables_ok(t) || mode < 0 || mode > 2) return SIM_ERR_ARG;
+    SimIntegrator ip{};
+    if (mode) {
+        if (!p || !p->step_ctr) return SIM_ERR_ARG;
+        ip = *p;
+    }
+    batch_set_attributes();
+    const bool ortho = b->e.box_orthogonal != 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (mode == 0) launch_bb_force<0>(*b, *t, ip, ortho, st);
+    else if (mode == 1) launch_bb_force<1>(*b, *t, ip, ortho, st);
+    else launch_bb_force<2>(*b, *t, ip, ortho, st);
+    return launch_status("sim_batch_eam_force");
+}
+
+extern "C" int sim_batch_first_half(const SimBatch* b, const SimIntegrator* p, void* stream) {
+    if (!batch_ok(b) || !p || !p->step_ctr) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    k_bb_first_half<<<(int)ceil_div(b->e.n, SIM_THREADS), SIM_THREADS, 0, st>>>(*b, *p);
+    k_bb_advance_step<<<1, 1, 0, st>>>(p->step_ctr);
+    return launch_status("sim_batch_first_half");
+}
+
+extern "C" int sim_batch_reduce(const SimBatch* b, const uint64_t* step, double* log, int32_t log_cap, void* stream) {
+    if (!batch_ok(b) || (log && (log_cap <= 0 || !step))) return SIM_ERR_ARG;
+    k_bb_reduce<<<b->n_rep, 256, 0, (cudaStream_t)stream>>>(*b, step, log, log_cap);
+    return launch_status("sim_batch_reduce");
+}
+
+extern "C" int sim_batched_step(const SimBatch* b, const SimEAMTables* t, const SimIntegrator* p, int32_t last,
+                                double* log, int32_t log_cap, void* stream) {
+    if (!batch_ok(b) || !batch_tables_ok(t) || !p || !p->step_ctr || (log && log_cap <= 0)) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = sim_batch_eam_density(b, t, stream);
+    if (rc != SIM_OK) return rc;
+    rc = sim_batch_eam_force(b, t, p, last ? 1 : 2, stream);
+    if (rc != SIM_OK) return rc;
+    rc = sim_batch_reduce(b, p->step_ctr, log, log_cap, stream);
+    if (rc != SIM_OK) return rc;
+    if (last) return SIM_OK;
+    k_bb_advance_step<<<1, 1, 0, st>>>(p->step_ctr);
+    rc = launch_status("sim_batched_step");
+    if (rc != SIM_OK) return rc;
+    return sim_batch_rebuild_if_needed(b, stream);
+}
+
+extern "C" int sim_batch_gather_f64(const SimBatch* b, const double* src_soa, double* out_rows, void* stream) {
+    if (!batch_ok(b) || !src_soa || !out_rows) return SIM_ERR_ARG;
+    k_bb_gather_f64<<<grid_slots(b->e.n), SIM_THREADS, 0, (cudaStream_t)stream>>>(*b, src_soa, out_rows);
+    return launch_status("sim_batch_gather_f64");
+}
+
+extern "C" int sim_batch_gather_f32(const SimBatch* b, const float* src_aos4, double* out_rows, void* stream) {
+    if (!batch_ok(b) || !src_aos4 || !out_rows) return SIM_ERR_ARG;
+    k_bb_gather_f32<<<grid_slots(b->e.n), SIM_THREADS, 0, (cudaStream_t)stream>>>(*b, src_aos4, out_rows);
+    return launch_status("sim_batch_gather_f32");
+}

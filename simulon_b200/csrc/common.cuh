@@ -13,6 +13,9 @@ void set_cuda_error(cudaError_t err, const char* where);
 void set_error_text(const char* msg);        // message returned by sim_last_cuda_error()
 int  launch_status(const char* where);   // checks cudaGetLastError after a launch
 void prepare_capture_stream();           // side stream used to capture IF-node bodies
+typedef int (*BodyFn)(const void* ctx, cudaStream_t s);
+int  launch_if_flag(cudaStream_t st, const int32_t* flag, BodyFn body, BodyFn eager, const void* ctx,
+                    const char* what);       // IF node on *flag while capturing, else eager()
 // Persistent grid: resident blocks per SM (cached occupancy query) x SM count,
 // capped by the number of atom tiles.
 int persistent_grid(const void* fn, int threads, size_t smem, int64_t n);
@@ -88,6 +91,11 @@ __device__ __forceinline__ double norm2_f64(double a, double b, double c) {
 }
 
 // ---- reductions -------------------------------------------------------------
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -211,10 +219,11 @@ __device__ __forceinline__ void second_half_atom(const SimEngine& e, const SimIn
 // x += v dt, refresh the fixed-point code in posq, and report whether the atom
 // moved more than skin/2 from its position at the last rebuild
 // (reader.py:136-163).  v_in: the velocity to kick (read from e.v when NULL).
-__device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimIntegrator& p, int64_t i, int type,
-                                                const double* f, const double* v_in, bool& bad) {
+__device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, int64_t i, int type, const double* xn);
+
+__device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimBox& b, const SimIntegrator& p, int64_t i,
+                                                int type, const double* f, const double* v_in, bool& bad) {
     const int64_t P = e.n_pad;
-    const SimBox& b = *e.box;
     const double m = e.mass[type];
     double xn[3];
 #pragma unroll
@@ -224,9 +233,23 @@ __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimInt
         const double vh = __dadd_rn(v0, __dmul_rn(__dmul_rn(0.5, a), p.dt));
         xn[c] = __dadd_rn(e.x[c * P + i], __dmul_rn(vh, p.dt));
         e.v[c * P + i] = vh;
-        e.x[c * P + i] = xn[c];
         bad |= !isfinite(xn[c]) || !isfinite(vh);
     }
+    return place_atom(e, b, i, type, xn);
+}
+
+__device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimIntegrator& p, int64_t i, int type,
+                                                const double* f, const double* v_in, bool& bad) {
+    return first_half_atom(e, *e.box, p, i, type, f, v_in, bad);
+}
+
+// Store position xn of slot i, refresh its fixed-point code in posq, and
+// report whether it is more than skin/2 from its position at the last rebuild
+// (reader.py:136-163).
+__device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, int64_t i, int type, const double* xn) {
+    const int64_t P = e.n_pad;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e.x[c * P + i] = xn[c];
     double s[3];
     cart_to_frac(b, xn[0], xn[1], xn[2], s);
     int4 q;

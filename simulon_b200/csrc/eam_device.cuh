@@ -1,0 +1,140 @@
+// EAM device helpers shared by the single-system and the batched kernels:
+// fixed-point displacement -> Cartesian vector, table interpolation
+// (eam_force_cu.py:437-459), the pass-1 density term and the pass-2 pair
+// force with its energy and virial accumulation.
+#pragma once
+#include "common.cuh"
+
+namespace simb200 {
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// _interp_rho for F and F' of type ti
+__device__ __forceinline__ void embed_lookup(const SimEAMTables& t, int ti, float rho, float& F, float& Fp) {
+    const float lo = t.rho_min[ti];
+    const float rc = fminf(fmaxf(rho, lo), t.rho_clamp_hi[ti]);
+    const float idx_f = (rc - lo) * t.inv_drho[ti];
+    const int i = (int)idx_f;
+    const int i1 = min(i + 1, t.n_rho - 1);
+    const float frac = idx_f - (float)i;
+    const float* e = t.embed + (size_t)ti * t.n_rho;
+    const float* d = t.embed_deriv + (size_t)ti * t.n_rho;
+    F = fmaf(frac, e[i1] - e[i], e[i]);
+    Fp = fmaf(frac, d[i1] - d[i], d[i]);
+}
+
+// Box terms in registers, with the 2^-32 of the fixed-point code folded in.
+struct BoxF {
+    float h[9];
+    __device__ __forceinline__ explicit BoxF(const SimBox& b) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) h[k] = b.Hf[k] * 2.3283064365386963e-10f;
+    }
+};
+template <bool ORTHO>
+__device__ __forceinline__ void rvec(const BoxF& b, const int4& qi, const int4& qj, float& r0, float& r1, float& r2) {
+    const float t0 = __int2float_rn((int32_t)((uint32_t)qi.x - (uint32_t)qj.x));
+    const float t1 = __int2float_rn((int32_t)((uint32_t)qi.y - (uint32_t)qj.y));
+    const float t2 = __int2float_rn((int32_t)((uint32_t)qi.z - (uint32_t)qj.z));
+    if (ORTHO) {
+        r0 = t0 * b.h[0];
+        r1 = t1 * b.h[4];
+        r2 = t2 * b.h[8];
+    } else {
+        r0 = fmaf(t2, b.h[6], fmaf(t1, b.h[3], t0 * b.h[0]));
+        r1 = fmaf(t2, b.h[7], fmaf(t1, b.h[4], t0 * b.h[1]));
+        r2 = fmaf(t2, b.h[8], fmaf(t1, b.h[5], t0 * b.h[2]));
+    }
+}
+
+// r inside the cutoff -> table row and fraction (_interp_r)
+struct Lerp {
+    int k;
+    float frac;
+};
+__device__ __forceinline__ Lerp lerp_r(float r, const SimEAMTables& t) {
+    const float idx_f = fminf(r, t.r_clamp_hi) * t.inv_dr;
+    const int k = (int)idx_f;
+    return Lerp{k, idx_f - (float)k};
+}
+
+// ---------------------------------------------------------------------------
+// pass 1
+// Shared-memory window of the r-tables: rows k in [k_lo, n_r) (r >= k_lo dr);
+// the rare shorter distances read the global table.
+struct Window {
+    int k_lo, n_win;
+};
+
+template <bool SMEM, bool ORTHO>
+__device__ __forceinline__ float density_term(const BoxF& b, const int4& qi, const int4& qj, float rc2,
+                                              const float2* g_i, const float2* s_i, Window w,
+                                              const SimEAMTables& t, bool& inside) {
+    float r0, r1, r2;
+    rvec<ORTHO>(b, qi, qj, r0, r1, r2);
+    const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
+    inside = d2 < rc2;
+    if (!inside) return 0.0f;
+    const Lerp l = lerp_r(d2 * rsqrt_approx(d2), t);
+    float2 v;
+    if (SMEM && l.k >= w.k_lo) v = s_i[qj.w * w.n_win + (l.k - w.k_lo)];
+    else v = __ldg(&g_i[(size_t)qj.w * t.n_r + l.k]);
+    return fmaf(l.frac, v.y, v.x);
+}
+
+// Lowest set bit of m as a list slot (clearing it), or -1 when m is empty.
+__device__ __forceinline__ int pop_slot(uint64_t& m) {
+    if (m == 0) return -1;
+    const int k = __ffsll((long long)m) - 1;
+    m &= m - 1;
+    return k;
+}
+
+// ---------------------------------------------------------------------------
+// pass 2.  Per-thread accumulators: acc[0] pair energy, acc[1] scalar virial,
+// acc[2..7] virial tensor (xx yy zz xy xz yz), acc[8] K, acc[9..14] K tensor;
+// only the three force components are per atom.
+__device__ __forceinline__ void pair_force(float s, float phi, float r, float inv_r, float r0, float r1, float r2,
+                                           float& fx, float& fy, float& fz, float (&acc)[15]) {
+    const float c = -s * inv_r;            // force on i = c * r_ij
+    const float ax = c * r0, ay = c * r1, az = c * r2;
+    fx += ax; fy += ay; fz += az;
+    acc[0] += phi;
+    acc[1] = fmaf(s, r, acc[1]);
+    acc[2] = fmaf(ax, r0, acc[2]); acc[3] = fmaf(ay, r1, acc[3]); acc[4] = fmaf(az, r2, acc[4]);
+    acc[5] = fmaf(ax, r1, acc[5]); acc[6] = fmaf(ax, r2, acc[6]); acc[7] = fmaf(ay, r2, acc[7]);
+}
+
+// One element type: f'_{ti,tj} = f'_{tj,ti}; tables {f', phi', df', dphi'} and
+// {phi, dphi} staged in shared memory.
+template <bool ORTHO>
+__device__ __forceinline__ void pair_single(const BoxF& b, const int4& pi, const int4& qj, float rc2, float fpi,
+                                            const float4* tab_d, const float2* tab_p, Window w,
+                                            const SimEAMTables& t, float& fx, float& fy, float& fz,
+                                            float (&acc)[15]) {
+    float r0, r1, r2;
+    rvec<ORTHO>(b, pi, qj, r0, r1, r2);
+    const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
+    if (!(d2 < rc2)) return;
+    const float inv_r = rsqrt_approx(d2);
+    const float r = d2 * inv_r;
+    const Lerp l = lerp_r(r, t);
+    float4 d;
+    float2 p;
+    if (l.k >= w.k_lo) {
+        d = tab_d[l.k - w.k_lo];
+        p = tab_p[l.k - w.k_lo];
+    } else {
+        d = __ldg(reinterpret_cast<const float4*>(t.deriv_vd) + l.k);
+        p = __ldg(reinterpret_cast<const float2*>(t.pair_vd) + l.k);
+    }
+    const float2 dd_dp = __ffma2_rn(make_float2(l.frac, l.frac), make_float2(d.z, d.w), make_float2(d.x, d.y));
+    const float phi = fmaf(l.frac, p.y, p.x);
+    pair_force(fmaf(fpi + __int_as_float(qj.w), dd_dp.x, dd_dp.y), phi, r, inv_r, r0, r1, r2, fx, fy, fz, acc);
+}
+
+}  // namespace simb200

@@ -303,10 +303,10 @@ extern "C" const char* sim_last_cuda_error(void) { return g_err; }
 extern "C" int sim_version(void) { return 1; }
 
 extern "C" int sim_struct_sizes(int64_t* out, int32_t n) {
-    const int64_t sizes[6] = {(int64_t)sizeof(SimBox), (int64_t)sizeof(SimEngine), (int64_t)sizeof(SimEAMTables),
+    const int64_t sizes[8] = {(int64_t)sizeof(SimBox), (int64_t)sizeof(SimEngine), (int64_t)sizeof(SimEAMTables),
                               (int64_t)sizeof(SimLJParams), (int64_t)sizeof(SimIntegrator),
-                              (int64_t)sizeof(SimBerendsen)};
-    if (!out || n < 6) return SIM_ERR_ARG;
-    for (int k = 0; k < 6; ++k) out[k] = sizes[k];
+                              (int64_t)sizeof(SimBerendsen), (int64_t)sizeof(SimRep), (int64_t)sizeof(SimBatch)};
+    if (!out || n < 8) return SIM_ERR_ARG;
+    for (int k = 0; k < 8; ++k) out[k] = sizes[k];
     return SIM_OK;
 }

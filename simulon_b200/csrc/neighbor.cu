@@ -14,7 +14,9 @@
 //   the exact floating-point operation sequence of the reference's torch
 //   code (core/box.py:109-130; gpu_kdtree.py:130-138) in the caller's dtype,
 //   so the (i, j, image) set is bit-identical.  Rows are emitted sorted by j.
+#include <cstdio>
 #include "common.cuh"
+#include "grid.cuh"
 
 namespace simb200 {
 
@@ -78,12 +80,6 @@ __global__ void k_scan_exclusive(const T* __restrict__ in, int64_t n, T* __restr
 
 // ---------------------------------------------------------------------------
 // engine rebuild kernels (gate = flags, kernel returns unless flags[0] != 0)
-
-__device__ __forceinline__ int cell_coord(double s, int n) {
-    s -= floor(s);
-    int c = (int)(s * (double)n);
-    return c < 0 ? 0 : (c >= n ? n - 1 : c);
-}
 
 __global__ void k_bin(SimEngine e, const int32_t* gate) {
     if (gate && __ldg(gate) == 0) return;
@@ -183,86 +179,17 @@ __global__ void k_slot_cells(SimEngine e, const int32_t* gate) {
     }
 }
 
-// unique stencil offsets along one axis: n>=3 -> {-1,0,1}; n==2 -> {0,1}; n==1 -> {0}
-__device__ __forceinline__ int stencil_count(int n) { return n >= 3 ? 3 : n; }
-__device__ __forceinline__ int stencil_cell(int c, int k, int n) {
-    if (n >= 3) { int v = c + k - 1; return v < 0 ? v + n : (v >= n ? v - n : v); }
-    return k;   // n <= 2: enumerate every cell once
-}
-
-#define ELL_SORT_MAX 128   // rows up to this length are sorted by distance
-
-// Full list in ELL layout.  Test in FP32 on fixed-point displacements; the
-// radius carries a 2e-6 relative margin so that an exact FP64/FP32 filter
-// applied later (half-list export, force cutoffs) always sees a superset.
+// Full list in ELL layout (row builder in grid.cuh).
 __global__ void __launch_bounds__(SIM_THREADS) k_build_ell(SimEngine e, const int32_t* cell_lin,
                                                           float rc2_list, const int32_t* gate) {
     if (gate && __ldg(gate) == 0) return;
-    const int64_t P = e.n_pad;
-    const SimBox& b = *e.box;
-    const int nx = e.ncell[0], ny = e.ncell[1], nz = e.ncell[2];
+    const CellGrid g{e.box, e.ncell[0], e.ncell[1], e.ncell[2], e.cell_rank, e.cell_start};
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
-    float key_d2[ELL_SORT_MAX];
+    uint32_t key_d2[ELL_SORT_MAX];
     int key_j[ELL_SORT_MAX];
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int4 qi = posq[i];
-    const int lin = cell_lin[e.cell_of[i]];
-    const int cx = lin % nx, cy = (lin / nx) % ny, cz = lin / (nx * ny);
-    int cnt = 0;
-    const int sx = stencil_count(nx), sy = stencil_count(ny), sz = stencil_count(nz);
-    for (int kz = 0; kz < sz; ++kz) {
-        int z = stencil_cell(cz, kz, nz);
-        for (int ky = 0; ky < sy; ++ky) {
-            int y = stencil_cell(cy, ky, ny);
-            for (int kx = 0; kx < sx; ++kx) {
-                int xx = stencil_cell(cx, kx, nx);
-                int r = e.cell_rank[xx + nx * (y + ny * z)];
-                int j0 = e.cell_start[r], j1 = e.cell_start[r + 1];
-                for (int j = j0; j < j1; ++j) {
-                    if (j == i) continue;
-                    const int4 qj = posq[j];
-                    float t0 = fixed_delta(qi.x, qj.x);
-                    float t1 = fixed_delta(qi.y, qj.y);
-                    float t2 = fixed_delta(qi.z, qj.z);
-                    float r0, r1, r2;
-                    frac_to_cart_f(b, t0, t1, t2, r0, r1, r2);
-                    float d2 = __fadd_rn(__fadd_rn(__fmul_rn(r0, r0), __fmul_rn(r1, r1)), __fmul_rn(r2, r2));
-                    if (d2 < rc2_list) {
-                        if (cnt < e.nbr_cap) {
-                            if (cnt < ELL_SORT_MAX) { key_d2[cnt] = d2; key_j[cnt] = j; }
-                            e.nbr[(int64_t)cnt * P + i] = j;
-                        }
-                        ++cnt;
-                    }
-                }
-            }
-        }
-    }
-    const int kept = cnt < e.nbr_cap ? cnt : e.nbr_cap;
-    if (kept <= ELL_SORT_MAX) {
-        // nearest first (ties by slot): in a crystal every row then lists the
-        // same shells in the same order, so a warp's lanes agree on which
-        // neighbours fall inside the force cutoff
-        for (int a = 1; a < kept; ++a) {
-            const float kd = key_d2[a];
-            const int kj = key_j[a];
-            int p = a - 1;
-            while (p >= 0 && (key_d2[p] > kd || (key_d2[p] == kd && key_j[p] > kj))) {
-                key_d2[p + 1] = key_d2[p];
-                key_j[p + 1] = key_j[p];
-                --p;
-            }
-            key_d2[p + 1] = kd;
-            key_j[p + 1] = kj;
-        }
-        for (int a = 0; a < kept; ++a) e.nbr[(int64_t)a * P + i] = key_j[a];
-    }
-    e.nnbr[i] = kept;
-    if (cnt > e.nbr_cap) {
-        atomicOr(&e.flags[1], SIM_STATUS_OVERFLOW);
-        atomicMax(&e.flags[2], cnt);
-    }
-    }
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x)
+        ell_row(posq, i, cell_lin[e.cell_of[i]], g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags,
+                key_d2, key_j);
 }
 
 // Count the rebuild (flags[3]) when it ran and clear the request.
@@ -528,22 +455,25 @@ void simb200::prepare_capture_stream() {
     if (!g_body_stream) cudaStreamCreateWithFlags(&g_body_stream, cudaStreamNonBlocking);
 }
 
-extern "C" int sim_rebuild_if_needed(const SimEngine* ep, void* stream) {
-    if (!ep || !ep->box || ep->n <= 0) return SIM_ERR_ARG;
-    cudaStream_t st = (cudaStream_t)stream;
+// While `st` is being captured: a one-thread kernel turns *flag into the value
+// of an IF node whose body is captured from body(ctx, body_stream); otherwise
+// run eager(ctx, st), which tests the flag on the device itself.
+int simb200::launch_if_flag(cudaStream_t st, const int32_t* flag, BodyFn body, BodyFn eager, const void* ctx,
+                            const char* what) {
+    char msg[160];
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaGraph_t graph = nullptr;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
     cudaError_t err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
-    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: capture info"); return SIM_ERR_CUDA; }
-    if (cs != cudaStreamCaptureStatusActive || !g_body_stream) return sim_rebuild(ep, 1, stream);
+    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: capture info", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
+    if (cs != cudaStreamCaptureStatusActive || !g_body_stream) return eager(ctx, st);
     cudaGraphConditionalHandle h;
     err = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
-    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: handle"); return SIM_ERR_CUDA; }
-    k_set_rebuild_condition<<<1, 1, 0, st>>>(h, ep->flags);
+    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: handle", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
+    k_set_rebuild_condition<<<1, 1, 0, st>>>(h, flag);
     err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
-    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: capture info 2"); return SIM_ERR_CUDA; }
+    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: capture info 2", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = h;
@@ -551,17 +481,25 @@ extern "C" int sim_rebuild_if_needed(const SimEngine* ep, void* stream) {
     cp.conditional.size = 1;
     cudaGraphNode_t node;
     err = cudaGraphAddNode(&node, graph, deps, ndeps, &cp);
-    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: add node"); return SIM_ERR_CUDA; }
+    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: add node", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
     err = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
-    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: deps"); return SIM_ERR_CUDA; }
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
-    err = cudaStreamBeginCaptureToGraph(g_body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
-    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: body capture"); return SIM_ERR_CUDA; }
-    int rc = sim_rebuild(ep, 0, g_body_stream);
+    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: deps", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
+    cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+    err = cudaStreamBeginCaptureToGraph(g_body_stream, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: body capture", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
+    int rc = body(ctx, g_body_stream);
     cudaGraph_t captured = nullptr;
     err = cudaStreamEndCapture(g_body_stream, &captured);
-    if (err != cudaSuccess) { set_cuda_error(err, "sim_rebuild_if_needed: end body capture"); return SIM_ERR_CUDA; }
+    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: end body capture", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
     return rc;
+}
+
+static int rebuild_body(const void* ctx, cudaStream_t s) { return sim_rebuild((const SimEngine*)ctx, 0, s); }
+static int rebuild_eager(const void* ctx, cudaStream_t s) { return sim_rebuild((const SimEngine*)ctx, 1, s); }
+
+extern "C" int sim_rebuild_if_needed(const SimEngine* ep, void* stream) {
+    if (!ep || !ep->box || ep->n <= 0) return SIM_ERR_ARG;
+    return launch_if_flag((cudaStream_t)stream, ep->flags, rebuild_body, rebuild_eager, ep, "sim_rebuild_if_needed");
 }
 
 extern "C" int sim_half_list_count(const void* pos, int32_t dtype_code, int64_t n, const SimBox* box_host,
