@@ -14,8 +14,8 @@
 // so a hot replica can rebuild every few steps without touching the others.
 //
 // Reductions: each warp writes the sums of its 32 slots to chunk_red; one
-// block per replica then adds its chunks in a fixed order in FP64 with Kahan
-// compensation (deterministic, no atomics).
+// block per replica then adds its chunks in a fixed order in FP64
+// (deterministic, no atomics).
 //
 // Pair arithmetic, table interpolation and integration are the single-system
 // engine's (eam_device.cuh, grid.cuh, common.cuh), so a replica advanced in a
@@ -199,20 +199,31 @@ __global__ void k_bb_slot_cells(SimBatch B, int only_flagged) {
     }
 }
 
-__global__ void __launch_bounds__(SIM_THREADS) k_bb_build_ell(SimBatch B, float rc2_list, int only_flagged) {
+#define BATCH_ELL_WARPS 8
+__global__ void __launch_bounds__(BATCH_ELL_WARPS * 32) k_bb_build_ell(SimBatch B, float rc2_list, int only_flagged) {
+    __shared__ uint32_t keys[BATCH_ELL_WARPS][ELL_SORT_MAX];
+    __shared__ int js[BATCH_ELL_WARPS][ELL_SORT_MAX];
     const SimEngine& e = B.e;
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
-    uint32_t key_d2[ELL_SORT_MAX];
-    int key_j[ELL_SORT_MAX];
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int warp = threadIdx.x >> 5;
+    // a warp takes 32 slots (one replica) at a time and skips them together
+    // when the replica is not being rebuilt
+    const int64_t n_chunks = e.n >> 5;
+    for (int64_t c = blockIdx.x * (int64_t)BATCH_ELL_WARPS + warp; c < n_chunks;
+         c += (int64_t)gridDim.x * BATCH_ELL_WARPS) {
         bool real;
-        const int k = slot_replica(B, i, real);
-        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+        const int k = slot_replica(B, c << 5, real);
+        if (only_flagged && B.rep_flags[k] == 0) continue;
         const SimRep& R = B.rep[k];
         const int32_t* rank = e.cell_rank + 2 * R.cell_off;
         const CellGrid g{&R.box, R.ncell[0], R.ncell[1], R.ncell[2], rank, e.cell_start + R.cell_off};
-        const int lin = rank[R.n_cells + (e.cell_of[i] - R.cell_off)];
-        ell_row(posq, i, lin, g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags, key_d2, key_j);
+        for (int s = 0; s < 32; ++s) {
+            const int64_t i = (c << 5) + s;
+            if (i - R.off >= R.n) break;                // padding slots close the replica's range
+            const int lin = rank[R.n_cells + (e.cell_of[i] - R.cell_off)];
+            ell_row_warp(posq, i, lin, g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags, keys[warp],
+                         js[warp]);
+        }
     }
 }
 
@@ -247,7 +258,8 @@ static int batch_rebuild(const SimBatch& B, int only_flagged, cudaStream_t st) {
     k_bb_commit<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
     k_bb_slot_cells<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
     const float rc2_list = (float)(B.e.x_rc * B.e.x_rc * (1.0 + 4e-6));
-    k_bb_build_ell<<<g, SIM_THREADS, 0, st>>>(B, rc2_list, only_flagged);
+    const int64_t ge = ceil_div(B.e.n >> 5, BATCH_ELL_WARPS);
+    k_bb_build_ell<<<(int)(ge > 148 * 64 ? 148 * 64 : ge), BATCH_ELL_WARPS * 32, 0, st>>>(B, rc2_list, only_flagged);
     k_bb_finish<<<1, 256, 0, st>>>(B, only_flagged);
     return launch_status("sim_batch_rebuild");
 }
@@ -404,10 +416,25 @@ __global__ void __launch_bounds__(BATCH_FORCE_THREADS, 1) k_bb_force(SimBatch B,
             const float fpi = __int_as_float(pi.w);
             float fx = 0.f, fy = 0.f, fz = 0.f;
             if (use_mask) {
+                // in-cutoff slots only; the next two list entries are fetched
+                // while the current pair is gathered and evaluated
                 uint64_t m = e.cut_mask[i];
-                for (int kk = pop_slot(m); kk >= 0; kk = pop_slot(m))
-                    pair_single<ORTHO>(b, pi, __ldg(&posfp[__ldg(&nbr[(int64_t)kk * P + i])]), rc2, fpi, tab_d,
-                                       tab_p, w, t, fx, fy, fz, acc);
+                int ka = pop_slot(m), kb = pop_slot(m);
+                int ja = ka >= 0 ? __ldg(&nbr[(int64_t)ka * P + i]) : 0;
+                int jb = kb >= 0 ? __ldg(&nbr[(int64_t)kb * P + i]) : 0;
+                while (kb >= 0) {
+                    const int j0 = ja, j1 = jb;
+                    ka = pop_slot(m);
+                    kb = pop_slot(m);
+                    if (ka >= 0) ja = __ldg(&nbr[(int64_t)ka * P + i]);
+                    if (kb >= 0) jb = __ldg(&nbr[(int64_t)kb * P + i]);
+                    const int4 q0 = __ldg(&posfp[j0]);
+                    const int4 q1 = __ldg(&posfp[j1]);
+                    pair_single<ORTHO>(b, pi, q0, rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
+                    pair_single<ORTHO>(b, pi, q1, rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
+                }
+                if (ka >= 0)
+                    pair_single<ORTHO>(b, pi, __ldg(&posfp[ja]), rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
             } else {
                 const int nn = e.nnbr[i];
                 for (int kk = 0; kk < nn; ++kk)
@@ -499,38 +526,46 @@ __global__ void k_bb_first_half(SimBatch B, SimIntegrator p) {
 
 __global__ void k_bb_advance_step(uint64_t* ctr) { *ctr += 1; }
 
-// One block per replica: FP64 Kahan sums of its warps' partials in a fixed
-// order; with a log, also into row (*step % cap).
-__global__ void __launch_bounds__(256) k_bb_reduce(SimBatch B, const uint64_t* step, double* log, int cap) {
+// One block per replica: FP64 sums of its warps' partials in a fixed order
+// (each thread a strided set of chunks, then butterfly sums within and across
+// warps: deterministic, no atomics); with a log, also into row (*step % cap).
+#define BATCH_REDUCE_THREADS 1024
+__global__ void __launch_bounds__(BATCH_REDUCE_THREADS) k_bb_reduce(SimBatch B, const uint64_t* step, double* log,
+                                                                    int cap) {
     const int k = blockIdx.x;
     const SimRep& R = B.rep[k];
     const int64_t c0 = R.off >> 5, c1 = (R.off + R.n_slots) >> 5;
-    __shared__ double part[256][SIM_RED_SLOTS + 1];
-    double s[SIM_RED_SLOTS], comp[SIM_RED_SLOTS];
+    __shared__ double part[SIM_RED_SLOTS][BATCH_REDUCE_THREADS / 32];
+    double s[SIM_RED_SLOTS];
 #pragma unroll
-    for (int q = 0; q < SIM_RED_SLOTS; ++q) { s[q] = 0.0; comp[q] = 0.0; }
+    for (int q = 0; q < SIM_RED_SLOTS; ++q) s[q] = 0.0;
     for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-        const double* src = B.chunk_red + c * SIM_RED_SLOTS;
+        const double2* src = reinterpret_cast<const double2*>(B.chunk_red + c * SIM_RED_SLOTS);
 #pragma unroll
-        for (int q = 0; q < SIM_RED_SLOTS; ++q) {
-            const double y = src[q] - comp[q];
-            const double tt = s[q] + y;
-            comp[q] = (tt - s[q]) - y;
-            s[q] = tt;
+        for (int q = 0; q < SIM_RED_SLOTS / 2; ++q) {
+            const double2 v = src[q];
+            s[2 * q] += v.x;
+            s[2 * q + 1] += v.y;
         }
     }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int q = 0; q < SIM_RED_SLOTS; ++q) part[threadIdx.x][q] = s[q];
+    for (int q = 0; q < SIM_RED_SLOTS; ++q) {
+        const double v = warp_sum(s[q]);
+        if (lane == 0) part[q][warp] = v;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int q = 0; q < SIM_RED_SLOTS; ++q) {
+            const double v = warp_sum(lane < (int)(blockDim.x >> 5) ? part[q][lane] : 0.0);
+            if (lane == 0) part[q][0] = v;
+        }
+    }
     __syncthreads();
     if (threadIdx.x < SIM_RED_SLOTS) {
         const int q = threadIdx.x;
-        double acc = 0.0, cc = 0.0;
-        for (int t = 0; t < (int)blockDim.x; ++t) {
-            const double y = part[t][q] - cc;
-            const double tt = acc + y;
-            cc = (tt - acc) - y;
-            acc = tt;
-        }
+        const double acc = part[q][0];
         B.rep_red[k * SIM_RED_SLOTS + q] = acc;
         if (log) log[((*step % (uint64_t)cap) * B.n_rep + k) * SIM_RED_SLOTS + q] = acc;
     }
@@ -672,7 +707,7 @@ extern "C" int sim_batch_first_half(const SimBatch* b, const SimIntegrator* p, v
 
 extern "C" int sim_batch_reduce(const SimBatch* b, const uint64_t* step, double* log, int32_t log_cap, void* stream) {
     if (!batch_ok(b) || (log && (log_cap <= 0 || !step))) return SIM_ERR_ARG;
-    k_bb_reduce<<<b->n_rep, 256, 0, (cudaStream_t)stream>>>(*b, step, log, log_cap);
+    k_bb_reduce<<<b->n_rep, BATCH_REDUCE_THREADS, 0, (cudaStream_t)stream>>>(*b, step, log, log_cap);
     return launch_status("sim_batch_reduce");
 }
 

@@ -30,69 +30,126 @@ struct CellGrid {
     const int32_t* start;
 };
 
-// Row i of the full list: every slot j != i of the 27 stencil cells around
-// cell `lin` with d^2 < rc2_list, tested in FP32 on fixed-point displacements
-// (the radius carries a 2e-6 relative margin so that an exact FP64/FP32 filter
-// applied later -- half-list export, force cutoffs -- always sees a superset).
-// Rows up to ELL_SORT_MAX entries are sorted nearest first, ties by slot: in a
-// crystal every row then lists the same shells in the same order, so a warp's
-// lanes agree on which neighbours fall inside the force cutoff.  A row longer
-// than cap sets SIM_STATUS_OVERFLOW and the longest length in flags[2].
-__device__ __forceinline__ void ell_row(const int4* __restrict__ posq, int64_t i, int lin, const CellGrid& g,
-                                        float rc2_list, int32_t* nbr, int64_t P, int cap, int32_t* nnbr,
-                                        int32_t* flags, uint32_t* key_d2, int* key_j) {
+// Row i of the full list, built by the 32 lanes of one warp: every slot j != i
+// of the 27 stencil cells around cell `lin` with d^2 < rc2_list, tested in FP32
+// on fixed-point displacements (the radius carries a 2e-6 relative margin so
+// that an exact FP64/FP32 filter applied later -- half-list export, force
+// cutoffs -- always sees a superset).  The stencil cells' slot ranges are
+// flattened into one candidate sequence (cells in kz, ky, kx order, slots
+// ascending); each lane tests one candidate per round and accepted entries are
+// compacted in order through a ballot into this warp's shared buffers (keys,
+// js; ELL_SORT_MAX entries each).  Rows of up to ELL_SORT_MAX kept entries are
+// written sorted nearest first, ties by slot -- each entry's rank is counted
+// against the others -- so in a crystal every row lists the same shells in the
+// same order and a warp's lanes agree on which neighbours fall inside the force
+// cutoff; longer rows keep the visiting order.  A row longer than cap sets
+// SIM_STATUS_OVERFLOW and the longest length in flags[2].  Every lane of the
+// warp must call this.
+__device__ __forceinline__ void ell_row_warp(const int4* __restrict__ posq, int64_t i, int lin, const CellGrid& g,
+                                             float rc2_list, int32_t* nbr, int64_t P, int cap, int32_t* nnbr,
+                                             int32_t* flags, uint32_t* keys, int* js) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     const SimBox& b = *g.box;
     const int4 qi = posq[i];
     const int cx = lin % g.nx, cy = (lin / g.nx) % g.ny, cz = lin / (g.nx * g.ny);
-    int cnt = 0;
     const int sx = stencil_count(g.nx), sy = stencil_count(g.ny), sz = stencil_count(g.nz);
-    for (int kz = 0; kz < sz; ++kz) {
-        const int z = stencil_cell(cz, kz, g.nz);
-        for (int ky = 0; ky < sy; ++ky) {
-            const int y = stencil_cell(cy, ky, g.ny);
-            for (int kx = 0; kx < sx; ++kx) {
-                const int xx = stencil_cell(cx, kx, g.nx);
-                const int r = g.rank[xx + g.nx * (y + g.ny * z)];
-                const int j0 = g.start[r], j1 = g.start[r + 1];
-                for (int j = j0; j < j1; ++j) {
-                    if (j == i) continue;
-                    const int4 qj = posq[j];
-                    float r0, r1, r2;
-                    frac_to_cart_f(b, fixed_delta(qi.x, qj.x), fixed_delta(qi.y, qj.y), fixed_delta(qi.z, qj.z),
-                                   r0, r1, r2);
-                    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(r0, r0), __fmul_rn(r1, r1)), __fmul_rn(r2, r2));
-                    if (d2 < rc2_list) {
-                        if (cnt < cap) {
-                            // non-negative floats order like their bit patterns
-                            if (cnt < ELL_SORT_MAX) { key_d2[cnt] = __float_as_uint(d2); key_j[cnt] = j; }
-                            nbr[(int64_t)cnt * P + i] = j;
-                        }
-                        ++cnt;
-                    }
-                }
-            }
-        }
+    const int n_st = sx * sy * sz;
+    int cs = 0, cn = 0;
+    if (lane < n_st) {
+        const int kx = lane % sx, ky = (lane / sx) % sy, kz = lane / (sx * sy);
+        const int r = g.rank[stencil_cell(cx, kx, g.nx) + g.nx * (stencil_cell(cy, ky, g.ny) +
+                                                                 g.ny * stencil_cell(cz, kz, g.nz))];
+        cs = g.start[r];
+        cn = g.start[r + 1] - cs;
     }
+    int incl = cn;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int excl = incl - cn;
+    const int total = __shfl_sync(FULL, incl, 31);
+    const unsigned below = (1u << lane) - 1u;
+    int cnt = 0;
+    for (int base = 0; base < total; base += 32) {
+        const int t = base + lane;
+        const int tt = t < total ? t : total - 1;
+        int c = 0;                                   // last stencil cell whose first candidate is <= tt
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int cc = c + step;
+            const int ex = __shfl_sync(FULL, excl, cc & 31);
+            if (cc < n_st && ex <= tt) c = cc;
+        }
+        const int j = __shfl_sync(FULL, cs, c) + (tt - __shfl_sync(FULL, excl, c));
+        bool acc = false;
+        float d2 = 0.0f;
+        if (t < total && j != i) {
+            const int4 qj = posq[j];
+            float r0, r1, r2;
+            frac_to_cart_f(b, fixed_delta(qi.x, qj.x), fixed_delta(qi.y, qj.y), fixed_delta(qi.z, qj.z), r0, r1, r2);
+            d2 = __fadd_rn(__fadd_rn(__fmul_rn(r0, r0), __fmul_rn(r1, r1)), __fmul_rn(r2, r2));
+            acc = d2 < rc2_list;
+        }
+        const unsigned m = __ballot_sync(FULL, acc);
+        const int pos = cnt + __popc(m & below);
+        if (acc && pos < ELL_SORT_MAX) {
+            keys[pos] = __float_as_uint(d2);        // non-negative floats order like their bits
+            js[pos] = j;
+        }
+        cnt += __popc(m);
+    }
+    __syncwarp();
     const int kept = cnt < cap ? cnt : cap;
     if (kept <= ELL_SORT_MAX) {
-        for (int a = 1; a < kept; ++a) {
-            const uint32_t kd = key_d2[a];
-            const int kj = key_j[a];
-            int p = a - 1;
-            while (p >= 0 && (key_d2[p] > kd || (key_d2[p] == kd && key_j[p] > kj))) {
-                key_d2[p + 1] = key_d2[p];
-                key_j[p + 1] = key_j[p];
-                --p;
+        for (int a = lane; a < kept; a += 32) {
+            const uint32_t ka = keys[a];
+            const int ja = js[a];
+            int rank = 0;
+            for (int f = 0; f < kept; ++f) {
+                const uint32_t kf = keys[f];
+                rank += (kf < ka || (kf == ka && js[f] < ja)) ? 1 : 0;
             }
-            key_d2[p + 1] = kd;
-            key_j[p + 1] = kj;
+            nbr[(int64_t)rank * P + i] = ja;
         }
-        for (int a = 0; a < kept; ++a) nbr[(int64_t)a * P + i] = key_j[a];
+    } else {
+        // longer than the sort buffer: the first `kept` entries in visiting order
+        int w = 0;
+        for (int base = 0; base < total && w < kept; base += 32) {
+            const int t = base + lane;
+            const int tt = t < total ? t : total - 1;
+            int c = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int cc = c + step;
+                const int ex = __shfl_sync(FULL, excl, cc & 31);
+                if (cc < n_st && ex <= tt) c = cc;
+            }
+            const int j = __shfl_sync(FULL, cs, c) + (tt - __shfl_sync(FULL, excl, c));
+            bool acc = false;
+            if (t < total && j != i) {
+                const int4 qj = posq[j];
+                float r0, r1, r2;
+                frac_to_cart_f(b, fixed_delta(qi.x, qj.x), fixed_delta(qi.y, qj.y), fixed_delta(qi.z, qj.z),
+                               r0, r1, r2);
+                const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(r0, r0), __fmul_rn(r1, r1)), __fmul_rn(r2, r2));
+                acc = d2 < rc2_list;
+            }
+            const unsigned m = __ballot_sync(FULL, acc);
+            const int pos = w + __popc(m & below);
+            if (acc && pos < kept) nbr[(int64_t)pos * P + i] = j;
+            w += __popc(m);
+        }
     }
-    nnbr[i] = kept;
-    if (cnt > cap) {
-        atomicOr(&flags[1], SIM_STATUS_OVERFLOW);
-        atomicMax(&flags[2], cnt);
+    __syncwarp();
+    if (lane == 0) {
+        nnbr[i] = kept;
+        if (cnt > cap) {
+            atomicOr(&flags[1], SIM_STATUS_OVERFLOW);
+            atomicMax(&flags[2], cnt);
+        }
     }
 }
 

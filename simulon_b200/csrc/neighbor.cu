@@ -179,17 +179,19 @@ __global__ void k_slot_cells(SimEngine e, const int32_t* gate) {
     }
 }
 
-// Full list in ELL layout (row builder in grid.cuh).
-__global__ void __launch_bounds__(SIM_THREADS) k_build_ell(SimEngine e, const int32_t* cell_lin,
-                                                          float rc2_list, const int32_t* gate) {
+// Full list in ELL layout, one warp per atom (row builder in grid.cuh).
+#define ELL_WARPS 8
+__global__ void __launch_bounds__(ELL_WARPS * 32) k_build_ell(SimEngine e, const int32_t* cell_lin,
+                                                             float rc2_list, const int32_t* gate) {
     if (gate && __ldg(gate) == 0) return;
+    __shared__ uint32_t keys[ELL_WARPS][ELL_SORT_MAX];
+    __shared__ int js[ELL_WARPS][ELL_SORT_MAX];
     const CellGrid g{e.box, e.ncell[0], e.ncell[1], e.ncell[2], e.cell_rank, e.cell_start};
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
-    uint32_t key_d2[ELL_SORT_MAX];
-    int key_j[ELL_SORT_MAX];
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x)
-        ell_row(posq, i, cell_lin[e.cell_of[i]], g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags,
-                key_d2, key_j);
+    const int warp = threadIdx.x >> 5;
+    for (int64_t i = blockIdx.x * (int64_t)ELL_WARPS + warp; i < e.n; i += (int64_t)gridDim.x * ELL_WARPS)
+        ell_row_warp(posq, i, cell_lin[e.cell_of[i]], g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags,
+                     keys[warp], js[warp]);
 }
 
 // Count the rebuild (flags[3]) when it ran and clear the request.
@@ -405,6 +407,11 @@ __global__ void __launch_bounds__(SIM_THREADS) k_engine_half(SimEngine e, double
     for (int64_t a = base; a < base + cnt; ++a) edge_i[a] = oi;
 }
 
+static int ell_grid(int64_t n) {
+    const int64_t g = ceil_div(n, ELL_WARPS);
+    return (int)(g < 1 ? 1 : (g > 148 * 64 ? 148 * 64 : g));
+}
+
 static int grid_for(int64_t n) {
     int64_t g = ceil_div(n, SIM_THREADS);
     return (int)(g < 1 ? 1 : (g > 148 * 8 ? 148 * 8 : g));
@@ -433,7 +440,7 @@ extern "C" int sim_rebuild(const SimEngine* ep, int32_t only_if_flagged, void* s
     k_slot_cells<<<g, SIM_THREADS, 0, st>>>(e, gate);
     const float rc2_list = (float)(e.x_rc * e.x_rc * (1.0 + 4e-6));
     // cell_lin (rank -> linear index) is stored right after cell_rank
-    k_build_ell<<<g, SIM_THREADS, 0, st>>>(e, e.cell_rank + e.n_cells, rc2_list, gate);
+    k_build_ell<<<ell_grid(e.n), ELL_WARPS * 32, 0, st>>>(e, e.cell_rank + e.n_cells, rc2_list, gate);
     launch_build_halo(e, gate, st);
     k_finish_rebuild<<<1, 1, 0, st>>>(e.flags, only_if_flagged ? 1 : 0);
     return launch_status("sim_rebuild");
