@@ -393,6 +393,8 @@ typedef struct SimBatch {
     int32_t* cell_rep;      /* [n_cell_entries] replica of each cell entry             */
     int32_t* rep_flags;     /* [n_rep] 1: rebuild this replica                         */
     int32_t* rep_rebuilds;  /* [n_rep] rebuilds performed                              */
+    int32_t* work;          /* [3 * (n_rep + 1)] rebuild work list, written by the rebuild:
+                               replicas to rebuild and their slot-chunk and cell prefixes */
     int8_t*  grip;          /* [atoms, original order] 0 free, 1 lower grip, 2 upper   */
     double*  gref;          /* [3][e.n_pad] grip reference positions, by original index */
     double*  rep_rff;       /* [n_rep] Langevin noise amplitude sqrt(kB T (1-damp^2)/m) */

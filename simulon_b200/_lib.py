@@ -90,7 +90,7 @@ class SimRep(ctypes.Structure):
 
 class SimBatch(ctypes.Structure):
     _fields_ = [("e", SimEngine), ("rep", c_p), ("n_rep", ctypes.c_int32), ("n_cell_entries", ctypes.c_int32),
-                ("slot_rep", c_p), ("cell_rep", c_p), ("rep_flags", c_p), ("rep_rebuilds", c_p), ("grip", c_p),
+                ("slot_rep", c_p), ("cell_rep", c_p), ("rep_flags", c_p), ("rep_rebuilds", c_p), ("work", c_p), ("grip", c_p),
                 ("gref", c_p), ("rep_rff", c_p), ("chunk_red", c_p), ("rep_red", c_p)]
 
 

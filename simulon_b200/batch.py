@@ -175,6 +175,7 @@ class BatchedEngine:
         self.slot_rep = torch.from_numpy(slot_rep).to(dev)
         self.rep_flags = torch.zeros(R, **i32)
         self.rep_rebuilds = torch.zeros(R, **i32)
+        self.work = torch.zeros(3 * (R + 1), **i32)
         grip = np.zeros(self.n_atoms, np.int8)
         gref = np.zeros((3, P), np.float64)
         for k, rp in enumerate(self.replicas):
@@ -235,8 +236,8 @@ class BatchedEngine:
         e.box_orthogonal = int(self.box_orthogonal)
         b.rep = p(self.rep_dev)
         b.n_rep, b.n_cell_entries = self.n_rep, plan.n_cell_entries
-        for name in ("slot_rep", "cell_rep", "rep_flags", "rep_rebuilds", "grip", "gref", "rep_rff", "chunk_red",
-                     "rep_red"):
+        for name in ("slot_rep", "cell_rep", "rep_flags", "rep_rebuilds", "work", "grip", "gref", "rep_rff",
+                     "chunk_red", "rep_red"):
             setattr(b, name, p(getattr(self, name)))
         self.st = b
         self.ref = ctypes.byref(b)

@@ -38,14 +38,81 @@ __device__ __forceinline__ int slot_replica(const SimBatch& B, int64_t i, bool& 
 }
 
 // ---------------------------------------------------------------------------
-// rebuild (gated per replica by rep_flags)
+// rebuild of the flagged replicas.  k_bb_plan lists them with prefix sums of
+// their 32-slot chunks and cells (B.work), and every later kernel walks only
+// those ranges, so a rebuild costs time in proportion to the atoms rebuilt.
+
+struct WorkList {
+    const int32_t* ids;     // flagged replicas
+    const int32_t* chunks;  // [nf + 1] prefix of their slot chunks
+    const int32_t* cells;   // [nf + 1] prefix of their cells
+    int nf;
+};
+__device__ __forceinline__ WorkList work_list(const SimBatch& B) {
+    const int32_t* w = B.work;
+    return WorkList{w + 1, w + (B.n_rep + 1), w + 2 * (B.n_rep + 1), w[0]};
+}
+// index f of the flagged replica whose prefix range [pre[f], pre[f+1]) holds x
+__device__ __forceinline__ int work_find(const int32_t* pre, int nf, int64_t x) {
+    int lo = 0, hi = nf;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pre[mid] <= x) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+// t-th slot of the flagged replicas (32 per chunk, padding included): false past the end
+__device__ __forceinline__ bool work_slot(const SimBatch& B, const WorkList& W, int64_t t, int64_t& slot, int& k) {
+    const int64_t chunk = t >> 5;
+    if (W.nf == 0 || chunk >= W.chunks[W.nf]) return false;
+    const int f = work_find(W.chunks, W.nf, chunk);
+    k = W.ids[f];
+    slot = B.rep[k].off + ((chunk - W.chunks[f]) << 5) + (t & 31);
+    return true;
+}
+
+// one warp: the replicas to rebuild (all when only_flagged == 0), in order
+__global__ void k_bb_plan(SimBatch B, int only_flagged) {
+    const int lane = threadIdx.x & 31;
+    int32_t* ids = B.work + 1;
+    int32_t* chunks = B.work + (B.n_rep + 1);
+    int32_t* cells = B.work + 2 * (B.n_rep + 1);
+    int nf = 0, cc = 0, ce = 0;
+    if (lane == 0) { chunks[0] = 0; cells[0] = 0; }
+    for (int base = 0; base < B.n_rep; base += 32) {
+        const int k = base + lane;
+        const bool on = k < B.n_rep && (!only_flagged || B.rep_flags[k] != 0);
+        const int nch = on ? (B.rep[k].n_slots >> 5) : 0;
+        const int nce = on ? B.rep[k].n_cells : 0;
+        const unsigned m = __ballot_sync(0xffffffffu, on);
+        int ich = nch, ice = nce;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int a = __shfl_up_sync(0xffffffffu, ich, o);
+            const int c = __shfl_up_sync(0xffffffffu, ice, o);
+            if (lane >= o) { ich += a; ice += c; }
+        }
+        if (on) {
+            const int pos = nf + __popc(m & ((1u << lane) - 1u));
+            ids[pos] = k;
+            chunks[pos + 1] = cc + ich;
+            cells[pos + 1] = ce + ice;
+        }
+        nf += __popc(m);
+        cc += __shfl_sync(0xffffffffu, ich, 31);
+        ce += __shfl_sync(0xffffffffu, ice, 31);
+    }
+    if (lane == 0) B.work[0] = nf;
+}
 
 __global__ void k_bb_bin(SimBatch B, int only_flagged) {
     const SimEngine& e = B.e;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
-        bool real;
-        const int k = slot_replica(B, i, real);
-        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+    const WorkList W = work_list(B);
+    int64_t i;
+    int k;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; work_slot(B, W, t, i, k);
+         t += (int64_t)gridDim.x * blockDim.x) {
+        if (i - B.rep[k].off >= B.rep[k].n) continue;   // padding
         const SimRep& R = B.rep[k];
         double s[3];
         cart_to_frac(R.box, e.x[i], e.x[e.n_pad + i], e.x[2 * e.n_pad + i], s);
@@ -62,9 +129,9 @@ __global__ void k_bb_bin(SimBatch B, int only_flagged) {
 // One block per replica: exclusive scan of its cell counts, based at its first
 // slot; counts are zeroed for the scatter.
 __global__ void __launch_bounds__(1024) k_bb_scan(SimBatch B, int only_flagged) {
-    const int k = blockIdx.x;
-    if (only_flagged && B.rep_flags[k] == 0) return;
-    const SimRep& R = B.rep[k];
+    const WorkList W = work_list(B);
+    if ((int)blockIdx.x >= W.nf) return;
+    const SimRep& R = B.rep[W.ids[blockIdx.x]];
     int32_t* cnt = B.e.cell_count + R.cell_off;
     int32_t* start = B.e.cell_start + R.cell_off;
     const int n = R.n_cells;
@@ -109,10 +176,12 @@ __global__ void __launch_bounds__(1024) k_bb_scan(SimBatch B, int only_flagged) 
 
 __global__ void k_bb_scatter(SimBatch B, int only_flagged) {
     const SimEngine& e = B.e;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
-        bool real;
-        const int k = slot_replica(B, i, real);
-        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+    const WorkList W = work_list(B);
+    int64_t i;
+    int k;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; work_slot(B, W, t, i, k);
+         t += (int64_t)gridDim.x * blockDim.x) {
+        if (i - B.rep[k].off >= B.rep[k].n) continue;   // padding
         const int c = e.cell_of[i];
         e.perm[e.cell_start[c] + atomicAdd(&e.cell_count[c], 1)] = (int32_t)i;
     }
@@ -122,10 +191,11 @@ __global__ void k_bb_scatter(SimBatch B, int only_flagged) {
 // are cleared for the next rebuild.
 __global__ void k_bb_sort_cells(SimBatch B, int only_flagged) {
     const SimEngine& e = B.e;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < B.n_cell_entries; c += gridDim.x * blockDim.x) {
-        const int k = B.cell_rep[c];
-        if (only_flagged && B.rep_flags[k] == 0) continue;
-        if (c - B.rep[k].cell_off >= B.rep[k].n_cells) continue;   // the closing entry
+    const WorkList W = work_list(B);
+    const int total = W.nf ? W.cells[W.nf] : 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int f = work_find(W.cells, W.nf, t);
+        const int c = B.rep[W.ids[f]].cell_off + (t - W.cells[f]);
         e.cell_count[c] = 0;
         const int b0 = e.cell_start[c], b1 = e.cell_start[c + 1];
         for (int a = b0 + 1; a < b1; ++a) {
@@ -144,10 +214,12 @@ __global__ void k_bb_sort_cells(SimBatch B, int only_flagged) {
 __global__ void k_bb_permute(SimBatch B, int only_flagged) {
     const SimEngine& e = B.e;
     const int64_t P = e.n_pad;
-    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < e.n; m += (int64_t)gridDim.x * blockDim.x) {
-        bool real;
-        const int k = slot_replica(B, m, real);
-        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+    const WorkList W = work_list(B);
+    int64_t m;
+    int k;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; work_slot(B, W, t, m, k);
+         t += (int64_t)gridDim.x * blockDim.x) {
+        if (m - B.rep[k].off >= B.rep[k].n) continue;   // padding
         const int64_t o = e.perm[m];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -163,10 +235,12 @@ __global__ void k_bb_permute(SimBatch B, int only_flagged) {
 __global__ void k_bb_commit(SimBatch B, int only_flagged) {
     const SimEngine& e = B.e;
     const int64_t P = e.n_pad;
-    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < e.n; m += (int64_t)gridDim.x * blockDim.x) {
-        bool real;
-        const int k = slot_replica(B, m, real);
-        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+    const WorkList W = work_list(B);
+    int64_t m;
+    int k;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; work_slot(B, W, t, m, k);
+         t += (int64_t)gridDim.x * blockDim.x) {
+        if (m - B.rep[k].off >= B.rep[k].n) continue;   // padding
         const double x0 = e.x_alt[m], x1 = e.x_alt[P + m], x2 = e.x_alt[2 * P + m];
         e.x[m] = x0; e.x[P + m] = x1; e.x[2 * P + m] = x2;
 #pragma unroll
@@ -185,10 +259,12 @@ __global__ void k_bb_commit(SimBatch B, int only_flagged) {
 // slot -> cell entry after the sort (binary search over the replica's starts)
 __global__ void k_bb_slot_cells(SimBatch B, int only_flagged) {
     const SimEngine& e = B.e;
-    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < e.n; m += (int64_t)gridDim.x * blockDim.x) {
-        bool real;
-        const int k = slot_replica(B, m, real);
-        if (!real || (only_flagged && B.rep_flags[k] == 0)) continue;
+    const WorkList W = work_list(B);
+    int64_t m;
+    int k;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; work_slot(B, W, t, m, k);
+         t += (int64_t)gridDim.x * blockDim.x) {
+        if (m - B.rep[k].off >= B.rep[k].n) continue;   // padding
         const SimRep& R = B.rep[k];
         int lo = R.cell_off, hi = R.cell_off + R.n_cells;
         while (hi - lo > 1) {
@@ -199,31 +275,23 @@ __global__ void k_bb_slot_cells(SimBatch B, int only_flagged) {
     }
 }
 
-#define BATCH_ELL_WARPS 8
+#define BATCH_ELL_WARPS 4
 __global__ void __launch_bounds__(BATCH_ELL_WARPS * 32) k_bb_build_ell(SimBatch B, float rc2_list, int only_flagged) {
-    __shared__ uint32_t keys[BATCH_ELL_WARPS][ELL_SORT_MAX];
-    __shared__ int js[BATCH_ELL_WARPS][ELL_SORT_MAX];
+    __shared__ uint64_t keys[BATCH_ELL_WARPS][ELL_SORT_MAX];
+    __shared__ int4 cq[BATCH_ELL_WARPS][ELL_CELL_CAND];
+    __shared__ int cj[BATCH_ELL_WARPS][ELL_CELL_CAND];
     const SimEngine& e = B.e;
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
     const int warp = threadIdx.x >> 5;
-    // a warp takes 32 slots (one replica) at a time and skips them together
-    // when the replica is not being rebuilt
-    const int64_t n_chunks = e.n >> 5;
-    for (int64_t c = blockIdx.x * (int64_t)BATCH_ELL_WARPS + warp; c < n_chunks;
-         c += (int64_t)gridDim.x * BATCH_ELL_WARPS) {
-        bool real;
-        const int k = slot_replica(B, c << 5, real);
-        if (only_flagged && B.rep_flags[k] == 0) continue;
-        const SimRep& R = B.rep[k];
+    const WorkList W = work_list(B);
+    const int total = W.nf ? W.cells[W.nf] : 0;
+    for (int t = blockIdx.x * BATCH_ELL_WARPS + warp; t < total; t += gridDim.x * BATCH_ELL_WARPS) {
+        const int f = work_find(W.cells, W.nf, t);
+        const SimRep& R = B.rep[W.ids[f]];
         const int32_t* rank = e.cell_rank + 2 * R.cell_off;
         const CellGrid g{&R.box, R.ncell[0], R.ncell[1], R.ncell[2], rank, e.cell_start + R.cell_off};
-        for (int s = 0; s < 32; ++s) {
-            const int64_t i = (c << 5) + s;
-            if (i - R.off >= R.n) break;                // padding slots close the replica's range
-            const int lin = rank[R.n_cells + (e.cell_of[i] - R.cell_off)];
-            ell_row_warp(posq, i, lin, g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags, keys[warp],
-                         js[warp]);
-        }
+        ell_cell_warp(posq, t - W.cells[f], rank + R.n_cells, g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr,
+                      e.flags, keys[warp], cq[warp], cj[warp]);
     }
 }
 
@@ -250,6 +318,7 @@ static int grid_slots(int64_t n) {
 
 static int batch_rebuild(const SimBatch& B, int only_flagged, cudaStream_t st) {
     const int g = grid_slots(B.e.n);
+    k_bb_plan<<<1, 32, 0, st>>>(B, only_flagged);
     k_bb_bin<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
     k_bb_scan<<<B.n_rep, 1024, 0, st>>>(B, only_flagged);
     k_bb_scatter<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
@@ -258,7 +327,7 @@ static int batch_rebuild(const SimBatch& B, int only_flagged, cudaStream_t st) {
     k_bb_commit<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
     k_bb_slot_cells<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
     const float rc2_list = (float)(B.e.x_rc * B.e.x_rc * (1.0 + 4e-6));
-    const int64_t ge = ceil_div(B.e.n >> 5, BATCH_ELL_WARPS);
+    const int64_t ge = ceil_div(B.n_cell_entries, BATCH_ELL_WARPS);
     k_bb_build_ell<<<(int)(ge > 148 * 64 ? 148 * 64 : ge), BATCH_ELL_WARPS * 32, 0, st>>>(B, rc2_list, only_flagged);
     k_bb_finish<<<1, 256, 0, st>>>(B, only_flagged);
     return launch_status("sim_batch_rebuild");

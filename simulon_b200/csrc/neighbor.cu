@@ -78,6 +78,85 @@ __global__ void k_scan_exclusive(const T* __restrict__ in, int64_t n, T* __restr
     if (tid == 0) out[n] = carry_s;
 }
 
+// Multi-block exclusive scan of int32 counts: tile sums, a scan of the tile
+// sums (k_scan_exclusive, one block), then each tile scanned with its offset.
+#define SCAN_TILE 4096
+__device__ __forceinline__ int warp_sum_i(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_tiles(const int32_t* __restrict__ in, int n, int32_t* tile_sum,
+                                                     const int32_t* gate) {
+    if (gate && __ldg(gate) == 0) return;
+    __shared__ int ws[32];
+    const int base = blockIdx.x * SCAN_TILE;
+    int v = 0;
+    for (int k = threadIdx.x; k < SCAN_TILE; k += blockDim.x) {
+        const int idx = base + k;
+        if (idx < n) v += in[idx];
+    }
+    v = warp_sum_i(v);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = warp_sum_i(threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0);
+        if (threadIdx.x == 0) tile_sum[blockIdx.x] = v;
+    }
+}
+
+// blockDim.x * 4 == SCAN_TILE: thread t owns elements 4t .. 4t+3 of its tile
+__global__ void __launch_bounds__(1024) k_scan_apply(const int32_t* __restrict__ in, int n, int32_t* out,
+                                                     int32_t* zero_after, const int32_t* tile_off,
+                                                     const int32_t* gate) {
+    if (gate && __ldg(gate) == 0) return;
+    __shared__ int ws[32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int base = blockIdx.x * SCAN_TILE + 4 * tid;
+    int v[4], local = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        v[q] = base + q < n ? in[base + q] : 0;
+        local += v[q];
+    }
+    int incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) ws[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0;
+        int wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        ws[lane] = wi - w;
+    }
+    __syncthreads();
+    int run = tile_off[blockIdx.x] + ws[warp] + (incl - local);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (base + q < n) {
+            out[base + q] = run;
+            if (zero_after) zero_after[base + q] = 0;
+        }
+        run += v[q];
+    }
+    if (blockIdx.x == gridDim.x - 1 && tid == 0) out[n] = tile_off[gridDim.x];
+}
+
+__global__ void k_zero_gated(int32_t* p, int64_t n, const int32_t* gate) {
+    if (gate && __ldg(gate) == 0) return;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        p[k] = 0;
+}
+
 // ---------------------------------------------------------------------------
 // engine rebuild kernels (gate = flags, kernel returns unless flags[0] != 0)
 
@@ -179,19 +258,20 @@ __global__ void k_slot_cells(SimEngine e, const int32_t* gate) {
     }
 }
 
-// Full list in ELL layout, one warp per atom (row builder in grid.cuh).
-#define ELL_WARPS 8
+// Full list in ELL layout, one warp per cell (row builders in grid.cuh).
+#define ELL_WARPS 4
 __global__ void __launch_bounds__(ELL_WARPS * 32) k_build_ell(SimEngine e, const int32_t* cell_lin,
                                                              float rc2_list, const int32_t* gate) {
     if (gate && __ldg(gate) == 0) return;
-    __shared__ uint32_t keys[ELL_WARPS][ELL_SORT_MAX];
-    __shared__ int js[ELL_WARPS][ELL_SORT_MAX];
+    __shared__ uint64_t keys[ELL_WARPS][ELL_SORT_MAX];
+    __shared__ int4 cq[ELL_WARPS][ELL_CELL_CAND];
+    __shared__ int cj[ELL_WARPS][ELL_CELL_CAND];
     const CellGrid g{e.box, e.ncell[0], e.ncell[1], e.ncell[2], e.cell_rank, e.cell_start};
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
     const int warp = threadIdx.x >> 5;
-    for (int64_t i = blockIdx.x * (int64_t)ELL_WARPS + warp; i < e.n; i += (int64_t)gridDim.x * ELL_WARPS)
-        ell_row_warp(posq, i, cell_lin[e.cell_of[i]], g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags,
-                     keys[warp], js[warp]);
+    for (int r = blockIdx.x * ELL_WARPS + warp; r < e.n_cells; r += gridDim.x * ELL_WARPS)
+        ell_cell_warp(posq, r, cell_lin, g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags, keys[warp], cq[warp],
+                      cj[warp]);
 }
 
 // Count the rebuild (flags[3]) when it ran and clear the request.
@@ -430,17 +510,25 @@ extern "C" int sim_rebuild(const SimEngine* ep, int32_t only_if_flagged, void* s
     // cell_count must be zero here: the scan of the previous rebuild leaves it zeroed,
     // and sim_engine_load zeroes it before the first rebuild.
     k_bin<<<g, SIM_THREADS, 0, st>>>(e, gate);
-    k_scan_exclusive<int32_t><<<1, 1024, 0, st>>>(e.cell_count, e.n_cells, e.cell_start, e.cell_count, gate);
+    // cell_start = exclusive scan of the counts (tile sums staged in perm, which
+    // the scatter fills next); the counts are zeroed for the scatter
+    const int n_tiles = (int)ceil_div(e.n_cells, SCAN_TILE);
+    int32_t* tile_sum = e.perm;
+    int32_t* tile_off = e.perm + n_tiles + 1;
+    k_scan_tiles<<<n_tiles, 1024, 0, st>>>(e.cell_count, e.n_cells, tile_sum, gate);
+    k_scan_exclusive<int32_t><<<1, 1024, 0, st>>>(tile_sum, n_tiles, tile_off, nullptr, gate);
+    k_scan_apply<<<n_tiles, SCAN_TILE / 4, 0, st>>>(e.cell_count, e.n_cells, e.cell_start, e.cell_count, tile_off,
+                                                    gate);
     k_scatter<<<g, SIM_THREADS, 0, st>>>(e, gate);
     k_sort_cells<<<grid_for(e.n_cells), SIM_THREADS, 0, st>>>(e, gate);
     k_permute<<<g, SIM_THREADS, 0, st>>>(e, gate);
     k_commit<<<g, SIM_THREADS, 0, st>>>(e, gate);
     // the scatter left cell_count == counts; zero them for the next rebuild
-    k_scan_exclusive<int32_t><<<1, 1024, 0, st>>>(e.cell_count, e.n_cells, e.cell_start, e.cell_count, gate);
+    k_zero_gated<<<grid_for(e.n_cells), SIM_THREADS, 0, st>>>(e.cell_count, e.n_cells, gate);
     k_slot_cells<<<g, SIM_THREADS, 0, st>>>(e, gate);
     const float rc2_list = (float)(e.x_rc * e.x_rc * (1.0 + 4e-6));
     // cell_lin (rank -> linear index) is stored right after cell_rank
-    k_build_ell<<<ell_grid(e.n), ELL_WARPS * 32, 0, st>>>(e, e.cell_rank + e.n_cells, rc2_list, gate);
+    k_build_ell<<<ell_grid(e.n_cells), ELL_WARPS * 32, 0, st>>>(e, e.cell_rank + e.n_cells, rc2_list, gate);
     launch_build_halo(e, gate, st);
     k_finish_rebuild<<<1, 1, 0, st>>>(e.flags, only_if_flagged ? 1 : 0);
     return launch_status("sim_rebuild");
