@@ -389,11 +389,12 @@ def batched_form(args, sb, pot, dev, world, rank, barrier):
                                  len(reps))
     total = int(sum(sizes))
     # a graph of k steps: first half + counter advance + IF condition, then per
-    # step pass 1, pass 2, per-replica sums, and (all but the last step) the
-    # counter advance and IF condition: 5k + 1; an eager tail of k steps runs
-    # the 10 gated rebuild kernels in place of each condition: 14k - 1
+    # step pass 1, pass 2, the two per-replica sum kernels, and (all but the
+    # last step) the counter advance and IF condition: 6k + 1; an eager tail of
+    # k steps runs the 10 rebuild kernels in place of each condition: 15k + 1.
+    # A rebuild event in a graph adds the 10 kernels of the IF body.
     full, rest = divmod(args.steps, G)
-    launches = full * (5 * G + 1) + (14 * rest - 1 if rest else 0) + 10 * events
+    launches = full * (6 * G + 1) + (15 * rest + 1 if rest else 0) + 10 * events
     return {"value": total * args.steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.steps,
             "replicas": len(reps), "atoms_total": total, "atoms_min": int(min(sizes)), "atoms_max": int(max(sizes)),
             "scaling": "strong", "status": status, "rebuild_events_in_timed": events,

@@ -379,6 +379,7 @@ typedef struct SimRep {
                                the upper grip as far above it                       */
 } SimRep;
 
+#define SIM_BATCH_RED_SPLIT 8   /* blocks that share one replica's reduction */
 typedef struct SimBatch {
     SimEngine e;            /* slot arrays; e.n = slots in use (sum of n_slots),
                                e.n_pad >= e.n, a multiple of 128.  e.box, e.ncell,
@@ -398,7 +399,8 @@ typedef struct SimBatch {
     int8_t*  grip;          /* [atoms, original order] 0 free, 1 lower grip, 2 upper   */
     double*  gref;          /* [3][e.n_pad] grip reference positions, by original index */
     double*  rep_rff;       /* [n_rep] Langevin noise amplitude sqrt(kB T (1-damp^2)/m) */
-    double*  chunk_red;     /* [e.n_pad / 32][SIM_RED_SLOTS] per-warp partial sums      */
+    double*  chunk_red;     /* [e.n_pad / 32 + SIM_BATCH_RED_SPLIT * n_rep][SIM_RED_SLOTS]:
+                               per-warp partial sums, then per-block sums of the reduction */
     double*  rep_red;       /* [n_rep][SIM_RED_SLOTS] per-replica FP64 sums            */
 } SimBatch;
 

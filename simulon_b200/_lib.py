@@ -20,6 +20,7 @@ SIM_STATUS_OVERFLOW = 8
 SIM_STATUS_NONFINITE = 16
 SIM_STATUS_HALO = 64
 SIM_STATIC_MAX_ATOMS = 262144   # atom-slot limit of sim_eam_forces_static
+SIM_BATCH_RED_SPLIT = 8         # blocks that share one replica's reduction
 
 RED_EPOT_EMBED, RED_EPOT_PAIR, RED_VIRIAL = 0, 1, 2
 RED_W = slice(3, 9)          # xx yy zz xy xz yz

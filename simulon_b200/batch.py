@@ -187,7 +187,7 @@ class BatchedEngine:
         self.gref = torch.from_numpy(gref).to(dev)
         self.temperatures = np.array([float(r.temperature) for r in self.replicas])
         self.rep_rff = torch.zeros(R, **f64)
-        self.chunk_red = torch.zeros(P // SLOT_ALIGN, _lib.RED_SLOTS, **f64)
+        self.chunk_red = torch.zeros(P // SLOT_ALIGN + _lib.SIM_BATCH_RED_SPLIT * R, _lib.RED_SLOTS, **f64)
         self.rep_red = torch.zeros(R, _lib.RED_SLOTS, **f64)
         self.step_ctr = torch.full((2,), -1, device=dev, dtype=torch.int64)
         self.log_capacity = int(log_capacity)

@@ -13,8 +13,8 @@
 // rebuild kernel skips the slots and cells of replicas that are not flagged,
 // so a hot replica can rebuild every few steps without touching the others.
 //
-// Reductions: each warp writes the sums of its 32 slots to chunk_red; one
-// block per replica then adds its chunks in a fixed order in FP64
+// Reductions: each warp writes the sums of its 32 slots to chunk_red; a few
+// blocks per replica then add its chunks in a fixed order in FP64
 // (deterministic, no atomics).
 //
 // Pair arithmetic, table interpolation and integration are the single-system
@@ -595,20 +595,22 @@ __global__ void k_bb_first_half(SimBatch B, SimIntegrator p) {
 
 __global__ void k_bb_advance_step(uint64_t* ctr) { *ctr += 1; }
 
-// One block per replica: FP64 sums of its warps' partials in a fixed order
-// (each thread a strided set of chunks, then butterfly sums within and across
-// warps: deterministic, no atomics); with a log, also into row (*step % cap).
-#define BATCH_REDUCE_THREADS 1024
-__global__ void __launch_bounds__(BATCH_REDUCE_THREADS) k_bb_reduce(SimBatch B, const uint64_t* step, double* log,
-                                                                    int cap) {
-    const int k = blockIdx.x;
+// Per-replica sums in two launches, both in a fixed order (deterministic, no
+// atomics): SIM_BATCH_RED_SPLIT blocks per replica each add a strided share of
+// its warps' partials (butterfly sums within and across warps) into the rows
+// after the per-warp area of chunk_red; then one warp per replica adds those
+// rows into rep_red and, with a log, into row (*step % cap).
+#define BATCH_REDUCE_THREADS 512
+__global__ void __launch_bounds__(BATCH_REDUCE_THREADS) k_bb_reduce(SimBatch B) {
+    const int k = blockIdx.x / SIM_BATCH_RED_SPLIT, sl = blockIdx.x % SIM_BATCH_RED_SPLIT;
     const SimRep& R = B.rep[k];
     const int64_t c0 = R.off >> 5, c1 = (R.off + R.n_slots) >> 5;
     __shared__ double part[SIM_RED_SLOTS][BATCH_REDUCE_THREADS / 32];
     double s[SIM_RED_SLOTS];
 #pragma unroll
     for (int q = 0; q < SIM_RED_SLOTS; ++q) s[q] = 0.0;
-    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    const int64_t stride = (int64_t)blockDim.x * SIM_BATCH_RED_SPLIT;
+    for (int64_t c = c0 + sl * (int64_t)blockDim.x + threadIdx.x; c < c1; c += stride) {
         const double2* src = reinterpret_cast<const double2*>(B.chunk_red + c * SIM_RED_SLOTS);
 #pragma unroll
         for (int q = 0; q < SIM_RED_SLOTS / 2; ++q) {
@@ -625,19 +627,24 @@ __global__ void __launch_bounds__(BATCH_REDUCE_THREADS) k_bb_reduce(SimBatch B, 
     }
     __syncthreads();
     if (warp == 0) {
+        double* dst = B.chunk_red + ((B.e.n_pad >> 5) + blockIdx.x) * SIM_RED_SLOTS;
 #pragma unroll
         for (int q = 0; q < SIM_RED_SLOTS; ++q) {
             const double v = warp_sum(lane < (int)(blockDim.x >> 5) ? part[q][lane] : 0.0);
-            if (lane == 0) part[q][0] = v;
+            if (lane == 0) dst[q] = v;
         }
     }
-    __syncthreads();
-    if (threadIdx.x < SIM_RED_SLOTS) {
-        const int q = threadIdx.x;
-        const double acc = part[q][0];
-        B.rep_red[k * SIM_RED_SLOTS + q] = acc;
-        if (log) log[((*step % (uint64_t)cap) * B.n_rep + k) * SIM_RED_SLOTS + q] = acc;
-    }
+}
+
+__global__ void k_bb_reduce_final(SimBatch B, const uint64_t* step, double* log, int cap) {
+    const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (k >= B.n_rep || lane >= SIM_RED_SLOTS) return;
+    const double* src = B.chunk_red + ((B.e.n_pad >> 5) + (int64_t)k * SIM_BATCH_RED_SPLIT) * SIM_RED_SLOTS;
+    double acc = 0.0;
+    for (int sl = 0; sl < SIM_BATCH_RED_SPLIT; ++sl) acc += src[sl * SIM_RED_SLOTS + lane];
+    B.rep_red[k * SIM_RED_SLOTS + lane] = acc;
+    if (log) log[((*step % (uint64_t)cap) * B.n_rep + k) * SIM_RED_SLOTS + lane] = acc;
 }
 
 __global__ void k_bb_gather_f64(SimBatch B, const double* __restrict__ src, double* __restrict__ out) {
@@ -776,7 +783,9 @@ extern "C" int sim_batch_first_half(const SimBatch* b, const SimIntegrator* p, v
 
 extern "C" int sim_batch_reduce(const SimBatch* b, const uint64_t* step, double* log, int32_t log_cap, void* stream) {
     if (!batch_ok(b) || (log && (log_cap <= 0 || !step))) return SIM_ERR_ARG;
-    k_bb_reduce<<<b->n_rep, BATCH_REDUCE_THREADS, 0, (cudaStream_t)stream>>>(*b, step, log, log_cap);
+    cudaStream_t st = (cudaStream_t)stream;
+    k_bb_reduce<<<b->n_rep * SIM_BATCH_RED_SPLIT, BATCH_REDUCE_THREADS, 0, st>>>(*b);
+    k_bb_reduce_final<<<(int)ceil_div(b->n_rep, 8), 256, 0, st>>>(*b, step, log, log_cap);
     return launch_status("sim_batch_reduce");
 }
 
