@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-extras", action="store_true", help="skip e2e / cpu baseline (profiling runs)")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-replica form")
+    p.add_argument("--no-lj", action="store_true", help="skip the LJ argon form")
+    p.add_argument("--lj-n", type=int, default=63, help="FCC cells per side of the LJ form (atoms = 4 n^3)")
     p.add_argument("--batch-replicas", type=int, default=48)
     p.add_argument("--batch-skin", type=float, default=0.75)
     return p.parse_args()
@@ -333,6 +335,8 @@ def run_b200(args):
 
     if not args.no_extras and rank == 0:
         line["e2e"] = e2e(model, mol, x, v, args, dev)
+    if not args.no_lj:
+        line["lj"] = lj_form(args, sb, dev, world)
     if not args.no_batched:
         line["batched"] = batched_form(args, sb, pot, dev, world, rank, barrier)
     if world > 1:
@@ -407,6 +411,81 @@ def batched_form(args, sb, pot, dev, world, rank, barrier):
                                    "precrack L_x/4, 3-layer grips opening 1e-4 A/step, T 50-1200 K Langevin "
                                    f"gamma 10/ps, dt 1 fs, skin {args.batch_skin} A",
                        "parallelism": f"LPT over {world} rank(s)", "graph_steps": G}}
+
+
+def lj_form(args, sb, dev, world):
+    """LJ argon scaling point: FCC 4 n^3 atoms, a = 5.26 A,
+    eps 0.0104 eV, sigma 3.405 A, cutoff 7.0 A, skin 0.5 A, NVE from 94.4 K
+    Maxwell-Boltzmann velocities, dt 2 fs; the FP32-pair / FP64-integration
+    form and the FP64 form, each timed like the plain EAM line, with the force
+    RMSE of the FP32 form against the FP64 form on the same positions and the
+    drift of the total energy per atom over the timed steps."""
+    import torch
+    import torch.distributed as dist
+    n = args.lj_n
+    a = 5.26
+    g = np.arange(n)
+    cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    x = ((cells[:, None, :] + basis[None]).reshape(-1, 3) * a).astype(np.float64)
+    L = n * a
+    N = len(x)
+    m = 39.948 * 1.036427e-4
+    rng = np.random.default_rng(7)
+    v = rng.standard_normal((N, 3)) * np.sqrt(8.617333262e-5 * 94.4 / m)
+    v -= v.mean(0)
+    G = args.graph_steps
+    out, f0 = {}, {}
+    for name, dtype in (("fp32_pair", torch.float32), ("fp64", torch.float64)):
+        old = torch.get_default_dtype()
+        torch.set_default_dtype(dtype)
+        try:
+            mol = sb.AtomFileReader.from_arrays(["Ar"] * N, x, L, 7.0, device=dev, skin_thickness=0.5,
+                                                parameter={"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}})
+            mol.atom_velocities = torch.tensor(v, dtype=dtype, device=dev)
+            ff = sb.LennardJonesForce(mol)
+            integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NVE")
+            model = sb.BaseModel(sb.SumBackboneInterface([ff], mol), integ, mol)
+        finally:
+            torch.set_default_dtype(old)
+        eng = mol.engine
+        ff.compute()
+        f0[name] = eng.gather("f").double()
+        model.run(max(args.warmup, G), graph_steps=G)
+        torch.cuda.synchronize()
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        first = model.steps_done
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        model.run(args.steps, graph_steps=G)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        k = min(args.steps, eng.log_capacity)
+        rows = model.step_log(first + args.steps - k, k).cpu().numpy()
+        etot = (rows[:, 0] + rows[:, 1] + rows[:, 9]) / N
+        t_ns = np.arange(k) * 0.002e-3
+        drift = float(np.polyfit(t_ns, etot, 1)[0]) if k > 1 else None
+        out[name] = {"value": world * N * args.steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.steps,
+                     "energy_drift_ev_per_atom_per_ns": drift, "status": eng.status(),
+                     "neighbors_mean": eng.neighbor_stats()["mean"]}
+        del model, mol, ff, integ, eng
+        torch.cuda.empty_cache()
+    rmse = float(torch.sqrt(((f0["fp32_pair"] - f0["fp64"]) ** 2).mean()))
+    out["fp32_pair"]["force_rmse_vs_fp64_ev_per_a"] = rmse
+    out["config"] = {"workload": f"LJ Ar FCC 4*{n}^3 = {N:,} atoms per GPU, a 5.26 A, eps 0.0104 eV, sigma 3.405 A, "
+                                 "rc 7.0 A, skin 0.5 A, NVE from 94.4 K, dt 2 fs", "scaling": "weak",
+                     "parallelism": f"replicas x{world}"}
+    return out
 
 
 def e2e(model, mol, x, v, args, dev):
