@@ -435,6 +435,58 @@ int sim_batched_step(const SimBatch* b, const SimEAMTables* t, const SimIntegrat
 int sim_batch_gather_f64(const SimBatch* b, const double* src_soa, double* out_rows, void* stream);
 int sim_batch_gather_f32(const SimBatch* b, const float* src_aos4, double* out_rows, void* stream);
 
+/* ==== group 4: descriptor-MLP surrogate (no counterpart in the reference) == *
+ * A learned stand-in for the EAM force field: per atom, 8 radial and 8
+ * angular symmetry-function descriptors of the in-cutoff neighbourhood
+ * (r < 4.4 A), a 16 -> 64 -> 64 -> 1 SiLU network giving the atom's energy,
+ * forces = -dE/dx.  The network's GEMMs run on the tensor cores in BF16 with
+ * FP32 accumulation; it is trained on the engine's own per-atom EAM energies
+ * with these kernels.  Parameters live in one FP32 array (offsets below); the
+ * kernels read BF16 operand images made from it by sim_mlp_pack. */
+#define SIM_MLP_OFF_W1 0        /* W1 [16][64]  */
+#define SIM_MLP_OFF_B1 1024     /* b1 [64]      */
+#define SIM_MLP_OFF_W2 1088     /* W2 [64][64]  */
+#define SIM_MLP_OFF_B2 5184     /* b2 [64]      */
+#define SIM_MLP_OFF_W3 5248     /* w3 [64]      */
+#define SIM_MLP_OFF_B3 5312     /* b3           */
+#define SIM_MLP_PARAMS 5313
+#define SIM_STATUS_MLP_NEIGHBORS 128  /* device: > 32 in-cutoff neighbours (extra ones ignored) */
+#define SIM_STATUS_MLP_TIMEOUT   256  /* device: a tensor-core completion wait timed out        */
+typedef struct SimMLP {
+    const uint16_t* w1t_img;  /* BF16 operand images from sim_mlp_pack (2, 8, 8, 2 KB) */
+    const uint16_t* w2t_img;
+    const uint16_t* w2_img;
+    const uint16_t* w1_img;
+    const float* b1;          /* [64] (inside the FP32 parameter array)         */
+    const float* b2;          /* [64]                                           */
+    const float* w3;          /* [64]                                           */
+    const float* b3;          /* [1]                                            */
+    const float* mu;          /* [16] descriptor means                          */
+    const float* inv_sigma;   /* [16] 1 / descriptor standard deviations        */
+} SimMLP;
+
+/* Descriptors of every slot: G [n_pad][16] FP32. */
+int sim_mlp_descriptors(const SimEngine* e, float* G, void* stream);
+/* Per-atom energies e_atom [n] and dE/dG [n][16] (with respect to the raw
+ * descriptors) for n rows of G; status gets SIM_STATUS_MLP_TIMEOUT on a
+ * tensor-core wait that did not complete. */
+int sim_mlp_forward(const SimMLP* m, const float* G, int64_t n, float* e_atom, float* dEdG, int32_t* status,
+                    void* stream);
+/* Forces -dE/dx into e->f32 (overwritten) from dE/dG of every slot. */
+int sim_mlp_forces(const SimEngine* e, const float* dEdG, void* stream);
+/* Training: gradient of mean_i (E_i - target_i)^2 over n rows with respect to
+ * every parameter into grads [SIM_MLP_PARAMS] (overwritten), loss into *loss. */
+int sim_mlp_train_grads(const SimMLP* m, const float* G, const float* target, int64_t n, float* grads,
+                        float* loss, int32_t* status, void* stream);
+/* BF16 operand images of W1, W2 from the FP32 parameter array. */
+int sim_mlp_pack(const float* params, uint16_t* w1t_img, uint16_t* w2t_img, uint16_t* w2_img, uint16_t* w1_img,
+                 void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on the parameter array; step >= 1. */
+int sim_mlp_adam(float* params, const float* grads, float* m1, float* m2, float lr, int32_t step, void* stream);
+/* Per-atom EAM energies F(rho_i) + 1/2 sum_j phi(r_ij) of every slot (one
+ * element type): the surrogate's training targets. */
+int sim_eam_atom_energy(const SimEngine* e, const SimEAMTables* t, float* e_atom, void* stream);
+
 /* Message for the last CUDA error seen by this library (host string). */
 const char* sim_last_cuda_error(void);
 int sim_version(void);

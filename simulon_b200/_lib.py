@@ -19,6 +19,8 @@ SIM_ERR_BOX = 4
 SIM_STATUS_OVERFLOW = 8
 SIM_STATUS_NONFINITE = 16
 SIM_STATUS_HALO = 64
+SIM_STATUS_MLP_NEIGHBORS = 128
+SIM_STATUS_MLP_TIMEOUT = 256
 SIM_STATIC_MAX_ATOMS = 262144   # atom-slot limit of sim_eam_forces_static
 SIM_BATCH_RED_SPLIT = 8         # blocks that share one replica's reduction
 
@@ -95,6 +97,11 @@ class SimBatch(ctypes.Structure):
                 ("gref", c_p), ("rep_rff", c_p), ("chunk_red", c_p), ("rep_red", c_p)]
 
 
+class SimMLP(ctypes.Structure):
+    _fields_ = [("w1t_img", c_p), ("w2t_img", c_p), ("w2_img", c_p), ("w1_img", c_p), ("b1", c_p), ("b2", c_p),
+                ("w3", c_p), ("b3", c_p), ("mu", c_p), ("inv_sigma", c_p)]
+
+
 _P = ctypes.POINTER
 # name -> argtypes (restype int unless listed in _RESTYPES)
 SIGNATURES = {
@@ -139,6 +146,13 @@ SIGNATURES = {
                          c_p],
     "sim_batch_gather_f64": [_P(SimBatch), c_p, c_p, c_p],
     "sim_batch_gather_f32": [_P(SimBatch), c_p, c_p, c_p],
+    "sim_mlp_descriptors": [_P(SimEngine), c_p, c_p],
+    "sim_mlp_forward": [_P(SimMLP), c_p, ctypes.c_int64, c_p, c_p, c_p, c_p],
+    "sim_mlp_forces": [_P(SimEngine), c_p, c_p],
+    "sim_mlp_train_grads": [_P(SimMLP), c_p, c_p, ctypes.c_int64, c_p, c_p, c_p, c_p],
+    "sim_mlp_pack": [c_p, c_p, c_p, c_p, c_p, c_p],
+    "sim_mlp_adam": [c_p, c_p, c_p, c_p, ctypes.c_float, ctypes.c_int32, c_p],
+    "sim_eam_atom_energy": [_P(SimEngine), _P(SimEAMTables), c_p, c_p],
     "sim_last_cuda_error": [],
     "sim_version": [],
     "sim_struct_sizes": [c_p, ctypes.c_int32],

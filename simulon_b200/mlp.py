@@ -1,0 +1,285 @@
+"""Descriptor-MLP surrogate of the EAM force field (C ABI group 4).
+
+No counterpart in the reference: this is the learned form of the force path.
+Per atom: 8 radial and 8 angular symmetry-function descriptors of the
+in-cutoff neighbourhood (r < 4.4 A, cosine cutoff), a 16 -> 64 -> 64 -> 1 SiLU
+network for the atom's energy (BF16 operands on the tensor cores, FP32
+accumulation), forces = -dE/dx through network and descriptors.
+
+* ``MLPNet`` holds the FP32 parameters and their BF16 operand images.
+* ``MLPForce`` is a force-field backbone with the ``BackboneInterface``
+  contract of the reference (core/md_model.py:9-12): energy, forces.
+* ``generate_dataset`` runs the engine's EAM at several temperatures and
+  strains and records descriptors with per-atom EAM energies.
+* ``train`` fits the network on the GPU with the library's own forward,
+  backward and Adam kernels.
+* ``SurrogateRun`` advances a system with MLP forces and checks them against
+  EAM every ``judge_every`` steps, switching to EAM when the force RMSE
+  exceeds ``tolerance``.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+
+import numpy as np
+import torch
+
+from . import _lib
+from .engine import MDEngine, integrator_params
+
+N_DESC, N_HID = 16, 64
+OFF = dict(W1=(0, (16, 64)), b1=(1024, (64,)), W2=(1088, (64, 64)), b2=(5184, (64,)), w3=(5248, (64,)),
+           b3=(5312, ()))
+N_PARAMS = 5313
+
+
+class MLPNet:
+    """Parameters (one FP32 device array) + descriptor normalisation + BF16 images."""
+
+    def __init__(self, device=None, params: dict | None = None, seed: int = 0):
+        self.device = torch.device(device or "cuda")
+        if self.device.type != "cuda":
+            raise RuntimeError("MLPNet runs on CUDA devices only (no CPU fallback)")
+        self.lib = _lib.load()
+        self.flat = torch.zeros(N_PARAMS, device=self.device, dtype=torch.float32)
+        self.mu = torch.zeros(N_DESC, device=self.device, dtype=torch.float32)
+        self.inv_sigma = torch.ones(N_DESC, device=self.device, dtype=torch.float32)
+        self.images = [torch.zeros(n, device=self.device, dtype=torch.int16) for n in (1024, 4096, 4096, 1024)]
+        self.status = torch.zeros(1, device=self.device, dtype=torch.int32)
+        if params is None:
+            params = init_params(seed)
+        self.load_dict(params)
+
+    # ---- parameters ------------------------------------------------------
+    def load_dict(self, p: dict):
+        flat = np.zeros(N_PARAMS, np.float32)
+        for k, (o, shp) in OFF.items():
+            flat[o:o + int(np.prod(shp)) if shp else o + 1] = np.asarray(p[k], np.float32).reshape(-1)
+        self.flat.copy_(torch.from_numpy(flat))
+        if "mu" in p:
+            self.mu.copy_(torch.as_tensor(np.asarray(p["mu"], np.float32)))
+        if "sigma" in p:
+            self.inv_sigma.copy_(torch.as_tensor(1.0 / np.asarray(p["sigma"], np.float32)))
+        self.pack()
+
+    def to_dict(self) -> dict:
+        flat = self.flat.cpu().numpy()
+        out = {k: flat[o:o + int(np.prod(shp))].reshape(shp) if shp else flat[o:o + 1].reshape(())
+               for k, (o, shp) in OFF.items()}
+        out["mu"] = self.mu.cpu().numpy()
+        out["sigma"] = 1.0 / self.inv_sigma.cpu().numpy()
+        return {k: np.asarray(v, np.float64) for k, v in out.items()}
+
+    def save(self, path: str):
+        np.savez(path, **self.to_dict())
+
+    @classmethod
+    def load(cls, path: str, device=None) -> "MLPNet":
+        with np.load(path) as z:
+            return cls(device, {k: z[k] for k in z.files})
+
+    def set_normalisation(self, G: torch.Tensor):
+        """Descriptor mean and standard deviation from rows of G."""
+        G = G.float()
+        self.mu.copy_(G.mean(0))
+        self.inv_sigma.copy_(1.0 / G.std(0).clamp_min(1e-6))
+
+    def pack(self):
+        p = _lib.ptr
+        _lib.call("sim_mlp_pack", p(self.flat), *(p(t) for t in self.images), self._stream())
+        self._make_struct()
+
+    def _make_struct(self):
+        s = _lib.SimMLP()
+        p = _lib.ptr
+        s.w1t_img, s.w2t_img, s.w2_img, s.w1_img = (p(t) for t in self.images)
+        base = self.flat.data_ptr()
+        s.b1, s.b2 = base + 4 * OFF["b1"][0], base + 4 * OFF["b2"][0]
+        s.w3, s.b3 = base + 4 * OFF["w3"][0], base + 4 * OFF["b3"][0]
+        s.mu, s.inv_sigma = p(self.mu), p(self.inv_sigma)
+        self.st = s
+        self.ref = ctypes.byref(s)
+
+    def _stream(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    # ---- kernels -----------------------------------------------------------
+    def forward(self, G: torch.Tensor, n: int):
+        """(E_i [n], dE/dG [n,16]) for the first n rows of G [>=n, 16] FP32."""
+        e = torch.empty(n, device=self.device, dtype=torch.float32)
+        d = torch.empty(n, N_DESC, device=self.device, dtype=torch.float32)
+        _lib.call("sim_mlp_forward", self.ref, _lib.ptr(G), int(n), _lib.ptr(e), _lib.ptr(d), _lib.ptr(self.status),
+                  self._stream())
+        return e, d
+
+    def train_grads(self, G: torch.Tensor, target: torch.Tensor, grads: torch.Tensor, loss: torch.Tensor):
+        _lib.call("sim_mlp_train_grads", self.ref, _lib.ptr(G), _lib.ptr(target), int(target.numel()),
+                  _lib.ptr(grads), _lib.ptr(loss), _lib.ptr(self.status), self._stream())
+
+
+def init_params(seed: int = 0) -> dict:
+    rng = np.random.default_rng(seed)
+    return dict(W1=rng.normal(0, 1 / math.sqrt(N_DESC), (N_DESC, N_HID)), b1=np.zeros(N_HID),
+                W2=rng.normal(0, 1 / math.sqrt(N_HID), (N_HID, N_HID)), b2=np.zeros(N_HID),
+                w3=rng.normal(0, 1 / math.sqrt(N_HID), N_HID), b3=np.array(0.0),
+                mu=np.zeros(N_DESC), sigma=np.ones(N_DESC))
+
+
+def descriptors(engine: MDEngine) -> torch.Tensor:
+    """G [n_pad, 16] of the engine's slots."""
+    G = torch.zeros(engine.n_pad, N_DESC, device=engine.device, dtype=torch.float32)
+    _lib.call("sim_mlp_descriptors", engine.st_ref, _lib.ptr(G), engine.stream)
+    return G
+
+
+def mlp_forces(engine: MDEngine, dEdG: torch.Tensor):
+    """-dE/dx of every slot into engine.f32 from dE/dG [n, 16]."""
+    _lib.call("sim_mlp_forces", engine.st_ref, _lib.ptr(dEdG), engine.stream)
+    engine._last_force_precision = 0
+    engine.forces_valid = True
+
+
+def eam_atom_energy(engine: MDEngine, tables) -> torch.Tensor:
+    """Per-atom EAM energies of the engine's slots [n_pad]."""
+    out = torch.zeros(engine.n_pad, device=engine.device, dtype=torch.float32)
+    _lib.call("sim_eam_atom_energy", engine.st_ref, tables.ref, _lib.ptr(out), engine.stream)
+    return out
+
+
+class MLPForce:
+    """Force-field backbone with MLP energies and forces (BackboneInterface contract)."""
+
+    def __init__(self, net: MLPNet, molecular):
+        self.net = net
+        self.molecular = molecular
+        self.force_precision = 0
+
+    def compute(self):
+        eng = self.molecular.engine
+        G = descriptors(eng)
+        e, d = self.net.forward(G, eng.n)
+        mlp_forces(eng, d)
+        self.atom_energy = e
+
+    def __call__(self):
+        return self.forward()
+
+    def forward(self):
+        self.compute()
+        eng = self.molecular.engine
+        return {"energy": self.atom_energy.sum(), "forces": eng.gather("f").to(self.molecular.dtype)}
+
+
+# ---------------------------------------------------------------------------
+# training data and training
+
+def bcc_cell(n: int, a: float = 3.165):
+    g = np.arange(n)
+    cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0.5]])
+    return (cells[:, None, :] + basis[None]).reshape(-1, 3).astype(np.float64) * a
+
+
+def generate_dataset(tables, *, n_cells: int = 10, temperatures=(300.0, 700.0, 1100.0, 1500.0),
+                     strains=(-0.03, 0.0, 0.03), frames_per_run: int = 20, stride: int = 20,
+                     equilibrate: int = 200, dt: float = 0.001, seed: int = 0, device=None,
+                     with_forces: bool = False):
+    """Descriptors and per-atom EAM energies (and optionally EAM forces and
+    positions) of frames from Langevin runs of BCC W (2 n^3 atoms) at each
+    temperature and isotropic strain."""
+    dev = torch.device(device or "cuda")
+    rng = np.random.default_rng(seed)
+    Gs, Es, frames = [], [], []
+    a0 = 3.165
+    for T in temperatures:
+        for eps in strains:
+            a = a0 * (1.0 + eps + rng.uniform(-0.005, 0.005))
+            x = bcc_cell(n_cells, a)
+            L = n_cells * a
+            m = 183.84 * 1.036427e-4
+            v = rng.normal(0.0, math.sqrt(8.617333262e-5 * T / m), x.shape)
+            eng = MDEngine(x, np.zeros(len(x), np.int32), [183.84], np.diag([L] * 3), 4.4, 0.5, velocities=v,
+                           device=dev)
+            ip = integrator_params(eng, dt, langevin=True, temperature=T, gamma=10.0, seed=int(rng.integers(1 << 30)))
+            eng.eam_forces(tables)
+
+            def advance(k):
+                for _ in range(k):
+                    eng.integrate_first(ip, 0)
+                    eng.rebuild_if_needed()
+                    eng.eam_forces_integrate(tables, ip)
+            advance(equilibrate)
+            for _ in range(frames_per_run):
+                advance(stride)
+                eng.eam_forces(tables)
+                G = descriptors(eng)[:eng.n].clone()
+                E = eam_atom_energy(eng, tables)[:eng.n].clone()
+                Gs.append(G)
+                Es.append(E)
+                if with_forces:
+                    frames.append(dict(x=eng.gather("x").cpu().numpy(), f=eng.gather("f").cpu().numpy(), H=np.diag([L] * 3)))
+            if eng.status() & ~_lib.SIM_STATUS_MLP_NEIGHBORS:
+                raise RuntimeError(f"EAM run for training data failed (status {eng.status():#x})")
+    G = torch.cat(Gs)
+    E = torch.cat(Es)
+    return (G, E, frames) if with_forces else (G, E)
+
+
+def train(net: MLPNet, G: torch.Tensor, E: torch.Tensor, *, steps: int = 2000, batch: int = 16384,
+          lr: float = 3e-3, lr_final: float = 1e-4, seed: int = 0, log_every: int = 0):
+    """Per-atom energy regression with Adam, all on the GPU.  Returns the
+    per-step losses (device tensor)."""
+    dev = net.device
+    n = G.shape[0]
+    net.set_normalisation(G)
+    with torch.no_grad():
+        p = net.to_dict()
+        p["b3"] = np.array(float(E.double().mean()))
+        net.load_dict(p)
+    grads = torch.zeros(N_PARAMS, device=dev, dtype=torch.float32)
+    m1 = torch.zeros_like(grads)
+    m2 = torch.zeros_like(grads)
+    loss = torch.zeros(1, device=dev, dtype=torch.float32)
+    losses = torch.zeros(steps, device=dev, dtype=torch.float32)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    Gb = torch.empty(batch, N_DESC, device=dev, dtype=torch.float32)
+    Eb = torch.empty(batch, device=dev, dtype=torch.float32)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    for s in range(steps):
+        idx = torch.randint(0, n, (batch,), device=dev, generator=gen)
+        torch.index_select(G, 0, idx, out=Gb)
+        torch.index_select(E, 0, idx, out=Eb)
+        net.train_grads(Gb, Eb, grads, loss)
+        frac = s / max(1, steps - 1)
+        lr_s = lr * (lr_final / lr) ** frac
+        _lib.call("sim_mlp_adam", _lib.ptr(net.flat), _lib.ptr(grads), _lib.ptr(m1), _lib.ptr(m2), float(lr_s),
+                  s + 1, st)
+        _lib.call("sim_mlp_pack", _lib.ptr(net.flat), *(_lib.ptr(t) for t in net.images), st)
+        losses[s:s + 1].copy_(loss)
+        if log_every and (s + 1) % log_every == 0:
+            print(f"step {s + 1}: loss {float(loss):.3e} eV^2", flush=True)
+    if int(net.status.item()):
+        raise RuntimeError(f"tensor-core wait timed out in training (status {int(net.status.item()):#x})")
+    return losses
+
+
+def force_rmse(net: MLPNet, tables, frames, device=None) -> float:
+    """RMSE of MLP forces against the recorded EAM forces of frames."""
+    dev = torch.device(device or "cuda")
+    se, cnt = 0.0, 0
+    for fr in frames:
+        eng = MDEngine(fr["x"], np.zeros(len(fr["x"]), np.int32), [183.84], fr["H"], 4.4, 0.5, device=dev)
+        G = descriptors(eng)
+        _, d = net.forward(G, eng.n)
+        mlp_forces(eng, d)
+        f = eng.gather("f").cpu().numpy()
+        se += float(((f - fr["f"]) ** 2).sum())
+        cnt += f.size
+    return math.sqrt(se / max(cnt, 1))
+
+
+def default_weights_path() -> str:
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "w_surrogate.npz")

@@ -163,7 +163,7 @@ def test_package_references_resolve():
     # status bits mirror the header
     hdr = open(os.path.join(ROOT, "include", "simb200.h")).read()
     for name in ("SIM_OK", "SIM_ERR_ARG", "SIM_ERR_CUDA", "SIM_STATUS_OVERFLOW", "SIM_STATUS_NONFINITE",
-                 "SIM_STATUS_HALO"):
+                 "SIM_STATUS_HALO", "SIM_STATUS_MLP_NEIGHBORS", "SIM_STATUS_MLP_TIMEOUT"):
         val = int(re.search(rf"#define {name}\s+(\d+)", hdr).group(1))
         assert getattr(_lib, name) == val, name
     assert engine.TILE == int(re.search(r"#define SIM_TILE\s+(\d+)", hdr).group(1))
