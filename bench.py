@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--no-extras", action="store_true", help="skip e2e / cpu baseline (profiling runs)")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-replica form")
     p.add_argument("--no-lj", action="store_true", help="skip the LJ argon form")
+    p.add_argument("--no-mlp", action="store_true", help="skip the MLP-surrogate form")
     p.add_argument("--lj-n", type=int, default=63, help="FCC cells per side of the LJ form (atoms = 4 n^3)")
     p.add_argument("--batch-replicas", type=int, default=48)
     p.add_argument("--batch-skin", type=float, default=0.75)
@@ -337,6 +338,8 @@ def run_b200(args):
         line["e2e"] = e2e(model, mol, x, v, args, dev)
     if not args.no_lj:
         line["lj"] = lj_form(args, sb, dev, world)
+    if not args.no_mlp:
+        line["mlp"] = mlp_form(args, sb, pot, dev, world)
     if not args.no_batched:
         line["batched"] = batched_form(args, sb, pot, dev, world, rank, barrier)
     if world > 1:
@@ -486,6 +489,57 @@ def lj_form(args, sb, dev, world):
                                  "rc 7.0 A, skin 0.5 A, NVE from 94.4 K, dt 2 fs", "scaling": "weak",
                      "parallelism": f"replicas x{world}"}
     return out
+
+
+def mlp_form(args, sb, pot, dev, world):
+    """MLP-surrogate form: the committed surrogate weights
+    (trained on the GPU by python -m simulon_b200.mlp on the engine's own EAM
+    data), 1,024,000 W atoms NVT at 300 K (Langevin gamma 10/ps, dt 2 fs), EAM
+    judging the force RMSE every 100 steps and taking over above 0.05 eV/A;
+    the judgements run inside the timed region."""
+    import torch
+    import torch.distributed as dist
+    from simulon_b200 import mlp
+    x, L = bcc(args.n)
+    N = len(x)
+    v = mb_velocities(N, 300.0, 2000 + int(os.environ.get("RANK", "0")))
+    parser = sb.EAMParser(pot)
+    tables = sb.EAMDeviceTables(parser, dev)
+    net = mlp.MLPNet.load(mlp.default_weights_path(), dev)
+    eng = sb.MDEngine(x, np.zeros(N, np.int32), [M_W], np.diag([L] * 3), parser.cutoff, 0.5, velocities=v, device=dev)
+    ip = sb.engine.integrator_params(eng, 0.002, langevin=True, temperature=300.0, gamma=10.0, seed=5)
+    run = mlp.SurrogateRun(eng, net, tables, ip, judge_every=100, tolerance=0.05)
+    run.run(max(args.warmup, 100) // 100 * 100)
+    torch.cuda.synchronize()
+    K = max(100, args.steps // 100 * 100)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    run.run(K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    rm = run.rmse_history
+    return {"value": world * N * K / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K, "steps": K,
+            "force_rmse_vs_eam_ev_per_a": {"last": rm[-1] if rm else None, "max": max(rm) if rm else None,
+                                           "judgements": len(rm)},
+            "fell_back_to_eam": not run.use_mlp, "status": eng.status(), "net_status": int(net.status.item()),
+            "config": {"workload": f"EAM-W surrogate: BCC 2*{args.n}^3 = {N:,} atoms per GPU, NVT 300 K Langevin "
+                                   "gamma 10/ps, dt 2 fs, skin 0.5 A; descriptors 8 radial + 8 angular (rc 4.4 A), "
+                                   "MLP 16-64-64-1 SiLU, BF16 tensor-core GEMMs with FP32 accumulation",
+                       "judge": "EAM force RMSE every 100 steps (inside the timed region), fallback above 0.05 eV/A",
+                       "training": "python -m simulon_b200.mlp: 1.2 M atom samples (2,000-atom BCC cells at "
+                                   "300/700/1100/1500 K and -3/0/+3 % strain), 20,000 Adam steps of 16,384 atoms "
+                                   "on per-atom EAM energies"}}
 
 
 def e2e(model, mol, x, v, args, dev):

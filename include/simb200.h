@@ -478,6 +478,17 @@ int sim_mlp_forces(const SimEngine* e, const float* dEdG, void* stream);
  * every parameter into grads [SIM_MLP_PARAMS] (overwritten), loss into *loss. */
 int sim_mlp_train_grads(const SimMLP* m, const float* G, const float* target, int64_t n, float* grads,
                         float* loss, int32_t* status, void* stream);
+/* Force matching, step 1: with ferr [n_pad][4] = F - F_target per slot
+ * (float4, .w unused), u [n][16] = sum_m ferr_m . dG_i/dx_m per atom. */
+int sim_mlp_force_contract(const SimEngine* e, const float* ferr, float* u, void* stream);
+/* Force matching, step 2: gradient of
+ *   w_energy mean_i (E_i - target_i)^2 + w_force sum_m |F_m - F_target,m|^2 / (3 n_force_atoms)
+ * with respect to every parameter into grads (overwritten), through the
+ * network and its directional derivative along u (held fixed); the energy
+ * term's mean square into *loss. */
+int sim_mlp_train_grads_fm(const SimMLP* m, const float* G, const float* target, const float* u, int64_t n,
+                           float w_energy, float w_force, int64_t n_force_atoms, float* grads, float* loss,
+                           int32_t* status, void* stream);
 /* BF16 operand images of W1, W2 from the FP32 parameter array. */
 int sim_mlp_pack(const float* params, uint16_t* w1t_img, uint16_t* w2t_img, uint16_t* w2_img, uint16_t* w1_img,
                  void* stream);

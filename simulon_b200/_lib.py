@@ -150,6 +150,9 @@ SIGNATURES = {
     "sim_mlp_forward": [_P(SimMLP), c_p, ctypes.c_int64, c_p, c_p, c_p, c_p],
     "sim_mlp_forces": [_P(SimEngine), c_p, c_p],
     "sim_mlp_train_grads": [_P(SimMLP), c_p, c_p, ctypes.c_int64, c_p, c_p, c_p, c_p],
+    "sim_mlp_force_contract": [_P(SimEngine), c_p, c_p, c_p],
+    "sim_mlp_train_grads_fm": [_P(SimMLP), c_p, c_p, c_p, ctypes.c_int64, ctypes.c_float, ctypes.c_float,
+                               ctypes.c_int64, c_p, c_p, c_p, c_p],
     "sim_mlp_pack": [c_p, c_p, c_p, c_p, c_p, c_p],
     "sim_mlp_adam": [c_p, c_p, c_p, c_p, ctypes.c_float, ctypes.c_int32, c_p],
     "sim_eam_atom_energy": [_P(SimEngine), _P(SimEAMTables), c_p, c_p],

@@ -574,6 +574,338 @@ __global__ void __launch_bounds__(MLP_TILE) k_mlp_net(SimMLP m, const float* __r
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" :: "r"(tm));
 }
 
+// Force-matching pieces.  With e = F - F_target per slot, the gradient of the
+// force loss with respect to the network's parameters needs, per atom, the
+// descriptor Jacobian contracted with the force errors of the atom and its
+// neighbours: u_i = sum_m e_m . dG_i/dx_m = sum_j (e_j - e_i) . dG_i/dd_j.
+template <bool ORTHO>
+__global__ void __launch_bounds__(128) k_mlp_ucontract(SimEngine e, const float* __restrict__ ferr,
+                                                        float* __restrict__ u) {
+    const BoxF b(*e.box);
+    const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
+    const float4* __restrict__ er = reinterpret_cast<const float4*>(ferr);
+    bool over = false;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+        float4 nb[MLP_MAXN];
+        float ex[MLP_MAXN], ey[MLP_MAXN], ez[MLP_MAXN], ea[MLP_MAXN], eda[MLP_MAXN];
+        const int4 qi = posq[i];
+        const float4 ei = er[i];
+        int cnt = 0;
+        for (int k = 0; k < e.nnbr[i]; ++k) {
+            const int j = __ldg(&e.nbr[(int64_t)k * e.n_pad + i]);
+            const int4 qj = __ldg(&posq[j]);
+            float d0, d1, d2;
+            mlp_dvec<ORTHO>(b, qi, qj, d0, d1, d2);
+            const float r2 = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+            if (!(r2 < MLP_RC * MLP_RC)) continue;
+            if (cnt == MLP_MAXN) { over = true; continue; }
+            const float4 ej = __ldg(&er[j]);
+            nb[cnt] = make_float4(d0, d1, d2, sqrtf(r2));
+            ex[cnt] = ej.x - ei.x; ey[cnt] = ej.y - ei.y; ez[cnt] = ej.z - ei.z;
+            ++cnt;
+        }
+        float g[MLP_D];
+#pragma unroll
+        for (int k = 0; k < MLP_D; ++k) g[k] = 0.0f;
+        for (int a = 0; a < cnt; ++a) {
+            const float r = nb[a].w, fc = mlp_fc(r), dfc = mlp_dfc(r);
+            const float q = (ex[a] * nb[a].x + ey[a] * nb[a].y + ez[a] * nb[a].z) / r;   // (de . d)/r
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float t = r - mlp_rs(k);
+                g[k] = fmaf(__expf(-4.0f * t * t) * fmaf(-8.0f * t, fc, dfc), q, g[k]);
+            }
+            const float xe = __expf(-0.01f * r * r);
+            ea[a] = xe * fc;
+            eda[a] = xe * fmaf(-0.02f * r, fc, dfc);
+        }
+        for (int a = 0; a < cnt; ++a) {
+            const float4 da = nb[a];
+            const float ira = 1.0f / da.w;
+            const float qaa = ex[a] * da.x + ey[a] * da.y + ez[a] * da.z;
+            for (int c = a + 1; c < cnt; ++c) {
+                const float4 dc = nb[c];
+                const float irc = 1.0f / dc.w;
+                const float cs = (da.x * dc.x + da.y * dc.y + da.z * dc.z) * ira * irc;
+                const float qac = ex[a] * dc.x + ey[a] * dc.y + ez[a] * dc.z;
+                const float qca = ex[c] * da.x + ey[c] * da.y + ez[c] * da.z;
+                const float qcc = ex[c] * dc.x + ey[c] * dc.y + ez[c] * dc.z;
+                const float rad = ea[a] * ea[c];
+                const float Xc = rad * ((qac + qca) * ira * irc - cs * (qaa * ira * ira + qcc * irc * irc));
+                const float Xe = eda[a] * ea[c] * qaa * ira + ea[a] * eda[c] * qcc * irc;
+                const float p1 = 1.0f + cs, m1 = 1.0f - cs;
+                const float p2 = p1 * p1, m2 = m1 * m1, p4 = p2 * p2, m4 = m2 * m2;
+                const float p3 = p2 * p1, m3 = m2 * m1, p7 = p4 * p3, m7 = m4 * m3, p8 = p4 * p4, m8 = m4 * m4;
+                // 2^(1-z) (1 + l c)^z and its derivative in c, for (z, l) = (1,+) (1,-) (2,+) ...
+                g[8] += Xc + p1 * Xe;
+                g[9] += -Xc + m1 * Xe;
+                g[10] += p1 * Xc + 0.5f * p2 * Xe;
+                g[11] += -m1 * Xc + 0.5f * m2 * Xe;
+                g[12] += 0.5f * p3 * Xc + 0.125f * p4 * Xe;
+                g[13] += -0.5f * m3 * Xc + 0.125f * m4 * Xe;
+                g[14] += 0.0625f * p7 * Xc + 0.0078125f * p8 * Xe;
+                g[15] += -0.0625f * m7 * Xc + 0.0078125f * m8 * Xe;
+            }
+        }
+        float4* out = reinterpret_cast<float4*>(u + i * MLP_D);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out[q] = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
+    }
+    if (over) atomicOr(&e.flags[1], SIM_STATUS_MLP_NEIGHBORS);
+}
+
+__device__ __forceinline__ float d2silu(float z) {
+    const float s = 1.0f / (1.0f + __expf(-z));
+    return s * (1.0f - s) * (2.0f + z * (1.0f - 2.0f * s));
+}
+
+struct MlpFmSmem {
+    __nv_bfloat16 w1t[MLP_H * MLP_D];     // B of Z1 = g W1 and Z1' = g' W1
+    __nv_bfloat16 w2t[MLP_H * MLP_H];     // B of Z2 = H1 W2 and Z2' = H1' W2
+    __nv_bfloat16 w2[MLP_H * MLP_H];      // B of P1 = P2 W2^T and Q1 = Q2 W2^T
+    __nv_bfloat16 g0[MLP_TILE * MLP_D];   // normalised descriptors g
+    __nv_bfloat16 gd[MLP_TILE * MLP_D];   // their tangent g' = u / sigma
+    __nv_bfloat16 h1[MLP_TILE * MLP_H];   // H1, later dJ/dz1
+    __nv_bfloat16 hd1[MLP_TILE * MLP_H];  // H1', later dJ/dz1'
+    __nv_bfloat16 p2[MLP_TILE * MLP_H];   // dJ/dz2'
+    __nv_bfloat16 q2[MLP_TILE * MLP_H];   // dJ/dz2
+    float b1[MLP_H], b2[MLP_H], w3[MLP_H], mu[MLP_D], isg[MLP_D], b3;
+    uint64_t bar;
+    uint32_t tmem;
+};
+
+// thread t owns column `col` of a 64-wide weight gradient over half the rows:
+// dst[k][col] += sum_r A[r][k] B[r][col] (+ C[r][k] D[r][col]) for k in rows
+__device__ __forceinline__ void outer_acc(const __nv_bfloat16* A, const __nv_bfloat16* B, const __nv_bfloat16* C,
+                                          const __nv_bfloat16* D, int KA, int k0, int k1, int col, float* dst) {
+    for (int k = k0; k < k1; ++k) {
+        float acc = 0.0f;
+        for (int r = 0; r < MLP_TILE; ++r) {
+            acc = fmaf(__bfloat162float(A[img_off(r, k, KA)]), __bfloat162float(B[img_off(r, col, MLP_H)]), acc);
+            acc = fmaf(__bfloat162float(C[img_off(r, k, KA)]), __bfloat162float(D[img_off(r, col, MLP_H)]), acc);
+        }
+        atomicAdd(&dst[k * MLP_H + col], acc);
+    }
+}
+
+// Gradient of J = sum_i [a_i E_i + beta dE_i] with dE_i = u_i . dE_i/dG_i and
+// a_i = alpha (E_i - target_i): the energy and force-matching terms of the
+// training loss, by reverse mode through the network and its directional
+// derivative.  Six tensor-core GEMMs per tile (Z1, Z1', Z2, Z2', and the two
+// back-propagations through W2); weight gradients summed on the CUDA cores.
+__global__ void __launch_bounds__(MLP_TILE) k_mlp_train_fm(SimMLP m, const float* __restrict__ G,
+                                                           const float* __restrict__ target,
+                                                           const float* __restrict__ u, int64_t n, float alpha,
+                                                           float beta, float inv_n, float* __restrict__ grads,
+                                                           float* __restrict__ loss, int32_t* status) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    MlpFmSmem& S = *reinterpret_cast<MlpFmSmem*>(smem_raw);
+    const int t = threadIdx.x, warp = t >> 5;
+    {
+        const uint4* src[3] = {reinterpret_cast<const uint4*>(m.w1t_img), reinterpret_cast<const uint4*>(m.w2t_img),
+                               reinterpret_cast<const uint4*>(m.w2_img)};
+        uint4* dst[3] = {reinterpret_cast<uint4*>(S.w1t), reinterpret_cast<uint4*>(S.w2t),
+                         reinterpret_cast<uint4*>(S.w2)};
+        const int cnt[3] = {MLP_H * MLP_D / 8, MLP_H * MLP_H / 8, MLP_H * MLP_H / 8};
+#pragma unroll
+        for (int w = 0; w < 3; ++w)
+            for (int q = t; q < cnt[w]; q += blockDim.x) dst[w][q] = src[w][q];
+        if (t < MLP_H) { S.b1[t] = m.b1[t]; S.b2[t] = m.b2[t]; S.w3[t] = m.w3[t]; }
+        if (t < MLP_D) { S.mu[t] = m.mu[t]; S.isg[t] = m.inv_sigma[t]; }
+        if (t == 0) S.b3 = *m.b3;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;"
+                     :: "r"((uint32_t)__cvta_generic_to_shared(&S.tmem)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"((uint32_t)__cvta_generic_to_shared(&S.bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tm = S.tmem;
+    const uint32_t lb = (uint32_t)(32 * warp) << 16;
+    uint32_t phase = 0;
+    bool failed = false;
+    const int n_tiles = (int)((n + MLP_TILE - 1) / MLP_TILE);
+    const int col = t & 63, half = t >> 6;
+    for (int tile = blockIdx.x; tile < n_tiles && !failed; tile += gridDim.x) {
+        const int64_t i = (int64_t)tile * MLP_TILE + t;
+        const bool live = i < n;
+        {
+            float a[MLP_D], d[MLP_D];
+            const float4* gs = reinterpret_cast<const float4*>(G + (live ? i : 0) * MLP_D);
+            const float4* us = reinterpret_cast<const float4*>(u + (live ? i : 0) * MLP_D);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 v = gs[q], w = us[q];
+                a[4 * q] = v.x; a[4 * q + 1] = v.y; a[4 * q + 2] = v.z; a[4 * q + 3] = v.w;
+                d[4 * q] = w.x; d[4 * q + 1] = w.y; d[4 * q + 2] = w.z; d[4 * q + 3] = w.w;
+            }
+#pragma unroll
+            for (int c = 0; c < MLP_D; ++c) {
+                a[c] = live ? (a[c] - S.mu[c]) * S.isg[c] : 0.0f;
+                d[c] = live ? d[c] * S.isg[c] : 0.0f;
+            }
+            img_store8(S.g0, t, 0, MLP_D, a);
+            img_store8(S.g0, t, 8, MLP_D, a + 8);
+            img_store8(S.gd, t, 0, MLP_D, d);
+            img_store8(S.gd, t, 8, MLP_D, d + 8);
+        }
+        async_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (t == 0) {   // Z1 -> [0, 64), Z1' -> [64, 128)
+            mma_bf16(tm, smem_desc(S.g0, MLP_D), smem_desc(S.w1t, MLP_D), mma_idesc(128, MLP_H), 0);
+            mma_bf16(tm + 64, smem_desc(S.gd, MLP_D), smem_desc(S.w1t, MLP_D), mma_idesc(128, MLP_H), 0);
+            mma_commit(&S.bar);
+        }
+        failed = __syncthreads_or(!mbar_wait(&S.bar, phase));
+        phase ^= 1;
+        if (failed) break;
+        tc_fence_after();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float z[16], zd[16], h[16], hd[16];
+            tmem_ld16(tm + lb + 16 * q, z);
+            tmem_ld16(tm + lb + 64 + 16 * q, zd);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                const float zz = z[c] + S.b1[16 * q + c];
+                h[c] = silu(zz);
+                hd[c] = dsilu(zz) * zd[c];
+            }
+            img_store8(S.h1, t, 16 * q, MLP_H, h);
+            img_store8(S.h1, t, 16 * q + 8, MLP_H, h + 8);
+            img_store8(S.hd1, t, 16 * q, MLP_H, hd);
+            img_store8(S.hd1, t, 16 * q + 8, MLP_H, hd + 8);
+        }
+        async_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (t == 0) {   // Z2 -> [128, 192), Z2' -> [192, 256)
+#pragma unroll
+            for (int s = 0; s < MLP_H / 16; ++s) {
+                mma_bf16(tm + 128, smem_desc(S.h1 + s * 128, MLP_H), smem_desc(S.w2t + s * 128, MLP_H),
+                         mma_idesc(128, MLP_H), s > 0);
+                mma_bf16(tm + 192, smem_desc(S.hd1 + s * 128, MLP_H), smem_desc(S.w2t + s * 128, MLP_H),
+                         mma_idesc(128, MLP_H), s > 0);
+            }
+            mma_commit(&S.bar);
+        }
+        failed = __syncthreads_or(!mbar_wait(&S.bar, phase));
+        phase ^= 1;
+        if (failed) break;
+        tc_fence_after();
+        // energy first (a_i needs the full E_i)
+        float E = S.b3;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float z[16];
+            tmem_ld16(tm + lb + 128 + 16 * q, z);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 16; ++c) E = fmaf(S.w3[16 * q + c], silu(z[c] + S.b2[16 * q + c]), E);
+        }
+        const float err = live ? E - target[i] : 0.0f;
+        const float a_i = alpha * err;
+        const float b_i = live ? beta : 0.0f;
+        {
+            const float l = warp_sum_f(err * err * inv_n);
+            if ((t & 31) == 0) atomicAdd(loss, l);
+            const float db3 = warp_sum_f(a_i);
+            if ((t & 31) == 0) atomicAdd(&grads[GRAD_B3], db3);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float z[16], zd[16], pp[16], qq[16];
+            tmem_ld16(tm + lb + 128 + 16 * q, z);
+            tmem_ld16(tm + lb + 192 + 16 * q, zd);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                const int k = 16 * q + c;
+                const float zz = z[c] + S.b2[k];
+                const float s1 = dsilu(zz), s2 = d2silu(zz);
+                pp[c] = b_i * S.w3[k] * s1;
+                qq[c] = a_i * S.w3[k] * s1 + b_i * S.w3[k] * s2 * zd[c];
+                const float gw3 = warp_sum_f(a_i * silu(zz) + b_i * s1 * zd[c]);
+                if ((t & 31) == 0) atomicAdd(&grads[GRAD_W3 + k], gw3);
+            }
+            img_store8(S.p2, t, 16 * q, MLP_H, pp);
+            img_store8(S.p2, t, 16 * q + 8, MLP_H, pp + 8);
+            img_store8(S.q2, t, 16 * q, MLP_H, qq);
+            img_store8(S.q2, t, 16 * q + 8, MLP_H, qq + 8);
+        }
+        async_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (t == 0) {   // P1 = P2 W2^T -> [128, 192), Q1 = Q2 W2^T -> [192, 256)
+#pragma unroll
+            for (int s = 0; s < MLP_H / 16; ++s) {
+                mma_bf16(tm + 128, smem_desc(S.p2 + s * 128, MLP_H), smem_desc(S.w2 + s * 128, MLP_H),
+                         mma_idesc(128, MLP_H), s > 0);
+                mma_bf16(tm + 192, smem_desc(S.q2 + s * 128, MLP_H), smem_desc(S.w2 + s * 128, MLP_H),
+                         mma_idesc(128, MLP_H), s > 0);
+            }
+            mma_commit(&S.bar);
+        }
+        // while the tensor cores work: dW2 += H1'^T P2 + H1^T Q2, db2 += sum Q2
+        outer_acc(S.hd1, S.p2, S.h1, S.q2, MLP_H, half * 32, half * 32 + 32, col, grads + GRAD_W2);
+        if (half == 0) {
+            float acc = 0.0f;
+            for (int r = 0; r < MLP_TILE; ++r) acc += __bfloat162float(S.q2[img_off(r, col, MLP_H)]);
+            atomicAdd(&grads[GRAD_B2 + col], acc);
+        }
+        failed = __syncthreads_or(!mbar_wait(&S.bar, phase));
+        phase ^= 1;
+        if (failed) break;
+        tc_fence_after();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float z[16], zd[16], pp[16], qq[16], p1[16], q1[16];
+            tmem_ld16(tm + lb + 16 * q, z);
+            tmem_ld16(tm + lb + 64 + 16 * q, zd);
+            tmem_ld16(tm + lb + 128 + 16 * q, pp);
+            tmem_ld16(tm + lb + 192 + 16 * q, qq);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                const float zz = z[c] + S.b1[16 * q + c];
+                const float s1 = dsilu(zz), s2 = d2silu(zz);
+                p1[c] = pp[c] * s1;
+                q1[c] = pp[c] * s2 * zd[c] + qq[c] * s1;
+            }
+            img_store8(S.hd1, t, 16 * q, MLP_H, p1);
+            img_store8(S.hd1, t, 16 * q + 8, MLP_H, p1 + 8);
+            img_store8(S.h1, t, 16 * q, MLP_H, q1);
+            img_store8(S.h1, t, 16 * q + 8, MLP_H, q1 + 8);
+        }
+        __syncthreads();
+        // dW1 += g'^T P1 + g^T Q1, db1 += sum Q1
+        outer_acc(S.gd, S.hd1, S.g0, S.h1, MLP_D, half * 8, half * 8 + 8, col, grads + GRAD_W1);
+        if (half == 0) {
+            float acc = 0.0f;
+            for (int r = 0; r < MLP_TILE; ++r) acc += __bfloat162float(S.h1[img_off(r, col, MLP_H)]);
+            atomicAdd(&grads[GRAD_B1 + col], acc);
+        }
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+    if (failed && t == 0) atomicOr(status, SIM_STATUS_MLP_TIMEOUT);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" :: "r"(tm));
+}
+
 // Operand images and vectors from the FP32 master parameters (flat layout
 // W1 [16][64], b1, W2 [64][64], b2, w3, b3).
 __global__ void k_mlp_pack(const float* __restrict__ p, __nv_bfloat16* w1t, __nv_bfloat16* w2t, __nv_bfloat16* w2,
@@ -704,3 +1036,44 @@ extern "C" int sim_mlp_adam(float* params, const float* grads, float* m1, float*
     k_mlp_adam<<<8, 256, 0, (cudaStream_t)stream>>>(params, grads, m1, m2, SIM_MLP_PARAMS, lr, b1, b2, 1e-8f, c1, c2);
     return launch_status("sim_mlp_adam");
 }
+
+extern "C" int sim_mlp_force_contract(const SimEngine* e, const float* ferr, float* u, void* stream) {
+    if (!e || !ferr || !u || e->n <= 0) return SIM_ERR_ARG;
+    const int g = (int)((e->n + 127) / 128 < 148 * 16 ? (e->n + 127) / 128 : 148 * 16);
+    if (e->box_orthogonal) k_mlp_ucontract<true><<<g, 128, 0, (cudaStream_t)stream>>>(*e, ferr, u);
+    else k_mlp_ucontract<false><<<g, 128, 0, (cudaStream_t)stream>>>(*e, ferr, u);
+    return launch_status("sim_mlp_force_contract");
+}
+
+extern "C" int sim_mlp_train_grads_fm(const SimMLP* m, const float* G, const float* target, const float* u,
+                                      int64_t n, float w_energy, float w_force, int64_t n_force_atoms, float* grads,
+                                      float* loss, int32_t* status, void* stream) {
+    if (!mlp_ok(m) || !G || !target || !u || n <= 0 || n_force_atoms <= 0 || !grads || !loss || !status)
+        return SIM_ERR_ARG;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_mlp_train_fm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpFmSmem));
+        cudaGetLastError();
+        attr = true;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t err = cudaMemsetAsync(grads, 0, sizeof(float) * SIM_MLP_PARAMS, st);
+    if (err == cudaSuccess) err = cudaMemsetAsync(loss, 0, sizeof(float), st);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_mlp_train_grads_fm: zero"); return SIM_ERR_CUDA; }
+    // every resident block holds 256 tensor-memory columns: at most 2 per SM
+    int per_sm = 0, dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_train_fm, MLP_TILE, sizeof(MlpFmSmem)) !=
+            cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    if (per_sm > 2) per_sm = 2;
+    const int64_t tiles = (n + MLP_TILE - 1) / MLP_TILE;
+    const int g = (int)(tiles < (int64_t)per_sm * sms ? tiles : (int64_t)per_sm * sms);
+    const float alpha = 2.0f * w_energy / (float)n;
+    const float beta = -2.0f * w_force / (3.0f * (float)n_force_atoms);
+    k_mlp_train_fm<<<g, MLP_TILE, sizeof(MlpFmSmem), st>>>(*m, G, target, u, n, alpha, beta, 1.0f / (float)n, grads,
+                                                           loss, status);
+    return launch_status("sim_mlp_train_grads_fm");
+}
+

@@ -114,9 +114,22 @@ class MLPNet:
                   self._stream())
         return e, d
 
+    def forward_into(self, G: torch.Tensor, n: int, e: torch.Tensor, d: torch.Tensor):
+        """forward() into preallocated e [>=n] and d [>=n,16] (no allocation)."""
+        _lib.call("sim_mlp_forward", self.ref, _lib.ptr(G), int(n), _lib.ptr(e), _lib.ptr(d), _lib.ptr(self.status),
+                  self._stream())
+
     def train_grads(self, G: torch.Tensor, target: torch.Tensor, grads: torch.Tensor, loss: torch.Tensor):
         _lib.call("sim_mlp_train_grads", self.ref, _lib.ptr(G), _lib.ptr(target), int(target.numel()),
                   _lib.ptr(grads), _lib.ptr(loss), _lib.ptr(self.status), self._stream())
+
+    def train_grads_fm(self, G: torch.Tensor, target: torch.Tensor, u: torch.Tensor, n: int, w_energy: float,
+                       w_force: float, n_force_atoms: int, grads: torch.Tensor, loss: torch.Tensor):
+        """Gradient of w_energy * mean (E - target)^2 + the force-matching term
+        whose descriptor contraction is u [n,16] (see ``force_contract``)."""
+        _lib.call("sim_mlp_train_grads_fm", self.ref, _lib.ptr(G), _lib.ptr(target), _lib.ptr(u), int(n),
+                  float(w_energy), float(w_force), int(n_force_atoms), _lib.ptr(grads), _lib.ptr(loss),
+                  _lib.ptr(self.status), self._stream())
 
 
 def init_params(seed: int = 0) -> dict:
@@ -139,6 +152,14 @@ def mlp_forces(engine: MDEngine, dEdG: torch.Tensor):
     _lib.call("sim_mlp_forces", engine.st_ref, _lib.ptr(dEdG), engine.stream)
     engine._last_force_precision = 0
     engine.forces_valid = True
+
+
+def force_contract(engine: MDEngine, ferr: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """u [n_pad,16] with u_i = sum_m ferr_m . dG_i/dx_m, from per-slot force
+    errors ferr [n_pad,4] (x, y, z, unused)."""
+    u = out if out is not None else torch.zeros(engine.n_pad, N_DESC, device=engine.device, dtype=torch.float32)
+    _lib.call("sim_mlp_force_contract", engine.st_ref, _lib.ptr(ferr), _lib.ptr(u), engine.stream)
+    return u
 
 
 def eam_atom_energy(engine: MDEngine, tables) -> torch.Tensor:
@@ -266,6 +287,65 @@ def train(net: MLPNet, G: torch.Tensor, E: torch.Tensor, *, steps: int = 2000, b
     return losses
 
 
+class ForceFrame:
+    """One EAM reference configuration for force matching: an engine holding
+    its positions and neighbour list, the descriptors G [n_pad,16], per-atom
+    EAM energies E [n] and EAM forces F [n_pad,4], all in the engine's slot order."""
+
+    def __init__(self, x, H, tables, device=None):
+        eng = MDEngine(x, np.zeros(len(x), np.int32), [183.84], H, 4.4, 0.5, device=device)
+        eng.eam_forces(tables)
+        self.F = eng.f32.clone()
+        self.E = eam_atom_energy(eng, tables)[:eng.n].clone()
+        self.G = descriptors(eng)
+        self.engine = eng
+        if eng.status() & ~_lib.SIM_STATUS_MLP_NEIGHBORS:
+            raise RuntimeError(f"EAM reference frame failed (status {eng.status():#x})")
+
+
+def train_forces(net: MLPNet, frames, *, steps: int = 4000, lr: float = 1e-3, lr_final: float = 1e-4,
+                 w_energy: float = 1.0, w_force: float = 1.0, seed: int = 0, log_every: int = 0):
+    """Energy and force matching on ``ForceFrame`` s with Adam, one frame per
+    step: loss = w_energy mean_i (E_i - E_i^EAM)^2
+               + w_force sum_m |F_m - F_m^EAM|^2 / (3 n).
+    The network keeps its normalisation (train on energies first).  Returns
+    the per-step force mean squares (device tensor, (eV/A)^2)."""
+    dev = net.device
+    grads = torch.zeros(N_PARAMS, device=dev, dtype=torch.float32)
+    m1 = torch.zeros_like(grads)
+    m2 = torch.zeros_like(grads)
+    loss = torch.zeros(1, device=dev, dtype=torch.float32)
+    fmse = torch.zeros(steps, device=dev, dtype=torch.float32)
+    P = max(fr.engine.n_pad for fr in frames)
+    e = torch.zeros(P, device=dev, dtype=torch.float32)
+    d = torch.zeros(P, N_DESC, device=dev, dtype=torch.float32)
+    ferr = torch.zeros(P, 4, device=dev, dtype=torch.float32)
+    u = torch.zeros(P, N_DESC, device=dev, dtype=torch.float32)
+    order = np.random.default_rng(seed).permutation(steps) % len(frames)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    for s in range(steps):
+        fr = frames[int(order[s])]
+        eng = fr.engine
+        n, np_ = eng.n, eng.n_pad
+        net.forward_into(fr.G, n, e, d)
+        _lib.call("sim_mlp_forces", eng.st_ref, _lib.ptr(d), eng.stream)
+        fe = ferr[:np_]
+        torch.sub(eng.f32, fr.F, out=fe)
+        fmse[s] = fe[:n, :3].square().mean()
+        _lib.call("sim_mlp_force_contract", eng.st_ref, _lib.ptr(fe), _lib.ptr(u), eng.stream)
+        net.train_grads_fm(fr.G, fr.E, u, n, w_energy, w_force, n, grads, loss)
+        lr_s = lr * (lr_final / lr) ** (s / max(1, steps - 1))
+        _lib.call("sim_mlp_adam", _lib.ptr(net.flat), _lib.ptr(grads), _lib.ptr(m1), _lib.ptr(m2), float(lr_s),
+                  s + 1, st)
+        _lib.call("sim_mlp_pack", _lib.ptr(net.flat), *(_lib.ptr(t) for t in net.images), st)
+        if log_every and (s + 1) % log_every == 0:
+            print(f"step {s + 1}: force RMSE {math.sqrt(float(fmse[s + 1 - log_every:s + 1].mean())):.4f} eV/A, "
+                  f"energy loss {float(loss):.3e} eV^2", flush=True)
+    if int(net.status.item()):
+        raise RuntimeError(f"tensor-core wait timed out in training (status {int(net.status.item()):#x})")
+    return fmse
+
+
 def force_rmse(net: MLPNet, tables, frames, device=None) -> float:
     """RMSE of MLP forces against the recorded EAM forces of frames."""
     dev = torch.device(device or "cuda")
@@ -283,3 +363,142 @@ def force_rmse(net: MLPNet, tables, frames, device=None) -> float:
 
 def default_weights_path() -> str:
     return os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "w_surrogate.npz")
+
+
+class SurrogateRun:
+    """MD of one system with MLP forces, judged against EAM.
+
+    Every ``judge_every`` steps the EAM forces of the current positions are
+    compared with the MLP forces; when their RMSE exceeds ``tolerance``
+    (eV/A) the run continues with EAM forces.  Steps between judgements are
+    captured in a CUDA graph: first half-step and conditional rebuild,
+    descriptors, network, forces, second half-step (Langevin when the
+    integrator parameters say so)."""
+
+    def __init__(self, engine: MDEngine, net: MLPNet, tables, integ, *, judge_every: int = 100,
+                 tolerance: float = 0.05):
+        self.eng, self.net, self.tables, self.integ = engine, net, tables, integ
+        self.judge_every, self.tolerance = int(judge_every), float(tolerance)
+        n = engine.n
+        self.G = torch.zeros(engine.n_pad, N_DESC, device=engine.device, dtype=torch.float32)
+        self.e = torch.zeros(n, device=engine.device, dtype=torch.float32)
+        self.d = torch.zeros(n, N_DESC, device=engine.device, dtype=torch.float32)
+        self.use_mlp = True
+        self.rmse_history: list[float] = []
+        self._graph = None
+        self._mlp_forces()
+
+    def _mlp_forces(self):
+        eng = self.eng
+        _lib.call("sim_mlp_descriptors", eng.st_ref, _lib.ptr(self.G), eng.stream)
+        self.net.forward_into(self.G, eng.n, self.e, self.d)
+        _lib.call("sim_mlp_forces", eng.st_ref, _lib.ptr(self.d), eng.stream)
+
+    def _step(self):
+        eng = self.eng
+        eng.integrate_first(self.integ, 0)
+        eng.rebuild_if_needed()
+        if self.use_mlp:
+            self._mlp_forces()
+            eng.integrate_second(self.integ, 0)
+        else:
+            eng.eam_forces_integrate(self.tables, self.integ)
+
+    def judge(self) -> float:
+        """Force RMSE of MLP against EAM at the current positions (synchronises);
+        leaves the forces of the model in use in the engine."""
+        eng = self.eng
+        f_mlp = eng.gather("f")
+        eng.eam_forces(self.tables)
+        f_eam = eng.gather("f")
+        rmse = float(torch.sqrt(((f_mlp - f_eam) ** 2).mean()))
+        self.rmse_history.append(rmse)
+        if rmse > self.tolerance:
+            self.use_mlp = False
+            self._graph = None
+        else:
+            self._mlp_forces()
+        return rmse
+
+    def run(self, n_steps: int, judge: bool = True):
+        done = 0
+        while done < n_steps:
+            k = min(self.judge_every, n_steps - done)
+            if k == self.judge_every:
+                if self._graph is None:
+                    s = torch.cuda.Stream(self.eng.device)
+                    s.wait_stream(torch.cuda.current_stream(self.eng.device))
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g, stream=s):
+                        for _ in range(k):
+                            self._step()
+                    torch.cuda.current_stream(self.eng.device).wait_stream(s)
+                    self._graph = g
+                self._graph.replay()
+            else:
+                for _ in range(k):
+                    self._step()
+            done += k
+            if judge and self.use_mlp and k == self.judge_every:
+                self.judge()
+        return self
+
+
+def main(argv=None):
+    """Train the surrogate on the engine's EAM data and save its weights:
+    python -m simulon_b200.mlp POTENTIAL OUT.npz [--steps N] [--fm-steps M] ...
+    Energy regression on per-atom EAM energies first, then energy and force
+    matching on whole frames."""
+    import argparse
+    import time
+    from .eam_parser import EAMDeviceTables, EAMParser
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("potential")
+    ap.add_argument("out")
+    ap.add_argument("--steps", type=int, default=20000, help="energy-regression steps")
+    ap.add_argument("--frames", type=int, default=50, help="frames per (temperature, strain) run")
+    ap.add_argument("--cells", type=int, default=10)
+    ap.add_argument("--batch", type=int, default=16384)
+    ap.add_argument("--fm-steps", type=int, default=12000, help="force-matching steps (one frame each)")
+    ap.add_argument("--fm-cells", type=int, default=16)
+    ap.add_argument("--fm-frames", type=int, default=10, help="force-matching frames per (temperature, strain) run")
+    ap.add_argument("--w-force", type=float, default=1.0)
+    ap.add_argument("--lr-fm", type=float, default=1e-3)
+    a = ap.parse_args(argv)
+    dev = torch.device("cuda")
+    tables = EAMDeviceTables(EAMParser(a.potential), dev)
+    t0 = time.perf_counter()
+    G, E = generate_dataset(tables, n_cells=a.cells, frames_per_run=a.frames, seed=0, device=dev)
+    _, _, fm_raw = generate_dataset(tables, n_cells=a.fm_cells, frames_per_run=a.fm_frames, stride=20,
+                                    equilibrate=200, seed=7, device=dev, with_forces=True)
+    fm_frames = [ForceFrame(fr["x"], fr["H"], tables, dev) for fr in fm_raw]
+    del fm_raw
+    val = {}
+    for T, seed in ((300.0, 99), (1500.0, 98)):
+        _, _, raw = generate_dataset(tables, n_cells=a.cells, temperatures=(T,), strains=(0.0,), frames_per_run=2,
+                                     stride=40, equilibrate=200, seed=seed, device=dev, with_forces=True)
+        val[T] = raw
+    t1 = time.perf_counter()
+    net = MLPNet(dev, seed=0)
+    losses = train(net, G, E, steps=a.steps, batch=a.batch, log_every=max(1, a.steps // 10))
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    before = {T: force_rmse(net, tables, fr, dev) for T, fr in val.items()}
+    fmse = train_forces(net, fm_frames, steps=a.fm_steps, lr=a.lr_fm, w_force=a.w_force,
+                        log_every=max(1, a.fm_steps // 10)) if a.fm_steps else torch.zeros(1)
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    after = {T: force_rmse(net, tables, fr, dev) for T, fr in val.items()}
+    net.save(a.out)
+    print(f"energy samples {G.shape[0]}, force frames {len(fm_frames)} x {fm_frames[0].engine.n} atoms; "
+          f"data {t1 - t0:.1f} s, energy fit {t2 - t1:.1f} s, force fit {t3 - t2:.1f} s")
+    print(f"energy loss {float(losses[-100:].mean()):.3e} eV^2, force MSE (last 5%) "
+          f"{float(fmse[-max(1, len(fmse) // 20):].mean()):.3e} (eV/A)^2")
+    for T in val:
+        print(f"validation force RMSE at {T:.0f} K: {before[T]:.4f} (energy fit) -> {after[T]:.4f} eV/A")
+    print(f"-> {a.out}")
+
+
+if __name__ == "__main__":
+    main()
+

@@ -170,3 +170,127 @@ def test_training_reduces_energy_and_force_errors(sb, tables):
     assert last < 0.1 * first, (first, last)
     rmse = mlp.force_rmse(net, tables, frames, DEV)
     assert rmse < 0.5 * rmse0, (rmse0, rmse)
+
+
+def test_surrogate_run_judges_and_falls_back(sb, tables):
+    """The committed weights keep a 300 K run on the surrogate (force RMSE
+    against EAM below 0.05 eV/A at each judgement); an untrained network is
+    caught at the first judgement and the run continues on EAM."""
+    from simulon_b200 import mlp
+    from simulon_b200.engine import integrator_params
+    x, L = oin.bcc_lattice(8)
+    v = oin.maxwell_boltzmann(np.full(len(x), oin.W_MASS), 300.0, 8)
+    for weights, expect_mlp in ((mlp.default_weights_path(), True), (None, False)):
+        eng = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], np.diag([L] * 3), 4.4, 0.5, velocities=v,
+                          device=DEV)
+        net = mlp.MLPNet.load(weights, DEV) if weights else mlp.MLPNet(DEV, seed=0)
+        ip = integrator_params(eng, 0.002, langevin=True, temperature=300.0, gamma=10.0, seed=1)
+        run = mlp.SurrogateRun(eng, net, tables, ip, judge_every=100, tolerance=0.05).run(300)
+        torch.cuda.synchronize()
+        assert eng.status() == 0 and int(net.status.item()) == 0
+        assert run.use_mlp == expect_mlp, run.rmse_history
+        assert len(run.rmse_history) == (3 if expect_mlp else 1)
+        assert np.isfinite(eng.gather("x").cpu().numpy()).all()
+
+
+def test_force_contraction_matches_directional_derivative(sb):
+    """u_i = sum_m e_m . dG_i/dx_m against a central difference of the FP64
+    descriptors along e: 3e-4 of the largest component (FP32 exponentials)."""
+    from simulon_b200 import mlp
+    x, H, eng, pi, pj = _system(sb, n=4, seed=9, tri=False)
+    rng = np.random.default_rng(10)
+    e = rng.normal(0.0, 1.0, x.shape)
+    ferr = torch.zeros(eng.n_pad, 4, device=DEV)
+    slots = eng.orig[:eng.n].long().cpu()
+    ferr[:eng.n, :3] = torch.tensor(e[slots.numpy()], dtype=torch.float32, device=DEV)
+    u = _slots_to_orig(eng, mlp.force_contract(eng, ferr)).cpu().double().numpy()
+    h = 1e-5
+    box = OracleBox(H)
+    Gp = omlp.descriptors(torch.tensor(x + h * e), box, pi, pj).numpy()
+    Gm = omlp.descriptors(torch.tensor(x - h * e), box, pi, pj).numpy()
+    want = (Gp - Gm) / (2 * h)
+    assert np.abs(u - want).max() <= 3e-4 * np.abs(want).max(), np.abs(u - want).max()
+    assert eng.status() == 0
+
+
+def test_force_matching_gradients_match_double_backward(sb):
+    """Kernel gradient of J = w_E mean (E - t)^2 + beta sum_i dE_i/dG_i . u_i
+    (u fixed) against torch double-backward in FP32: 5% of each parameter
+    block's gradient norm (BF16 operands of six GEMMs and the outer products);
+    b3's gradient within 2 w_E x the 5e-3 energy tolerance."""
+    from simulon_b200 import mlp
+    n = 700
+    G = _random_rows(n, 11)
+    rng = np.random.default_rng(12)
+    u = torch.tensor(rng.normal(0.0, 1.0, (n, 16)), dtype=torch.float32, device=DEV) * G.std(0)
+    target = torch.tensor(rng.normal(-8.0, 0.3, n), dtype=torch.float32, device=DEV)
+    p = omlp.random_net(13, mu=G.mean(0).cpu().numpy(), sigma=G.std(0).cpu().numpy())
+    net = mlp.MLPNet(DEV, p)
+    grads = torch.zeros(mlp.N_PARAMS, device=DEV)
+    loss = torch.zeros(1, device=DEV)
+    w_e, w_f, n_f = 0.7, 1.3, 500
+    net.train_grads_fm(G, target, u, n, w_e, w_f, n_f, grads, loss)
+    torch.cuda.synchronize()
+    assert int(net.status.item()) == 0
+    leaves = {k: torch.tensor(np.asarray(p[k], np.float32), device=DEV, requires_grad=True)
+              for k in ("W1", "b1", "W2", "b2", "w3", "b3")}
+    ref = {k: torch.as_tensor(np.asarray(v, np.float32), device=DEV) for k, v in p.items()}
+    ref.update(leaves)
+    Gr = G.clone().requires_grad_(True)
+    E = omlp.atom_energies(Gr, ref)
+    (dEdG,) = torch.autograd.grad(E.sum(), Gr, create_graph=True)
+    beta = -2.0 * w_f / (3.0 * n_f)
+    J = w_e * ((E - target) ** 2).mean() + beta * (dEdG * u).sum()
+    J.backward()
+    mse = float(((E - target) ** 2).mean().detach())
+    assert abs(float(loss) - mse) <= 2e-3 * mse
+    for k, (o, shp) in mlp.OFF.items():
+        cnt = int(np.prod(shp)) if shp else 1
+        got = grads[o:o + cnt].cpu()
+        want = leaves[k].grad.reshape(-1).cpu()
+        if k == "b3":   # 2 w_E mean(E - t): a cancelling sum, bounded by the 5e-3 energy error
+            assert abs(float(got - want)) <= 2 * w_e * 5e-3, (float(got), float(want))
+            continue
+        assert float((got - want).norm()) <= 0.05 * float(want.norm()) + 1e-7, (k, float((got - want).norm()),
+                                                                                float(want.norm()))
+
+
+def test_force_loss_gradient_matches_oracle(sb):
+    """Whole force-matching chain (network, forces, contraction, gradient)
+    against autograd of sum |F - F_t|^2 / (3n) through the FP64 oracle
+    descriptors and network: 5% of each block's gradient norm."""
+    from simulon_b200 import mlp
+    x, H, eng, pi, pj = _system(sb, n=4, seed=14)
+    G = mlp.descriptors(eng)
+    Gn = G[:eng.n].double().cpu()
+    p = omlp.random_net(15, mu=Gn.mean(0).numpy(), sigma=Gn.std(0).numpy())
+    net = mlp.MLPNet(DEV, p)
+    rng = np.random.default_rng(16)
+    f_t = rng.normal(0.0, 0.5, x.shape)
+    F_slots = torch.zeros(eng.n_pad, 4, device=DEV)
+    slots = eng.orig[:eng.n].long().cpu().numpy()
+    F_slots[:eng.n, :3] = torch.tensor(f_t[slots], dtype=torch.float32, device=DEV)
+    e, d = net.forward(G, eng.n)
+    mlp.mlp_forces(eng, d)
+    ferr = eng.f32 - F_slots
+    u = mlp.force_contract(eng, ferr)
+    grads = torch.zeros(mlp.N_PARAMS, device=DEV)
+    loss = torch.zeros(1, device=DEV)
+    net.train_grads_fm(G, torch.zeros(eng.n, device=DEV), u, eng.n, 0.0, 1.0, eng.n, grads, loss)
+    torch.cuda.synchronize()
+    leaves = {k: torch.tensor(np.asarray(p[k]), dtype=torch.float64, requires_grad=True)
+              for k in ("W1", "b1", "W2", "b2", "w3", "b3")}
+    ref = {k: torch.as_tensor(np.asarray(v), dtype=torch.float64) for k, v in p.items()}
+    ref.update(leaves)
+    xt = torch.tensor(x, dtype=torch.float64, requires_grad=True)
+    Eo = omlp.atom_energies(omlp.descriptors(xt, OracleBox(H), pi, pj), ref)
+    (gx,) = torch.autograd.grad(Eo.sum(), xt, create_graph=True)
+    L = ((-gx - torch.tensor(f_t)) ** 2).sum() / (3 * len(x))
+    L.backward()
+    for k, (o, shp) in mlp.OFF.items():
+        cnt = int(np.prod(shp)) if shp else 1
+        got = grads[o:o + cnt].cpu().double()
+        g = leaves[k].grad   # None for b3: a constant shift moves no force
+        want = torch.zeros(cnt, dtype=torch.float64) if g is None else g.reshape(-1)
+        assert float((got - want).norm()) <= 0.05 * float(want.norm()) + 1e-9, (k, float((got - want).norm()),
+                                                                                float(want.norm()))
