@@ -417,7 +417,7 @@ def batched_form(args, sb, pot, dev, world, rank, barrier):
 
 
 def lj_form(args, sb, dev, world):
-    """LJ argon scaling point (SURVEY 8(d) item 2): FCC 4 n^3 atoms, a = 5.26 A,
+    """LJ argon scaling point: FCC 4 n^3 atoms, a = 5.26 A,
     eps 0.0104 eV, sigma 3.405 A, cutoff 7.0 A, skin 0.5 A, NVE from 94.4 K
     Maxwell-Boltzmann velocities, dt 2 fs; the FP32-pair / FP64-integration
     form and the FP64 form, each timed like the plain EAM line, with the force
@@ -492,7 +492,7 @@ def lj_form(args, sb, dev, world):
 
 
 def mlp_form(args, sb, pot, dev, world):
-    """MLP-surrogate form (SURVEY 8(d) item 5): the committed surrogate weights
+    """MLP-surrogate form: the committed surrogate weights
     (trained on the GPU by python -m simulon_b200.mlp on the engine's own EAM
     data), 1,024,000 W atoms NVT at 300 K (Langevin gamma 10/ps, dt 2 fs), EAM
     judging the force RMSE every 100 steps and taking over above 0.05 eV/A;

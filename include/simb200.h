@@ -127,6 +127,11 @@ typedef struct SimEngine {
      * cut_mask[i] for slot k of atom i) and pass 2 visits only those; needs
      * nbr_cap <= 64.  NULL: pass 2 tests every slot itself.                      */
     uint64_t* cut_mask;   /* [n_pad] or NULL */
+    /* launch shapes (0: built-in default), as picked by sim_autotune_*:
+     * [0] EAM pass-1 threads per block (128, 256, 512), [1] EAM pass-2 threads
+     * per block (256, 512, 1024), [2] / [3] threads per atom of the MLP
+     * descriptor / force kernels (4, 8).                                        */
+    int32_t launch[4];
 } SimEngine;
 
 /* reduction slot layout (FP64 Kahan-compensated sums over all atoms) */
@@ -324,6 +329,12 @@ int sim_integrate_first(const SimEngine* e, const SimIntegrator* p, int32_t forc
 int sim_integrate_second(const SimEngine* e, const SimIntegrator* p, int32_t force_precision,
                          void* stream);
 
+/* second_half of step s and first_half of step s+1 with the same forces, in
+ * one pass (for force fields that cannot finish the step inside their own
+ * kernel); advances step_ctr like sim_eam_force_integrate_drift. */
+int sim_integrate_second_first(const SimEngine* e, const SimIntegrator* p, int32_t force_precision,
+                               void* stream);
+
 /* Berendsen: reads red_out (K tensor, W tensor) and the device box, computes
  * P (bar) and mu on the device in FP64, scales box, coordinates (mu^power),
  * velocities; writes pressure_out[0] = P (bar), pressure_out[1] = mu. */
@@ -473,7 +484,7 @@ int sim_mlp_descriptors(const SimEngine* e, float* G, void* stream);
 int sim_mlp_forward(const SimMLP* m, const float* G, int64_t n, float* e_atom, float* dEdG, int32_t* status,
                     void* stream);
 /* Forces -dE/dx into e->f32 (overwritten) from dE/dG of every slot. */
-int sim_mlp_forces(const SimEngine* e, const float* dEdG, void* stream);
+int sim_mlp_backward(const SimEngine* e, const float* dEdG, void* stream);
 /* Training: gradient of mean_i (E_i - target_i)^2 over n rows with respect to
  * every parameter into grads [SIM_MLP_PARAMS] (overwritten), loss into *loss. */
 int sim_mlp_train_grads(const SimMLP* m, const float* G, const float* target, int64_t n, float* grads,
@@ -494,9 +505,37 @@ int sim_mlp_pack(const float* params, uint16_t* w1t_img, uint16_t* w2t_img, uint
                  void* stream);
 /* One Adam step (beta 0.9 / 0.999, eps 1e-8) on the parameter array; step >= 1. */
 int sim_mlp_adam(float* params, const float* grads, float* m1, float* m2, float lr, int32_t step, void* stream);
+/* One training step on the parameter array params [SIM_MLP_PARAMS] (the
+ * array m's vectors point into; the four images are m's, rewritten): the
+ * gradient (u NULL: sim_mlp_train_grads, energy term only, w_energy and
+ * w_force unused; else sim_mlp_train_grads_fm), one Adam step with moments
+ * adam_m, adam_v, and sim_mlp_pack. */
+int sim_mlp_train_step(const SimMLP* m, float* params, uint16_t* w1t_img, uint16_t* w2t_img, uint16_t* w2_img,
+                       uint16_t* w1_img, const float* G, const float* target, const float* u, int64_t n,
+                       float w_energy, float w_force, int64_t n_force_atoms, float* grads, float* adam_m,
+                       float* adam_v, float lr, int32_t step, float* loss, int32_t* status, void* stream);
 /* Per-atom EAM energies F(rho_i) + 1/2 sum_j phi(r_ij) of every slot (one
  * element type): the surrogate's training targets. */
 int sim_eam_atom_energy(const SimEngine* e, const SimEAMTables* t, float* e_atom, void* stream);
+
+/* ---- group 5: launch-shape autotuning (SimEngine.launch) ------------------
+ * Each call times every candidate shape of its kernels on the engine's
+ * current state with CUDA events (reps launches after one untimed launch;
+ * synchronises the stream, so never while a stream is being captured) and
+ * returns the mean milliseconds and the fastest shapes; the caller stores
+ * them in SimEngine.launch.  No counterpart in the reference (whose kernels
+ * have fixed launch shapes).
+ * sim_autotune_eam: ms[0..2] pass 1 at 128/256/512 threads, ms[3..5] pass 2
+ *   (forces, energy, virial; no integrator epilogue) at 256/512/1024;
+ *   best[0] = pass-1 threads, best[1] = pass-2 threads.  Rewrites the
+ *   engine's posfp, cut_mask, f32 and red_out (as sim_eam_forces does).
+ * sim_autotune_mlp: ms[0..1] descriptors at 4/8 threads per atom, ms[2..3]
+ *   forces from dEdG at 4/8; best[0] / best[1] = descriptor / force threads
+ *   per atom.  Rewrites G [n_pad][16] and the engine's f32.               */
+int sim_autotune_eam(const SimEngine* e, const SimEAMTables* t, int32_t reps, float* ms, int32_t* best,
+                     void* stream);
+int sim_autotune_mlp(const SimEngine* e, const float* dEdG, float* G, int32_t reps, float* ms, int32_t* best,
+                     void* stream);
 
 /* Message for the last CUDA error seen by this library (host string). */
 const char* sim_last_cuda_error(void);

@@ -53,7 +53,8 @@ class SimEngine(ctypes.Structure):
                 ("flags", c_p), ("partials", c_p), ("red_counter", c_p), ("red_out", c_p),
                 ("n_blocks_max", ctypes.c_int32), ("box_orthogonal", ctypes.c_int32),
                 ("n_tiles", ctypes.c_int32), ("halo_cap", ctypes.c_int32),
-                ("halo", c_p), ("halo_n", c_p), ("nbr16", c_p), ("cut_mask", c_p)]
+                ("halo", c_p), ("halo_n", c_p), ("nbr16", c_p), ("cut_mask", c_p),
+                ("launch", ctypes.c_int32 * 4)]
 
 
 class SimEAMTables(ctypes.Structure):
@@ -127,6 +128,7 @@ SIGNATURES = {
     "sim_lj_forces": [_P(SimEngine), _P(SimLJParams), ctypes.c_int32, c_p],
     "sim_integrate_first": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_integrate_second": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
+    "sim_integrate_second_first": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_berendsen": [_P(SimEngine), _P(SimBerendsen), c_p, c_p],
     "sim_gather_original_f64": [_P(SimEngine), c_p, c_p, c_p],
     "sim_gather_original_f32": [_P(SimEngine), c_p, c_p, c_p],
@@ -148,12 +150,17 @@ SIGNATURES = {
     "sim_batch_gather_f32": [_P(SimBatch), c_p, c_p, c_p],
     "sim_mlp_descriptors": [_P(SimEngine), c_p, c_p],
     "sim_mlp_forward": [_P(SimMLP), c_p, ctypes.c_int64, c_p, c_p, c_p, c_p],
-    "sim_mlp_forces": [_P(SimEngine), c_p, c_p],
+    "sim_mlp_backward": [_P(SimEngine), c_p, c_p],
     "sim_mlp_train_grads": [_P(SimMLP), c_p, c_p, ctypes.c_int64, c_p, c_p, c_p, c_p],
     "sim_mlp_force_contract": [_P(SimEngine), c_p, c_p, c_p],
     "sim_mlp_train_grads_fm": [_P(SimMLP), c_p, c_p, c_p, ctypes.c_int64, ctypes.c_float, ctypes.c_float,
                                ctypes.c_int64, c_p, c_p, c_p, c_p],
+    "sim_mlp_train_step": [_P(SimMLP), c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p, ctypes.c_int64, ctypes.c_float,
+                           ctypes.c_float, ctypes.c_int64, c_p, c_p, c_p, ctypes.c_float, ctypes.c_int32, c_p, c_p,
+                           c_p],
     "sim_mlp_pack": [c_p, c_p, c_p, c_p, c_p, c_p],
+    "sim_autotune_eam": [_P(SimEngine), _P(SimEAMTables), ctypes.c_int32, c_p, c_p, c_p],
+    "sim_autotune_mlp": [_P(SimEngine), c_p, c_p, ctypes.c_int32, c_p, c_p, c_p],
     "sim_mlp_adam": [c_p, c_p, c_p, c_p, ctypes.c_float, ctypes.c_int32, c_p],
     "sim_eam_atom_energy": [_P(SimEngine), _P(SimEAMTables), c_p, c_p],
     "sim_last_cuda_error": [],

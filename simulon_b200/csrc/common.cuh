@@ -27,6 +27,25 @@ int launch_eam_force_tiled(const SimEngine& e, const SimEAMTables& t, const SimI
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Mean duration in ms of reps calls of launch() on stream st, after one
+// untimed call (CUDA events on st; synchronises); negative on a CUDA error.
+template <class F>
+inline float time_launches(F launch, int reps, cudaStream_t st) {
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess) return -1.0f;
+    if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return -1.0f; }
+    launch();
+    cudaEventRecord(a, st);
+    for (int r = 0; r < reps; ++r) launch();
+    cudaEventRecord(b, st);
+    float ms = -1.0f;
+    if (cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) == cudaSuccess) ms /= (float)reps;
+    else ms = -1.0f;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms;
+}
+
 // ---- fixed-point fractional coordinates -----------------------------------
 // u = frac(s) * 2^32 stored as uint32; the difference of two codes read as
 // int32 is the minimum-image fractional displacement in [-1/2, 1/2).
@@ -122,8 +141,11 @@ __device__ __forceinline__ void block_partials(double (&vals)[NV], double* parti
 }
 
 // The last block to finish sums all partial rows for slots [slot0, slot0+NV)
-// with Kahan compensation in block order and resets the counter (so a
-// captured graph can replay).  Must be called by every thread of every block.
+// and resets the counter (so a captured graph can replay).  Warp k sums slot
+// k: lane l adds rows l, l+32, ... with Kahan compensation, then the 32
+// compensated sums combine in a fixed tree (TwoSum of the sums, the
+// compensations added): the order depends only on the grid size.  Must be
+// called by every thread of every block (blockDim.x a multiple of 32).
 template <int NV>
 __device__ __forceinline__ bool last_block_finalize(double* partials, uint32_t* counter,
                                                     double* out, int slot0) {
@@ -137,15 +159,25 @@ __device__ __forceinline__ bool last_block_finalize(double* partials, uint32_t* 
     __syncthreads();
     if (!is_last) return false;
     __threadfence();
-    if (threadIdx.x < NV) {
-        double s = 0.0, c = 0.0;
-        for (unsigned b = 0; b < gridDim.x; ++b) {
-            double y = __ldcg(&partials[(size_t)b * SIM_RED_SLOTS + slot0 + threadIdx.x]) - c;
-            double t = s + y;
+    const int lane = threadIdx.x & 31, nw = (int)(blockDim.x >> 5);
+    for (int k = (int)(threadIdx.x >> 5); k < NV; k += nw) {
+        double s = 0.0, c = 0.0;   // value s - c
+        for (unsigned b = lane; b < gridDim.x; b += 32) {
+            const double y = __ldcg(&partials[(size_t)b * SIM_RED_SLOTS + slot0 + k]) - c;
+            const double t = s + y;
             c = (t - s) - y;
             s = t;
         }
-        out[slot0 + threadIdx.x] = s;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double s2 = __shfl_down_sync(0xffffffffu, s, o);
+            const double c2 = __shfl_down_sync(0xffffffffu, c, o);
+            const double t = s + s2, bp = t - s;
+            const double err = (s - (t - bp)) + (s2 - bp);   // s + s2 = t + err exactly
+            c = c + c2 - err;
+            s = t;
+        }
+        if (lane == 0) out[slot0 + k] = s - c;
     }
     if (threadIdx.x == 0) *counter = 0u;
     return true;

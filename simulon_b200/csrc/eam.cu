@@ -296,11 +296,24 @@ static bool valid_tables(const SimEAMTables& t) {
            t.rho_clamp_hi && t.dens_vd && t.deriv_vd && t.pair_vd;
 }
 
+// launch[0] / launch[1] choose the threads per block of pass 1 / pass 2
+// (within each kernel's launch bound; 0: the built-in shape)
+static int density_threads(const SimEngine& e) {
+    const int t = e.launch[0];
+    return t == 0 ? EAM_DENSITY_THREADS : (t == 128 || t == 256 || t == 512) && t <= EAM_DENSITY_THREADS ? t : -1;
+}
+static int force_threads(const SimEngine& e) {
+    const int t = e.launch[1];
+    return t == 0 ? EAM_FORCE_THREADS : (t == 256 || t == 512 || t == 1024) && t <= EAM_FORCE_THREADS ? t : -1;
+}
+
 template <bool SMEM, bool ORTHO>
 static int launch_density(const SimEngine& e, const SimEAMTables& t, size_t smem, cudaStream_t st) {
-    const int g = persistent_grid((const void*)k_eam_density<SMEM, ORTHO>, EAM_DENSITY_THREADS, smem, e.n);
+    const int threads = density_threads(e);
+    if (threads < 0) return SIM_ERR_ARG;
+    const int g = persistent_grid((const void*)k_eam_density<SMEM, ORTHO>, threads, smem, e.n);
     if (g > e.n_blocks_max) return SIM_ERR_ARG;
-    k_eam_density<SMEM, ORTHO><<<g, EAM_DENSITY_THREADS, smem, st>>>(e, t, table_window(t));
+    k_eam_density<SMEM, ORTHO><<<g, threads, smem, st>>>(e, t, table_window(t));
     return SIM_OK;
 }
 
@@ -325,9 +338,11 @@ extern "C" int sim_eam_density(const SimEngine* ep, const SimEAMTables* tp, void
 template <bool SINGLE, int INTEG, bool ORTHO>
 static int launch_force(const SimEngine& e, const SimEAMTables& t, const SimIntegrator& ip, cudaStream_t st) {
     const size_t smem = SINGLE ? smem_pass2(t) : 0;
-    const int g = persistent_grid((const void*)k_eam_force<SINGLE, INTEG, ORTHO>, EAM_FORCE_THREADS, smem, e.n);
+    const int threads = force_threads(e);
+    if (threads < 0) return SIM_ERR_ARG;
+    const int g = persistent_grid((const void*)k_eam_force<SINGLE, INTEG, ORTHO>, threads, smem, e.n);
     if (g > e.n_blocks_max) return SIM_ERR_ARG;
-    k_eam_force<SINGLE, INTEG, ORTHO><<<g, EAM_FORCE_THREADS, smem, st>>>(e, t, ip, table_window(t));
+    k_eam_force<SINGLE, INTEG, ORTHO><<<g, threads, smem, st>>>(e, t, ip, table_window(t));
     return SIM_OK;
 }
 
@@ -382,3 +397,39 @@ extern "C" int sim_eam_forces(const SimEngine* ep, const SimEAMTables* tp, void*
     if (rc != SIM_OK) return rc;
     return sim_eam_force(ep, tp, stream);
 }
+
+extern "C" int sim_autotune_eam(const SimEngine* ep, const SimEAMTables* tp, int32_t reps, float* ms, int32_t* best,
+                                void* stream) {
+    if (!ep || !tp || !ms || !best || reps < 1 || ep->n <= 0) return SIM_ERR_ARG;
+    if (tiled_eam_usable(*ep, *tp)) {
+        set_error_text("sim_autotune_eam: the neighbour-tile kernels have fixed shapes");
+        return SIM_ERR_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    SimEngine e = *ep;
+    const int d_cand[3] = {128, 256, 512}, f_cand[3] = {256, 512, 1024};
+    for (int k = 0; k < 3; ++k) {
+        e.launch[0] = d_cand[k];
+        int rc = SIM_OK;
+        ms[k] = time_launches([&] { if (rc == SIM_OK) rc = sim_eam_density(&e, tp, stream); }, reps, st);
+        if (rc != SIM_OK) return rc;
+    }
+    e.launch[0] = ep->launch[0];
+    for (int k = 0; k < 3; ++k) {
+        e.launch[1] = f_cand[k];
+        int rc = SIM_OK;
+        ms[3 + k] = time_launches([&] { if (rc == SIM_OK) rc = sim_eam_force(&e, tp, stream); }, reps, st);
+        if (rc != SIM_OK) return rc;
+    }
+    for (int k = 0; k < 6; ++k)
+        if (ms[k] < 0.0f) return SIM_ERR_CUDA;
+    int bd = 0, bf = 0;
+    for (int k = 1; k < 3; ++k) {
+        if (ms[k] < ms[bd]) bd = k;
+        if (ms[3 + k] < ms[3 + bf]) bf = k;
+    }
+    best[0] = d_cand[bd];
+    best[1] = f_cand[bf];
+    return SIM_OK;
+}
+

@@ -81,28 +81,59 @@ __global__ void __launch_bounds__(SIM_THREADS) k_first_half(SimEngine e, SimInte
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
 }
 
+__device__ __forceinline__ void ke_terms(double m, const double* v, double* vals) {
+    const double hm = 0.5 * m;
+    vals[0] += hm * v[0] * v[0] + hm * v[1] * v[1] + hm * v[2] * v[2];
+    vals[1] += m * v[0] * v[0];
+    vals[2] += m * v[1] * v[1];
+    vals[3] += m * v[2] * v[2];
+    vals[4] += m * v[0] * v[1];
+    vals[5] += m * v[0] * v[2];
+    vals[6] += m * v[1] * v[2];
+}
+
+// Second half of the step (grid-stride over the atoms): kick, Langevin O-step,
+// kinetic energy and tensor.
 __global__ void __launch_bounds__(SIM_THREADS) k_second_half(SimEngine e, SimIntegrator p, int prec) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     double vals[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (i < e.n) {
+    bool bad = false;
+    const uint64_t step = *p.step_ctr;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
         const int type = e.posq[4 * i + 3];
-        const double m = e.mass[type];
         double v[3];
-        bool bad = false;
-        second_half_atom(e, p, i, type, *p.step_ctr, load_force(e, prec, i, 0), load_force(e, prec, i, 1),
+        second_half_atom(e, p, i, type, step, load_force(e, prec, i, 0), load_force(e, prec, i, 1),
                          load_force(e, prec, i, 2), v, bad);
-        const double hm = 0.5 * m;
-        vals[0] = hm * v[0] * v[0] + hm * v[1] * v[1] + hm * v[2] * v[2];
-        vals[1] = m * v[0] * v[0];
-        vals[2] = m * v[1] * v[1];
-        vals[3] = m * v[2] * v[2];
-        vals[4] = m * v[0] * v[1];
-        vals[5] = m * v[0] * v[2];
-        vals[6] = m * v[1] * v[2];
-        if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+        ke_terms(e.mass[type], v, vals);
     }
+    if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
     block_partials<7>(vals, e.partials, SIM_RED_KE);
     last_block_finalize<7>(e.partials, e.red_counter + 2, e.red_out, SIM_RED_KE);
+}
+
+// Second half of step s and first half of step s+1 with the same forces (for
+// force fields whose kernel cannot finish the step itself, e.g. one that
+// scatters forces with atomics): kinetic terms of step s, then kick, drift,
+// posq refresh and the skin/2 trigger; the last block advances the step
+// counter (step_ctr[0] = s + 1, step_ctr[1] = s for the step log).
+__global__ void __launch_bounds__(SIM_THREADS) k_second_first(SimEngine e, SimIntegrator p, int prec) {
+    double vals[7] = {0, 0, 0, 0, 0, 0, 0};
+    bool bad = false, trig = false;
+    const uint64_t step = *p.step_ctr;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int type = e.posq[4 * i + 3];
+        const double f[3] = {load_force(e, prec, i, 0), load_force(e, prec, i, 1), load_force(e, prec, i, 2)};
+        double v[3];
+        second_half_atom(e, p, i, type, step, f[0], f[1], f[2], v, bad, false);
+        ke_terms(e.mass[type], v, vals);
+        trig |= first_half_atom(e, p, i, type, f, v, bad);
+    }
+    if (__any_sync(0xffffffffu, trig) && (threadIdx.x & 31) == 0) e.flags[0] = 1;
+    if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+    block_partials<7>(vals, e.partials, SIM_RED_KE);
+    if (last_block_finalize<7>(e.partials, e.red_counter + 2, e.red_out, SIM_RED_KE) && threadIdx.x == 0) {
+        p.step_ctr[1] = step;
+        p.step_ctr[0] = step + 1;
+    }
 }
 
 // ---- Berendsen -------------------------------------------------------------
@@ -244,10 +275,20 @@ extern "C" int sim_integrate_first(const SimEngine* ep, const SimIntegrator* p, 
 extern "C" int sim_integrate_second(const SimEngine* ep, const SimIntegrator* p, int32_t force_precision, void* stream) {
     if (!ep || !p || ep->n <= 0 || (force_precision == 1 && !ep->f64)) return SIM_ERR_ARG;
     if (p->langevin && !p->rff) return SIM_ERR_ARG;
-    const int blocks = (int)ceil_div(ep->n, SIM_THREADS);
-    if (blocks > ep->n_blocks_max) return SIM_ERR_ARG;
+    int blocks = persistent_grid((const void*)k_second_half, SIM_THREADS, 0, ep->n);
+    if (blocks > ep->n_blocks_max) blocks = (int)ep->n_blocks_max;
     k_second_half<<<blocks, SIM_THREADS, 0, (cudaStream_t)stream>>>(*ep, *p, force_precision);
     return launch_status("sim_integrate_second");
+}
+
+extern "C" int sim_integrate_second_first(const SimEngine* ep, const SimIntegrator* p, int32_t force_precision,
+                                          void* stream) {
+    if (!ep || !p || ep->n <= 0 || !p->step_ctr || (force_precision == 1 && !ep->f64)) return SIM_ERR_ARG;
+    if (p->langevin && !p->rff) return SIM_ERR_ARG;
+    int blocks = persistent_grid((const void*)k_second_first, SIM_THREADS, 0, ep->n);
+    if (blocks > ep->n_blocks_max) blocks = (int)ep->n_blocks_max;
+    k_second_first<<<blocks, SIM_THREADS, 0, (cudaStream_t)stream>>>(*ep, *p, force_precision);
+    return launch_status("sim_integrate_second_first");
 }
 
 extern "C" int sim_berendsen(const SimEngine* ep, const SimBerendsen* p, double* pressure_out, void* stream) {

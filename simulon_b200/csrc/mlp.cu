@@ -52,150 +52,228 @@ __device__ __forceinline__ void mlp_dvec(const BoxF& b, const int4& qi, const in
     rvec<ORTHO>(b, qj, qi, d0, d1, d2);
 }
 
-// In-cutoff neighbours of slot i as {d, r}; returns the count (capped).
-template <bool ORTHO>
-__device__ __forceinline__ int mlp_neighbours(const SimEngine& e, const BoxF& b, int64_t i, float4* nb, bool& over) {
+// Descriptor and force kernels: GRP threads per atom (4 or 8), 128 / GRP
+// atoms per 128-thread block.  The group first gathers the atom's in-cutoff list
+// entries into a shared-memory table (entry-major, so the eight atoms of a
+// warp read eight consecutive elements), then splits the pair loops by the
+// first neighbour a (a = sub, sub + 4, ...).
+#define MLP_APB_MAX 32
+
+template <int APB>
+struct MlpTableU {
+    float4 u[MLP_MAXN][APB];     // unit vector d/r, e(r)
+};
+template <int APB>
+struct MlpTable {
+    float4 u[MLP_MAXN][APB];     // unit vector d/r, e(r)
+    float2 w[MLP_MAXN][APB];     // e'(r), e(r)/r                      (forces)
+    int32_t j[MLP_MAXN][APB];    // neighbour slot                      (forces)
+    float srad[MLP_MAXN][APB];   // sum_k dE/dG_k dphi_k/dr (radial)    (forces)
+};
+
+// Fills the table of local atom g (slot i) and returns the in-cutoff count
+// (capped at MLP_MAXN; more sets `over`).  FORCE: radial derivative sums
+// from dE/dG (gr[0..7]); otherwise the radial descriptors are added to
+// rad[0..7] (this lane's share of the atom's neighbours).
+template <bool ORTHO, bool FORCE, int GRP, class Table>
+__device__ __forceinline__ int mlp_table(const SimEngine& e, const BoxF& b, int64_t i, bool live, int g, int sub,
+                                         Table& T, const float* gr, float* rad, bool& over) {
+    const int lane = threadIdx.x & 31;
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
-    const int4 qi = posq[i];
-    const int nn = e.nnbr[i];
+    const int4 qi = live ? posq[i] : make_int4(0, 0, 0, 0);
+    const int nn = live ? e.nnbr[i] : 0;
+    const int nn_max = __reduce_max_sync(0xffffffffu, nn);
     int cnt = 0;
-    for (int k = 0; k < nn; ++k) {
-        const int4 qj = __ldg(&posq[__ldg(&e.nbr[(int64_t)k * e.n_pad + i])]);
-        float d0, d1, d2;
-        mlp_dvec<ORTHO>(b, qi, qj, d0, d1, d2);
-        const float r2 = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
-        if (!(r2 < MLP_RC * MLP_RC)) continue;
-        if (cnt == MLP_MAXN) { over = true; continue; }
-        nb[cnt++] = make_float4(d0, d1, d2, sqrtf(r2));
+    for (int k0 = 0; k0 < nn_max; k0 += GRP) {
+        const int k = k0 + sub;
+        bool inside = false;
+        float d0 = 0.f, d1 = 0.f, d2 = 0.f, r2 = 0.f;
+        int j = 0;
+        if (k < nn) {
+            j = __ldg(&e.nbr[(int64_t)k * e.n_pad + i]);
+            const int4 qj = __ldg(&posq[j]);
+            mlp_dvec<ORTHO>(b, qi, qj, d0, d1, d2);
+            r2 = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+            inside = r2 < MLP_RC * MLP_RC;
+        }
+        const unsigned grp = (__ballot_sync(0xffffffffu, inside) >> (lane & ~(GRP - 1))) & ((1u << GRP) - 1u);
+        const int pos = cnt + __popc(grp & ((1u << sub) - 1u));
+        if (inside) {
+            if (pos < MLP_MAXN) {
+                const float r = sqrtf(r2), ir = 1.0f / r;
+                const float fc = mlp_fc(r), ex = __expf(-0.01f * r2), ev = ex * fc;
+                T.u[pos][g] = make_float4(d0 * ir, d1 * ir, d2 * ir, ev);
+                // exp(-4 (r - R_k)^2) by the recurrence over k (R_k = 2 + k h):
+                // x_{k+1} = x_k exp(8 h t0) exp(-4 h^2 (2k + 1)), t0 = r - 2
+                const float step[8] = {0.6248747f, 0.24399385f, 0.09527189f, 0.037200667f,
+                                       0.014525686f, 0.005671822f, 0.0022146674f, 0.0008647577f};
+                const float t0 = r - 2.0f, q8 = __expf(2.7428572f * t0);
+                float gk = __expf(-4.0f * t0 * t0);
+                if constexpr (FORCE) {
+                    const float dfc = mlp_dfc(r);
+                    T.w[pos][g] = make_float2(ex * fmaf(-0.02f * r, fc, dfc), ev * ir);
+                    T.j[pos][g] = j;
+                    float sr = 0.0f;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const float t = fmaf(-0.34285715f, (float)q, t0);
+                        sr = fmaf(gr[q], gk * fmaf(-8.0f * t, fc, dfc), sr);
+                        gk *= q8 * step[q];
+                    }
+                    T.srad[pos][g] = sr;
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        rad[q] = fmaf(gk, fc, rad[q]);
+                        gk *= q8 * step[q];
+                    }
+                }
+            } else {
+                over = true;
+            }
+        }
+        cnt += __popc(grp);
     }
-    return cnt;
+    __syncwarp();
+    return cnt < MLP_MAXN ? cnt : MLP_MAXN;
 }
 
-template <bool ORTHO>
+template <int GRP>
+__device__ __forceinline__ float grp_sum(float v) {
+#pragma unroll
+    for (int o = 1; o < GRP; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <bool ORTHO, int GRP>
 __global__ void __launch_bounds__(128) k_mlp_desc(SimEngine e, float* __restrict__ G) {
+    constexpr int APB = 128 / GRP;
+    __shared__ MlpTableU<APB> T;
     const BoxF b(*e.box);
+    const int g = threadIdx.x / GRP, sub = threadIdx.x % GRP;
     bool over = false;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
-        float4 nb[MLP_MAXN];
-        float ea[MLP_MAXN];
-        const int cnt = mlp_neighbours<ORTHO>(e, b, i, nb, over);
-        float g[MLP_D];
+    for (int64_t base = blockIdx.x * (int64_t)APB; base < e.n; base += (int64_t)gridDim.x * APB) {
+        const int64_t i = base + g;
+        const bool live = i < e.n;
+        float d[MLP_D];
 #pragma unroll
-        for (int k = 0; k < MLP_D; ++k) g[k] = 0.0f;
-        for (int a = 0; a < cnt; ++a) {
-            const float r = nb[a].w, fc = mlp_fc(r);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const float t = r - mlp_rs(k);
-                g[k] = fmaf(__expf(-4.0f * t * t), fc, g[k]);
-            }
-            ea[a] = __expf(-0.01f * r * r) * fc;
-        }
-        for (int a = 0; a < cnt; ++a) {
-            const float4 da = nb[a];
+        for (int q = 0; q < MLP_D; ++q) d[q] = 0.0f;
+        const int cnt = mlp_table<ORTHO, false, GRP>(e, b, i, live, g, sub, T, nullptr, d, over);
+        // angular: raw powers (1 +- c)^z summed over a < c; the 2^(1-z) after the
+        // reduction.  Lane sub takes a = sub and 2 GRP - 1 - sub of every block of
+        // 2 GRP (a long and a short row of the triangle: the lanes' pair counts balance)
+        for (int k = 0; k < 2 * ((cnt + 2 * GRP - 1) / (2 * GRP)); ++k) {
+            const int a = (k >> 1) * 2 * GRP + ((k & 1) ? 2 * GRP - 1 - sub : sub);
+            if (a >= cnt) continue;
+            const float4 ua = T.u[a][g];
             for (int c = a + 1; c < cnt; ++c) {
-                const float4 dc = nb[c];
-                const float cs = (da.x * dc.x + da.y * dc.y + da.z * dc.z) / (da.w * dc.w);
-                const float rad = ea[a] * ea[c];
+                const float4 uc = T.u[c][g];
+                const float cs = fmaf(ua.z, uc.z, fmaf(ua.y, uc.y, ua.x * uc.x));
+                const float rad = ua.w * uc.w;
                 const float p1 = 1.0f + cs, m1 = 1.0f - cs;
-                const float p2 = p1 * p1, m2 = m1 * m1, p4 = p2 * p2, m4 = m2 * m2, p8 = p4 * p4, m8 = m4 * m4;
-                g[8] = fmaf(p1, rad, g[8]);
-                g[9] = fmaf(m1, rad, g[9]);
-                g[10] = fmaf(0.5f * p2, rad, g[10]);
-                g[11] = fmaf(0.5f * m2, rad, g[11]);
-                g[12] = fmaf(0.125f * p4, rad, g[12]);
-                g[13] = fmaf(0.125f * m4, rad, g[13]);
-                g[14] = fmaf(0.0078125f * p8, rad, g[14]);
-                g[15] = fmaf(0.0078125f * m8, rad, g[15]);
+                const float p2 = p1 * p1, m2 = m1 * m1, p4 = p2 * p2, m4 = m2 * m2;
+                d[8] = fmaf(p1, rad, d[8]);
+                d[9] = fmaf(m1, rad, d[9]);
+                d[10] = fmaf(p2, rad, d[10]);
+                d[11] = fmaf(m2, rad, d[11]);
+                d[12] = fmaf(p4, rad, d[12]);
+                d[13] = fmaf(m4, rad, d[13]);
+                d[14] = fmaf(p4 * p4, rad, d[14]);
+                d[15] = fmaf(m4 * m4, rad, d[15]);
             }
         }
-        float4* out = reinterpret_cast<float4*>(G + i * MLP_D);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) out[q] = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
+        for (int q = 0; q < MLP_D; ++q) d[q] = grp_sum<GRP>(d[q]);
+        d[10] *= 0.5f; d[11] *= 0.5f; d[12] *= 0.125f; d[13] *= 0.125f; d[14] *= 0.0078125f; d[15] *= 0.0078125f;
+        if (live && sub < 4) {   // lane sub writes float4 number sub of the row
+            float4 v = make_float4(d[0], d[1], d[2], d[3]);
+#pragma unroll
+            for (int q = 1; q < 4; ++q)
+                if (q == sub) v = make_float4(d[4 * q], d[4 * q + 1], d[4 * q + 2], d[4 * q + 3]);
+            reinterpret_cast<float4*>(G + i * MLP_D)[sub] = v;
+        }
+        __syncwarp();
     }
     if (over) atomicOr(&e.flags[1], SIM_STATUS_MLP_NEIGHBORS);
 }
 
-// Forces from dE/dG (already including the 1/sigma of the normalisation):
-// each centre i accumulates dE_i/dd_j for its in-cutoff neighbours j and adds
-// -dE_i/dd_j to atom j and +sum_j dE_i/dd_j to itself (float atomics: the
-// summation order, and so the last bits, vary from run to run).
-template <bool ORTHO>
+// Forces from dE/dG (already including the 1/sigma of the normalisation).
+// With the angular part of E_i written as sum_{a<c} S(cos_ac) e_a e_c,
+//   S(x) = sum_(z,l) dE/dG_zl 2^(1-z) (1 + l x)^z = sum_m s_m x^m  (degree 8),
+// the derivative of E_i with respect to d_a is
+//   g_a = srad_a u_a + (e_a / r_a) (A_a - B_a u_a) + e'_a C_a u_a,
+//   A_a = sum_{c != a} S'(cos_ac) e_c u_c, B_a = sum_{c != a} S'(cos_ac) e_c cos_ac,
+//   C_a = sum_{c != a} S(cos_ac) e_c,
+// (each ordered pair evaluated by the lane owning a).  Atom j_a receives
+// -g_a, atom i +sum_a g_a, by float4 atomics (the summation order, and so
+// the last bits, vary from run to run).
+template <bool ORTHO, int GRP>
 __global__ void __launch_bounds__(128) k_mlp_force(SimEngine e, const float* __restrict__ dEdG) {
+    constexpr int APB = 128 / GRP;
+    __shared__ MlpTable<APB> T;
     const BoxF b(*e.box);
-    float* f = e.f32;
+    float4* f = reinterpret_cast<float4*>(e.f32);
+    const int g = threadIdx.x / GRP, sub = threadIdx.x % GRP;
     bool over = false;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
-        float4 nb[MLP_MAXN];
-        float gx[MLP_MAXN], gy[MLP_MAXN], gz[MLP_MAXN], ea[MLP_MAXN], eda[MLP_MAXN];
-        const int cnt = mlp_neighbours<ORTHO>(e, b, i, nb, over);
-        float g[MLP_D];
-        const float4* gin = reinterpret_cast<const float4*>(dEdG + i * MLP_D);
+    for (int64_t base = blockIdx.x * (int64_t)APB; base < e.n; base += (int64_t)gridDim.x * APB) {
+        const int64_t i = base + g;
+        const bool live = i < e.n;
+        float gr[MLP_D];
+        {
+            const float4* src = reinterpret_cast<const float4*>(dEdG + (live ? i : 0) * MLP_D);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const float4 v = gin[q];
-            g[4 * q] = v.x; g[4 * q + 1] = v.y; g[4 * q + 2] = v.z; g[4 * q + 3] = v.w;
-        }
-        for (int a = 0; a < cnt; ++a) {
-            const float r = nb[a].w, fc = mlp_fc(r), dfc = mlp_dfc(r);
-            float s = 0.0f;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const float t = r - mlp_rs(k);
-                const float ex = __expf(-4.0f * t * t);
-                s = fmaf(g[k], ex * fmaf(-8.0f * t, fc, dfc), s);
-            }
-            const float ir = 1.0f / r;
-            gx[a] = s * nb[a].x * ir; gy[a] = s * nb[a].y * ir; gz[a] = s * nb[a].z * ir;
-            const float ex = __expf(-0.01f * r * r);
-            ea[a] = ex * fc;
-            eda[a] = ex * fmaf(-0.02f * r, fc, dfc);     // d e / d r
-        }
-        for (int a = 0; a < cnt; ++a) {
-            const float4 da = nb[a];
-            const float ira = 1.0f / da.w;
-            for (int c = a + 1; c < cnt; ++c) {
-                const float4 dc = nb[c];
-                const float irc = 1.0f / dc.w;
-                const float cs = (da.x * dc.x + da.y * dc.y + da.z * dc.z) * ira * irc;
-                const float p1 = 1.0f + cs, m1 = 1.0f - cs;
-                const float p2 = p1 * p1, m2 = m1 * m1, p4 = p2 * p2, m4 = m2 * m2;
-                const float p3 = p2 * p1, m3 = m2 * m1, p7 = p4 * p3, m7 = m4 * m3, p8 = p4 * p4, m8 = m4 * m4;
-                // S_A = sum_l g_l 2^(1-z) (1 + l c)^z ; S_dA = sum_l g_l 2^(1-z) z l (1 + l c)^(z-1)
-                const float SA = g[8] * p1 + g[9] * m1 + 0.5f * (g[10] * p2 + g[11] * m2) +
-                                 0.125f * (g[12] * p4 + g[13] * m4) + 0.0078125f * (g[14] * p8 + g[15] * m8);
-                const float SdA = (g[8] - g[9]) + (g[10] * p1 - g[11] * m1) + 0.5f * (g[12] * p3 - g[13] * m3) +
-                                  0.0625f * (g[14] * p7 - g[15] * m7);
-                const float rad = ea[a] * ea[c];
-                // dc/dd_a = d_c/(r_a r_c) - c d_a / r_a^2 (and a <-> c)
-                const float wc = SdA * rad * ira * irc;
-                const float ka = SdA * rad * cs * ira * ira - SA * eda[a] * ea[c] * ira;
-                const float kc = SdA * rad * cs * irc * irc - SA * ea[a] * eda[c] * irc;
-                gx[a] += wc * dc.x - ka * da.x; gy[a] += wc * dc.y - ka * da.y; gz[a] += wc * dc.z - ka * da.z;
-                gx[c] += wc * da.x - kc * dc.x; gy[c] += wc * da.y - kc * dc.y; gz[c] += wc * da.z - kc * dc.z;
+            for (int q = 0; q < 4; ++q) {
+                const float4 v = live ? __ldg(&src[q]) : make_float4(0.f, 0.f, 0.f, 0.f);
+                gr[4 * q] = v.x; gr[4 * q + 1] = v.y; gr[4 * q + 2] = v.z; gr[4 * q + 3] = v.w;
             }
         }
-        // gx[a] = dE_i / dd_a; the neighbour's slot is needed again: walk the list once more
-        const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
-        const int4 qi = posq[i];
-        const int nn = e.nnbr[i];
-        float sx = 0.f, sy = 0.f, sz = 0.f;
-        int a = 0;
-        for (int k = 0; k < nn && a < cnt; ++k) {
-            const int j = __ldg(&e.nbr[(int64_t)k * e.n_pad + i]);
-            const int4 qj = __ldg(&posq[j]);
-            float d0, d1, d2;
-            mlp_dvec<ORTHO>(b, qi, qj, d0, d1, d2);
-            if (!(fmaf(d2, d2, fmaf(d1, d1, d0 * d0)) < MLP_RC * MLP_RC)) continue;
-            atomicAdd(&f[4 * j], -gx[a]);
-            atomicAdd(&f[4 * j + 1], -gy[a]);
-            atomicAdd(&f[4 * j + 2], -gz[a]);
-            sx += gx[a]; sy += gy[a]; sz += gz[a];
-            ++a;
+        // monomial coefficients of S: 2^(1-z) binom(z, m) (g_z+ + (-1)^m g_z-)
+        const float P1 = gr[8] + gr[9], M1 = gr[8] - gr[9], P2 = gr[10] + gr[11], M2 = gr[10] - gr[11];
+        const float P4 = gr[12] + gr[13], M4 = gr[12] - gr[13], P8 = gr[14] + gr[15], M8 = gr[14] - gr[15];
+        float s[9];
+        s[0] = P1 + 0.5f * P2 + 0.125f * P4 + 0.0078125f * P8;
+        s[1] = M1 + M2 + 0.5f * M4 + 0.0625f * M8;
+        s[2] = 0.5f * P2 + 0.75f * P4 + 0.21875f * P8;
+        s[3] = 0.5f * M4 + 0.4375f * M8;
+        s[4] = 0.125f * P4 + 0.546875f * P8;
+        s[5] = 0.4375f * M8;
+        s[6] = 0.21875f * P8;
+        s[7] = 0.0625f * M8;
+        s[8] = 0.0078125f * P8;
+        float sd[8];   // coefficients of S': (m + 1) s_(m+1)
+#pragma unroll
+        for (int m = 0; m < 8; ++m) sd[m] = (float)(m + 1) * s[m + 1];
+        const int cnt = mlp_table<ORTHO, true, GRP>(e, b, i, live, g, sub, T, gr, nullptr, over);
+        float fx = 0.f, fy = 0.f, fz = 0.f;
+        for (int a = sub; a < cnt; a += GRP) {
+            const float4 ua = T.u[a][g];
+            float Ax = 0.f, Ay = 0.f, Az = 0.f, B = 0.f, C = 0.f;
+            for (int c = 0; c < cnt; ++c) {
+                const float4 uc = T.u[c][g];
+                const float x = fmaf(ua.z, uc.z, fmaf(ua.y, uc.y, ua.x * uc.x));
+                float S = s[8], Sp = sd[7];
+#pragma unroll
+                for (int m = 7; m >= 1; --m) {
+                    S = fmaf(S, x, s[m]);
+                    Sp = fmaf(Sp, x, sd[m - 1]);
+                }
+                S = fmaf(S, x, s[0]);
+                if (c != a) {
+                    const float t1 = Sp * uc.w;
+                    Ax = fmaf(t1, uc.x, Ax); Ay = fmaf(t1, uc.y, Ay); Az = fmaf(t1, uc.z, Az);
+                    B = fmaf(t1, x, B);
+                    C = fmaf(S, uc.w, C);
+                }
+            }
+            const float2 wa = T.w[a][g];
+            const float k = T.srad[a][g] - wa.y * B + wa.x * C;
+            const float gx = fmaf(wa.y, Ax, k * ua.x), gy = fmaf(wa.y, Ay, k * ua.y), gz = fmaf(wa.y, Az, k * ua.z);
+            atomicAdd(&f[T.j[a][g]], make_float4(-gx, -gy, -gz, 0.0f));
+            fx += gx; fy += gy; fz += gz;
         }
-        atomicAdd(&f[4 * i], sx);
-        atomicAdd(&f[4 * i + 1], sy);
-        atomicAdd(&f[4 * i + 2], sz);
+        fx = grp_sum<GRP>(fx); fy = grp_sum<GRP>(fy); fz = grp_sum<GRP>(fz);
+        if (live && sub == 0) atomicAdd(&f[i], make_float4(fx, fy, fz, 0.0f));
+        __syncwarp();
     }
     if (over) atomicOr(&e.flags[1], SIM_STATUS_MLP_NEIGHBORS);
 }
@@ -293,9 +371,11 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// logistic sigmoid with the fast divide (1 + exp(-z) above 2^126 gives 0)
+__device__ __forceinline__ float sigm(float z) { return __fdividef(1.0f, 1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu(float z) { return z * sigm(z); }
 __device__ __forceinline__ float dsilu(float z) {
-    const float s = 1.0f / (1.0f + __expf(-z));
+    const float s = sigm(z);
     return s * (1.0f + z * (1.0f - s));
 }
 
@@ -320,6 +400,199 @@ struct MlpSmem {
     uint64_t bar;
     uint32_t tmem;
 };
+
+// Inference: E_i and dE/dG (scaled by 1/sigma) per atom.  One activation
+// image serves every layer (H1, then dZ2, then dZ1: each MMA has completed
+// before its operand is overwritten), so four blocks fit on an SM (tensor
+// memory: 4 x 128 columns); the epilogues walk the accumulators 16 columns
+// at a time, and the next tile's descriptors load while this tile's MMAs run.
+struct MlpFwdSmem {
+    __nv_bfloat16 w1t[MLP_H * MLP_D];
+    __nv_bfloat16 w2t[MLP_H * MLP_H];
+    __nv_bfloat16 w2[MLP_H * MLP_H];
+    __nv_bfloat16 w1[MLP_D * MLP_H];
+    __nv_bfloat16 a0[MLP_TILE * MLP_D];
+    __nv_bfloat16 a1[MLP_TILE * MLP_H];
+    float b1[MLP_H], b2[MLP_H], w3[MLP_H], mu[MLP_D], isg[MLP_D], b3;
+    uint64_t bar;
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ void mlp_load_row(const float* G, int64_t i, bool live, float* v) {
+    const float4* src = reinterpret_cast<const float4*>(G + (live ? i : 0) * MLP_D);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 x = live ? __ldg(&src[q]) : make_float4(0.f, 0.f, 0.f, 0.f);
+        v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
+    }
+}
+
+__global__ void __launch_bounds__(MLP_TILE) k_mlp_fwd(SimMLP m, const float* __restrict__ G, int64_t n,
+                                                      float* __restrict__ e_atom, float* __restrict__ dEdG,
+                                                      int32_t* status) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    MlpFwdSmem& S = *reinterpret_cast<MlpFwdSmem*>(smem_raw);
+    const int t = threadIdx.x, warp = t >> 5;
+    {
+        const uint4* src[4] = {reinterpret_cast<const uint4*>(m.w1t_img), reinterpret_cast<const uint4*>(m.w2t_img),
+                               reinterpret_cast<const uint4*>(m.w2_img), reinterpret_cast<const uint4*>(m.w1_img)};
+        uint4* dst[4] = {reinterpret_cast<uint4*>(S.w1t), reinterpret_cast<uint4*>(S.w2t),
+                         reinterpret_cast<uint4*>(S.w2), reinterpret_cast<uint4*>(S.w1)};
+        const int cnt[4] = {MLP_H * MLP_D / 8, MLP_H * MLP_H / 8, MLP_H * MLP_H / 8, MLP_D * MLP_H / 8};
+#pragma unroll
+        for (int w = 0; w < 4; ++w)
+            for (int q = t; q < cnt[w]; q += blockDim.x) dst[w][q] = src[w][q];
+        if (t < MLP_H) { S.b1[t] = m.b1[t]; S.b2[t] = m.b2[t]; S.w3[t] = m.w3[t]; }
+        if (t < MLP_D) { S.mu[t] = m.mu[t]; S.isg[t] = m.inv_sigma[t]; }
+        if (t == 0) S.b3 = *m.b3;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;"
+                     :: "r"((uint32_t)__cvta_generic_to_shared(&S.tmem)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"((uint32_t)__cvta_generic_to_shared(&S.bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tm = S.tmem;
+    const uint32_t lb = (uint32_t)(32 * warp) << 16;
+    uint32_t phase = 0;
+    bool failed = false;
+    const int n_tiles = (int)((n + MLP_TILE - 1) / MLP_TILE);
+    float gn[MLP_D];
+    {
+        const int64_t i0 = (int64_t)blockIdx.x * MLP_TILE + t;
+        mlp_load_row(G, i0, i0 < n, gn);
+    }
+    for (int tile = blockIdx.x; tile < n_tiles && !failed; tile += gridDim.x) {
+        const int64_t i = (int64_t)tile * MLP_TILE + t;
+        const bool live = i < n;
+#pragma unroll
+        for (int c = 0; c < MLP_D; ++c) gn[c] = live ? (gn[c] - S.mu[c]) * S.isg[c] : 0.0f;
+        img_store8(S.a0, t, 0, MLP_D, gn);
+        img_store8(S.a0, t, 8, MLP_D, gn + 8);
+        async_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (t == 0) {   // Z1 = g W1 -> [0, 64)
+            mma_bf16(tm, smem_desc(S.a0, MLP_D), smem_desc(S.w1t, MLP_D), mma_idesc(128, MLP_H), 0);
+            mma_commit(&S.bar);
+        }
+        {   // the next tile's rows, in flight while the tensor cores work
+            const int64_t inext = i + (int64_t)gridDim.x * MLP_TILE;
+            mlp_load_row(G, inext, inext < n, gn);
+        }
+        failed = __syncthreads_or(!mbar_wait(&S.bar, phase));
+        phase ^= 1;
+        if (failed) break;
+        tc_fence_after();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float z[16];
+            tmem_ld16(tm + lb + 16 * q, z);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 16; ++c) z[c] = silu(z[c] + S.b1[16 * q + c]);
+            img_store8(S.a1, t, 16 * q, MLP_H, z);
+            img_store8(S.a1, t, 16 * q + 8, MLP_H, z + 8);
+        }
+        async_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (t == 0) {   // Z2 = H1 W2 -> [64, 128)
+#pragma unroll
+            for (int s = 0; s < MLP_H / 16; ++s)
+                mma_bf16(tm + 64, smem_desc(S.a1 + s * 128, MLP_H), smem_desc(S.w2t + s * 128, MLP_H),
+                         mma_idesc(128, MLP_H), s > 0);
+            mma_commit(&S.bar);
+        }
+        failed = __syncthreads_or(!mbar_wait(&S.bar, phase));
+        phase ^= 1;
+        if (failed) break;
+        tc_fence_after();
+        float E = S.b3;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float z[16];
+            tmem_ld16(tm + lb + 64 + 16 * q, z);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                const int k = 16 * q + c;
+                const float zz = z[c] + S.b2[k], sg = sigm(zz);
+                E = fmaf(S.w3[k], zz * sg, E);
+                z[c] = live ? S.w3[k] * sg * fmaf(zz, 1.0f - sg, 1.0f) : 0.0f;   // dZ2
+            }
+            img_store8(S.a1, t, 16 * q, MLP_H, z);
+            img_store8(S.a1, t, 16 * q + 8, MLP_H, z + 8);
+        }
+        if (live) e_atom[i] = E;
+        async_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (t == 0) {   // D1 = dZ2 W2^T -> [64, 128)
+#pragma unroll
+            for (int s = 0; s < MLP_H / 16; ++s)
+                mma_bf16(tm + 64, smem_desc(S.a1 + s * 128, MLP_H), smem_desc(S.w2 + s * 128, MLP_H),
+                         mma_idesc(128, MLP_H), s > 0);
+            mma_commit(&S.bar);
+        }
+        failed = __syncthreads_or(!mbar_wait(&S.bar, phase));
+        phase ^= 1;
+        if (failed) break;
+        tc_fence_after();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float z[16], d[16];
+            tmem_ld16(tm + lb + 16 * q, z);
+            tmem_ld16(tm + lb + 64 + 16 * q, d);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 16; ++c) d[c] *= dsilu(z[c] + S.b1[16 * q + c]);   // dZ1
+            img_store8(S.a1, t, 16 * q, MLP_H, d);
+            img_store8(S.a1, t, 16 * q + 8, MLP_H, d + 8);
+        }
+        async_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (t == 0) {   // dG = dZ1 W1^T -> [0, 16)
+#pragma unroll
+            for (int s = 0; s < MLP_H / 16; ++s)
+                mma_bf16(tm, smem_desc(S.a1 + s * 128, MLP_H), smem_desc(S.w1 + s * 128, MLP_H),
+                         mma_idesc(128, MLP_D), s > 0);
+            mma_commit(&S.bar);
+        }
+        failed = __syncthreads_or(!mbar_wait(&S.bar, phase));
+        phase ^= 1;
+        if (failed) break;
+        tc_fence_after();
+        float gv[MLP_D];
+        tmem_ld16(tm + lb, gv);
+        tmem_wait_ld();
+        if (live) {
+            float4* out = reinterpret_cast<float4*>(dEdG + i * MLP_D);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                out[q] = make_float4(gv[4 * q] * S.isg[4 * q], gv[4 * q + 1] * S.isg[4 * q + 1],
+                                     gv[4 * q + 2] * S.isg[4 * q + 2], gv[4 * q + 3] * S.isg[4 * q + 3]);
+        }
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+    if (failed && t == 0) atomicOr(status, SIM_STATUS_MLP_TIMEOUT);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" :: "r"(tm));
+}
 
 // TRAIN = false: E_i and dE/dG (scaled by 1/sigma) per atom.
 // TRAIN = true : per-atom loss (E_i - target_i)^2 / n_batch, its gradient
@@ -946,45 +1219,127 @@ static bool mlp_ok(const SimMLP* m) {
            m->inv_sigma;
 }
 
+// Dynamic shared memory of the inference kernel, padded so that at most four
+// blocks fit on an SM: four x 128 columns is all of its tensor memory, so a
+// fifth block would wait in tcgen05.alloc.
+static size_t mlp_fwd_smem() {
+    static size_t bytes = 0;
+    if (bytes == 0) {
+        int dev = 0, smem_sm = 228 * 1024;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        const size_t pad = (size_t)smem_sm / 4 - 1024;
+        bytes = pad > sizeof(MlpFwdSmem) ? pad : sizeof(MlpFwdSmem);
+    }
+    return bytes;
+}
+
 static void mlp_set_attributes() {
     static bool done = false;   // the first call happens before any stream capture
     if (done) return;
-    cudaFuncSetAttribute(k_mlp_net<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
+    cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_fwd_smem());
     cudaFuncSetAttribute(k_mlp_net<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
     cudaGetLastError();
     done = true;
 }
 
-static int mlp_grid(const void* fn, int64_t n_tiles) {
-    // every resident block holds 128 tensor-memory columns: never more than 4 per SM
-    int per_sm = 0, dev = 0, sms = 148;
+// Resident blocks per SM of a tensor-memory kernel, from its registers, its
+// shared memory and the 512 tensor-memory columns of an SM (the occupancy
+// query does not count tensor memory, and answers one block for these
+// kernels, so the limits are worked out here).
+static int mlp_resident(const void* fn, size_t smem, int tmem_cols) {
+    int dev = 0, smem_sm = 228 * 1024, regs_sm = 65536;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaFuncAttributes fa;
+    int by_regs = 1;
+    if (cudaFuncGetAttributes(&fa, fn) == cudaSuccess && fa.numRegs > 0) {
+        const int per_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
+        by_regs = regs_sm / (per_warp * (MLP_TILE / 32));
+        smem += fa.sharedSizeBytes;
+    }
+    cudaGetLastError();
+    const int by_smem = (int)((size_t)smem_sm / (smem + 1024));
+    int per_sm = 512 / tmem_cols;
+    if (by_regs < per_sm) per_sm = by_regs;
+    if (by_smem < per_sm) per_sm = by_smem;
+    return per_sm < 1 ? 1 : per_sm;
+}
+
+static int mlp_grid(const void* fn, int64_t n_tiles, size_t smem, int tmem_cols) {
+    static const void* fns[4];
+    static int cached[4], n_cached = 0;
+    int per_sm = 0;
+    for (int k = 0; k < n_cached; ++k)
+        if (fns[k] == fn) per_sm = cached[k];
+    if (per_sm == 0) {   // the first call happens before any stream capture
+        per_sm = mlp_resident(fn, smem, tmem_cols);
+        if (n_cached < 4) { fns[n_cached] = fn; cached[n_cached++] = per_sm; }
+    }
+    int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, MLP_TILE, sizeof(MlpSmem)) != cudaSuccess ||
-        per_sm < 1)
-        per_sm = 1;
-    if (per_sm > 4) per_sm = 4;
     const int64_t g = (int64_t)per_sm * sms;
     return (int)(n_tiles < g ? (n_tiles < 1 ? 1 : n_tiles) : g);
 }
 
+template <int GRP>
+static void launch_mlp_desc(const SimEngine& e, float* G, cudaStream_t st) {
+    const int64_t groups = (e.n + 128 / GRP - 1) / (128 / GRP);
+    const int g = (int)(groups < 148 * 12 ? groups : 148 * 12);
+    if (e.box_orthogonal) k_mlp_desc<true, GRP><<<g, 128, 0, st>>>(e, G);
+    else k_mlp_desc<false, GRP><<<g, 128, 0, st>>>(e, G);
+}
+
+template <int GRP>
+static void launch_mlp_force(const SimEngine& e, const float* dEdG, cudaStream_t st) {
+    const int64_t groups = (e.n + 128 / GRP - 1) / (128 / GRP);
+    const int g = (int)(groups < 148 * 12 ? groups : 148 * 12);
+    if (e.box_orthogonal) k_mlp_force<true, GRP><<<g, 128, 0, st>>>(e, dEdG);
+    else k_mlp_force<false, GRP><<<g, 128, 0, st>>>(e, dEdG);
+}
+
+// launch[2] / launch[3]: threads per atom of the descriptor / force kernel (4 or 8; 0: 4)
+static bool mlp_group_ok(int g) { return g == 0 || g == 4 || g == 8; }
+
 extern "C" int sim_mlp_descriptors(const SimEngine* e, float* G, void* stream) {
-    if (!e || !G || e->n <= 0) return SIM_ERR_ARG;
-    const int g = (int)((e->n + 127) / 128 < 148 * 16 ? (e->n + 127) / 128 : 148 * 16);
-    if (e->box_orthogonal) k_mlp_desc<true><<<g, 128, 0, (cudaStream_t)stream>>>(*e, G);
-    else k_mlp_desc<false><<<g, 128, 0, (cudaStream_t)stream>>>(*e, G);
+    if (!e || !G || e->n <= 0 || !mlp_group_ok(e->launch[2])) return SIM_ERR_ARG;
+    if (e->launch[2] == 8) launch_mlp_desc<8>(*e, G, (cudaStream_t)stream);
+    else launch_mlp_desc<4>(*e, G, (cudaStream_t)stream);
     return launch_status("sim_mlp_descriptors");
 }
 
-extern "C" int sim_mlp_forces(const SimEngine* e, const float* dEdG, void* stream) {
-    if (!e || !dEdG || e->n <= 0) return SIM_ERR_ARG;
+extern "C" int sim_mlp_backward(const SimEngine* e, const float* dEdG, void* stream) {
+    if (!e || !dEdG || e->n <= 0 || !mlp_group_ok(e->launch[3])) return SIM_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t err = cudaMemsetAsync(e->f32, 0, sizeof(float) * 4 * e->n_pad, st);
-    if (err != cudaSuccess) { set_cuda_error(err, "sim_mlp_forces: zero forces"); return SIM_ERR_CUDA; }
-    const int g = (int)((e->n + 127) / 128 < 148 * 16 ? (e->n + 127) / 128 : 148 * 16);
-    if (e->box_orthogonal) k_mlp_force<true><<<g, 128, 0, st>>>(*e, dEdG);
-    else k_mlp_force<false><<<g, 128, 0, st>>>(*e, dEdG);
-    return launch_status("sim_mlp_forces");
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_mlp_backward: zero forces"); return SIM_ERR_CUDA; }
+    if (e->launch[3] == 8) launch_mlp_force<8>(*e, dEdG, st);
+    else launch_mlp_force<4>(*e, dEdG, st);
+    return launch_status("sim_mlp_backward");
+}
+
+extern "C" int sim_autotune_mlp(const SimEngine* e, const float* dEdG, float* G, int32_t reps, float* ms,
+                                int32_t* best, void* stream) {
+    if (!e || !dEdG || !G || !ms || !best || reps < 1 || e->n <= 0) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const SimEngine& en = *e;
+    ms[0] = time_launches([&] { launch_mlp_desc<4>(en, G, st); }, reps, st);
+    ms[1] = time_launches([&] { launch_mlp_desc<8>(en, G, st); }, reps, st);
+    // the force pass accumulates; zeroed once per launch like sim_mlp_backward
+    ms[2] = time_launches([&] {
+        cudaMemsetAsync(en.f32, 0, sizeof(float) * 4 * en.n_pad, st);
+        launch_mlp_force<4>(en, dEdG, st);
+    }, reps, st);
+    ms[3] = time_launches([&] {
+        cudaMemsetAsync(en.f32, 0, sizeof(float) * 4 * en.n_pad, st);
+        launch_mlp_force<8>(en, dEdG, st);
+    }, reps, st);
+    if (ms[0] < 0.f || ms[1] < 0.f || ms[2] < 0.f || ms[3] < 0.f) return SIM_ERR_CUDA;
+    best[0] = ms[1] < ms[0] ? 8 : 4;
+    best[1] = ms[3] < ms[2] ? 8 : 4;
+    return launch_status("sim_autotune_mlp");
 }
 
 extern "C" int sim_eam_atom_energy(const SimEngine* e, const SimEAMTables* t, float* e_atom, void* stream) {
@@ -998,9 +1353,9 @@ extern "C" int sim_mlp_forward(const SimMLP* m, const float* G, int64_t n, float
                                int32_t* status, void* stream) {
     if (!mlp_ok(m) || !G || n <= 0 || !e_atom || !dEdG || !status) return SIM_ERR_ARG;
     mlp_set_attributes();
-    const int g = mlp_grid((const void*)k_mlp_net<false>, (n + MLP_TILE - 1) / MLP_TILE);
-    k_mlp_net<false><<<g, MLP_TILE, sizeof(MlpSmem), (cudaStream_t)stream>>>(*m, G, n, e_atom, dEdG, nullptr, 0.0f,
-                                                                            nullptr, nullptr, status);
+    const size_t smem = mlp_fwd_smem();
+    const int g = mlp_grid((const void*)k_mlp_fwd, (n + MLP_TILE - 1) / MLP_TILE, smem, 128);
+    k_mlp_fwd<<<g, MLP_TILE, smem, (cudaStream_t)stream>>>(*m, G, n, e_atom, dEdG, status);
     return launch_status("sim_mlp_forward");
 }
 
@@ -1012,7 +1367,7 @@ extern "C" int sim_mlp_train_grads(const SimMLP* m, const float* G, const float*
     cudaError_t err = cudaMemsetAsync(grads, 0, sizeof(float) * SIM_MLP_PARAMS, st);
     if (err == cudaSuccess) err = cudaMemsetAsync(loss, 0, sizeof(float), st);
     if (err != cudaSuccess) { set_cuda_error(err, "sim_mlp_train_grads: zero"); return SIM_ERR_CUDA; }
-    const int g = mlp_grid((const void*)k_mlp_net<true>, (n + MLP_TILE - 1) / MLP_TILE);
+    const int g = mlp_grid((const void*)k_mlp_net<true>, (n + MLP_TILE - 1) / MLP_TILE, sizeof(MlpSmem), 128);
     k_mlp_net<true><<<g, MLP_TILE, sizeof(MlpSmem), st>>>(*m, G, n, nullptr, nullptr, target, 1.0f / (float)n, grads,
                                                          loss, status);
     return launch_status("sim_mlp_train_grads");
@@ -1060,20 +1415,25 @@ extern "C" int sim_mlp_train_grads_fm(const SimMLP* m, const float* G, const flo
     cudaError_t err = cudaMemsetAsync(grads, 0, sizeof(float) * SIM_MLP_PARAMS, st);
     if (err == cudaSuccess) err = cudaMemsetAsync(loss, 0, sizeof(float), st);
     if (err != cudaSuccess) { set_cuda_error(err, "sim_mlp_train_grads_fm: zero"); return SIM_ERR_CUDA; }
-    // every resident block holds 256 tensor-memory columns: at most 2 per SM
-    int per_sm = 0, dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_train_fm, MLP_TILE, sizeof(MlpFmSmem)) !=
-            cudaSuccess || per_sm < 1)
-        per_sm = 1;
-    if (per_sm > 2) per_sm = 2;
-    const int64_t tiles = (n + MLP_TILE - 1) / MLP_TILE;
-    const int g = (int)(tiles < (int64_t)per_sm * sms ? tiles : (int64_t)per_sm * sms);
+    const int g = mlp_grid((const void*)k_mlp_train_fm, (n + MLP_TILE - 1) / MLP_TILE, sizeof(MlpFmSmem), 256);
     const float alpha = 2.0f * w_energy / (float)n;
     const float beta = -2.0f * w_force / (3.0f * (float)n_force_atoms);
     k_mlp_train_fm<<<g, MLP_TILE, sizeof(MlpFmSmem), st>>>(*m, G, target, u, n, alpha, beta, 1.0f / (float)n, grads,
                                                            loss, status);
     return launch_status("sim_mlp_train_grads_fm");
+}
+
+extern "C" int sim_mlp_train_step(const SimMLP* m, float* params, uint16_t* w1t_img, uint16_t* w2t_img,
+                                  uint16_t* w2_img, uint16_t* w1_img, const float* G, const float* target,
+                                  const float* u, int64_t n, float w_energy, float w_force, int64_t n_force_atoms,
+                                  float* grads, float* adam_m, float* adam_v, float lr, int32_t step, float* loss,
+                                  int32_t* status, void* stream) {
+    if (!params || !adam_m || !adam_v || step < 1) return SIM_ERR_ARG;
+    int rc = u ? sim_mlp_train_grads_fm(m, G, target, u, n, w_energy, w_force, n_force_atoms, grads, loss, status,
+                                        stream)
+               : sim_mlp_train_grads(m, G, target, n, grads, loss, status, stream);
+    if (rc == SIM_OK) rc = sim_mlp_adam(params, grads, adam_m, adam_v, lr, step, stream);
+    if (rc == SIM_OK) rc = sim_mlp_pack(params, w1t_img, w2t_img, w2_img, w1_img, stream);
+    return rc;
 }
 

@@ -171,6 +171,9 @@ class MDEngine:
         if int(self.types.min()) < 0 or int(self.types.max()) >= self.n_types:
             raise ValueError(f"atom types must lie in [0, {self.n_types})")
         self.rebuilds_host = 0
+        # launch shapes (SimEngine.launch; 0 = built-in): EAM pass-1 / pass-2
+        # threads per block, MLP descriptor / force threads per atom
+        self.launch = [0, 0, 0, 0]
         self._make_struct()
         vel = None if velocities is None else torch.as_tensor(velocities).to(dev, torch.float64).contiguous()
         self.load(pos, vel)
@@ -194,12 +197,23 @@ class MDEngine:
         s.n_tiles, s.halo_cap = self.n_tiles, self.halo_cap
         s.halo, s.halo_n, s.nbr16 = _lib.ptr(self.halo), _lib.ptr(self.halo_n), _lib.ptr(self.nbr16)
         s.cut_mask = _lib.ptr(self.cut_mask)
+        s.launch[:] = list(self.launch)
         self.st = s
         self.st_ref = ctypes.byref(s)
 
     @property
     def stream(self):
         return torch.cuda.current_stream(self.device).cuda_stream
+
+    def set_launch(self, eam_density_threads: int | None = None, eam_force_threads: int | None = None,
+                   mlp_desc_group: int | None = None, mlp_force_group: int | None = None):
+        """Launch shapes of the EAM and MLP kernels (0 = built-in); see
+        simulon_b200.autotune for measuring them.  Graphs captured before the
+        change keep the shapes they were captured with."""
+        for k, v in enumerate((eam_density_threads, eam_force_threads, mlp_desc_group, mlp_force_group)):
+            if v is not None:
+                self.launch[k] = int(v)
+        self.st.launch[:] = list(self.launch)
 
     # ---- state in/out ------------------------------------------------------
     def load(self, positions, velocities=None):
@@ -323,6 +337,10 @@ class MDEngine:
 
     def integrate_second(self, integ, precision: int):
         _lib.call("sim_integrate_second", self.st_ref, integ.ref, int(precision), self.stream)
+
+    def integrate_second_first(self, integ, precision: int):
+        """Second half of this step and first half of the next with the same forces."""
+        _lib.call("sim_integrate_second_first", self.st_ref, integ.ref, int(precision), self.stream)
 
     def berendsen(self, params):
         _lib.call("sim_berendsen", self.st_ref, params.ref, _lib.ptr(self.extra), self.stream)

@@ -7,6 +7,8 @@ network for the atom's energy (BF16 operands on the tensor cores, FP32
 accumulation), forces = -dE/dx through network and descriptors.
 
 * ``MLPNet`` holds the FP32 parameters and their BF16 operand images.
+* ``MLPEnergy`` / ``mlp_energy``: the energy as a ``torch.autograd.Function``
+  whose backward is the library's force kernel.
 * ``MLPForce`` is a force-field backbone with the ``BackboneInterface``
   contract of the reference (core/md_model.py:9-12): energy, forces.
 * ``generate_dataset`` runs the engine's EAM at several temperatures and
@@ -123,6 +125,17 @@ class MLPNet:
         _lib.call("sim_mlp_train_grads", self.ref, _lib.ptr(G), _lib.ptr(target), int(target.numel()),
                   _lib.ptr(grads), _lib.ptr(loss), _lib.ptr(self.status), self._stream())
 
+    def train_step(self, G: torch.Tensor, target: torch.Tensor, n: int, grads: torch.Tensor, adam_m: torch.Tensor,
+                   adam_v: torch.Tensor, lr: float, step: int, loss: torch.Tensor, u: torch.Tensor | None = None,
+                   w_energy: float = 1.0, w_force: float = 1.0, n_force_atoms: int = 0):
+        """Gradient (energy only, or energy and force matching along u), Adam
+        step and BF16 repack in one library call."""
+        p = _lib.ptr
+        _lib.call("sim_mlp_train_step", self.ref, p(self.flat), *(p(t) for t in self.images), p(G), p(target),
+                  p(u) if u is not None else None, int(n), float(w_energy), float(w_force),
+                  int(n_force_atoms or n), p(grads), p(adam_m), p(adam_v), float(lr), int(step), p(loss),
+                  p(self.status), self._stream())
+
     def train_grads_fm(self, G: torch.Tensor, target: torch.Tensor, u: torch.Tensor, n: int, w_energy: float,
                        w_force: float, n_force_atoms: int, grads: torch.Tensor, loss: torch.Tensor):
         """Gradient of w_energy * mean (E - target)^2 + the force-matching term
@@ -149,7 +162,7 @@ def descriptors(engine: MDEngine) -> torch.Tensor:
 
 def mlp_forces(engine: MDEngine, dEdG: torch.Tensor):
     """-dE/dx of every slot into engine.f32 from dE/dG [n, 16]."""
-    _lib.call("sim_mlp_forces", engine.st_ref, _lib.ptr(dEdG), engine.stream)
+    _lib.call("sim_mlp_backward", engine.st_ref, _lib.ptr(dEdG), engine.stream)
     engine._last_force_precision = 0
     engine.forces_valid = True
 
@@ -167,6 +180,32 @@ def eam_atom_energy(engine: MDEngine, tables) -> torch.Tensor:
     out = torch.zeros(engine.n_pad, device=engine.device, dtype=torch.float32)
     _lib.call("sim_eam_atom_energy", engine.st_ref, tables.ref, _lib.ptr(out), engine.stream)
     return out
+
+
+class MLPEnergy(torch.autograd.Function):
+    """Total surrogate energy of positions x [N,3] (original atom order) as a
+    differentiable torch function.  forward: the engine is loaded with x
+    (cell sort and list build), then descriptors, network and the backward
+    kernels run; backward: dE/dx = -forces, times the incoming gradient."""
+
+    @staticmethod
+    def forward(ctx, x, engine, net):
+        engine.set_positions(x.detach())
+        G = descriptors(engine)
+        e, d = net.forward(G, engine.n)
+        mlp_forces(engine, d)
+        ctx.save_for_backward(-engine.gather("f").to(x.dtype))
+        return e.sum().to(x.dtype)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (dEdx,) = ctx.saved_tensors
+        return grad_out * dEdx, None, None
+
+
+def mlp_energy(x: torch.Tensor, engine: MDEngine, net: MLPNet) -> torch.Tensor:
+    """E(x) with forces = -dE/dx from the library's backward kernels."""
+    return MLPEnergy.apply(x, engine, net)
 
 
 class MLPForce:
@@ -268,17 +307,12 @@ def train(net: MLPNet, G: torch.Tensor, E: torch.Tensor, *, steps: int = 2000, b
     gen.manual_seed(seed)
     Gb = torch.empty(batch, N_DESC, device=dev, dtype=torch.float32)
     Eb = torch.empty(batch, device=dev, dtype=torch.float32)
-    st = torch.cuda.current_stream(dev).cuda_stream
     for s in range(steps):
         idx = torch.randint(0, n, (batch,), device=dev, generator=gen)
         torch.index_select(G, 0, idx, out=Gb)
         torch.index_select(E, 0, idx, out=Eb)
-        net.train_grads(Gb, Eb, grads, loss)
-        frac = s / max(1, steps - 1)
-        lr_s = lr * (lr_final / lr) ** frac
-        _lib.call("sim_mlp_adam", _lib.ptr(net.flat), _lib.ptr(grads), _lib.ptr(m1), _lib.ptr(m2), float(lr_s),
-                  s + 1, st)
-        _lib.call("sim_mlp_pack", _lib.ptr(net.flat), *(_lib.ptr(t) for t in net.images), st)
+        lr_s = lr * (lr_final / lr) ** (s / max(1, steps - 1))
+        net.train_step(Gb, Eb, batch, grads, m1, m2, lr_s, s + 1, loss)
         losses[s:s + 1].copy_(loss)
         if log_every and (s + 1) % log_every == 0:
             print(f"step {s + 1}: loss {float(loss):.3e} eV^2", flush=True)
@@ -322,22 +356,19 @@ def train_forces(net: MLPNet, frames, *, steps: int = 4000, lr: float = 1e-3, lr
     ferr = torch.zeros(P, 4, device=dev, dtype=torch.float32)
     u = torch.zeros(P, N_DESC, device=dev, dtype=torch.float32)
     order = np.random.default_rng(seed).permutation(steps) % len(frames)
-    st = torch.cuda.current_stream(dev).cuda_stream
     for s in range(steps):
         fr = frames[int(order[s])]
         eng = fr.engine
         n, np_ = eng.n, eng.n_pad
         net.forward_into(fr.G, n, e, d)
-        _lib.call("sim_mlp_forces", eng.st_ref, _lib.ptr(d), eng.stream)
+        _lib.call("sim_mlp_backward", eng.st_ref, _lib.ptr(d), eng.stream)
         fe = ferr[:np_]
         torch.sub(eng.f32, fr.F, out=fe)
         fmse[s] = fe[:n, :3].square().mean()
         _lib.call("sim_mlp_force_contract", eng.st_ref, _lib.ptr(fe), _lib.ptr(u), eng.stream)
-        net.train_grads_fm(fr.G, fr.E, u, n, w_energy, w_force, n, grads, loss)
         lr_s = lr * (lr_final / lr) ** (s / max(1, steps - 1))
-        _lib.call("sim_mlp_adam", _lib.ptr(net.flat), _lib.ptr(grads), _lib.ptr(m1), _lib.ptr(m2), float(lr_s),
-                  s + 1, st)
-        _lib.call("sim_mlp_pack", _lib.ptr(net.flat), *(_lib.ptr(t) for t in net.images), st)
+        net.train_step(fr.G, fr.E, n, grads, m1, m2, lr_s, s + 1, loss, u=u, w_energy=w_energy, w_force=w_force,
+                       n_force_atoms=n)
         if log_every and (s + 1) % log_every == 0:
             print(f"step {s + 1}: force RMSE {math.sqrt(float(fmse[s + 1 - log_every:s + 1].mean())):.4f} eV/A, "
                   f"energy loss {float(loss):.3e} eV^2", flush=True)
@@ -371,9 +402,10 @@ class SurrogateRun:
     Every ``judge_every`` steps the EAM forces of the current positions are
     compared with the MLP forces; when their RMSE exceeds ``tolerance``
     (eV/A) the run continues with EAM forces.  Steps between judgements are
-    captured in a CUDA graph: first half-step and conditional rebuild,
-    descriptors, network, forces, second half-step (Langevin when the
-    integrator parameters say so)."""
+    captured in a CUDA graph: first half-step and conditional rebuild, then
+    per step descriptors, network and forces followed by one pass that
+    finishes the step and starts the next (Langevin when the integrator
+    parameters say so), the last step ending with a plain second half."""
 
     def __init__(self, engine: MDEngine, net: MLPNet, tables, integ, *, judge_every: int = 100,
                  tolerance: float = 0.05):
@@ -392,17 +424,28 @@ class SurrogateRun:
         eng = self.eng
         _lib.call("sim_mlp_descriptors", eng.st_ref, _lib.ptr(self.G), eng.stream)
         self.net.forward_into(self.G, eng.n, self.e, self.d)
-        _lib.call("sim_mlp_forces", eng.st_ref, _lib.ptr(self.d), eng.stream)
+        _lib.call("sim_mlp_backward", eng.st_ref, _lib.ptr(self.d), eng.stream)
 
-    def _step(self):
+    def _chunk(self, k: int):
+        """k steps, launches only: the second half of each step but the last
+        runs together with the first half of the next (same forces)."""
         eng = self.eng
         eng.integrate_first(self.integ, 0)
         eng.rebuild_if_needed()
-        if self.use_mlp:
-            self._mlp_forces()
-            eng.integrate_second(self.integ, 0)
-        else:
-            eng.eam_forces_integrate(self.tables, self.integ)
+        for s in range(k):
+            last = s == k - 1
+            if self.use_mlp:
+                self._mlp_forces()
+                if last:
+                    eng.integrate_second(self.integ, 0)
+                else:
+                    eng.integrate_second_first(self.integ, 0)
+            elif last:
+                eng.eam_forces_integrate(self.tables, self.integ)
+            else:
+                eng.eam_forces_integrate_drift(self.tables, self.integ)
+            if not last:
+                eng.rebuild_if_needed()
 
     def judge(self) -> float:
         """Force RMSE of MLP against EAM at the current positions (synchronises);
@@ -430,14 +473,12 @@ class SurrogateRun:
                     s.wait_stream(torch.cuda.current_stream(self.eng.device))
                     g = torch.cuda.CUDAGraph()
                     with torch.cuda.graph(g, stream=s):
-                        for _ in range(k):
-                            self._step()
+                        self._chunk(k)
                     torch.cuda.current_stream(self.eng.device).wait_stream(s)
                     self._graph = g
                 self._graph.replay()
             else:
-                for _ in range(k):
-                    self._step()
+                self._chunk(k)
             done += k
             if judge and self.use_mlp and k == self.judge_every:
                 self.judge()

@@ -294,3 +294,36 @@ def test_force_loss_gradient_matches_oracle(sb):
         want = torch.zeros(cnt, dtype=torch.float64) if g is None else g.reshape(-1)
         assert float((got - want).norm()) <= 0.05 * float(want.norm()) + 1e-9, (k, float((got - want).norm()),
                                                                                 float(want.norm()))
+
+
+def test_autograd_function_matches_fp64_and_finite_differences(sb):
+    """mlp_energy (torch.autograd.Function): its gradient against autograd of
+    the FP64 restatement with the same weights (3% of the gradient norm: BF16
+    network operands), whose own gradient matches central finite differences
+    along random directions (1e-6 relative)."""
+    from simulon_b200 import mlp
+    x, H, eng, pi, pj = _system(sb, n=4, seed=22)
+    net = mlp.MLPNet.load(mlp.default_weights_path(), DEV)
+    p64 = {k: torch.as_tensor(v, dtype=torch.float64) for k, v in net.to_dict().items()}
+    xt = torch.tensor(x, device=DEV, requires_grad=True)
+    E = mlp.mlp_energy(xt, eng, net)
+    (g,) = torch.autograd.grad(E, xt)
+    g = g.cpu()
+    box = OracleBox(H)
+
+    def e64(xx):
+        return omlp.atom_energies(omlp.descriptors(xx, box, pi, pj), p64).sum()
+    xo = torch.tensor(x, requires_grad=True)
+    Eo = e64(xo)
+    (go,) = torch.autograd.grad(Eo, xo)
+    assert abs(float(E.detach()) - float(Eo.detach())) <= 2e-3 * len(x)
+    assert float((g - go).norm()) <= 0.03 * float(go.norm()), (float((g - go).norm()), float(go.norm()))
+    rng = np.random.default_rng(23)
+    h = 1e-4
+    with torch.no_grad():
+        for _ in range(3):
+            v = torch.tensor(rng.normal(size=x.shape))
+            v /= v.norm()
+            fd = (e64(torch.tensor(x) + h * v) - e64(torch.tensor(x) - h * v)) / (2 * h)
+            assert abs(float(fd) - float((go * v).sum())) <= 1e-6 * float(go.norm()) + 1e-9
+    assert eng.status() == 0

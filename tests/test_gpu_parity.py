@@ -306,9 +306,10 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
     res = []
     from simulon_b200.engine import integrator_params
     # (graph?, conditional IF-node rebuild?, second half fused into EAM pass 2?);
-    # fused == "drift": the next step's first half is fused in as well
+    # fused == "drift": the next step's first half is fused in as well;
+    # fused == "sf": standalone forces, then sim_integrate_second_first
     modes = [(False, False, False), (True, False, False), (True, True, False), (True, True, True), (False, True, True),
-             (False, True, "drift"), (True, True, "drift")]
+             (False, True, "drift"), (True, True, "drift"), (False, True, "sf"), (True, True, "sf")]
     for use_graph, cond, fused in modes:
         eng, tables, parser = _eam_engine(sb, fsw_path, x, np.diag([L] * 3), v)
         # an NVT integrator exercises the noise and triggers rebuilds
@@ -320,9 +321,17 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
             eng.rebuild_if_needed()
             for s in range(k):
                 if s < k - 1:
-                    eng.eam_forces_integrate_drift(tables, integ)
+                    if fused == "sf":
+                        eng.eam_forces(tables)
+                        eng.integrate_second_first(integ, 0)
+                    else:
+                        eng.eam_forces_integrate_drift(tables, integ)
                     eng.log_step(after_drift=True)
                     eng.rebuild_if_needed()
+                elif fused == "sf":
+                    eng.eam_forces(tables)
+                    eng.integrate_second(integ, 0)
+                    eng.log_step()
                 else:
                     eng.eam_forces_integrate(tables, integ)
                     eng.log_step()
@@ -344,7 +353,7 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
             s.wait_stream(torch.cuda.current_stream())
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=s):
-                if fused == "drift":
+                if fused in ("drift", "sf"):
                     drift_steps(20)
                 else:
                     for _ in range(20):
@@ -353,7 +362,7 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
             torch.cuda.current_stream().wait_stream(s)
             for _ in range(steps // 20):
                 g.replay()
-        elif fused == "drift":
+        elif fused in ("drift", "sf"):
             for _ in range(steps // 20):
                 drift_steps(20)
         else:
