@@ -147,13 +147,15 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def measured_peaks():
+def measured_peaks(key: str = "hbm_gbs"):
+    """(peak, "measured"|"fallback"): HBM GB/s, or dense BF16 TFLOP/s (burst)."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
         with open(path) as fh:
             d = json.load(fh)
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        if key in d:
+            return float(d[key]), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}[key], "fallback"
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle port)
@@ -248,6 +250,9 @@ def run_b200(args):
     model = sb.BaseModel(sb.SumBackboneInterface([ff], mol), integ, mol)
     eng = mol.engine
     G = args.graph_steps
+    # launch shapes of the two EAM passes, timed on this system (not cached)
+    from simulon_b200 import autotune
+    shapes = autotune.tune_eam(eng, ff.tables, reps=10, use_cache=False)
 
     # warm-up (captures the graph, runs W steps)
     model.run(max(args.warmup, G), graph_steps=G)
@@ -321,6 +326,8 @@ def run_b200(args):
                        "form": "plain", "atoms_per_gpu": N, "graph_steps": G,
                        "l2": "state ~0.4 GB > 126 MB L2 (no flush needed)",
                        "neighbors_mean": nbar, "neighbor_capacity": nbr["cap"], "rebuilds_in_timed": rebuilds,
+                       "launch_shapes": {"density_threads": shapes["density_threads"],
+                                         "force_threads": shapes["force_threads"], "autotune_ms": shapes["ms"]},
                        "parallelism": f"replicas x{world}"},
             "status": status,
             "roofline": {"bound": "hbm", "kernel": "k_eam_force<single,integ,ortho> (EAM pass 2 + second half-step)",
@@ -508,6 +515,10 @@ def mlp_form(args, sb, pot, dev, world):
     net = mlp.MLPNet.load(mlp.default_weights_path(), dev)
     eng = sb.MDEngine(x, np.zeros(N, np.int32), [M_W], np.diag([L] * 3), parser.cutoff, 0.5, velocities=v, device=dev)
     ip = sb.engine.integrator_params(eng, 0.002, langevin=True, temperature=300.0, gamma=10.0, seed=5)
+    from simulon_b200 import autotune
+    G0 = mlp.descriptors(eng)
+    _, d0 = net.forward(G0, N)
+    shapes = autotune.tune_mlp(eng, reps=10, use_cache=False, dEdG=d0)
     run = mlp.SurrogateRun(eng, net, tables, ip, judge_every=100, tolerance=0.05)
     run.run(max(args.warmup, 100) // 100 * 100)
     torch.cuda.synchronize()
@@ -529,7 +540,32 @@ def mlp_form(args, sb, pot, dev, world):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     rm = run.rmse_history
+    # the step's kernels timed alone (events, 20 launches each, after the run)
+    from simulon_b200 import _lib
+
+    def each(fn, reps=20):
+        fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+    k_ms = {"descriptors": each(lambda: _lib.call("sim_mlp_descriptors", eng.st_ref, _lib.ptr(run.G), eng.stream)),
+            "network": each(lambda: net.forward_into(run.G, N, run.e, run.d)),
+            "forces": each(lambda: _lib.call("sim_mlp_backward", eng.st_ref, _lib.ptr(run.d), eng.stream))}
+    flops = 2 * (16 * 64 + 64 * 64 + 64 * 64 + 64 * 16) * N     # the four BF16 GEMMs per atom
+    tf = flops / (k_ms["network"] / 1e3) / 1e12
+    peak_tf, kind_tf = measured_peaks("bf16_tflops")
     return {"value": world * N * K / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K, "steps": K,
+            "kernels_ms": k_ms,
+            "tensor": {"kernel": "k_mlp_fwd (Z1, Z2, dZ2 W2^T, dZ1 W1^T on tcgen05, BF16 in, FP32 in TMEM)",
+                       "flops_per_atom": flops // N, "achieved": tf, "peak": peak_tf, "peak_kind": kind_tf,
+                       "unit": "TFLOP/s", "frac": tf / peak_tf},
+            "launch_shapes": {"desc_group": shapes["desc_group"], "force_group": shapes["force_group"],
+                              "autotune_ms": shapes["ms"]},
             "force_rmse_vs_eam_ev_per_a": {"last": rm[-1] if rm else None, "max": max(rm) if rm else None,
                                            "judgements": len(rm)},
             "fell_back_to_eam": not run.use_mlp, "status": eng.status(), "net_status": int(net.status.item()),
@@ -537,9 +573,7 @@ def mlp_form(args, sb, pot, dev, world):
                                    "gamma 10/ps, dt 2 fs, skin 0.5 A; descriptors 8 radial + 8 angular (rc 4.4 A), "
                                    "MLP 16-64-64-1 SiLU, BF16 tensor-core GEMMs with FP32 accumulation",
                        "judge": "EAM force RMSE every 100 steps (inside the timed region), fallback above 0.05 eV/A",
-                       "training": "python -m simulon_b200.mlp: 1.2 M atom samples (2,000-atom BCC cells at "
-                                   "300/700/1100/1500 K and -3/0/+3 % strain), 20,000 Adam steps of 16,384 atoms "
-                                   "on per-atom EAM energies"}}
+                       "training": mlp.TRAINING_NOTE}}
 
 
 def e2e(model, mol, x, v, args, dev):

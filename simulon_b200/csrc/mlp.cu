@@ -84,55 +84,67 @@ __device__ __forceinline__ int mlp_table(const SimEngine& e, const BoxF& b, int6
     const int nn = live ? e.nnbr[i] : 0;
     const int nn_max = __reduce_max_sync(0xffffffffu, nn);
     int cnt = 0;
-    for (int k0 = 0; k0 < nn_max; k0 += GRP) {
-        const int k = k0 + sub;
-        bool inside = false;
-        float d0 = 0.f, d1 = 0.f, d2 = 0.f, r2 = 0.f;
-        int j = 0;
-        if (k < nn) {
-            j = __ldg(&e.nbr[(int64_t)k * e.n_pad + i]);
-            const int4 qj = __ldg(&posq[j]);
-            mlp_dvec<ORTHO>(b, qi, qj, d0, d1, d2);
-            r2 = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
-            inside = r2 < MLP_RC * MLP_RC;
+    // R rounds of GRP entries at a time: their list entries, then their
+    // positions, are all in flight before the first distance is needed
+    constexpr int R = 4;
+    for (int k0 = 0; k0 < nn_max; k0 += GRP * R) {
+        int jj[R];
+        int4 qq[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int k = k0 + r * GRP + sub;
+            jj[r] = k < nn ? __ldg(&e.nbr[(int64_t)k * e.n_pad + i]) : -1;
         }
-        const unsigned grp = (__ballot_sync(0xffffffffu, inside) >> (lane & ~(GRP - 1))) & ((1u << GRP) - 1u);
-        const int pos = cnt + __popc(grp & ((1u << sub) - 1u));
-        if (inside) {
-            if (pos < MLP_MAXN) {
-                const float r = sqrtf(r2), ir = 1.0f / r;
-                const float fc = mlp_fc(r), ex = __expf(-0.01f * r2), ev = ex * fc;
-                T.u[pos][g] = make_float4(d0 * ir, d1 * ir, d2 * ir, ev);
-                // exp(-4 (r - R_k)^2) by the recurrence over k (R_k = 2 + k h):
-                // x_{k+1} = x_k exp(8 h t0) exp(-4 h^2 (2k + 1)), t0 = r - 2
-                const float step[8] = {0.6248747f, 0.24399385f, 0.09527189f, 0.037200667f,
-                                       0.014525686f, 0.005671822f, 0.0022146674f, 0.0008647577f};
-                const float t0 = r - 2.0f, q8 = __expf(2.7428572f * t0);
-                float gk = __expf(-4.0f * t0 * t0);
-                if constexpr (FORCE) {
-                    const float dfc = mlp_dfc(r);
-                    T.w[pos][g] = make_float2(ex * fmaf(-0.02f * r, fc, dfc), ev * ir);
-                    T.j[pos][g] = j;
-                    float sr = 0.0f;
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const float t = fmaf(-0.34285715f, (float)q, t0);
-                        sr = fmaf(gr[q], gk * fmaf(-8.0f * t, fc, dfc), sr);
-                        gk *= q8 * step[q];
-                    }
-                    T.srad[pos][g] = sr;
-                } else {
+        for (int r = 0; r < R; ++r) qq[r] = jj[r] >= 0 ? __ldg(&posq[jj[r]]) : make_int4(0, 0, 0, 0);
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        rad[q] = fmaf(gk, fc, rad[q]);
-                        gk *= q8 * step[q];
-                    }
-                }
-            } else {
-                over = true;
+        for (int r = 0; r < R; ++r) {
+            bool inside = false;
+            float d0 = 0.f, d1 = 0.f, d2 = 0.f, r2 = 0.f;
+            const int j = jj[r];
+            if (j >= 0) {
+                mlp_dvec<ORTHO>(b, qi, qq[r], d0, d1, d2);
+                r2 = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+                inside = r2 < MLP_RC * MLP_RC;
             }
+            const unsigned grp = (__ballot_sync(0xffffffffu, inside) >> (lane & ~(GRP - 1))) & ((1u << GRP) - 1u);
+            const int pos = cnt + __popc(grp & ((1u << sub) - 1u));
+            if (inside) {
+                if (pos < MLP_MAXN) {
+                    const float r = sqrtf(r2), ir = 1.0f / r;
+                    const float fc = mlp_fc(r), ex = __expf(-0.01f * r2), ev = ex * fc;
+                    T.u[pos][g] = make_float4(d0 * ir, d1 * ir, d2 * ir, ev);
+                    // exp(-4 (r - R_k)^2) by the recurrence over k (R_k = 2 + k h):
+                    // x_{k+1} = x_k exp(8 h t0) exp(-4 h^2 (2k + 1)), t0 = r - 2
+                    const float step[8] = {0.6248747f, 0.24399385f, 0.09527189f, 0.037200667f,
+                                           0.014525686f, 0.005671822f, 0.0022146674f, 0.0008647577f};
+                    const float t0 = r - 2.0f, q8 = __expf(2.7428572f * t0);
+                    float gk = __expf(-4.0f * t0 * t0);
+                    if constexpr (FORCE) {
+                        const float dfc = mlp_dfc(r);
+                        T.w[pos][g] = make_float2(ex * fmaf(-0.02f * r, fc, dfc), ev * ir);
+                        T.j[pos][g] = j;
+                        float sr = 0.0f;
+    #pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const float t = fmaf(-0.34285715f, (float)q, t0);
+                            sr = fmaf(gr[q], gk * fmaf(-8.0f * t, fc, dfc), sr);
+                            gk *= q8 * step[q];
+                        }
+                        T.srad[pos][g] = sr;
+                    } else {
+    #pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            rad[q] = fmaf(gk, fc, rad[q]);
+                            gk *= q8 * step[q];
+                        }
+                    }
+                } else {
+                    over = true;
+                }
+            }
+            cnt += __popc(grp);
         }
-        cnt += __popc(grp);
     }
     __syncwarp();
     return cnt < MLP_MAXN ? cnt : MLP_MAXN;

@@ -337,38 +337,128 @@ class ForceFrame:
             raise RuntimeError(f"EAM reference frame failed (status {eng.status():#x})")
 
 
+class FramePool:
+    """Frames of BCC-W cells (2 n_cells^3 atoms) from the engine's own EAM
+    runs: n_runs Langevin runs, each at a temperature drawn uniformly from
+    t_range and under a diagonal strain with components drawn uniformly from
+    +-strain; every `stride`-th step after `equilibrate` steps is a frame.
+    Kept per frame: positions (FP64, device), and for energy regression the
+    descriptors G and per-atom EAM energies E (rows concatenated over frames).
+    pool[k] loads frame k into its run's engine and returns a ForceFrame-like
+    view with the EAM forces and energies of those positions as targets
+    (buffers reused by the next pool[k])."""
+
+    def __init__(self, tables, *, n_frames: int = 20000, n_cells: int = 10, n_runs: int = 40, stride: int = 10,
+                 equilibrate: int = 200, t_range=(300.0, 1500.0), strain: float = 0.03, dt: float = 0.001,
+                 seed: int = 0, device=None):
+        dev = torch.device(device or "cuda")
+        rng = np.random.default_rng(seed)
+        self.tables = tables
+        self.engines, self.run_T, self.run_strain = [], [], []
+        per_run = [n_frames // n_runs + (1 if r < n_frames % n_runs else 0) for r in range(n_runs)]
+        x0 = bcc_cell(n_cells)
+        n = len(x0)
+        self.n = n
+        self.X = torch.empty(n_frames, n, 3, device=dev, dtype=torch.float64)
+        self.G = torch.empty(n_frames * n, N_DESC, device=dev, dtype=torch.float32)
+        self.E = torch.empty(n_frames * n, device=dev, dtype=torch.float32)
+        self.run_of = np.empty(n_frames, np.int64)
+        m = 183.84 * 1.036427e-4
+        f = 0
+        for r in range(n_runs):
+            T = float(rng.uniform(*t_range))
+            eps = rng.uniform(-strain, strain, 3)
+            H = np.diag(n_cells * 3.165 * (1.0 + eps))
+            x = x0 * (1.0 + eps)
+            v = rng.normal(0.0, math.sqrt(8.617333262e-5 * T / m), x.shape)
+            eng = MDEngine(x, np.zeros(n, np.int32), [183.84], H, 4.4, 0.5, velocities=v, device=dev)
+            ip = integrator_params(eng, dt, langevin=True, temperature=T, gamma=10.0, seed=int(rng.integers(1 << 30)))
+            eng.eam_forces(tables)
+
+            def advance(k):
+                for _ in range(k):
+                    eng.integrate_first(ip, 0)
+                    eng.rebuild_if_needed()
+                    eng.eam_forces_integrate(tables, ip)
+            advance(equilibrate)
+            for _ in range(per_run[r]):
+                advance(stride)
+                eng.eam_forces(tables)
+                self.X[f].copy_(eng.gather("x"))
+                self.G[f * n:(f + 1) * n].copy_(descriptors(eng)[:n])
+                self.E[f * n:(f + 1) * n].copy_(eam_atom_energy(eng, tables)[:n])
+                self.run_of[f] = r
+                f += 1
+            if eng.status() & ~_lib.SIM_STATUS_MLP_NEIGHBORS:
+                raise RuntimeError(f"EAM run for training data failed (status {eng.status():#x})")
+            self.engines.append(eng)
+            self.run_T.append(T)
+            self.run_strain.append(eps)
+        P = self.engines[0].n_pad
+        self._F = torch.zeros(P, 4, device=dev, dtype=torch.float32)
+        self._Et = torch.zeros(P, device=dev, dtype=torch.float32)
+        self._G = torch.zeros(P, N_DESC, device=dev, dtype=torch.float32)
+
+    def __len__(self):
+        return self.X.shape[0]
+
+    def __getitem__(self, k):
+        eng = self.engines[int(self.run_of[k])]
+        eng.load(self.X[k])
+        eng.eam_forces(self.tables)
+        self._F.copy_(eng.f32)
+        self._Et.copy_(eam_atom_energy(eng, self.tables))
+        _lib.call("sim_mlp_descriptors", eng.st_ref, _lib.ptr(self._G), eng.stream)
+
+        class View:
+            pass
+        fr = View()
+        fr.engine, fr.G, fr.E, fr.F = eng, self._G, self._Et[:eng.n], self._F
+        return fr
+
+
 def train_forces(net: MLPNet, frames, *, steps: int = 4000, lr: float = 1e-3, lr_final: float = 1e-4,
-                 w_energy: float = 1.0, w_force: float = 1.0, seed: int = 0, log_every: int = 0):
-    """Energy and force matching on ``ForceFrame`` s with Adam, one frame per
-    step: loss = w_energy mean_i (E_i - E_i^EAM)^2
-               + w_force sum_m |F_m - F_m^EAM|^2 / (3 n).
+                 w_energy: float = 1.0, w_force: float = 1.0, frames_per_step: int = 1, seed: int = 0,
+                 log_every: int = 0):
+    """Energy and force matching with Adam on ``frames`` (a list of
+    ``ForceFrame`` or a ``FramePool``), frames_per_step frames per step (their
+    gradients averaged): loss per frame = w_energy mean_i (E_i - E_i^EAM)^2
+                                       + w_force sum_m |F_m - F_m^EAM|^2 / (3 n).
     The network keeps its normalisation (train on energies first).  Returns
     the per-step force mean squares (device tensor, (eV/A)^2)."""
     dev = net.device
     grads = torch.zeros(N_PARAMS, device=dev, dtype=torch.float32)
+    gsum = torch.zeros_like(grads)
     m1 = torch.zeros_like(grads)
     m2 = torch.zeros_like(grads)
     loss = torch.zeros(1, device=dev, dtype=torch.float32)
     fmse = torch.zeros(steps, device=dev, dtype=torch.float32)
-    P = max(fr.engine.n_pad for fr in frames)
+    P = max(fr.engine.n_pad for fr in frames) if isinstance(frames, list) else frames.engines[0].n_pad
     e = torch.zeros(P, device=dev, dtype=torch.float32)
     d = torch.zeros(P, N_DESC, device=dev, dtype=torch.float32)
     ferr = torch.zeros(P, 4, device=dev, dtype=torch.float32)
     u = torch.zeros(P, N_DESC, device=dev, dtype=torch.float32)
-    order = np.random.default_rng(seed).permutation(steps) % len(frames)
+    B = max(1, int(frames_per_step))
+    order = np.random.default_rng(seed).permutation(steps * B) % len(frames)
+    st = torch.cuda.current_stream(dev).cuda_stream
     for s in range(steps):
-        fr = frames[int(order[s])]
-        eng = fr.engine
-        n, np_ = eng.n, eng.n_pad
-        net.forward_into(fr.G, n, e, d)
-        _lib.call("sim_mlp_backward", eng.st_ref, _lib.ptr(d), eng.stream)
-        fe = ferr[:np_]
-        torch.sub(eng.f32, fr.F, out=fe)
-        fmse[s] = fe[:n, :3].square().mean()
-        _lib.call("sim_mlp_force_contract", eng.st_ref, _lib.ptr(fe), _lib.ptr(u), eng.stream)
+        gsum.zero_()
+        for b in range(B):
+            fr = frames[int(order[s * B + b])]
+            eng = fr.engine
+            n, np_ = eng.n, eng.n_pad
+            net.forward_into(fr.G, n, e, d)
+            _lib.call("sim_mlp_backward", eng.st_ref, _lib.ptr(d), eng.stream)
+            fe = ferr[:np_]
+            torch.sub(eng.f32, fr.F, out=fe)
+            fmse[s] += fe[:n, :3].square().mean() / B
+            _lib.call("sim_mlp_force_contract", eng.st_ref, _lib.ptr(fe), _lib.ptr(u), eng.stream)
+            net.train_grads_fm(fr.G, fr.E, u, n, w_energy / B, w_force / B, n, grads, loss)
+            gsum += grads
         lr_s = lr * (lr_final / lr) ** (s / max(1, steps - 1))
-        net.train_step(fr.G, fr.E, n, grads, m1, m2, lr_s, s + 1, loss, u=u, w_energy=w_energy, w_force=w_force,
-                       n_force_atoms=n)
+        _lib.call("sim_mlp_adam", _lib.ptr(net.flat), _lib.ptr(gsum), _lib.ptr(m1), _lib.ptr(m2), float(lr_s), s + 1,
+                  st)
+        _lib.call("sim_mlp_pack", _lib.ptr(net.flat), *(_lib.ptr(t) for t in net.images), st)
         if log_every and (s + 1) % log_every == 0:
             print(f"step {s + 1}: force RMSE {math.sqrt(float(fmse[s + 1 - log_every:s + 1].mean())):.4f} eV/A, "
                   f"energy loss {float(loss):.3e} eV^2", flush=True)
@@ -485,54 +575,60 @@ class SurrogateRun:
         return self
 
 
+TRAINING_NOTE = ("python -m simulon_b200.mlp: 20,000 frames of 2,000-atom BCC-W cells from 40 Langevin EAM runs "
+                 "(T uniform in 300-1500 K, diagonal strain uniform in +-3 %, every 10th step of dt 1 fs after 200), "
+                 "per-atom EAM energies and EAM forces as targets; 20,000 Adam steps of energy regression "
+                 "(16,384 atoms each), then 12,000 steps of energy + force matching (4 frames each)")
+
+
 def main(argv=None):
     """Train the surrogate on the engine's EAM data and save its weights:
-    python -m simulon_b200.mlp POTENTIAL OUT.npz [--steps N] [--fm-steps M] ...
+    python -m simulon_b200.mlp POTENTIAL OUT.npz [--frames F] [--steps N] [--fm-steps M] ...
     Energy regression on per-atom EAM energies first, then energy and force
-    matching on whole frames."""
+    matching on whole frames (targets recomputed from the frame's positions)."""
     import argparse
     import time
     from .eam_parser import EAMDeviceTables, EAMParser
     ap = argparse.ArgumentParser(description=main.__doc__)
     ap.add_argument("potential")
     ap.add_argument("out")
+    ap.add_argument("--frames", type=int, default=20000, help="training frames")
+    ap.add_argument("--runs", type=int, default=40, help="EAM runs the frames come from")
+    ap.add_argument("--cells", type=int, default=10, help="BCC cells per side (2 n^3 atoms per frame)")
+    ap.add_argument("--stride", type=int, default=10, help="MD steps between frames")
     ap.add_argument("--steps", type=int, default=20000, help="energy-regression steps")
-    ap.add_argument("--frames", type=int, default=50, help="frames per (temperature, strain) run")
-    ap.add_argument("--cells", type=int, default=10)
-    ap.add_argument("--batch", type=int, default=16384)
-    ap.add_argument("--fm-steps", type=int, default=12000, help="force-matching steps (one frame each)")
-    ap.add_argument("--fm-cells", type=int, default=16)
-    ap.add_argument("--fm-frames", type=int, default=10, help="force-matching frames per (temperature, strain) run")
+    ap.add_argument("--batch", type=int, default=16384, help="atoms per energy-regression step")
+    ap.add_argument("--fm-steps", type=int, default=12000, help="force-matching steps")
+    ap.add_argument("--fm-batch", type=int, default=4, help="frames per force-matching step")
     ap.add_argument("--w-force", type=float, default=1.0)
     ap.add_argument("--lr-fm", type=float, default=1e-3)
     a = ap.parse_args(argv)
     dev = torch.device("cuda")
     tables = EAMDeviceTables(EAMParser(a.potential), dev)
     t0 = time.perf_counter()
-    G, E = generate_dataset(tables, n_cells=a.cells, frames_per_run=a.frames, seed=0, device=dev)
-    _, _, fm_raw = generate_dataset(tables, n_cells=a.fm_cells, frames_per_run=a.fm_frames, stride=20,
-                                    equilibrate=200, seed=7, device=dev, with_forces=True)
-    fm_frames = [ForceFrame(fr["x"], fr["H"], tables, dev) for fr in fm_raw]
-    del fm_raw
+    pool = FramePool(tables, n_frames=a.frames, n_cells=a.cells, n_runs=a.runs, stride=a.stride, seed=0,
+                     device=dev)
     val = {}
     for T, seed in ((300.0, 99), (1500.0, 98)):
         _, _, raw = generate_dataset(tables, n_cells=a.cells, temperatures=(T,), strains=(0.0,), frames_per_run=2,
                                      stride=40, equilibrate=200, seed=seed, device=dev, with_forces=True)
         val[T] = raw
+    torch.cuda.synchronize()
     t1 = time.perf_counter()
     net = MLPNet(dev, seed=0)
-    losses = train(net, G, E, steps=a.steps, batch=a.batch, log_every=max(1, a.steps // 10))
+    losses = train(net, pool.G, pool.E, steps=a.steps, batch=a.batch, log_every=max(1, a.steps // 10))
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     before = {T: force_rmse(net, tables, fr, dev) for T, fr in val.items()}
-    fmse = train_forces(net, fm_frames, steps=a.fm_steps, lr=a.lr_fm, w_force=a.w_force,
+    fmse = train_forces(net, pool, steps=a.fm_steps, lr=a.lr_fm, w_force=a.w_force, frames_per_step=a.fm_batch,
                         log_every=max(1, a.fm_steps // 10)) if a.fm_steps else torch.zeros(1)
     torch.cuda.synchronize()
     t3 = time.perf_counter()
     after = {T: force_rmse(net, tables, fr, dev) for T, fr in val.items()}
     net.save(a.out)
-    print(f"energy samples {G.shape[0]}, force frames {len(fm_frames)} x {fm_frames[0].engine.n} atoms; "
-          f"data {t1 - t0:.1f} s, energy fit {t2 - t1:.1f} s, force fit {t3 - t2:.1f} s")
+    print(f"frames {len(pool)} x {pool.n} atoms from {len(pool.engines)} runs "
+          f"(T {min(pool.run_T):.0f}-{max(pool.run_T):.0f} K); data {t1 - t0:.1f} s, "
+          f"energy fit {t2 - t1:.1f} s, force fit {t3 - t2:.1f} s")
     print(f"energy loss {float(losses[-100:].mean()):.3e} eV^2, force MSE (last 5%) "
           f"{float(fmse[-max(1, len(fmse) // 20):].mean()):.3e} (eV/A)^2")
     for T in val:
