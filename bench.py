@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the batched-replica form")
     p.add_argument("--no-lj", action="store_true", help="skip the LJ argon form")
     p.add_argument("--no-mlp", action="store_true", help="skip the MLP-surrogate form")
+    p.add_argument("--forms", default="plain,lj,mlp,batched",
+                   help="forms to run (profiling runs: e.g. --forms mlp prints only the mlp object)")
     p.add_argument("--lj-n", type=int, default=63, help="FCC cells per side of the LJ form (atoms = 4 n^3)")
     p.add_argument("--batch-replicas", type=int, default=48)
     p.add_argument("--batch-skin", type=float, default=0.75)
@@ -237,11 +239,25 @@ def run_b200(args):
         if world > 1:
             dist.barrier()
 
+    forms = set(f.strip() for f in args.forms.split(",") if f.strip())
+    tmp = tempfile.mkdtemp()
+    pot = write_potential(os.path.join(tmp, "W_synthetic.eam.fs"))
+    if "plain" not in forms:   # profiling runs of single forms
+        line = {"metric": METRIC, "unit": UNIT, "n_gpus": world, "forms": sorted(forms)}
+        if "lj" in forms and not args.no_lj:
+            line["lj"] = lj_form(args, sb, dev, world)
+        if "mlp" in forms and not args.no_mlp:
+            line["mlp"] = mlp_form(args, sb, pot, dev, world)
+        if "batched" in forms and not args.no_batched:
+            line["batched"] = batched_form(args, sb, pot, dev, world, rank, barrier)
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
     x, L = bcc(args.n)
     N = len(x)
     v = mb_velocities(N, 300.0, 1000 + rank)
-    tmp = tempfile.mkdtemp()
-    pot = write_potential(os.path.join(tmp, "W_synthetic.eam.fs"))
     parser = sb.EAMParser(pot)
     mol = sb.AtomFileReader.from_arrays(["W"] * N, x, L, parser.cutoff, device=dev, skin_thickness=0.5, is_fs=True)
     mol.atom_velocities = torch.tensor(v, device=dev)
@@ -343,11 +359,11 @@ def run_b200(args):
 
     if not args.no_extras and rank == 0:
         line["e2e"] = e2e(model, mol, x, v, args, dev)
-    if not args.no_lj:
+    if not args.no_lj and "lj" in forms:
         line["lj"] = lj_form(args, sb, dev, world)
-    if not args.no_mlp:
+    if not args.no_mlp and "mlp" in forms:
         line["mlp"] = mlp_form(args, sb, pot, dev, world)
-    if not args.no_batched:
+    if not args.no_batched and "batched" in forms:
         line["batched"] = batched_form(args, sb, pot, dev, world, rank, barrier)
     if world > 1:
         dist.destroy_process_group()
