@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "atom-steps/s (EAM-W, 1 B200): plain vs batched vs MLP at stated force RMSE"
 UNIT = "atom-steps/s"
-PASS2_DRAM_BYTES_PER_ATOM = (78706432 + 6443776) / 524288   # k_eam_force<1,1,1>, ncu --set full
+PASS2_DRAM_BYTES_PER_ATOM = (66975232 + 2780416) / 524288   # k_eam_force<1,1,1>, ncu --set full
 A_W, M_W = 3.165, 183.84
 
 
@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the batched-replica form")
     p.add_argument("--no-lj", action="store_true", help="skip the LJ argon form")
     p.add_argument("--no-mlp", action="store_true", help="skip the MLP-surrogate form")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the built-in launch shapes (profiling runs: fewer launches before the timed ones)")
     p.add_argument("--forms", default="plain,lj,mlp,batched",
                    help="forms to run (profiling runs: e.g. --forms mlp prints only the mlp object)")
     p.add_argument("--lj-n", type=int, default=63, help="FCC cells per side of the LJ form (atoms = 4 n^3)")
@@ -268,7 +270,8 @@ def run_b200(args):
     G = args.graph_steps
     # launch shapes of the two EAM passes, timed on this system (not cached)
     from simulon_b200 import autotune
-    shapes = autotune.tune_eam(eng, ff.tables, reps=10, use_cache=False)
+    shapes = {"density_threads": 0, "force_threads": 0, "ms": {}} if args.no_autotune else \
+        autotune.tune_eam(eng, ff.tables, reps=10, use_cache=False)
 
     # warm-up (captures the graph, runs W steps)
     model.run(max(args.warmup, G), graph_steps=G)
@@ -534,7 +537,8 @@ def mlp_form(args, sb, pot, dev, world):
     from simulon_b200 import autotune
     G0 = mlp.descriptors(eng)
     _, d0 = net.forward(G0, N)
-    shapes = autotune.tune_mlp(eng, reps=10, use_cache=False, dEdG=d0)
+    shapes = {"desc_group": 0, "force_group": 0, "ms": {}} if args.no_autotune else \
+        autotune.tune_mlp(eng, reps=10, use_cache=False, dEdG=d0)
     run = mlp.SurrogateRun(eng, net, tables, ip, judge_every=100, tolerance=0.05)
     run.run(max(args.warmup, 100) // 100 * 100)
     torch.cuda.synchronize()

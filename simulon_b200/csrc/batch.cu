@@ -378,10 +378,12 @@ __global__ void k_bb_flag_all(SimBatch B) {
 template <bool ORTHO>
 __global__ void __launch_bounds__(BATCH_DENSITY_THREADS, 3) k_bb_density(SimBatch B, SimEAMTables t, Window w) {
     extern __shared__ float2 s_dens[];
+    pdl_trigger();
     const SimEngine& e = B.e;
     const float2* dens = reinterpret_cast<const float2*>(t.dens_vd);
     for (int k = threadIdx.x; k < w.n_win; k += blockDim.x) s_dens[k] = __ldg(&dens[w.k_lo + k]);
     __syncthreads();
+    pdl_wait();   // the table is constant; positions, boxes and lists come from earlier kernels
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
     int4* __restrict__ posfp = reinterpret_cast<int4*>(e.posfp);
     const int32_t* __restrict__ nbr = e.nbr;
@@ -453,6 +455,7 @@ template <int MODE, bool ORTHO>
 __global__ void __launch_bounds__(BATCH_FORCE_THREADS, 1) k_bb_force(SimBatch B, SimEAMTables t, SimIntegrator ip,
                                                                      Window w) {
     extern __shared__ float4 s_tab4[];
+    pdl_trigger();
     const SimEngine& e = B.e;
     float4* tab_d = s_tab4;
     float2* tab_p = reinterpret_cast<float2*>(s_tab4 + w.n_win);
@@ -465,6 +468,7 @@ __global__ void __launch_bounds__(BATCH_FORCE_THREADS, 1) k_bb_force(SimBatch B,
         }
         __syncthreads();
     }
+    pdl_wait();   // pass 1's posfp and F' come from the previous kernel
     const int4* __restrict__ posfp = reinterpret_cast<const int4*>(e.posfp);
     const int32_t* __restrict__ nbr = e.nbr;
     const int64_t P = e.n_pad;
@@ -593,7 +597,11 @@ __global__ void k_bb_first_half(SimBatch B, SimIntegrator p) {
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
 }
 
-__global__ void k_bb_advance_step(uint64_t* ctr) { *ctr += 1; }
+__global__ void k_bb_advance_step(uint64_t* ctr) {
+    pdl_trigger();
+    pdl_wait();
+    *ctr += 1;
+}
 
 // Per-replica sums in two launches, both in a fixed order (deterministic, no
 // atomics): SIM_BATCH_RED_SPLIT blocks per replica each add a strided share of
@@ -602,6 +610,8 @@ __global__ void k_bb_advance_step(uint64_t* ctr) { *ctr += 1; }
 // rows into rep_red and, with a log, into row (*step % cap).
 #define BATCH_REDUCE_THREADS 512
 __global__ void __launch_bounds__(BATCH_REDUCE_THREADS) k_bb_reduce(SimBatch B) {
+    pdl_trigger();
+    pdl_wait();
     const int k = blockIdx.x / SIM_BATCH_RED_SPLIT, sl = blockIdx.x % SIM_BATCH_RED_SPLIT;
     const SimRep& R = B.rep[k];
     const int64_t c0 = R.off >> 5, c1 = (R.off + R.n_slots) >> 5;
@@ -637,6 +647,8 @@ __global__ void __launch_bounds__(BATCH_REDUCE_THREADS) k_bb_reduce(SimBatch B) 
 }
 
 __global__ void k_bb_reduce_final(SimBatch B, const uint64_t* step, double* log, int cap) {
+    pdl_trigger();
+    pdl_wait();
     const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (k >= B.n_rep || lane >= SIM_RED_SLOTS) return;
@@ -740,8 +752,8 @@ extern "C" int sim_batch_eam_density(const SimBatch* b, const SimEAMTables* t, v
     const void* fn = ortho ? (const void*)k_bb_density<true> : (const void*)k_bb_density<false>;
     const int g = persistent_grid(fn, BATCH_DENSITY_THREADS, smem, b->e.n);
     cudaStream_t st = (cudaStream_t)stream;
-    if (ortho) k_bb_density<true><<<g, BATCH_DENSITY_THREADS, smem, st>>>(*b, *t, w);
-    else k_bb_density<false><<<g, BATCH_DENSITY_THREADS, smem, st>>>(*b, *t, w);
+    if (ortho) launch_pdl(k_bb_density<true>, dim3(g), dim3(BATCH_DENSITY_THREADS), smem, st, *b, *t, w);
+    else launch_pdl(k_bb_density<false>, dim3(g), dim3(BATCH_DENSITY_THREADS), smem, st, *b, *t, w);
     return launch_status("sim_batch_eam_density");
 }
 
@@ -752,8 +764,8 @@ static void launch_bb_force(const SimBatch& b, const SimEAMTables& t, const SimI
     const size_t smem = (size_t)w.n_win * (sizeof(float4) + sizeof(float2));
     const void* fn = ortho ? (const void*)k_bb_force<MODE, true> : (const void*)k_bb_force<MODE, false>;
     const int g = persistent_grid(fn, BATCH_FORCE_THREADS, smem, b.e.n);
-    if (ortho) k_bb_force<MODE, true><<<g, BATCH_FORCE_THREADS, smem, st>>>(b, t, ip, w);
-    else k_bb_force<MODE, false><<<g, BATCH_FORCE_THREADS, smem, st>>>(b, t, ip, w);
+    if (ortho) launch_pdl(k_bb_force<MODE, true>, dim3(g), dim3(BATCH_FORCE_THREADS), smem, st, b, t, ip, w);
+    else launch_pdl(k_bb_force<MODE, false>, dim3(g), dim3(BATCH_FORCE_THREADS), smem, st, b, t, ip, w);
 }
 
 extern "C" int sim_batch_eam_force(const SimBatch* b, const SimEAMTables* t, const SimIntegrator* p, int32_t mode,
@@ -784,8 +796,8 @@ extern "C" int sim_batch_first_half(const SimBatch* b, const SimIntegrator* p, v
 extern "C" int sim_batch_reduce(const SimBatch* b, const uint64_t* step, double* log, int32_t log_cap, void* stream) {
     if (!batch_ok(b) || (log && (log_cap <= 0 || !step))) return SIM_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    k_bb_reduce<<<b->n_rep * SIM_BATCH_RED_SPLIT, BATCH_REDUCE_THREADS, 0, st>>>(*b);
-    k_bb_reduce_final<<<(int)ceil_div(b->n_rep, 8), 256, 0, st>>>(*b, step, log, log_cap);
+    launch_pdl(k_bb_reduce, dim3(b->n_rep * SIM_BATCH_RED_SPLIT), dim3(BATCH_REDUCE_THREADS), 0, st, *b);
+    launch_pdl(k_bb_reduce_final, dim3((unsigned)ceil_div(b->n_rep, 8)), dim3(256), 0, st, *b, step, log, log_cap);
     return launch_status("sim_batch_reduce");
 }
 
@@ -800,7 +812,7 @@ extern "C" int sim_batched_step(const SimBatch* b, const SimEAMTables* t, const 
     rc = sim_batch_reduce(b, p->step_ctr, log, log_cap, stream);
     if (rc != SIM_OK) return rc;
     if (last) return SIM_OK;
-    k_bb_advance_step<<<1, 1, 0, st>>>(p->step_ctr);
+    launch_pdl(k_bb_advance_step, dim3(1), dim3(1), 0, st, p->step_ctr);
     rc = launch_status("sim_batched_step");
     if (rc != SIM_OK) return rc;
     return sim_batch_rebuild_if_needed(b, stream);

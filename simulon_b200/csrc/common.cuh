@@ -27,6 +27,31 @@ int launch_eam_force_tiled(const SimEngine& e, const SimEAMTables& t, const SimI
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Programmatic dependent launch (sm_90 and later).  A kernel launched by
+// launch_pdl may be scheduled while its predecessor in the stream (or graph)
+// is still finishing: pdl_wait() returns once the predecessor has completed
+// and its writes are visible (at once when there is no programmatic
+// dependency), so everything before it may only read data the predecessor
+// does not write; pdl_trigger() lets the successor be scheduled from now on.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Mean duration in ms of reps calls of launch() on stream st, after one
 // untimed call (CUDA events on st; synchronises); negative on a CUDA error.
 template <class F>

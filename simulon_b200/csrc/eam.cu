@@ -49,6 +49,7 @@ namespace simb200 {
 template <bool SMEM, bool ORTHO>
 __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k_eam_density(SimEngine e, SimEAMTables t, Window w) {
     extern __shared__ float2 s_dens[];
+    pdl_trigger();
     const float2* dens = reinterpret_cast<const float2*>(t.dens_vd);
     const int nt = t.n_types;
     if (SMEM) {
@@ -57,6 +58,7 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k
                 s_dens[tt * w.n_win + k] = __ldg(&dens[(size_t)tt * t.n_r + w.k_lo + k]);
         __syncthreads();
     }
+    pdl_wait();   // the tables are constant; positions, box and list come from earlier kernels
     const BoxF b(*e.box);
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
     int4* __restrict__ posfp = reinterpret_cast<int4*>(e.posfp);
@@ -122,6 +124,7 @@ template <bool SINGLE, int INTEG, bool ORTHO>
 __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam_force(SimEngine e, SimEAMTables t, SimIntegrator ip,
                                                                     Window w) {
     extern __shared__ float4 s_tab4[];
+    pdl_trigger();
     float4* tab_d = s_tab4;
     float2* tab_p = reinterpret_cast<float2*>(s_tab4 + w.n_win);
     if (SINGLE) {
@@ -133,6 +136,7 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
         }
         __syncthreads();
     }
+    pdl_wait();   // pass 1's posfp and F', the box and the list come from earlier kernels
     const BoxF b(*e.box);
     const int4* __restrict__ posfp = reinterpret_cast<const int4*>(e.posfp);
     const int32_t* __restrict__ nbr = e.nbr;
@@ -313,7 +317,9 @@ static int launch_density(const SimEngine& e, const SimEAMTables& t, size_t smem
     if (threads < 0) return SIM_ERR_ARG;
     const int g = persistent_grid((const void*)k_eam_density<SMEM, ORTHO>, threads, smem, e.n);
     if (g > e.n_blocks_max) return SIM_ERR_ARG;
-    k_eam_density<SMEM, ORTHO><<<g, threads, smem, st>>>(e, t, table_window(t));
+    const cudaError_t err = launch_pdl(k_eam_density<SMEM, ORTHO>, dim3(g), dim3(threads), smem, st, e, t,
+                                       table_window(t));
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_eam_density: launch"); return SIM_ERR_CUDA; }
     return SIM_OK;
 }
 
@@ -342,7 +348,9 @@ static int launch_force(const SimEngine& e, const SimEAMTables& t, const SimInte
     if (threads < 0) return SIM_ERR_ARG;
     const int g = persistent_grid((const void*)k_eam_force<SINGLE, INTEG, ORTHO>, threads, smem, e.n);
     if (g > e.n_blocks_max) return SIM_ERR_ARG;
-    k_eam_force<SINGLE, INTEG, ORTHO><<<g, threads, smem, st>>>(e, t, ip, table_window(t));
+    const cudaError_t err = launch_pdl(k_eam_force<SINGLE, INTEG, ORTHO>, dim3(g), dim3(threads), smem, st, e, t, ip,
+                                       table_window(t));
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_eam_force: launch"); return SIM_ERR_CUDA; }
     return SIM_OK;
 }
 

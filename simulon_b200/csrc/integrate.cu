@@ -70,6 +70,8 @@ __device__ __forceinline__ double load_force(const SimEngine& e, int prec, int64
 }
 
 __global__ void __launch_bounds__(SIM_THREADS) k_first_half(SimEngine e, SimIntegrator p, int prec) {
+    pdl_trigger();
+    pdl_wait();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     bool trigger = false, bad = false;
     if (i == 0 && p.step_ctr) *p.step_ctr += 1;   // the step index sim_integrate_second reads
@@ -95,6 +97,8 @@ __device__ __forceinline__ void ke_terms(double m, const double* v, double* vals
 // Second half of the step (grid-stride over the atoms): kick, Langevin O-step,
 // kinetic energy and tensor.
 __global__ void __launch_bounds__(SIM_THREADS) k_second_half(SimEngine e, SimIntegrator p, int prec) {
+    pdl_trigger();
+    pdl_wait();
     double vals[7] = {0, 0, 0, 0, 0, 0, 0};
     bool bad = false;
     const uint64_t step = *p.step_ctr;
@@ -116,6 +120,8 @@ __global__ void __launch_bounds__(SIM_THREADS) k_second_half(SimEngine e, SimInt
 // posq refresh and the skin/2 trigger; the last block advances the step
 // counter (step_ctr[0] = s + 1, step_ctr[1] = s for the step log).
 __global__ void __launch_bounds__(SIM_THREADS) k_second_first(SimEngine e, SimIntegrator p, int prec) {
+    pdl_trigger();
+    pdl_wait();
     double vals[7] = {0, 0, 0, 0, 0, 0, 0};
     bool bad = false, trig = false;
     const uint64_t step = *p.step_ctr;
@@ -238,6 +244,8 @@ __global__ void k_scatter_f64(SimEngine e, const double* __restrict__ rows, doub
 }
 
 __global__ void k_log_step(SimEngine e, const uint64_t* ctr, const double* extra, int n_extra, double* log, int cap) {
+    pdl_trigger();
+    pdl_wait();
     const int w = SIM_RED_SLOTS + n_extra + 1;
     const uint64_t s = ctr ? *ctr : 0;
     double* row = log + (size_t)(s % (uint64_t)cap) * w;
@@ -268,7 +276,9 @@ using namespace simb200;
 
 extern "C" int sim_integrate_first(const SimEngine* ep, const SimIntegrator* p, int32_t force_precision, void* stream) {
     if (!ep || !p || ep->n <= 0 || (force_precision == 1 && !ep->f64)) return SIM_ERR_ARG;
-    k_first_half<<<(int)ceil_div(ep->n, SIM_THREADS), SIM_THREADS, 0, (cudaStream_t)stream>>>(*ep, *p, force_precision);
+    const cudaError_t err = launch_pdl(k_first_half, dim3((unsigned)ceil_div(ep->n, SIM_THREADS)), dim3(SIM_THREADS), 0,
+                                       (cudaStream_t)stream, *ep, *p, force_precision);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_integrate_first: launch"); return SIM_ERR_CUDA; }
     return launch_status("sim_integrate_first");
 }
 
@@ -277,7 +287,9 @@ extern "C" int sim_integrate_second(const SimEngine* ep, const SimIntegrator* p,
     if (p->langevin && !p->rff) return SIM_ERR_ARG;
     int blocks = persistent_grid((const void*)k_second_half, SIM_THREADS, 0, ep->n);
     if (blocks > ep->n_blocks_max) blocks = (int)ep->n_blocks_max;
-    k_second_half<<<blocks, SIM_THREADS, 0, (cudaStream_t)stream>>>(*ep, *p, force_precision);
+    const cudaError_t err = launch_pdl(k_second_half, dim3(blocks), dim3(SIM_THREADS), 0, (cudaStream_t)stream, *ep,
+                                       *p, force_precision);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_integrate_second: launch"); return SIM_ERR_CUDA; }
     return launch_status("sim_integrate_second");
 }
 
@@ -287,7 +299,9 @@ extern "C" int sim_integrate_second_first(const SimEngine* ep, const SimIntegrat
     if (p->langevin && !p->rff) return SIM_ERR_ARG;
     int blocks = persistent_grid((const void*)k_second_first, SIM_THREADS, 0, ep->n);
     if (blocks > ep->n_blocks_max) blocks = (int)ep->n_blocks_max;
-    k_second_first<<<blocks, SIM_THREADS, 0, (cudaStream_t)stream>>>(*ep, *p, force_precision);
+    const cudaError_t err = launch_pdl(k_second_first, dim3(blocks), dim3(SIM_THREADS), 0, (cudaStream_t)stream, *ep,
+                                       *p, force_precision);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_integrate_second_first: launch"); return SIM_ERR_CUDA; }
     return launch_status("sim_integrate_second_first");
 }
 
@@ -330,7 +344,9 @@ extern "C" int sim_scatter_original_f64(const SimEngine* ep, const double* rows,
 extern "C" int sim_log_step(const SimEngine* ep, const uint64_t* step_ctr, const double* extra, int32_t n_extra,
                             double* log, int32_t capacity, void* stream) {
     if (!ep || !log || capacity <= 0 || n_extra < 0 || n_extra > 32 || (n_extra > 0 && !extra)) return SIM_ERR_ARG;
-    k_log_step<<<1, 64, 0, (cudaStream_t)stream>>>(*ep, step_ctr, extra, n_extra, log, capacity);
+    const cudaError_t err = launch_pdl(k_log_step, dim3(1), dim3(64), 0, (cudaStream_t)stream, *ep, step_ctr, extra,
+                                       n_extra, log, capacity);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_log_step: launch"); return SIM_ERR_CUDA; }
     return launch_status("sim_log_step");
 }
 

@@ -161,6 +161,8 @@ template <bool ORTHO, int GRP>
 __global__ void __launch_bounds__(128) k_mlp_desc(SimEngine e, float* __restrict__ G) {
     constexpr int APB = 128 / GRP;
     __shared__ MlpTableU<APB> T;
+    pdl_trigger();
+    pdl_wait();
     const BoxF b(*e.box);
     const int g = threadIdx.x / GRP, sub = threadIdx.x % GRP;
     bool over = false;
@@ -445,6 +447,7 @@ __global__ void __launch_bounds__(MLP_TILE) k_mlp_fwd(SimMLP m, const float* __r
     extern __shared__ __align__(128) unsigned char smem_raw[];
     MlpFwdSmem& S = *reinterpret_cast<MlpFwdSmem*>(smem_raw);
     const int t = threadIdx.x, warp = t >> 5;
+    pdl_trigger();
     {
         const uint4* src[4] = {reinterpret_cast<const uint4*>(m.w1t_img), reinterpret_cast<const uint4*>(m.w2t_img),
                                reinterpret_cast<const uint4*>(m.w2_img), reinterpret_cast<const uint4*>(m.w1_img)};
@@ -476,6 +479,7 @@ __global__ void __launch_bounds__(MLP_TILE) k_mlp_fwd(SimMLP m, const float* __r
     bool failed = false;
     const int n_tiles = (int)((n + MLP_TILE - 1) / MLP_TILE);
     float gn[MLP_D];
+    pdl_wait();   // weights and tensor memory are set up; the descriptors come from the previous kernel
     {
         const int64_t i0 = (int64_t)blockIdx.x * MLP_TILE + t;
         mlp_load_row(G, i0, i0 < n, gn);
@@ -1300,8 +1304,8 @@ template <int GRP>
 static void launch_mlp_desc(const SimEngine& e, float* G, cudaStream_t st) {
     const int64_t groups = (e.n + 128 / GRP - 1) / (128 / GRP);
     const int g = (int)(groups < 148 * 12 ? groups : 148 * 12);
-    if (e.box_orthogonal) k_mlp_desc<true, GRP><<<g, 128, 0, st>>>(e, G);
-    else k_mlp_desc<false, GRP><<<g, 128, 0, st>>>(e, G);
+    if (e.box_orthogonal) launch_pdl(k_mlp_desc<true, GRP>, dim3(g), dim3(128), 0, st, e, G);
+    else launch_pdl(k_mlp_desc<false, GRP>, dim3(g), dim3(128), 0, st, e, G);
 }
 
 template <int GRP>
@@ -1367,7 +1371,7 @@ extern "C" int sim_mlp_forward(const SimMLP* m, const float* G, int64_t n, float
     mlp_set_attributes();
     const size_t smem = mlp_fwd_smem();
     const int g = mlp_grid((const void*)k_mlp_fwd, (n + MLP_TILE - 1) / MLP_TILE, smem, 128);
-    k_mlp_fwd<<<g, MLP_TILE, smem, (cudaStream_t)stream>>>(*m, G, n, e_atom, dEdG, status);
+    launch_pdl(k_mlp_fwd, dim3(g), dim3(MLP_TILE), smem, (cudaStream_t)stream, *m, G, n, e_atom, dEdG, status);
     return launch_status("sim_mlp_forward");
 }
 

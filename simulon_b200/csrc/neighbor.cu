@@ -541,6 +541,7 @@ extern "C" int sim_rebuild(const SimEngine* ep, int32_t only_if_flagged, void* s
 // launch instead of the whole rebuild sequence.
 
 __global__ void k_set_rebuild_condition(cudaGraphConditionalHandle h, const int32_t* flags) {
+    pdl_wait();
     cudaGraphSetConditional(h, flags[0] != 0 ? 1u : 0u);
 }
 
@@ -566,7 +567,8 @@ int simb200::launch_if_flag(cudaStream_t st, const int32_t* flag, BodyFn body, B
     cudaGraphConditionalHandle h;
     err = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
     if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: handle", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
-    k_set_rebuild_condition<<<1, 1, 0, st>>>(h, flag);
+    err = launch_pdl(k_set_rebuild_condition, dim3(1), dim3(1), 0, st, h, flag);
+    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: condition kernel", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
     err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
     if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: capture info 2", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
     cudaGraphNodeParams cp = {};
