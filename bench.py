@@ -598,29 +598,36 @@ def mlp_form(args, sb, pot, dev, world):
 
 def e2e(model, mol, x, v, args, dev):
     """Same metric through the public API with host buffers: pinned H2D of the
-    state, K steps, D2H of every step's scalars and of the final state."""
+    state, K steps, D2H of every step's scalars and of the final state into
+    pinned buffers.  One untimed pass of the same path first (it loads the
+    kernels this path uses that the device-resident run does not)."""
     import torch
     N = len(x)
     xh = torch.tensor(x).pin_memory()
     vh = torch.tensor(v).pin_memory()
     K = args.steps
-    log_h = torch.empty(K, model.engine.log.shape[1], dtype=torch.float64).pin_memory()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    mol.update_coordinates(xh)          # H2D + cell sort + list build
-    mol.atom_velocities = vh            # H2D
-    done = 0
     G = args.graph_steps
-    while done < K:
-        k = min(G * 5, K - done)
-        model.run(k, graph_steps=G)
-        log_h[done:done + k].copy_(model.step_log(model.steps_done - k, k), non_blocking=True)
-        done += k
-    x_out = mol.coordinates.cpu()
-    v_out = mol.atom_velocities.cpu()
-    torch.cuda.synchronize()
+    log_h = torch.empty(K, model.engine.log.shape[1], dtype=torch.float64).pin_memory()
+    x_out = torch.empty(N, 3, dtype=torch.float64).pin_memory()
+    v_out = torch.empty(N, 3, dtype=torch.float64).pin_memory()
+
+    def one_pass(n_steps):
+        mol.update_coordinates(xh)          # H2D + cell sort + list build
+        mol.atom_velocities = vh            # H2D
+        done = 0
+        while done < n_steps:
+            k = min(G * 5, n_steps - done)
+            model.run(k, graph_steps=G)
+            log_h[done:done + k].copy_(model.step_log(model.steps_done - k, k), non_blocking=True)
+            done += k
+        x_out.copy_(mol.coordinates)
+        v_out.copy_(mol.atom_velocities)
+        torch.cuda.synchronize()
+    one_pass(min(K, G * 5))
+    t0 = time.perf_counter()
+    one_pass(K)
     dt = time.perf_counter() - t0
-    assert torch.isfinite(x_out).all() and torch.isfinite(log_h).all()
+    assert torch.isfinite(x_out).all() and torch.isfinite(v_out).all() and torch.isfinite(log_h).all()
     row_bytes = log_h.shape[1] * 8
     return {"value": N * K / dt, "unit": UNIT, "h2d_bytes_per_step": 2 * N * 24 / K,
             "d2h_bytes_per_step": row_bytes + 2 * N * 24 / K, "seconds": dt,
