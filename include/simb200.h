@@ -55,6 +55,8 @@ extern "C" {
 #define SIM_STATUS_NONFINITE 16  /* device: NaN/Inf in forces, positions or velocities         */
 #define SIM_STATUS_CELLCAP   32  /* device: half-list export row capacity exceeded             */
 #define SIM_STATUS_HALO      64  /* device: a tile's halo exceeded halo_cap (flags[4] = size)  */
+#define SIM_STATUS_CELLS     512 /* device: the box shrank below the cell grid's rc + skin width
+                                    (a rebuild may miss pairs: rebuild the grid, MDEngine.regrid) */
 
 #define SIM_TILE 1024            /* atoms per neighbour tile (= threads of a tiled block)      */
 
@@ -200,6 +202,28 @@ typedef struct SimIntegrator {
     int32_t pad;
 } SimIntegrator;
 
+/* ---- anisotropic pressure control (barostat.py:78-208) and box scaling --- */
+typedef struct SimAniso {
+    double target_bar[3];      /* per lattice axis                                  */
+    double tau_p, gamma_p, max_eta_dot, kappa_bar_inv, tol_bar, dt, temperature;
+    double* eta_dot;           /* [3] device state: log strain rate per axis (1/ps) */
+    uint64_t* counter;         /* [1] device: calls so far (Philox counter of the noise) */
+    int32_t control[3];        /* 1 = the axis is controlled                        */
+    int32_t stochastic;        /* 1 = add the reference's thermal noise (Philox)    */
+    int32_t reset_reference;   /* 1 = last_positions reset after the step (reference) */
+    uint32_t seed;
+} SimAniso;
+/* work buffer of sim_aniso_npt / sim_box_scale: SIM_BOXSCALE_WORK doubles;
+ * [0..2] axis pressures (bar), [3..5] box scale, [6..8] velocity scale, then
+ * the new box (SimBox layout, from double 16). */
+#define SIM_BOXSCALE_WORK 64
+typedef struct SimBoxScale {
+    double scale[3];           /* H <- diag(scale) H                                 */
+    double vel_scale[3];       /* v_c <- v_c * vel_scale[c]                           */
+    int32_t reset_reference;   /* 1 = last_positions reset (loading.py:78)            */
+    int32_t pad;
+} SimBoxScale;
+
 /* ---- Berendsen (barostat.py:21-68) -------------------------------------- */
 typedef struct SimBerendsen {
     double target_bar, tau, kappa, mu_max, dt;
@@ -339,6 +363,19 @@ int sim_integrate_second_first(const SimEngine* e, const SimIntegrator* p, int32
  * P (bar) and mu on the device in FP64, scales box, coordinates (mu^power),
  * velocities; writes pressure_out[0] = P (bar), pressure_out[1] = mu. */
 int sim_berendsen(const SimEngine* e, const SimBerendsen* p, double* pressure_out, void* stream);
+
+/* AnisotropicNPTBarostat.step (barostat.py:137-208) on the device in FP64:
+ * axis pressures from the kinetic and virial tensors in red_out projected on
+ * the normalised lattice rows, the deadband, the damped strain-rate update
+ * (clamped, masked), H <- diag(exp(dt eta_dot)) H, positions through
+ * fractional coordinates into the new box and wrapped (box.py:132-142),
+ * velocities * exp(-dt eta_dot), posq refreshed, the skin test against the
+ * last rebuild and (reset_reference) the reference reset.  work: see
+ * SIM_BOXSCALE_WORK. */
+int sim_aniso_npt(const SimEngine* e, const SimAniso* p, double* work, void* stream);
+/* UniaxialTensileLoader.step's box update (loading.py:41-80): H <- diag(scale) H
+ * and the same position, velocity (vel_scale), posq and reference handling. */
+int sim_box_scale(const SimEngine* e, const SimBoxScale* p, double* work, void* stream);
 
 /* Scatter caller rows into slots: dst_soa[c*n_pad + k] = rows[orig[k]*3 + c]. */
 int sim_scatter_original_f64(const SimEngine* e, const double* rows, double* dst_soa, void* stream);
@@ -541,8 +578,8 @@ int sim_autotune_mlp(const SimEngine* e, const float* dEdG, float* G, int32_t re
 const char* sim_last_cuda_error(void);
 int sim_version(void);
 /* sizeof of SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator,
- * SimBerendsen, SimRep, SimBatch (host-only; lets bindings verify their
- * struct layouts; n >= 8). */
+ * SimBerendsen, SimRep, SimBatch, SimMLP, SimAniso, SimBoxScale (host-only;
+ * lets bindings verify their struct layouts; n >= 11). */
 int sim_struct_sizes(int64_t* out, int32_t n);
 
 #ifdef __cplusplus

@@ -82,6 +82,54 @@ def berendsen(box: OracleBox, coords, vel, dt, K_t, W_t, P0, tau, kappa=4.57e-5,
     return coords, vel * mu, P, mu
 
 
+def aniso_npt(box: OracleBox, coords, vel, eta_dot, dt, K_t, W_t, target_bar, tau_p=0.2, gamma_p=2.0,
+              control=(True, True, True), max_eta_dot=0.05, kappa=3.2e-7, tol=25.0):
+    """AnisotropicNPTBarostat.step without its optional noise (barostat.py:137-208):
+    returns (new wrapped coordinates, velocities, axis pressures in bar, eta_dot);
+    box.H is updated."""
+    f64 = torch.float64
+    p_int = (K_t.to(f64) + W_t.to(f64)) / box.volume
+    axes = box.H / torch.linalg.norm(box.H, dim=1, keepdim=True).clamp_min(1e-12)
+    p_axis_bar = torch.einsum("ai,ij,aj->a", axes, p_int, axes) * EV_ANG3_TO_BAR
+    target = torch.as_tensor(target_bar, dtype=f64).reshape(-1).expand(3)
+    ctrl = torch.as_tensor(control, dtype=torch.bool)
+    delta = p_axis_bar - target
+    within = delta.abs() <= tol
+    accel = kappa * torch.where(within, torch.zeros_like(delta), delta) / max(tau_p ** 2, 1e-12)
+    if gamma_p > 0.0:
+        accel = accel - gamma_p * eta_dot
+    if bool(within.any()):
+        accel = torch.where(within, -max(gamma_p, 5.0) * eta_dot, accel)
+    eta = torch.clamp(eta_dot + dt * accel, -max_eta_dot, max_eta_dot)
+    eta = torch.where(ctrl, eta, torch.zeros_like(eta))
+    eta = torch.where(within & (eta.abs() < 1e-7), torch.zeros_like(eta), eta)
+    scale = torch.where(ctrl, torch.exp(dt * eta), torch.ones_like(eta))
+    frac = coords.to(f64) @ box.H_inv
+    box.H = torch.diag(scale) @ box.H
+    box._refresh()
+    new = box.wrap_positions(frac @ box.H)
+    vs = torch.where(ctrl, torch.exp(-dt * eta), torch.ones_like(eta))
+    return new, vel * vs.unsqueeze(0), p_axis_bar, eta
+
+
+def uniaxial_box_step(box: OracleBox, coords, dt, axis=0, strain_rate=1e-3, lateral_mode="fixed",
+                      poisson_ratio=0.28, max_lateral_scale_step=2e-3):
+    """UniaxialTensileLoader.step's box and coordinate update (loading.py:41-73):
+    returns the new wrapped coordinates; box.H is updated."""
+    dstrain = strain_rate * float(dt)
+    scale = torch.ones(3, dtype=torch.float64)
+    scale[axis] = 1.0 + dstrain
+    if lateral_mode == "poisson":
+        lat = max(1.0 - poisson_ratio * dstrain, 1.0 - max_lateral_scale_step)
+        for ax in range(3):
+            if ax != axis:
+                scale[ax] = lat
+    frac = coords.to(torch.float64) @ box.H_inv
+    box.H = torch.diag(scale) @ box.H
+    box._refresh()
+    return box.wrap_positions(frac @ box.H)
+
+
 class OracleMD:
     """CPU restatement of one reference MD step (the timed CPU baseline too).
 
@@ -107,6 +155,7 @@ class OracleMD:
         self.F = None
         self.step_index = 0
         self.rebuilds = 0
+        self.eta_dot = torch.zeros(3, dtype=torch.float64)
         self._rebuild()
 
     def _rebuild(self):
@@ -131,6 +180,15 @@ class OracleMD:
             return
         self.x = xn
 
+    def load_step(self, **loader):
+        """UniaxialTensileLoader.step (loading.py:41-80): box and coordinates,
+        update_coordinates, last_positions reset; returns the axis strain."""
+        L0 = float(torch.linalg.norm(self.box.H[loader.get("axis", 0)]))
+        xn = uniaxial_box_step(self.box, self.x, self.integ.dt, **loader)
+        self.update_coordinates(xn.to(self.dtype))
+        self.last = self.x.clone()
+        return float(torch.linalg.norm(self.box.H[loader.get("axis", 0)])) / L0
+
     def step(self):
         if self.F is None:
             self.F = self.force_fn(self.x, self.i, self.j)["forces"].to(self.dtype)
@@ -145,8 +203,14 @@ class OracleMD:
         if self.barostat is not None:
             m = self.integ.atom_mass[:, :1]
             K_t = torch.einsum("ni,nj->ij", m * self.v, self.v)
-            self.x, self.v, P, mu = berendsen(self.box, self.x, self.v, self.integ.dt, K_t,
-                                              out["virial_tensor"], **self.barostat)
+            if self.barostat.get("kind") == "aniso":
+                kw = {k: v for k, v in self.barostat.items() if k != "kind"}
+                xn, self.v, P, self.eta_dot = aniso_npt(self.box, self.x, self.v, self.eta_dot, self.integ.dt, K_t,
+                                                        out["virial_tensor"], **kw)
+                self.update_coordinates(xn.to(self.dtype))
+            else:
+                self.x, self.v, P, mu = berendsen(self.box, self.x, self.v, self.integ.dt, K_t,
+                                                  out["virial_tensor"], **self.barostat)
             self.last = self.x.clone()
             res["pressure"] = P
         self.step_index += 1

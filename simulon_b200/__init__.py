@@ -4,15 +4,16 @@ Hand-written CUDA kernels behind a C ABI (include/simb200.h, libsimb200.so)
 with a Python host layer that mirrors the reference's plugin interfaces:
 
     AtomFileReader, Box, EAMParser, EAMForceCUDAExt / EAMForce, LennardJonesForce,
-    VerletIntegrator, BerendsenBarostat, SumBackboneInterface, BaseModel,
-    MDSimulator, find_neighbors_gpu_pbc, and the legacy ``simulon_cuda`` module.
+    VerletIntegrator, BerendsenBarostat, AnisotropicNPTBarostat,
+    UniaxialTensileLoader, SumBackboneInterface, BaseModel, MDSimulator,
+    find_neighbors_gpu_pbc, and the legacy ``simulon_cuda`` module.
 """
 from __future__ import annotations
 
 import sys
 
 from . import _lib
-from .barostat import BerendsenBarostat
+from .barostat import AnisotropicNPTBarostat, BerendsenBarostat
 from .batch import BatchedEngine, Replica, crack_slab, crack_sweep, partition_replicas
 from .box import Box
 from .eam_parser import EAMDeviceTables, EAMParser
@@ -21,6 +22,7 @@ from .forces import BackboneInterface, EAMForce, EAMForceCUDA, EAMForceCUDAExt, 
 from .integrator import IntegratorInterface, VerletIntegrator
 from .md_model import BaseModel, SumBackboneInterface
 from .md_simulation import MDSimulator
+from .mechanics import UniaxialTensileLoader
 from .neighbor import find_neighbors_gpu_pbc
 from .reader import AtomFileReader
 
@@ -38,4 +40,4 @@ __all__ = ["AtomFileReader", "Box", "EAMParser", "EAMDeviceTables", "EAMForce", 
            "LennardJonesForce", "BackboneInterface", "IntegratorInterface", "VerletIntegrator",
            "BerendsenBarostat", "SumBackboneInterface", "BaseModel", "MDSimulator", "MDEngine",
            "find_neighbors_gpu_pbc", "install_simulon_cuda", "BatchedEngine", "Replica", "crack_slab",
-           "crack_sweep", "partition_replicas"]
+           "crack_sweep", "partition_replicas", "AnisotropicNPTBarostat", "UniaxialTensileLoader"]

@@ -21,6 +21,8 @@ SIM_STATUS_NONFINITE = 16
 SIM_STATUS_HALO = 64
 SIM_STATUS_MLP_NEIGHBORS = 128
 SIM_STATUS_MLP_TIMEOUT = 256
+SIM_STATUS_CELLS = 512
+BOXSCALE_WORK = 64          # doubles of the sim_aniso_npt / sim_box_scale work buffer
 SIM_STATIC_MAX_ATOMS = 262144   # atom-slot limit of sim_eam_forces_static
 SIM_BATCH_RED_SPLIT = 8         # blocks that share one replica's reduction
 
@@ -85,6 +87,19 @@ class SimBerendsen(ctypes.Structure):
                 ("coordinate_scale_power", ctypes.c_int32), ("reset_reference", ctypes.c_int32)]
 
 
+class SimAniso(ctypes.Structure):
+    _fields_ = [("target_bar", ctypes.c_double * 3), ("tau_p", ctypes.c_double), ("gamma_p", ctypes.c_double),
+                ("max_eta_dot", ctypes.c_double), ("kappa_bar_inv", ctypes.c_double), ("tol_bar", ctypes.c_double),
+                ("dt", ctypes.c_double), ("temperature", ctypes.c_double), ("eta_dot", ctypes.c_void_p),
+                ("counter", ctypes.c_void_p), ("control", ctypes.c_int32 * 3), ("stochastic", ctypes.c_int32),
+                ("reset_reference", ctypes.c_int32), ("seed", ctypes.c_uint32)]
+
+
+class SimBoxScale(ctypes.Structure):
+    _fields_ = [("scale", ctypes.c_double * 3), ("vel_scale", ctypes.c_double * 3),
+                ("reset_reference", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
 class SimRep(ctypes.Structure):
     _fields_ = [("box", SimBox), ("off", ctypes.c_int64), ("first", ctypes.c_int64),
                 ("n", ctypes.c_int32), ("n_slots", ctypes.c_int32), ("ncell", ctypes.c_int32 * 3),
@@ -130,6 +145,8 @@ SIGNATURES = {
     "sim_integrate_second": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_integrate_second_first": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_berendsen": [_P(SimEngine), _P(SimBerendsen), c_p, c_p],
+    "sim_aniso_npt": [_P(SimEngine), _P(SimAniso), c_p, c_p],
+    "sim_box_scale": [_P(SimEngine), _P(SimBoxScale), c_p, c_p],
     "sim_gather_original_f64": [_P(SimEngine), c_p, c_p, c_p],
     "sim_gather_original_f32": [_P(SimEngine), c_p, c_p, c_p],
     "sim_scatter_original_f64": [_P(SimEngine), c_p, c_p, c_p],
@@ -167,7 +184,8 @@ SIGNATURES = {
     "sim_version": [],
     "sim_struct_sizes": [c_p, ctypes.c_int32],
 }
-STRUCTS = (SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator, SimBerendsen, SimRep, SimBatch)
+STRUCTS = (SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator, SimBerendsen, SimRep, SimBatch, SimMLP,
+           SimAniso, SimBoxScale)
 _RESTYPES = {"sim_last_cuda_error": ctypes.c_char_p}
 
 _lib = None

@@ -142,6 +142,151 @@ __global__ void __launch_bounds__(SIM_THREADS) k_second_first(SimEngine e, SimIn
     }
 }
 
+// ---- anisotropic pressure control and box scaling ---------------------------
+// (barostat.py:137-208, loading.py:41-80)  The new box is prepared by one
+// thread into work (from double 16), the atoms are mapped through fractional
+// coordinates of the old box into the new one and wrapped, then the box is
+// committed.
+
+__device__ double det3(const double* H);
+
+__device__ __forceinline__ SimBox& work_box(double* work) { return *reinterpret_cast<SimBox*>(work + 16); }
+
+// new box = diag(scale) H; H^-1 columns divided by the same factors
+__device__ void prepare_scaled_box(const SimBox& b, const double* scale, SimBox& nb) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            nb.H[3 * r + c] = scale[r] * b.H[3 * r + c];
+            nb.Hinv[3 * r + c] = b.Hinv[3 * r + c] / scale[c];
+            nb.Hf[3 * r + c] = (float)nb.H[3 * r + c];
+        }
+    nb.orthogonal = b.orthogonal;
+    nb.pad[0] = nb.pad[1] = nb.pad[2] = 0;
+}
+
+__global__ void k_aniso_control(SimEngine e, SimAniso p, double* work) {
+    pdl_wait();
+    const SimBox& b = *e.box;
+    const double* H = b.H;
+    const double* r = e.red_out;
+    const double V = fabs(det3(H));
+    const double kt[6] = {r[SIM_RED_K_XX] + r[SIM_RED_W_XX], r[SIM_RED_K_YY] + r[SIM_RED_W_YY],
+                          r[SIM_RED_K_ZZ] + r[SIM_RED_W_ZZ], r[SIM_RED_K_XY] + r[SIM_RED_W_XY],
+                          r[SIM_RED_K_XZ] + r[SIM_RED_W_XZ], r[SIM_RED_K_YZ] + r[SIM_RED_W_YZ]};
+    const double pm[3][3] = {{kt[0] / V, kt[3] / V, kt[4] / V}, {kt[3] / V, kt[1] / V, kt[5] / V},
+                             {kt[4] / V, kt[5] / V, kt[2] / V}};
+    double p_bar[3], delta[3];
+    bool within[3], any_within = false;
+    for (int a = 0; a < 3; ++a) {
+        const double* row = H + 3 * a;
+        const double nrm = fmax(sqrt(row[0] * row[0] + row[1] * row[1] + row[2] * row[2]), 1e-12);
+        const double ax[3] = {row[0] / nrm, row[1] / nrm, row[2] / nrm};
+        double pa = 0.0;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) pa += ax[i] * pm[i][j] * ax[j];
+        p_bar[a] = pa * 1602176.6208;
+        delta[a] = p_bar[a] - p.target_bar[a];
+        within[a] = fabs(delta[a]) <= p.tol_bar;
+        any_within |= within[a];
+    }
+    float z[3] = {0.f, 0.f, 0.f};
+    if (p.stochastic) langevin_normals(0xA5150u, *p.counter, p.seed, z[0], z[1], z[2]);
+    const double noise_sd = p.kappa_bar_inv * 8.617333262e-5 * fmax(p.temperature, 1.0) / fmax(p.tau_p, 1e-12);
+    double scale[3], vscale[3];
+    for (int a = 0; a < 3; ++a) {
+        const double eta = p.eta_dot[a];
+        double accel = p.kappa_bar_inv * (within[a] ? 0.0 : delta[a]) / fmax(p.tau_p * p.tau_p, 1e-12);
+        if (p.gamma_p > 0.0) accel -= p.gamma_p * eta;
+        if (p.stochastic) accel += (double)z[a] * noise_sd;
+        if (any_within && within[a]) accel = -fmax(p.gamma_p, 5.0) * eta;
+        double en = eta + p.dt * accel;
+        en = fmin(fmax(en, -p.max_eta_dot), p.max_eta_dot);
+        if (!p.control[a]) en = 0.0;
+        if (within[a] && fabs(en) < 1e-7) en = 0.0;
+        p.eta_dot[a] = en;
+        scale[a] = p.control[a] ? exp(p.dt * en) : 1.0;
+        vscale[a] = p.control[a] ? exp(-p.dt * en) : 1.0;
+        work[a] = p_bar[a];
+        work[3 + a] = scale[a];
+        work[6 + a] = vscale[a];
+    }
+    if (p.stochastic) *p.counter += 1;
+    prepare_scaled_box(b, scale, work_box(work));
+}
+
+__global__ void k_box_prepare(SimEngine e, SimBoxScale p, double* work) {
+    pdl_wait();
+    for (int a = 0; a < 3; ++a) {
+        work[a] = 0.0;
+        work[3 + a] = p.scale[a];
+        work[6 + a] = p.vel_scale[a];
+    }
+    prepare_scaled_box(*e.box, p.scale, work_box(work));
+}
+
+// Positions through fractional coordinates of the old box into the new one,
+// wrapped into [0, 1) of it (box.py:132-142), velocities scaled per Cartesian
+// component (the reference applies the axis factors to columns), posq, the
+// skin test and (reset) the reference reset.
+__global__ void __launch_bounds__(SIM_THREADS) k_scale_atoms(SimEngine e, const double* work, int reset) {
+    pdl_trigger();
+    pdl_wait();
+    const int64_t P = e.n_pad;
+    const SimBox& ob = *e.box;
+    const SimBox& nb = *reinterpret_cast<const SimBox*>(work + 16);
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool trig = false, bad = false;
+    if (i < e.n) {
+        double s[3], xn[3];
+        cart_to_frac(ob, e.x[i], e.x[P + i], e.x[2 * P + i], s);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) xn[c] = fma(s[2], nb.H[6 + c], fma(s[1], nb.H[3 + c], s[0] * nb.H[c]));
+        if (nb.orthogonal) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const double d = nb.H[4 * c];
+                xn[c] = xn[c] - floor(xn[c] / d) * d;
+            }
+        } else {
+            double t[3];
+            cart_to_frac(nb, xn[0], xn[1], xn[2], t);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) t[c] -= floor(t[c]);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) xn[c] = fma(t[2], nb.H[6 + c], fma(t[1], nb.H[3 + c], t[0] * nb.H[c]));
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double vc = e.v[c * P + i] * work[6 + c];
+            e.v[c * P + i] = vc;
+            bad |= !isfinite(xn[c]) || !isfinite(vc);
+        }
+        trig = place_atom(e, nb, i, e.posq[4 * i + 3], xn);
+        if (reset) {
+            e.xref[i] = e.posq[4 * i];
+            e.xref[P + i] = e.posq[4 * i + 1];
+            e.xref[2 * P + i] = e.posq[4 * i + 2];
+        }
+    }
+    if (__any_sync(0xffffffffu, trig) && (threadIdx.x & 31) == 0) e.flags[0] = 1;
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+}
+
+__global__ void k_box_commit(SimEngine e, const double* work) {
+    pdl_wait();
+    *e.box = *reinterpret_cast<const SimBox*>(work + 16);
+}
+
+static int launch_box_scale(const SimEngine& e, double* work, int reset, cudaStream_t st, const char* what) {
+    cudaError_t err = launch_pdl(k_scale_atoms, dim3((unsigned)ceil_div(e.n, SIM_THREADS)), dim3(SIM_THREADS), 0, st,
+                                 e, (const double*)work, reset);
+    if (err == cudaSuccess) err = launch_pdl(k_box_commit, dim3(1), dim3(1), 0, st, e, (const double*)work);
+    if (err != cudaSuccess) { set_cuda_error(err, what); return SIM_ERR_CUDA; }
+    return launch_status(what);
+}
+
 // ---- Berendsen -------------------------------------------------------------
 __device__ double det3(const double* H) {
     return H[0] * (H[4] * H[8] - H[5] * H[7]) - H[1] * (H[3] * H[8] - H[5] * H[6]) +
@@ -360,10 +505,30 @@ extern "C" const char* sim_last_cuda_error(void) { return g_err; }
 extern "C" int sim_version(void) { return 1; }
 
 extern "C" int sim_struct_sizes(int64_t* out, int32_t n) {
-    const int64_t sizes[8] = {(int64_t)sizeof(SimBox), (int64_t)sizeof(SimEngine), (int64_t)sizeof(SimEAMTables),
-                              (int64_t)sizeof(SimLJParams), (int64_t)sizeof(SimIntegrator),
-                              (int64_t)sizeof(SimBerendsen), (int64_t)sizeof(SimRep), (int64_t)sizeof(SimBatch)};
-    if (!out || n < 8) return SIM_ERR_ARG;
-    for (int k = 0; k < 8; ++k) out[k] = sizes[k];
+    const int64_t sizes[11] = {(int64_t)sizeof(SimBox), (int64_t)sizeof(SimEngine), (int64_t)sizeof(SimEAMTables),
+                               (int64_t)sizeof(SimLJParams), (int64_t)sizeof(SimIntegrator),
+                               (int64_t)sizeof(SimBerendsen), (int64_t)sizeof(SimRep), (int64_t)sizeof(SimBatch),
+                               (int64_t)sizeof(SimMLP), (int64_t)sizeof(SimAniso), (int64_t)sizeof(SimBoxScale)};
+    if (!out || n < 11) return SIM_ERR_ARG;
+    for (int k = 0; k < 11; ++k) out[k] = sizes[k];
     return SIM_OK;
 }
+
+extern "C" int sim_aniso_npt(const SimEngine* ep, const SimAniso* p, double* work, void* stream) {
+    if (!ep || !p || !work || ep->n <= 0 || !p->eta_dot || (p->stochastic && !p->counter)) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const cudaError_t err = launch_pdl(k_aniso_control, dim3(1), dim3(1), 0, st, *ep, *p, work);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_aniso_npt: control"); return SIM_ERR_CUDA; }
+    return launch_box_scale(*ep, work, p->reset_reference, st, "sim_aniso_npt");
+}
+
+extern "C" int sim_box_scale(const SimEngine* ep, const SimBoxScale* p, double* work, void* stream) {
+    if (!ep || !p || !work || ep->n <= 0) return SIM_ERR_ARG;
+    for (int a = 0; a < 3; ++a)
+        if (!(p->scale[a] > 0.0) || !(p->vel_scale[a] > 0.0)) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const cudaError_t err = launch_pdl(k_box_prepare, dim3(1), dim3(1), 0, st, *ep, *p, work);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_box_scale: prepare"); return SIM_ERR_CUDA; }
+    return launch_box_scale(*ep, work, p->reset_reference, st, "sim_box_scale");
+}
+

@@ -160,9 +160,27 @@ __global__ void k_zero_gated(int32_t* p, int64_t n, const int32_t* gate) {
 // ---------------------------------------------------------------------------
 // engine rebuild kernels (gate = flags, kernel returns unless flags[0] != 0)
 
+// Cells must stay at least rc + skin wide across each face for the 27-cell
+// stencil to see every pair; a box that shrank below that (a barostat, a
+// loader) is reported for the host to rebuild the grid (MDEngine.regrid).
+__device__ bool cells_cover(const SimEngine& e, const SimBox& b) {
+    const double* H = b.H;
+    const double V = fabs(H[0] * (H[4] * H[8] - H[5] * H[7]) - H[1] * (H[3] * H[8] - H[5] * H[6]) +
+                          H[2] * (H[3] * H[7] - H[4] * H[6]));
+    for (int a = 0; a < 3; ++a) {
+        if (e.ncell[a] < 3) continue;   // a 1- or 2-cell axis enumerates every cell
+        const double* u = H + 3 * ((a + 1) % 3);
+        const double* w = H + 3 * ((a + 2) % 3);
+        const double cx = u[1] * w[2] - u[2] * w[1], cy = u[2] * w[0] - u[0] * w[2], cz = u[0] * w[1] - u[1] * w[0];
+        if (V / sqrt(cx * cx + cy * cy + cz * cz) < e.x_rc * (double)e.ncell[a]) return false;
+    }
+    return true;
+}
+
 __global__ void k_bin(SimEngine e, const int32_t* gate) {
     if (gate && __ldg(gate) == 0) return;
     const SimBox& b = *e.box;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && !cells_cover(e, b)) atomicOr(&e.flags[1], SIM_STATUS_CELLS);
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < e.n; k += (int64_t)gridDim.x * blockDim.x) {
         double s[3];
         cart_to_frac(b, e.x[k], e.x[e.n_pad + k], e.x[2 * e.n_pad + k], s);

@@ -174,6 +174,9 @@ class MDEngine:
         # launch shapes (SimEngine.launch; 0 = built-in): EAM pass-1 / pass-2
         # threads per block, MLP descriptor / force threads per atom
         self.launch = [0, 0, 0, 0]
+        # bumped whenever device buffers are reallocated: CUDA graphs captured
+        # before then hold stale pointers
+        self.generation = 0
         self._make_struct()
         vel = None if velocities is None else torch.as_tensor(velocities).to(dev, torch.float64).contiguous()
         self.load(pos, vel)
@@ -257,6 +260,7 @@ class MDEngine:
             self._alloc_lists()
             self.flags.zero_()
             self._make_struct()
+            self.generation += 1
             _lib.call("sim_rebuild", self.st_ref, 0, self.stream)
             grew = True
         raise _lib.SimError("neighbour list / halo overflow persists after growing the capacity")
@@ -293,6 +297,34 @@ class MDEngine:
     def box_matrix(self) -> np.ndarray:
         raw = self.box_dev.cpu().numpy().tobytes()
         return box_from_struct(_lib.SimBox.from_buffer_copy(raw))
+
+    def cells_valid(self, H=None) -> bool:
+        """Whether every axis of the cell grid with 3 or more cells is still at
+        least rc + skin wide per cell for box H (default: the device box)."""
+        H = self.box_matrix() if H is None else np.asarray(H, np.float64)
+        w = perpendicular_widths(H)
+        return all(int(n) < 3 or w[k] / int(n) >= self.x_rc for k, n in enumerate(self.ncell))
+
+    def regrid(self) -> bool:
+        """Cell grid for the current device box (after a barostat or a loader
+        shrank cells below rc + skin, SIM_STATUS_CELLS) and a full reload: the
+        list is rebuilt on the new grid.  Synchronises; True if the grid changed."""
+        H = self.box_matrix()
+        nc = cell_grid(H, self.x_rc, self.n)
+        if np.array_equal(nc, self.ncell) and self.cells_valid(H):
+            return False
+        x, v = self.gather("x"), self.gather("v")
+        self.ncell = nc
+        self.n_cells = int(np.prod(nc))
+        i32 = dict(device=self.device, dtype=torch.int32)
+        self.cell_count = torch.zeros(self.n_cells + 1, **i32)
+        self.cell_start = torch.zeros(self.n_cells + 1, **i32)
+        r, lin = morton_rank(nc)
+        self.cell_rank = torch.from_numpy(np.concatenate([r, lin])).to(self.device)
+        self._make_struct()
+        self.generation += 1
+        self.load(x, v)
+        return True
 
     def set_box(self, H):
         self.box = make_box(H)

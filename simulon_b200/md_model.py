@@ -109,7 +109,7 @@ class BaseModel(nn.Module):
                     kinetic_energy=ke,
                     temperature=lambda: (2.0 / 3.0) * ke() / (n * kB))
         if self.barostat is not None:
-            prod["pressure"] = lambda: eng.extra[0]
+            prod["pressure"] = self.barostat.pressure
         return LazyOutputs(**prod)
 
     def _prime(self):
@@ -129,6 +129,9 @@ class BaseModel(nn.Module):
 
     # ---- graph-captured multi-step execution ------------------------------
     def _graph(self, k: int):
+        if getattr(self, "_graph_generation", None) != self.engine.generation:
+            self._graphs = {}   # the engine's buffers were reallocated (MDEngine.regrid)
+            self._graph_generation = self.engine.generation
         if k not in self._graphs:
             s = torch.cuda.Stream(self.engine.device)
             s.wait_stream(torch.cuda.current_stream(self.engine.device))

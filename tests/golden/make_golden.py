@@ -13,6 +13,7 @@ small .npz next to this script; the tests read only those files.
 """
 from __future__ import annotations
 
+import json
 import os
 import sys
 import tempfile
@@ -233,6 +234,53 @@ def md_cases(tmp):
               rebuilds=mol.profile["neighbor_builds"], **{k: np.array(v) for k, v in rec.items() if v})
 
 
+def mech_cases(tmp):
+    """Tensile-workflow callers of the force path (LJ argon 108, FP64, NVE, 20
+    steps): UniaxialTensileLoader on axis 0 with the AnisotropicNPTBarostat on
+    the lateral axes (run_scripts/w_tensile.py's stress-free mode), and the
+    barostat alone on all axes towards 500 bar."""
+    from core.force.lennard_jones_force import LennardJonesForce
+    from core.integrator.integrator import VerletIntegrator
+    from core.md_model import BaseModel, SumBackboneInterface
+    from core.barostat import AnisotropicNPTBarostat
+    from core.mechanics.loading import UniaxialTensileLoader
+
+    torch.set_default_dtype(torch.float64)
+    try:
+        x, L = oin.fcc_lattice(3)
+        x = oin.jitter(x, 0.05, 0)
+        v0 = oin.maxwell_boltzmann(np.full(len(x), oin.AR_MASS), 94.4, 1)
+        params = {"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}}
+        cases = {
+            "tensile": (dict(axis=0, strain_rate=2.0, lateral_mode="fixed"),
+                        dict(target_pressure_bar=[0.0, 0.0, 0.0], control_axes=(False, True, True))),
+            "aniso": (None, dict(target_pressure_bar=[500.0, 500.0, 500.0], control_axes=(True, True, True))),
+        }
+        for name, (load, baro_kw) in cases.items():
+            mol = _reader(tmp, f"ar108{name}", x, "Ar", L, 7.0, 0.5, params=params)
+            integ = VerletIntegrator(mol, dt=0.002, ensemble="NVE")
+            mol.atom_velocities = torch.tensor(v0)
+            baro = AnisotropicNPTBarostat(mol, temperature_k=94.4, tau_p=0.2, gamma_p=2.0,
+                                          compressibility_bar_inv=3.2e-5, pressure_tolerance_bar=25.0, **baro_kw)
+            model = BaseModel(SumBackboneInterface([LennardJonesForce(mol)], mol), integ, mol, barostat=baro)
+            loader = UniaxialTensileLoader(mol, **load) if load else None
+            rec = {k: [] for k in ("energy", "kinetic_energy", "pressure", "strain", "H", "eta_dot")}
+            for _ in range(20):
+                rec["strain"].append(loader.step(0.002) if loader else 0.0)
+                out = model()
+                rec["energy"].append(float(out["energy"]))
+                rec["kinetic_energy"].append(float(out["kinetic_energy"]))
+                rec["pressure"].append(out["pressure"].detach().numpy().copy())
+                rec["H"].append(mol.box.H.detach().numpy().copy())
+                rec["eta_dot"].append(baro.eta_dot.detach().numpy().copy())
+            _save(f"mech_ar108_{name}_f64", x0=x, v0=v0, box0=L, dt=0.002, steps=20, x=mol.coordinates,
+                  v=mol.atom_velocities, rebuilds=mol.profile["neighbor_builds"],
+                  load=np.array(json.dumps(load)), baro=np.array(json.dumps(baro_kw)),
+                  **{k: np.array(v) for k, v in rec.items()})
+    finally:
+        torch.set_default_dtype(torch.float32)
+
+
 def main():
     if not os.path.isdir(REF):
         raise SystemExit(f"reference checkout not found at {REF}")
@@ -246,6 +294,7 @@ def main():
             lj_cases(tmp)
             eam_cases(tmp)
             md_cases(tmp)
+            mech_cases(tmp)
         finally:
             builtins.print = quiet
 

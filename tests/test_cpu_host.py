@@ -41,8 +41,8 @@ def test_library_exports_every_declared_symbol(lib):
 
 def test_struct_layouts_match(lib):
     from simulon_b200 import _lib
-    out = np.zeros(8, np.int64)
-    assert lib.sim_struct_sizes(out.ctypes.data, 8) == 0
+    out = np.zeros(len(_lib.STRUCTS), np.int64)
+    assert lib.sim_struct_sizes(out.ctypes.data, len(_lib.STRUCTS)) == 0
     assert list(out) == [ctypes.sizeof(s) for s in _lib.STRUCTS]
     assert lib.sim_version() == 1
 

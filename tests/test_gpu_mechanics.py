@@ -1,0 +1,122 @@
+"""Tensile-workflow callers of the force path on the GPU: the device
+UniaxialTensileLoader and AnisotropicNPTBarostat against the reference's own
+run (tests/golden/mech_ar108_*_f64.npz, written by running the unmodified
+reference; the oracle's restatement is pinned to the same vectors by
+tests/test_oracle_golden.py).  LJ argon 108 atoms, FP64 forces, NVE: energies
+and axis pressures to 1e-8 relative, box to 1e-12, strain rates to 1e-7,
+final wrapped positions to 1e-8 A and velocities to 1e-7 A/ps.  Also: the
+cell-grid guard reports a box that shrank below the list cutoff per cell, and
+MDEngine.regrid repairs it."""
+import json
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import inputs as oin
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda")
+
+
+@pytest.fixture(scope="module")
+def sb():
+    import simulon_b200
+    simulon_b200._lib.load()
+    return simulon_b200
+
+
+def _golden(name):
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    with np.load(os.path.join(here, name + ".npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+@pytest.mark.parametrize("name", ["tensile", "aniso"])
+@pytest.mark.parametrize("graph", [False, True])
+def test_tensile_and_aniso_npt_match_reference(sb, tmp_path, name, graph):
+    from simulon_b200.barostat import AnisotropicNPTBarostat
+    from simulon_b200.mechanics import UniaxialTensileLoader
+    g = _golden(f"mech_ar108_{name}_f64")
+    load_kw = json.loads(str(g["load"]))
+    baro_kw = json.loads(str(g["baro"]))
+    torch.set_default_dtype(torch.float64)
+    try:
+        path = oin.write_xyz(str(tmp_path / "ar.xyz"), g["x0"], "Ar")
+        mol = sb.AtomFileReader(path, float(g["box0"]), 7.0, device=DEV,
+                                parameter={"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}}, skin_thickness=0.5)
+        integ = sb.VerletIntegrator(mol, dt=float(g["dt"]), ensemble="NVE")
+        mol.atom_velocities = torch.tensor(g["v0"], device=DEV)
+        baro = AnisotropicNPTBarostat(mol, temperature_k=94.4, tau_p=0.2, gamma_p=2.0, compressibility_bar_inv=3.2e-5,
+                                      pressure_tolerance_bar=25.0, **baro_kw)
+        model = sb.BaseModel(sb.SumBackboneInterface([sb.LennardJonesForce(mol)], mol), integ, mol, barostat=baro)
+        loader = UniaxialTensileLoader(mol, **load_kw) if load_kw else None
+        E, P, H, eta, strain = [], [], [], [], []
+        for s in range(int(g["steps"])):
+            strain.append(loader.step(float(g["dt"])) if loader else 0.0)
+            if graph and loader is None and s == 0:
+                model.run(int(g["steps"]), graph_steps=5)    # whole run as CUDA graphs: no per-step record
+                break
+            out = model()
+            E.append(float(out["energy"]))
+            P.append(out["pressure"].cpu().numpy().copy())
+            H.append(mol.engine.box_matrix())
+            eta.append(baro.eta_dot.cpu().numpy().copy())
+        if E:
+            np.testing.assert_allclose(E, g["energy"], rtol=1e-9)
+            np.testing.assert_allclose(np.array(P), g["pressure"], rtol=1e-8, atol=1e-6)
+            np.testing.assert_allclose(np.array(H), g["H"], rtol=1e-12, atol=1e-12)
+            np.testing.assert_allclose(np.array(eta), g["eta_dot"], rtol=1e-7, atol=1e-12)
+            np.testing.assert_allclose(strain, g["strain"], rtol=1e-12)
+        else:
+            np.testing.assert_allclose(mol.engine.box_matrix(), g["H"][-1], rtol=1e-12, atol=1e-12)
+            np.testing.assert_allclose(baro.eta_dot.cpu().numpy(), g["eta_dot"][-1], rtol=1e-7, atol=1e-12)
+        np.testing.assert_allclose(mol.coordinates.cpu().numpy(), g["x"], atol=1e-8)
+        np.testing.assert_allclose(mol.atom_velocities.cpu().numpy(), g["v"], atol=1e-7)
+        assert mol.engine.status() == 0
+    finally:
+        torch.set_default_dtype(torch.float32)
+
+
+def test_cell_guard_and_regrid(sb, tmp_path):
+    """A loader that contracts the lateral axes (Poisson) below the grid's
+    rc + skin per cell: the rebuild reports SIM_STATUS_CELLS unless the loader
+    regrids, and after the regrid the list equals a fresh engine's list."""
+    from simulon_b200 import _lib
+    from simulon_b200.mechanics import UniaxialTensileLoader
+    x, L = oin.bcc_lattice(12)                      # 37.98 A: 7 cells of 5.43 A at rc + skin = 4.9 A
+    x = oin.jitter(x, 0.03, 5)
+    eng = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], np.diag([L] * 3), 4.4, 0.5, device=DEV)
+    assert list(eng.ncell) == [7, 7, 7]
+    # shrink y and z by 12 % directly: the next rebuild must flag the grid
+    work = torch.zeros(_lib.BOXSCALE_WORK, dtype=torch.float64, device=DEV)
+    s = _lib.SimBoxScale()
+    s.scale[:] = [1.0, 0.88, 0.88]
+    s.vel_scale[:] = [1.0, 1.0, 1.0]
+    s.reset_reference = 1
+    import ctypes
+    _lib.call("sim_box_scale", eng.st_ref, ctypes.byref(s), _lib.ptr(work), eng.stream)
+    eng.rebuild(only_if_flagged=False)
+    assert eng.status() & _lib.SIM_STATUS_CELLS
+    assert not eng.cells_valid()
+    assert eng.regrid()
+    assert eng.status() == 0 and eng.cells_valid()
+    assert list(eng.ncell) == [7, 6, 6]
+    ref = sb.MDEngine(eng.gather("x").cpu().numpy(), np.zeros(len(x), np.int32), [oin.W_MASS], eng.box_matrix(),
+                      4.4, 0.5, device=DEV)
+    a, _ = eng.half_list(4.9 ** 2)
+    b, _ = ref.half_list(4.9 ** 2)
+    pa = set(zip(a[0].tolist(), a[1].tolist()))
+    pb = set(zip(b[0].tolist(), b[1].tolist()))
+    assert pa == pb and len(pa) > 0
+    # the loader regrids by itself
+    eng2 = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], np.diag([L] * 3), 4.4, 0.5, device=DEV)
+
+    class Mol:
+        engine = eng2
+    loader = UniaxialTensileLoader(Mol(), axis=0, strain_rate=50.0, lateral_mode="poisson", poisson_ratio=0.3,
+                                   max_lateral_scale_step=0.05)
+    for _ in range(10):
+        loader.step(0.002)
+    assert loader.regrids >= 1 and eng2.cells_valid() and eng2.status() == 0

@@ -188,3 +188,35 @@ def test_md_eam_fp32_matches_reference(fsw, ens):
         np.testing.assert_allclose([r["pressure"] for r in e], g["pressure"], rtol=1e-3, atol=50.0)
         np.testing.assert_allclose(box.H.numpy(), g["box"], rtol=1e-6)
     np.testing.assert_allclose(md.x.numpy(), g["x"], atol=1e-4)
+
+
+@pytest.mark.parametrize("name", ["tensile", "aniso"])
+def test_tensile_and_aniso_npt_match_reference(name):
+    """UniaxialTensileLoader + AnisotropicNPTBarostat (lateral axes) and the
+    barostat alone, LJ argon FP64: the oracle's restatement against the
+    reference's own run (energies, axis pressures, box, strain rates, final
+    positions and velocities)."""
+    import json
+    g = load(f"mech_ar108_{name}_f64")
+    box = OracleBox(float(g["box0"]))
+    load_kw = json.loads(str(g["load"]))
+    baro_kw = json.loads(str(g["baro"]))
+    baro = dict(kind="aniso", target_bar=baro_kw["target_pressure_bar"], control=tuple(baro_kw["control_axes"]),
+                tau_p=0.2, gamma_p=2.0, kappa=3.2e-5, tol=25.0)
+    md = OracleMD(g["x0"], g["v0"], np.full(108, oin.AR_MASS), box, _lj_force_fn(box, 0.0104, 3.405),
+                  cutoff=7.0, skin=0.5, dt=float(g["dt"]), barostat=baro)
+    E, P, H, eta = [], [], [], []
+    for _ in range(int(g["steps"])):
+        if load_kw:
+            md.load_step(**load_kw)
+        r = md.step()
+        E.append(float(r["energy"]))
+        P.append(r["pressure"].numpy())
+        H.append(box.H.numpy().copy())
+        eta.append(md.eta_dot.numpy().copy())
+    np.testing.assert_allclose(E, g["energy"], rtol=1e-9)
+    np.testing.assert_allclose(np.array(P), g["pressure"], rtol=1e-8, atol=1e-6)
+    np.testing.assert_allclose(np.array(H), g["H"], rtol=1e-12)
+    np.testing.assert_allclose(np.array(eta), g["eta_dot"], rtol=1e-8, atol=1e-12)
+    np.testing.assert_allclose(md.x.numpy(), g["x"], atol=1e-9)
+    np.testing.assert_allclose(md.v.numpy(), g["v"], atol=1e-9)
