@@ -224,6 +224,14 @@ typedef struct SimBoxScale {
     int32_t pad;
 } SimBoxScale;
 
+/* ---- spherical indenter (core/mechanics/indenter.py:7-68) --------------- */
+typedef struct SimIndenter {
+    const double* center;      /* [3] device (settable between graph replays)      */
+    double radius, stiffness;  /* R (A), K (eV/A^3)                                  */
+    double* out;               /* [11] device: energy, force on the indenter (3),
+                                  contact atoms, virial xx yy zz xy xz yz            */
+} SimIndenter;
+
 /* ---- Berendsen (barostat.py:21-68) -------------------------------------- */
 typedef struct SimBerendsen {
     double target_bar, tau, kappa, mu_max, dt;
@@ -376,6 +384,14 @@ int sim_aniso_npt(const SimEngine* e, const SimAniso* p, double* work, void* str
 /* UniaxialTensileLoader.step's box update (loading.py:41-80): H <- diag(scale) H
  * and the same position, velocity (vel_scale), posq and reference handling. */
 int sim_box_scale(const SimEngine* e, const SimBoxScale* p, double* work, void* stream);
+
+/* SphericalIndenterForce.forward (indenter.py:40-68) added to the engine's
+ * forces (force_precision 0: f32, 1: f64) after a force field's pass: for
+ * atoms with d = |x - c| < R, F = K (R - d)^2 (x - c)/d, U = K/3 (R - d)^3,
+ * virial F (x) x; the energy, the trace and the tensor's upper triangle are
+ * added to red_out (EPOT_PAIR, VIRIAL, W), and out[] gets the indenter's own
+ * sums.  Positions are the FP64 unwrapped ones, without periodic images. */
+int sim_indenter_add(const SimEngine* e, const SimIndenter* p, int32_t force_precision, void* stream);
 
 /* Scatter caller rows into slots: dst_soa[c*n_pad + k] = rows[orig[k]*3 + c]. */
 int sim_scatter_original_f64(const SimEngine* e, const double* rows, double* dst_soa, void* stream);
@@ -578,8 +594,8 @@ int sim_autotune_mlp(const SimEngine* e, const float* dEdG, float* G, int32_t re
 const char* sim_last_cuda_error(void);
 int sim_version(void);
 /* sizeof of SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator,
- * SimBerendsen, SimRep, SimBatch, SimMLP, SimAniso, SimBoxScale (host-only;
- * lets bindings verify their struct layouts; n >= 11). */
+ * SimBerendsen, SimRep, SimBatch, SimMLP, SimAniso, SimBoxScale, SimIndenter
+ * (host-only; lets bindings verify their struct layouts; n >= 12). */
 int sim_struct_sizes(int64_t* out, int32_t n);
 
 #ifdef __cplusplus

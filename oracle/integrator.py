@@ -130,6 +130,26 @@ def uniaxial_box_step(box: OracleBox, coords, dt, axis=0, strain_rate=1e-3, late
     return box.wrap_positions(frac @ box.H)
 
 
+def indenter(x, center, radius, stiffness):
+    """SphericalIndenterForce.forward (indenter.py:40-68): forces, energy,
+    virial (F (x) x), force on the indenter and contact count, FP64."""
+    x = x.to(torch.float64)
+    disp = x - torch.as_tensor(center, dtype=torch.float64)
+    dist = torch.linalg.norm(disp, dim=1).clamp_min(1e-12)
+    pen = radius - dist
+    act = pen > 0.0
+    F = torch.zeros_like(x)
+    W = torch.zeros(3, 3, dtype=torch.float64)
+    E = torch.zeros((), dtype=torch.float64)
+    if bool(act.any()):
+        fv = stiffness * pen[act].pow(2).unsqueeze(1) * (disp[act] / dist[act].unsqueeze(1))
+        F[act] = fv
+        E = stiffness / 3.0 * pen[act].pow(3).sum()
+        W = torch.einsum("ni,nj->ij", fv, x[act])
+    return dict(forces=F, energy=E, virial=torch.trace(W), virial_tensor=W, force_on_indenter=-F.sum(0),
+                contact_atoms=int(act.sum()))
+
+
 class OracleMD:
     """CPU restatement of one reference MD step (the timed CPU baseline too).
 

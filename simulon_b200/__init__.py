@@ -5,7 +5,7 @@ with a Python host layer that mirrors the reference's plugin interfaces:
 
     AtomFileReader, Box, EAMParser, EAMForceCUDAExt / EAMForce, LennardJonesForce,
     VerletIntegrator, BerendsenBarostat, AnisotropicNPTBarostat,
-    UniaxialTensileLoader, SumBackboneInterface, BaseModel, MDSimulator,
+    UniaxialTensileLoader, SphericalIndenterForce, SumBackboneInterface, BaseModel, MDSimulator,
     find_neighbors_gpu_pbc, and the legacy ``simulon_cuda`` module.
 """
 from __future__ import annotations
@@ -22,7 +22,7 @@ from .forces import BackboneInterface, EAMForce, EAMForceCUDA, EAMForceCUDAExt, 
 from .integrator import IntegratorInterface, VerletIntegrator
 from .md_model import BaseModel, SumBackboneInterface
 from .md_simulation import MDSimulator
-from .mechanics import UniaxialTensileLoader
+from .mechanics import SphericalIndenterForce, UniaxialTensileLoader
 from .neighbor import find_neighbors_gpu_pbc
 from .reader import AtomFileReader
 
@@ -40,4 +40,5 @@ __all__ = ["AtomFileReader", "Box", "EAMParser", "EAMDeviceTables", "EAMForce", 
            "LennardJonesForce", "BackboneInterface", "IntegratorInterface", "VerletIntegrator",
            "BerendsenBarostat", "SumBackboneInterface", "BaseModel", "MDSimulator", "MDEngine",
            "find_neighbors_gpu_pbc", "install_simulon_cuda", "BatchedEngine", "Replica", "crack_slab",
-           "crack_sweep", "partition_replicas", "AnisotropicNPTBarostat", "UniaxialTensileLoader"]
+           "crack_sweep", "partition_replicas", "AnisotropicNPTBarostat", "UniaxialTensileLoader",
+           "SphericalIndenterForce"]

@@ -100,6 +100,11 @@ class SimBoxScale(ctypes.Structure):
                 ("reset_reference", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
+class SimIndenter(ctypes.Structure):
+    _fields_ = [("center", ctypes.c_void_p), ("radius", ctypes.c_double), ("stiffness", ctypes.c_double),
+                ("out", ctypes.c_void_p)]
+
+
 class SimRep(ctypes.Structure):
     _fields_ = [("box", SimBox), ("off", ctypes.c_int64), ("first", ctypes.c_int64),
                 ("n", ctypes.c_int32), ("n_slots", ctypes.c_int32), ("ncell", ctypes.c_int32 * 3),
@@ -147,6 +152,7 @@ SIGNATURES = {
     "sim_berendsen": [_P(SimEngine), _P(SimBerendsen), c_p, c_p],
     "sim_aniso_npt": [_P(SimEngine), _P(SimAniso), c_p, c_p],
     "sim_box_scale": [_P(SimEngine), _P(SimBoxScale), c_p, c_p],
+    "sim_indenter_add": [_P(SimEngine), _P(SimIndenter), ctypes.c_int32, c_p],
     "sim_gather_original_f64": [_P(SimEngine), c_p, c_p, c_p],
     "sim_gather_original_f32": [_P(SimEngine), c_p, c_p, c_p],
     "sim_scatter_original_f64": [_P(SimEngine), c_p, c_p, c_p],
@@ -185,7 +191,7 @@ SIGNATURES = {
     "sim_struct_sizes": [c_p, ctypes.c_int32],
 }
 STRUCTS = (SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator, SimBerendsen, SimRep, SimBatch, SimMLP,
-           SimAniso, SimBoxScale)
+           SimAniso, SimBoxScale, SimIndenter)
 _RESTYPES = {"sim_last_cuda_error": ctypes.c_char_p}
 
 _lib = None

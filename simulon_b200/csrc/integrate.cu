@@ -142,6 +142,50 @@ __global__ void __launch_bounds__(SIM_THREADS) k_second_first(SimEngine e, SimIn
     }
 }
 
+// ---- spherical indenter (indenter.py:40-68) ----------------------------------
+__global__ void __launch_bounds__(SIM_THREADS) k_indenter(SimEngine e, SimIndenter p, int prec) {
+    pdl_trigger();
+    pdl_wait();
+    const int64_t P = e.n_pad;
+    const double c0 = p.center[0], c1 = p.center[1], c2 = p.center[2];
+    double vals[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double x0 = e.x[i], x1 = e.x[P + i], x2 = e.x[2 * P + i];
+        const double d0 = x0 - c0, d1 = x1 - c1, d2 = x2 - c2;
+        const double d = fmax(sqrt(d0 * d0 + d1 * d1 + d2 * d2), 1e-12);
+        const double pen = p.radius - d;
+        if (!(pen > 0.0)) continue;
+        const double k = p.stiffness * pen * pen;
+        const double f0 = k * (d0 / d), f1 = k * (d1 / d), f2 = k * (d2 / d);
+        if (prec == 1) {
+            e.f64[i] += f0;
+            e.f64[P + i] += f1;
+            e.f64[2 * P + i] += f2;
+        } else {
+            float4* f = reinterpret_cast<float4*>(e.f32) + i;
+            float4 v = *f;
+            v.x += (float)f0; v.y += (float)f1; v.z += (float)f2;
+            *f = v;
+        }
+        vals[0] += p.stiffness / 3.0 * pen * pen * pen;
+        vals[1] += f0; vals[2] += f1; vals[3] += f2;
+        vals[4] += 1.0;
+        vals[5] += f0 * x0; vals[6] += f1 * x1; vals[7] += f2 * x2;
+        vals[8] += f0 * x1; vals[9] += f0 * x2; vals[10] += f1 * x2;
+    }
+    block_partials<11>(vals, e.partials, 0);
+    if (last_block_finalize<11>(e.partials, e.red_counter + 3, p.out, 0)) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double* r = e.red_out;
+            r[SIM_RED_EPOT_PAIR] += p.out[0];
+            r[SIM_RED_VIRIAL] += p.out[5] + p.out[6] + p.out[7];
+            for (int k = 0; k < 6; ++k) r[SIM_RED_W_XX + k] += p.out[5 + k];
+            for (int k = 1; k < 4; ++k) p.out[k] = -p.out[k];   // force on the indenter
+        }
+    }
+}
+
 // ---- anisotropic pressure control and box scaling ---------------------------
 // (barostat.py:137-208, loading.py:41-80)  The new box is prepared by one
 // thread into work (from double 16), the atoms are mapped through fractional
@@ -505,12 +549,13 @@ extern "C" const char* sim_last_cuda_error(void) { return g_err; }
 extern "C" int sim_version(void) { return 1; }
 
 extern "C" int sim_struct_sizes(int64_t* out, int32_t n) {
-    const int64_t sizes[11] = {(int64_t)sizeof(SimBox), (int64_t)sizeof(SimEngine), (int64_t)sizeof(SimEAMTables),
+    const int64_t sizes[12] = {(int64_t)sizeof(SimBox), (int64_t)sizeof(SimEngine), (int64_t)sizeof(SimEAMTables),
                                (int64_t)sizeof(SimLJParams), (int64_t)sizeof(SimIntegrator),
                                (int64_t)sizeof(SimBerendsen), (int64_t)sizeof(SimRep), (int64_t)sizeof(SimBatch),
-                               (int64_t)sizeof(SimMLP), (int64_t)sizeof(SimAniso), (int64_t)sizeof(SimBoxScale)};
-    if (!out || n < 11) return SIM_ERR_ARG;
-    for (int k = 0; k < 11; ++k) out[k] = sizes[k];
+                               (int64_t)sizeof(SimMLP), (int64_t)sizeof(SimAniso), (int64_t)sizeof(SimBoxScale),
+                               (int64_t)sizeof(SimIndenter)};
+    if (!out || n < 12) return SIM_ERR_ARG;
+    for (int k = 0; k < 12; ++k) out[k] = sizes[k];
     return SIM_OK;
 }
 
@@ -530,5 +575,17 @@ extern "C" int sim_box_scale(const SimEngine* ep, const SimBoxScale* p, double* 
     const cudaError_t err = launch_pdl(k_box_prepare, dim3(1), dim3(1), 0, st, *ep, *p, work);
     if (err != cudaSuccess) { set_cuda_error(err, "sim_box_scale: prepare"); return SIM_ERR_CUDA; }
     return launch_box_scale(*ep, work, p->reset_reference, st, "sim_box_scale");
+}
+
+extern "C" int sim_indenter_add(const SimEngine* ep, const SimIndenter* p, int32_t force_precision, void* stream) {
+    if (!ep || !p || !p->center || !p->out || ep->n <= 0 || (force_precision == 1 && !ep->f64) ||
+        !(p->radius >= 0.0))
+        return SIM_ERR_ARG;
+    int blocks = persistent_grid((const void*)k_indenter, SIM_THREADS, 0, ep->n);
+    if (blocks > ep->n_blocks_max) blocks = (int)ep->n_blocks_max;
+    const cudaError_t err = launch_pdl(k_indenter, dim3(blocks), dim3(SIM_THREADS), 0, (cudaStream_t)stream, *ep, *p,
+                                       force_precision);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_indenter_add: launch"); return SIM_ERR_CUDA; }
+    return launch_status("sim_indenter_add");
 }
 

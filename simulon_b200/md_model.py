@@ -23,8 +23,11 @@ __all__ = ["BackboneInterface", "IntegratorInterface", "SumBackboneInterface", "
 
 
 class SumBackboneInterface(nn.Module):
-    """Sum of force-field backbones (md_model.py:19-52).  One device
-    backbone per system is supported (its outputs are returned as they are)."""
+    """Sum of force-field backbones (md_model.py:19-52).  The first backbone
+    is the device force field (it writes the engine's forces, energy and
+    virial); each further one must add its terms on the device
+    (``add_to_engine``, e.g. ``SphericalIndenterForce``).  The outputs are
+    the engine's sums, as the reference's summed buffers."""
 
     def __init__(self, backbones, molecular):
         super().__init__()
@@ -32,15 +35,28 @@ class SumBackboneInterface(nn.Module):
         self.molecular = molecular
         self.device = molecular.device
         self.atom_num = molecular.atom_count
-        if len(self.backbones) != 1:
-            raise NotImplementedError("exactly one device force field per system is supported")
+        if len(self.backbones) < 1:
+            raise ValueError("at least one force field is needed")
+        for b in list(self.backbones)[1:]:
+            if not hasattr(b, "add_to_engine"):
+                raise NotImplementedError(f"{type(b).__name__} cannot be summed on the device (needs add_to_engine)")
         self.force_precision = getattr(self.backbones[0], "force_precision", 0)
+
+    @property
+    def single(self) -> bool:
+        return len(self.backbones) == 1
 
     def compute(self):
         self.backbones[0].compute()
+        for b in list(self.backbones)[1:]:
+            b.add_to_engine(self.force_precision)
 
     def forward(self):
-        return self.backbones[0]()
+        if self.single:
+            return self.backbones[0]()
+        self.compute()
+        from .forces import _force_outputs
+        return _force_outputs(self.molecular)
 
 
 class BaseModel(nn.Module):
@@ -60,7 +76,7 @@ class BaseModel(nn.Module):
     # one step, launches only (no host sync)
     def _step_launches(self):
         self.Integrator.first_half()
-        fused = getattr(self.sum_bone.backbones[0], "compute_and_finish", None)
+        fused = getattr(self.sum_bone.backbones[0], "compute_and_finish", None) if self.sum_bone.single else None
         if fused is not None and hasattr(self.Integrator, "params"):
             fused(self.Integrator)        # EAM: second half fused into pass 2
         else:
@@ -72,7 +88,7 @@ class BaseModel(nn.Module):
 
     def _drift_fusable(self) -> bool:
         bone = self.sum_bone.backbones[0]
-        return (self.barostat is None and hasattr(bone, "compute_finish_and_drift")
+        return (self.barostat is None and self.sum_bone.single and hasattr(bone, "compute_finish_and_drift")
                 and hasattr(self.Integrator, "params") and not self.engine.use_tiles)
 
     def _launch_steps(self, k: int):

@@ -1,5 +1,8 @@
-"""Uniaxial tensile loading with the interface of core/mechanics/loading.py:6-81.
+"""Mechanics callers of the force path: uniaxial tensile loading
+(core/mechanics/loading.py:6-81) and the spherical indenter backbone
+(core/mechanics/indenter.py:7-68).
 
+Loader:
 The box update runs on the device in FP64 (``sim_box_scale``): H <- diag(s) H,
 positions through fractional coordinates of the old box into the new one and
 wrapped (box.py:132-142), posq refreshed, the skin test against the last
@@ -21,6 +24,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .forces import BackboneInterface, _force_outputs
 
 
 class UniaxialTensileLoader:
@@ -85,3 +89,69 @@ class UniaxialTensileLoader:
 
     def current_lengths(self) -> torch.Tensor:
         return torch.tensor(np.linalg.norm(self.molecular.engine.box_matrix(), axis=1), dtype=torch.float64)
+
+
+class SphericalIndenterForce(BackboneInterface):
+    """Repulsive sphere (indenter.py:7-68): for atoms with d = |x - c| < R,
+    U = K/3 (R - d)^3 and F = K (R - d)^2 (x - c)/d.  On the device: added to
+    the engine's forces, energy and virial after the force field's pass (as a
+    further backbone of SumBackboneInterface), with its own energy, force on
+    the indenter and contact count in ``out``.  The centre is device memory,
+    so ``set_center`` between CUDA-graph replays takes effect.  Positions are
+    the unwrapped ones, without periodic images (as the reference).  The
+    engine's virial tensor is symmetric: the indenter's F (x) x enters it with
+    its upper triangle."""
+
+    def __init__(self, molecular, radius: float, stiffness: float, center):
+        super().__init__()
+        self.molecular = molecular
+        self.device = molecular.device
+        self.radius = float(radius)
+        self.stiffness = float(stiffness)
+        c = torch.as_tensor(center, dtype=torch.float64).reshape(-1)
+        if c.numel() != 3:
+            raise ValueError("center must have three components")
+        self._center = c.to(self.device).clone()
+        self.out = torch.zeros(11, dtype=torch.float64, device=self.device)
+        self._st = _lib.SimIndenter()
+        self._st.center, self._st.out = _lib.ptr(self._center), _lib.ptr(self.out)
+        self._st.radius, self._st.stiffness = self.radius, self.stiffness
+        self._ref = ctypes.byref(self._st)
+        self.force_precision = 0
+
+    @property
+    def center(self) -> torch.Tensor:
+        return self._center
+
+    def set_center(self, center) -> None:
+        self._center.copy_(torch.as_tensor(center, dtype=torch.float64).reshape(3))
+
+    @property
+    def force_on_indenter(self) -> torch.Tensor:
+        return self.out[1:4]
+
+    @property
+    def last_energy(self) -> torch.Tensor:
+        return self.out[0]
+
+    @property
+    def contact_atoms(self) -> int:
+        return int(self.out[4].item())
+
+    def add_to_engine(self, force_precision: int = 0):
+        eng = self.molecular.engine
+        _lib.call("sim_indenter_add", eng.st_ref, self._ref, int(force_precision), eng.stream)
+
+    def compute(self):
+        """Alone (the only backbone): the engine's forces and sums are zeroed first."""
+        eng = self.molecular.engine
+        eng.f32.zero_()
+        if eng.f64 is not None:
+            eng.f64.zero_()
+        eng.red_out.zero_()
+        self.add_to_engine(self.force_precision)
+        eng.forces_valid = True
+
+    def forward(self):
+        self.compute()
+        return _force_outputs(self.molecular)

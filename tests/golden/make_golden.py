@@ -281,6 +281,47 @@ def mech_cases(tmp):
         torch.set_default_dtype(torch.float32)
 
 
+def indenter_cases(tmp):
+    """LJ argon 108 (FP64, NVE, 20 steps) with the SphericalIndenterForce as a
+    second backbone, its centre lowered 0.05 A per step into the top layer."""
+    from core.force.lennard_jones_force import LennardJonesForce
+    from core.integrator.integrator import VerletIntegrator
+    from core.md_model import BaseModel, SumBackboneInterface
+    from core.mechanics.indenter import SphericalIndenterForce
+
+    torch.set_default_dtype(torch.float64)
+    try:
+        x, L = oin.fcc_lattice(3)
+        x = oin.jitter(x, 0.05, 0)
+        v0 = oin.maxwell_boltzmann(np.full(len(x), oin.AR_MASS), 94.4, 1)
+        params = {"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}}
+        mol = _reader(tmp, "ar108ind", x, "Ar", L, 7.0, 0.5, params=params)
+        integ = VerletIntegrator(mol, dt=0.002, ensemble="NVE")
+        mol.atom_velocities = torch.tensor(v0)
+        R, K = 4.0, 0.05
+        c0 = np.array([0.5 * L, 0.5 * L, float(np.max(x[:, 2])) + R - 0.5])
+        ind = SphericalIndenterForce(mol, radius=R, stiffness=K, center=c0)
+        model = BaseModel(SumBackboneInterface([LennardJonesForce(mol), ind], mol), integ, mol)
+        rec = {k: [] for k in ("energy", "kinetic_energy", "virial", "virial_tensor", "force_on_indenter",
+                               "indenter_energy", "contact_atoms", "center")}
+        for s in range(20):
+            c = c0 - np.array([0.0, 0.0, 0.05 * s])
+            ind.set_center(c)
+            out = model()
+            rec["energy"].append(float(out["energy"]))
+            rec["kinetic_energy"].append(float(out["kinetic_energy"]))
+            rec["virial"].append(float(out["virial"]))
+            rec["virial_tensor"].append(out["virial_tensor"].detach().numpy().copy())
+            rec["force_on_indenter"].append(ind.force_on_indenter.detach().numpy().copy())
+            rec["indenter_energy"].append(float(ind.last_energy))
+            rec["contact_atoms"].append(int(ind.contact_atoms))
+            rec["center"].append(c)
+        _save("ind_ar108_f64", x0=x, v0=v0, box0=L, dt=0.002, steps=20, radius=R, stiffness=K, x=mol.coordinates,
+              v=mol.atom_velocities, **{k: np.array(v) for k, v in rec.items()})
+    finally:
+        torch.set_default_dtype(torch.float32)
+
+
 def main():
     if not os.path.isdir(REF):
         raise SystemExit(f"reference checkout not found at {REF}")
@@ -295,6 +336,7 @@ def main():
             eam_cases(tmp)
             md_cases(tmp)
             mech_cases(tmp)
+            indenter_cases(tmp)
         finally:
             builtins.print = quiet
 

@@ -120,3 +120,90 @@ def test_cell_guard_and_regrid(sb, tmp_path):
     for _ in range(10):
         loader.step(0.002)
     assert loader.regrids >= 1 and eng2.cells_valid() and eng2.status() == 0
+
+
+def test_indenter_backbone_matches_reference(sb, tmp_path):
+    """LJ (FP64) + SphericalIndenterForce as a second backbone, centre moved
+    every step: energies, virial (trace and upper triangle of the reference's
+    F (x) x tensor), force on the indenter, contacts and the final state."""
+    from simulon_b200.mechanics import SphericalIndenterForce
+    g = _golden("ind_ar108_f64")
+    torch.set_default_dtype(torch.float64)
+    try:
+        path = oin.write_xyz(str(tmp_path / "ar.xyz"), g["x0"], "Ar")
+        mol = sb.AtomFileReader(path, float(g["box0"]), 7.0, device=DEV,
+                                parameter={"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}}, skin_thickness=0.5)
+        integ = sb.VerletIntegrator(mol, dt=float(g["dt"]), ensemble="NVE")
+        mol.atom_velocities = torch.tensor(g["v0"], device=DEV)
+        ind = SphericalIndenterForce(mol, radius=float(g["radius"]), stiffness=float(g["stiffness"]),
+                                     center=g["center"][0])
+        model = sb.BaseModel(sb.SumBackboneInterface([sb.LennardJonesForce(mol), ind], mol), integ, mol)
+        E, V, W, Fi, n, Ei = [], [], [], [], [], []
+        for s in range(int(g["steps"])):
+            ind.set_center(g["center"][s])
+            out = model()
+            E.append(float(out["energy"]))
+            V.append(float(out["virial"]))
+            W.append(out["virial_tensor"].cpu().numpy())
+            Fi.append(ind.force_on_indenter.cpu().numpy().copy())
+            Ei.append(float(ind.last_energy))
+            n.append(ind.contact_atoms)
+        np.testing.assert_allclose(E, g["energy"], rtol=1e-9)
+        np.testing.assert_allclose(V, g["virial"], rtol=1e-9, atol=1e-12)
+        iu = np.triu_indices(3)
+        np.testing.assert_allclose(np.array(W)[:, iu[0], iu[1]], g["virial_tensor"][:, iu[0], iu[1]], rtol=1e-8,
+                                   atol=1e-12)
+        np.testing.assert_allclose(np.array(Fi), g["force_on_indenter"], rtol=1e-8, atol=1e-13)
+        np.testing.assert_allclose(Ei, g["indenter_energy"], rtol=1e-8, atol=1e-15)
+        assert n == list(g["contact_atoms"])
+        np.testing.assert_allclose(mol.coordinates.cpu().numpy(), g["x"], atol=1e-8)
+        np.testing.assert_allclose(mol.atom_velocities.cpu().numpy(), g["v"], atol=1e-7)
+        assert mol.engine.status() == 0
+    finally:
+        torch.set_default_dtype(torch.float32)
+
+
+def test_indenter_alone_and_with_eam_in_graphs(sb, tmp_path):
+    """The indenter as the only backbone (forces against the FP64
+    restatement), and EAM + indenter stepped eagerly and through CUDA graphs
+    with the centre changed between replays: identical states."""
+    from oracle.integrator import indenter
+    from simulon_b200.mechanics import SphericalIndenterForce
+    x, L = oin.bcc_lattice(6)
+    x = oin.jitter(x, 0.05, 9)
+    c = np.array([0.5 * L, 0.5 * L, float(x[:, 2].max()) + 1.5])
+    eng = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], np.diag([L] * 3), 4.4, 0.5, device=DEV)
+
+    class Mol:
+        engine = eng
+        device = DEV
+        dtype = torch.float64
+    ind = SphericalIndenterForce(Mol(), radius=3.0, stiffness=1.0, center=c)
+    ind.compute()
+    o = indenter(torch.tensor(x), c, 3.0, 1.0)
+    np.testing.assert_allclose(eng.gather("f").cpu().numpy(), o["forces"].numpy(), rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(float(eng.potential_energy()), float(o["energy"]), rtol=1e-12)
+    assert ind.contact_atoms == o["contact_atoms"] > 0
+    from oracle import inputs as oi
+    pot = oi.write_fs_w_setfl(str(tmp_path / "W.eam.fs"))
+    parser = sb.EAMParser(pot)
+    res = []
+    for graph in (False, True):
+        p = oi.write_xyz(str(tmp_path / f"w{int(graph)}.xyz"), x, "W")
+        mol = sb.AtomFileReader(p, L, parser.cutoff, device=DEV, skin_thickness=0.5, is_fs=True)
+        mol.atom_velocities = torch.tensor(oi.maxwell_boltzmann(np.full(len(x), oi.W_MASS), 300.0, 4), device=DEV)
+        integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NVE")
+        ind = SphericalIndenterForce(mol, radius=3.0, stiffness=1.0, center=c)
+        model = sb.BaseModel(sb.SumBackboneInterface([sb.EAMForceCUDAExt(parser, mol), ind], mol), integ, mol)
+        for chunk in range(4):
+            ind.set_center(c - np.array([0.0, 0.0, 0.1 * chunk]))
+            if graph:
+                model.run(5, graph_steps=5)
+            else:
+                for _ in range(5):
+                    model()
+        torch.cuda.synchronize()
+        res.append((mol.coordinates.cpu(), mol.atom_velocities.cpu(), ind.out.cpu()))
+        assert mol.engine.status() == 0
+    assert torch.equal(res[0][0], res[1][0]) and torch.equal(res[0][1], res[1][1])
+    assert torch.equal(res[0][2], res[1][2]) and res[0][2][4] > 0

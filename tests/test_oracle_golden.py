@@ -220,3 +220,35 @@ def test_tensile_and_aniso_npt_match_reference(name):
     np.testing.assert_allclose(np.array(eta), g["eta_dot"], rtol=1e-8, atol=1e-12)
     np.testing.assert_allclose(md.x.numpy(), g["x"], atol=1e-9)
     np.testing.assert_allclose(md.v.numpy(), g["v"], atol=1e-9)
+
+
+def test_indenter_backbone_matches_reference():
+    """LJ + SphericalIndenterForce (summed backbones) over 20 NVE steps with a
+    moving centre: the oracle's restatement against the reference's run."""
+    from oracle.integrator import indenter
+    g = load("ind_ar108_f64")
+    box = OracleBox(float(g["box0"]))
+    lj = _lj_force_fn(box, 0.0104, 3.405)
+    state = {"c": g["center"][0], "last": None}
+
+    def ff(x, i, j):
+        a = lj(x, i, j)
+        b = indenter(x, state["c"], float(g["radius"]), float(g["stiffness"]))
+        state["last"] = b
+        return dict(forces=a["forces"] + b["forces"], energy=a["energy"] + b["energy"],
+                    virial=a["virial"] + b["virial"], virial_tensor=a["virial_tensor"] + b["virial_tensor"])
+    md = OracleMD(g["x0"], g["v0"], np.full(108, oin.AR_MASS), box, ff, cutoff=7.0, skin=0.5, dt=float(g["dt"]))
+    E, Fi, n, W = [], [], [], []
+    for s in range(int(g["steps"])):
+        state["c"] = g["center"][s]
+        r = md.step()
+        E.append(float(r["energy"]))
+        W.append(r["virial_tensor"].numpy())
+        Fi.append(state["last"]["force_on_indenter"].numpy())
+        n.append(state["last"]["contact_atoms"])
+    np.testing.assert_allclose(E, g["energy"], rtol=1e-10)
+    np.testing.assert_allclose(np.array(W), g["virial_tensor"], rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(np.array(Fi), g["force_on_indenter"], rtol=1e-9, atol=1e-14)
+    assert n == list(g["contact_atoms"])
+    np.testing.assert_allclose(md.x.numpy(), g["x"], atol=1e-10)
+    np.testing.assert_allclose(md.v.numpy(), g["v"], atol=1e-9)
