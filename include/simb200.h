@@ -590,12 +590,38 @@ int sim_autotune_eam(const SimEngine* e, const SimEAMTables* t, int32_t reps, fl
 int sim_autotune_mlp(const SimEngine* e, const float* dEdG, float* G, int32_t reps, float* ms, int32_t* best,
                      void* stream);
 
+/* ---- group 6: crack observables of the batched form (w_crack.py:113-188) --
+ * Per replica, from the current positions: the crack-mouth opening (mean
+ * height of the upper mouth atoms minus that of the lower ones, minus its
+ * initial value), the crack length (positions binned along the crack axis;
+ * a bin is open where the lowest atom above the crack plane and the highest
+ * below it are at least `threshold` apart; the open run through the bins
+ * inside the initial crack, grown to both sides), and the projected stress
+ * ((K + W)/V in bar on the normalised box rows; the reference reports the
+ * negated y component as the opening stress).  No counterpart in the
+ * reference's kernels (its script computes these on the host each step). */
+typedef struct SimCrack {
+    double x_unit[3], y_unit[3];    /* normalised box rows 0 and 1                    */
+    double y_plane, x_min, x_max, x_center, half_length, threshold, initial_cmod;
+    int32_t bins, bin_off;          /* bins (0: not a crack replica), first bin        */
+    int32_t n_upper, n_lower;       /* mouth atoms (tags 1 and 2)                      */
+} SimCrack;
+#define SIM_CRACK_OUT 8   /* per replica: stress_bar, native_stress_yy_bar, cmod, signed_cmod,
+                             crack_length, crack_extension, open bins, 0 */
+/* crack [n_rep] device; mouth [atoms, original order] 0 / 1 upper / 2 lower;
+ * bins [2 * total bins] and sums [2 * n_rep] scratch; out [n_rep][SIM_CRACK_OUT].
+ * Reads the per-replica sums of the last sim_batch_reduce for the stress.
+ * The mouth heights are summed with FP64 atomics: the last bits of the
+ * opening vary from run to run. */
+int sim_batch_crack_observe(const SimBatch* b, const SimCrack* crack, const int8_t* mouth, int32_t total_bins,
+                            uint64_t* bins, double* sums, double* out, void* stream);
+
 /* Message for the last CUDA error seen by this library (host string). */
 const char* sim_last_cuda_error(void);
 int sim_version(void);
 /* sizeof of SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator,
- * SimBerendsen, SimRep, SimBatch, SimMLP, SimAniso, SimBoxScale, SimIndenter
- * (host-only; lets bindings verify their struct layouts; n >= 12). */
+ * SimBerendsen, SimRep, SimBatch, SimMLP, SimAniso, SimBoxScale, SimIndenter,
+ * SimCrack (host-only; lets bindings verify their struct layouts; n >= 13). */
 int sim_struct_sizes(int64_t* out, int32_t n);
 
 #ifdef __cplusplus

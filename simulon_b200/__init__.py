@@ -14,7 +14,7 @@ import sys
 
 from . import _lib
 from .barostat import AnisotropicNPTBarostat, BerendsenBarostat
-from .batch import BatchedEngine, Replica, crack_slab, crack_sweep, partition_replicas
+from .batch import BatchedEngine, CrackObserver, Replica, crack_slab, crack_sweep, partition_replicas
 from .box import Box
 from .eam_parser import EAMDeviceTables, EAMParser
 from .engine import MDEngine
@@ -41,4 +41,4 @@ __all__ = ["AtomFileReader", "Box", "EAMParser", "EAMDeviceTables", "EAMForce", 
            "BerendsenBarostat", "SumBackboneInterface", "BaseModel", "MDSimulator", "MDEngine",
            "find_neighbors_gpu_pbc", "install_simulon_cuda", "BatchedEngine", "Replica", "crack_slab",
            "crack_sweep", "partition_replicas", "AnisotropicNPTBarostat", "UniaxialTensileLoader",
-           "SphericalIndenterForce"]
+           "SphericalIndenterForce", "CrackObserver"]

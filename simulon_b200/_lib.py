@@ -105,6 +105,17 @@ class SimIndenter(ctypes.Structure):
                 ("out", ctypes.c_void_p)]
 
 
+class SimCrack(ctypes.Structure):
+    _fields_ = [("x_unit", ctypes.c_double * 3), ("y_unit", ctypes.c_double * 3), ("y_plane", ctypes.c_double),
+                ("x_min", ctypes.c_double), ("x_max", ctypes.c_double), ("x_center", ctypes.c_double),
+                ("half_length", ctypes.c_double), ("threshold", ctypes.c_double), ("initial_cmod", ctypes.c_double),
+                ("bins", ctypes.c_int32), ("bin_off", ctypes.c_int32), ("n_upper", ctypes.c_int32),
+                ("n_lower", ctypes.c_int32)]
+
+
+SIM_CRACK_OUT = 8
+
+
 class SimRep(ctypes.Structure):
     _fields_ = [("box", SimBox), ("off", ctypes.c_int64), ("first", ctypes.c_int64),
                 ("n", ctypes.c_int32), ("n_slots", ctypes.c_int32), ("ncell", ctypes.c_int32 * 3),
@@ -153,6 +164,7 @@ SIGNATURES = {
     "sim_aniso_npt": [_P(SimEngine), _P(SimAniso), c_p, c_p],
     "sim_box_scale": [_P(SimEngine), _P(SimBoxScale), c_p, c_p],
     "sim_indenter_add": [_P(SimEngine), _P(SimIndenter), ctypes.c_int32, c_p],
+    "sim_batch_crack_observe": [c_p, c_p, c_p, ctypes.c_int32, c_p, c_p, c_p, c_p],
     "sim_gather_original_f64": [_P(SimEngine), c_p, c_p, c_p],
     "sim_gather_original_f32": [_P(SimEngine), c_p, c_p, c_p],
     "sim_scatter_original_f64": [_P(SimEngine), c_p, c_p, c_p],
@@ -191,7 +203,7 @@ SIGNATURES = {
     "sim_struct_sizes": [c_p, ctypes.c_int32],
 }
 STRUCTS = (SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator, SimBerendsen, SimRep, SimBatch, SimMLP,
-           SimAniso, SimBoxScale, SimIndenter)
+           SimAniso, SimBoxScale, SimIndenter, SimCrack)
 _RESTYPES = {"sim_last_cuda_error": ctypes.c_char_p}
 
 _lib = None

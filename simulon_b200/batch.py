@@ -386,7 +386,8 @@ def crack_slab(n_target: int, a: float = 3.165, *, vacuum: float = 15.0, crack_g
     free = grip == 0
     v[free] -= v[free].mean(axis=0)
     return Replica(positions=x, H=H, velocities=v, temperature=temperature, grip=grip, grip_axis=1,
-                   grip_rate=grip_rate, meta={"cells": (nx, ny, nz), "removed": int(crack.sum())})
+                   grip_rate=grip_rate, meta={"cells": (nx, ny, nz), "removed": int(crack.sum()),
+                                              "crack_plane_y": float(y_plane), "crack_half_length": Lx / 8.0})
 
 
 def crack_sweep(n_replicas: int = 48, n_min: int = 2000, n_max: int = 250000, t_min: float = 50.0,
@@ -398,3 +399,88 @@ def crack_sweep(n_replicas: int = 48, n_min: int = 2000, n_max: int = 250000, t_
     temps = np.linspace(t_min, t_max, n_replicas)
     return [crack_slab(int(s), temperature=float(T), seed=seed + 1 + k, **kw)
             for k, (s, T) in enumerate(zip(sizes, temps))]
+
+
+# ---------------------------------------------------------------------------
+# crack observables (w_crack.py:113-188) on the device
+
+def select_mouth_groups(vx, vy, x_center: float, y_center: float, crack_half_length: float):
+    """Atoms at the crack mouth above and below the crack plane, in windows
+    growing until both groups are non-empty (w_crack.py:125-133)."""
+    mouth_x = x_center + crack_half_length
+    for xw in (0.8, 1.2, 1.8, 2.5):
+        for yw in (0.8, 1.2, 1.8, 2.5):
+            near = np.abs(vx - mouth_x) <= xw
+            upper = near & (vy > y_center) & ((vy - y_center) <= yw)
+            lower = near & (vy < y_center) & ((y_center - vy) <= yw)
+            if upper.any() and lower.any():
+                return upper, lower
+    raise ValueError("failed to find crack-mouth atoms; increase replicas or crack size")
+
+
+class CrackObserver:
+    """Per-replica crack-mouth opening, crack length and projected stress of a
+    BatchedEngine, computed on the device (``sim_batch_crack_observe``) from
+    the current positions and the last reduction, so a sweep needs no host
+    round trip per step (the reference's script computes them on the host,
+    w_crack.py:113-188, 474-496).  Set-up as the reference's: the lattice
+    axes are the normalised box rows 0 and 1; the crack-axis range and centre
+    and the mouth groups come from the reference positions (default: the
+    engine's current ones), the opening is measured from their initial
+    value.  Replicas without crack metadata (``crack_plane_y``,
+    ``crack_half_length``) report only the stress."""
+
+    COLUMNS = ("stress_bar", "native_stress_yy_bar", "cmod_A", "signed_cmod_A", "crack_length_A",
+               "crack_extension_A", "open_bins", "reserved")
+
+    def __init__(self, batch: "BatchedEngine", threshold: float = 1.0, bins: int = 160, reference_positions=None):
+        self.batch = batch
+        dev = batch.device
+        x = (batch.gather("x") if reference_positions is None else torch.as_tensor(reference_positions))
+        x = x.to(torch.float64).cpu().numpy()
+        R = batch.n_rep
+        table = (_lib.SimCrack * R)()
+        mouth = np.zeros(batch.n_atoms, np.int8)
+        off = 0
+        self.initial_cmod = np.zeros(R)
+        for k, rep in enumerate(batch.replicas):
+            c = table[k]
+            H = np.asarray(rep.H, np.float64)
+            xu = H[0] / max(np.linalg.norm(H[0]), 1e-12)
+            yu = H[1] / max(np.linalg.norm(H[1]), 1e-12)
+            c.x_unit[:], c.y_unit[:] = xu.tolist(), yu.tolist()
+            if "crack_plane_y" not in rep.meta or "crack_half_length" not in rep.meta:
+                c.bins = 0
+                continue
+            sl = batch.replica_slice(k)
+            xs = x[sl]
+            vx, vy = xs @ xu, xs @ yu
+            c.x_min, c.x_max = float(vx.min()), float(vx.max())
+            c.x_center = 0.5 * (c.x_min + c.x_max)
+            c.y_plane = float(rep.meta["crack_plane_y"])
+            c.half_length = float(rep.meta["crack_half_length"])
+            c.threshold = float(threshold)
+            up, lo = select_mouth_groups(vx, vy, c.x_center, c.y_plane, c.half_length)
+            c.initial_cmod = float(vy[up].mean() - vy[lo].mean())
+            self.initial_cmod[k] = c.initial_cmod
+            c.n_upper, c.n_lower = int(up.sum()), int(lo.sum())
+            first = sl.start
+            mouth[first + np.nonzero(up)[0]] = 1
+            mouth[first + np.nonzero(lo)[0]] = 2
+            c.bins = int(max(8, bins))
+            c.bin_off = off
+            off += c.bins
+        self.total_bins = off
+        raw = bytes(table)
+        self.table = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(dev)
+        self.mouth = torch.from_numpy(mouth).to(dev)
+        self.bins = torch.zeros(max(1, 2 * off), dtype=torch.int64, device=dev)
+        self.sums = torch.zeros(2 * R, dtype=torch.float64, device=dev)
+        self.out = torch.zeros(R, _lib.SIM_CRACK_OUT, dtype=torch.float64, device=dev)
+
+    def observe(self) -> torch.Tensor:
+        """[n_rep, 8] device tensor, columns ``COLUMNS`` (no synchronisation)."""
+        b = self.batch
+        _lib.call("sim_batch_crack_observe", b.ref, _lib.ptr(self.table), _lib.ptr(self.mouth), int(self.total_bins),
+                  _lib.ptr(self.bins), _lib.ptr(self.sums), _lib.ptr(self.out), b.stream)
+        return self.out

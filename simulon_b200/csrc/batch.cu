@@ -829,3 +829,122 @@ extern "C" int sim_batch_gather_f32(const SimBatch* b, const float* src_aos4, do
     k_bb_gather_f32<<<grid_slots(b->e.n), SIM_THREADS, 0, (cudaStream_t)stream>>>(*b, src_aos4, out_rows);
     return launch_status("sim_batch_gather_f32");
 }
+
+// ---- crack observables (w_crack.py:113-188) ---------------------------------
+// Doubles as 64-bit keys whose unsigned order is the numeric order, so the
+// per-bin extremes are exact atomic min / max.
+__device__ __forceinline__ unsigned long long dkey(double v) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dkey_value(unsigned long long k) {
+    const unsigned long long u = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
+    return __longlong_as_double((long long)u);
+}
+
+__global__ void k_crack_init(int total_bins, int n_rep, unsigned long long* bins, double* sums) {
+    const unsigned long long up0 = dkey(__longlong_as_double(0x7FF0000000000000ll));   // +inf
+    const unsigned long long lo0 = dkey(__longlong_as_double((long long)0xFFF0000000000000ull));   // -inf
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * total_bins + 2 * n_rep; t += gridDim.x * blockDim.x) {
+        if (t < total_bins) bins[t] = up0;
+        else if (t < 2 * total_bins) bins[t] = lo0;
+        else sums[t - 2 * total_bins] = 0.0;
+    }
+}
+
+__global__ void k_crack_scan(SimBatch B, const SimCrack* __restrict__ crack, const int8_t* __restrict__ mouth,
+                             int total_bins, unsigned long long* bins, double* sums) {
+    const SimEngine& e = B.e;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+        bool real;
+        const int k = slot_replica(B, i, real);
+        if (!real) continue;
+        const SimCrack& c = crack[k];
+        if (c.bins <= 0) continue;
+        const double x0 = e.x[i], x1 = e.x[e.n_pad + i], x2 = e.x[2 * e.n_pad + i];
+        const double vx = x0 * c.x_unit[0] + x1 * c.x_unit[1] + x2 * c.x_unit[2];
+        const double vy = x0 * c.y_unit[0] + x1 * c.y_unit[1] + x2 * c.y_unit[2];
+        const double span = fmax(1.0e-12, c.x_max - c.x_min);
+        double bf = floor((vx - c.x_min) / span * (double)c.bins);
+        bf = fmin(fmax(bf, 0.0), (double)(c.bins - 1));
+        const int bin = c.bin_off + (int)bf;
+        if (vy > c.y_plane) atomicMin(&bins[bin], dkey(vy));
+        else if (vy < c.y_plane) atomicMax(&bins[total_bins + bin], dkey(vy));
+        const int tag = mouth[e.orig[i]];
+        if (tag == 1) atomicAdd(&sums[2 * k], vy);
+        else if (tag == 2) atomicAdd(&sums[2 * k + 1], vy);
+    }
+}
+
+__global__ void k_crack_finish(SimBatch B, const SimCrack* __restrict__ crack, int total_bins,
+                               const unsigned long long* __restrict__ bins, const double* __restrict__ sums,
+                               double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= B.n_rep) return;
+    const SimCrack& c = crack[k];
+    double* o = out + (size_t)k * SIM_CRACK_OUT;
+    // projected stress from the replica's sums (the last sim_batch_reduce)
+    const SimBox& bx = B.rep[k].box;
+    const double* H = bx.H;
+    const double V = fabs(H[0] * (H[4] * H[8] - H[5] * H[7]) - H[1] * (H[3] * H[8] - H[5] * H[6]) +
+                          H[2] * (H[3] * H[7] - H[4] * H[6]));
+    const double* r = B.rep_red + (size_t)k * SIM_RED_SLOTS;
+    const double t[6] = {r[SIM_RED_K_XX] + r[SIM_RED_W_XX], r[SIM_RED_K_YY] + r[SIM_RED_W_YY],
+                         r[SIM_RED_K_ZZ] + r[SIM_RED_W_ZZ], r[SIM_RED_K_XY] + r[SIM_RED_W_XY],
+                         r[SIM_RED_K_XZ] + r[SIM_RED_W_XZ], r[SIM_RED_K_YZ] + r[SIM_RED_W_YZ]};
+    const double s[3][3] = {{t[0], t[3], t[4]}, {t[3], t[1], t[5]}, {t[4], t[5], t[2]}};
+    const double* row = H + 3;
+    const double nrm = fmax(sqrt(row[0] * row[0] + row[1] * row[1] + row[2] * row[2]), 1e-12);
+    const double ax[3] = {row[0] / nrm, row[1] / nrm, row[2] / nrm};
+    double pyy = 0.0;
+    for (int a = 0; a < 3; ++a)
+        for (int b2 = 0; b2 < 3; ++b2) pyy += ax[a] * s[a][b2] * ax[b2];
+    pyy = pyy / V * 1602176.6208;
+    o[0] = -pyy;
+    o[1] = pyy;
+    for (int q = 2; q < SIM_CRACK_OUT; ++q) o[q] = 0.0;
+    if (c.bins <= 0) return;
+    if (c.n_upper > 0 && c.n_lower > 0) {
+        const double sc = (sums[2 * k] / c.n_upper - sums[2 * k + 1] / c.n_lower) - c.initial_cmod;
+        o[2] = fabs(sc);
+        o[3] = sc;
+    }
+    // open bins: gap between the lowest atom above and the highest below the plane
+    const double span = fmax(1.0e-12, c.x_max - c.x_min), width = span / c.bins;
+    int lo_seed = -1, hi_seed = -1, n_open = 0;
+    auto open_bin = [&](int q) {
+        const double g = dkey_value(bins[c.bin_off + q]) - dkey_value(bins[total_bins + c.bin_off + q]);
+        return isfinite(g) && g >= c.threshold;
+    };
+    for (int q = 0; q < c.bins; ++q) {
+        if (!open_bin(q)) continue;
+        ++n_open;
+        const double center = c.x_min + (q + 0.5) * width;
+        if (center >= c.x_center - c.half_length && center <= c.x_center + c.half_length) {
+            if (lo_seed < 0) lo_seed = q;
+            hi_seed = q;
+        }
+    }
+    o[6] = (double)n_open;
+    if (lo_seed < 0) return;
+    while (lo_seed > 0 && open_bin(lo_seed - 1)) --lo_seed;
+    while (hi_seed < c.bins - 1 && open_bin(hi_seed + 1)) ++hi_seed;
+    const double length = (hi_seed - lo_seed + 1) * width;
+    o[4] = length;
+    o[5] = fmax(0.0, length - 2.0 * c.half_length);
+}
+
+extern "C" int sim_batch_crack_observe(const SimBatch* b, const SimCrack* crack, const int8_t* mouth,
+                                       int32_t total_bins, uint64_t* bins, double* sums, double* out, void* stream) {
+    if (!batch_ok(b) || !crack || !mouth || total_bins < 0 || (total_bins > 0 && !bins) || !sums || !out)
+        return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned long long* kb = reinterpret_cast<unsigned long long*>(bins);
+    const int n_init = 2 * total_bins + 2 * b->n_rep;
+    k_crack_init<<<(n_init + 255) / 256, 256, 0, st>>>(total_bins, b->n_rep, kb, sums);
+    if (total_bins > 0)
+        k_crack_scan<<<grid_slots(b->e.n), SIM_THREADS, 0, st>>>(*b, crack, mouth, total_bins, kb, sums);
+    k_crack_finish<<<(b->n_rep + 63) / 64, 64, 0, st>>>(*b, crack, total_bins, kb, sums, out);
+    return launch_status("sim_batch_crack_observe");
+}
+

@@ -322,6 +322,53 @@ def indenter_cases(tmp):
         torch.set_default_dtype(torch.float32)
 
 
+def crack_cases(tmp):
+    """Crack observables of run_scripts/w_crack.py (_select_mouth_groups,
+    _estimate_crack_length, _project_to_lattice_axes) on a precracked BCC-W
+    slab as built and with its upper half opened (a smooth opening profile
+    around the crack plus seeded jitter), and the stress projection of a
+    seeded symmetric tensor."""
+    for name in ("matplotlib", "matplotlib.pyplot"):
+        if name not in sys.modules:
+            m = types.ModuleType(name)
+            m.use = lambda *a, **k: None
+            m.rcParams = {}
+            sys.modules[name] = m
+    sys.modules["matplotlib"].pyplot = sys.modules["matplotlib.pyplot"]
+    from run_scripts.w_crack import _estimate_crack_length, _project_to_lattice_axes, _select_mouth_groups
+    from simulon_b200.batch import crack_slab
+
+    rep = crack_slab(3000, seed=5)
+    H = torch.tensor(rep.H)
+    x0 = torch.tensor(rep.positions)
+    x_unit = H[0] / torch.linalg.norm(H[0])
+    y_unit = H[1] / torch.linalg.norm(H[1])
+    yc = float(rep.meta["crack_plane_y"])
+    half = float(rep.meta["crack_half_length"])
+    vx, vy = x0 @ x_unit, x0 @ y_unit
+    x_min, x_max = float(vx.min()), float(vx.max())
+    xc = 0.5 * (x_min + x_max)
+    up, lo = _select_mouth_groups(vx, vy, xc, yc, half)
+    cmod0 = float(vy[up].mean() - vy[lo].mean())
+    rng = np.random.default_rng(6)
+    x1 = x0.clone()
+    sel = vy > yc
+    open_by = 1.8 * torch.exp(-((vx - xc) / (1.6 * half)) ** 2)
+    x1[sel, 1] += open_by[sel]
+    x1 += torch.tensor(rng.normal(0.0, 0.05, x1.shape))
+    res = {}
+    for tag, xx in (("0", x0), ("1", x1)):
+        L, ext = _estimate_crack_length(xx, x_unit, y_unit, yc, x_min, x_max, xc, half, 1.0, 160)
+        vyy = xx @ y_unit
+        res[f"length{tag}"], res[f"extension{tag}"] = L, ext
+        res[f"cmod{tag}"] = float(vyy[up].mean() - vyy[lo].mean()) - cmod0
+    A = rng.normal(0.0, 1.0e4, (3, 3))
+    sigma = torch.tensor(A + A.T)
+    proj = _project_to_lattice_axes(sigma, types.SimpleNamespace(H=H))
+    _save("crack_obs_w3000", x0=x0, x1=x1, H=H, crack_plane_y=yc, half_length=half, upper=up.numpy(),
+          lower=lo.numpy(), sigma=sigma, projected=proj, threshold=1.0, bins=160, **res)
+
+
 def main():
     if not os.path.isdir(REF):
         raise SystemExit(f"reference checkout not found at {REF}")
@@ -337,6 +384,7 @@ def main():
             md_cases(tmp)
             mech_cases(tmp)
             indenter_cases(tmp)
+            crack_cases(tmp)
         finally:
             builtins.print = quiet
 
