@@ -25,6 +25,7 @@ from .md_simulation import MDSimulator
 from .mechanics import SphericalIndenterForce, UniaxialTensileLoader
 from .neighbor import find_neighbors_gpu_pbc
 from .reader import AtomFileReader
+from .restart import load_checkpoint, save_checkpoint
 
 __version__ = "0.1.0"
 
@@ -41,4 +42,4 @@ __all__ = ["AtomFileReader", "Box", "EAMParser", "EAMDeviceTables", "EAMForce", 
            "BerendsenBarostat", "SumBackboneInterface", "BaseModel", "MDSimulator", "MDEngine",
            "find_neighbors_gpu_pbc", "install_simulon_cuda", "BatchedEngine", "Replica", "crack_slab",
            "crack_sweep", "partition_replicas", "AnisotropicNPTBarostat", "UniaxialTensileLoader",
-           "SphericalIndenterForce", "CrackObserver"]
+           "SphericalIndenterForce", "CrackObserver", "save_checkpoint", "load_checkpoint"]

@@ -8,17 +8,31 @@ log.  When ``store_outputs`` is on (the reference does this whenever
 num_steps <= 2000, md_simulation.py:57-68,190-194) forces, energies and
 coordinates of every step are kept on the device in float16, which forces a
 per-step path.
+
+Output files as the reference's (md_simulation.py:30-100,125-168):
+``output_dir`` with ``traj.xyz`` every ``traj_interval`` steps ("n", "Step s,
+Energy = E", "type x y z"), ``energies.csv`` (step, potential, kinetic, total,
+temperature; every step or every ``energies_interval``) and
+``forces/forces_<step>.pt``.  The run stays in CUDA graphs up to each
+output step; positions, forces and the step log rows go to pinned host
+buffers by asynchronous copies, and the files are written while the device
+runs on (no synchronisation per output step).
 """
 from __future__ import annotations
 
+import os
 import time
+from pathlib import Path
 
 import torch
 
 
 class MDSimulator:
     def __init__(self, model, num_steps: int, print_interval: int = 10, store_outputs: bool | None = None,
-                 graph_steps: int = 20, verbose: bool = True, **unused):
+                 graph_steps: int = 20, verbose: bool = True, output_dir: str | None = None, dump_interval: int = 0,
+                 dump_format: str = "xyz", write_forces: bool = False, write_energies: bool = False,
+                 traj_interval: int | None = None, forces_interval: int | None = None,
+                 energies_interval: int | None = None, **unused):
         self.model = model
         self.num_steps = int(num_steps)
         self.print_interval = int(print_interval)
@@ -35,6 +49,102 @@ class MDSimulator:
             self.gpu_energies = torch.empty(k, device=self.device, dtype=torch.float16)
         self.sim_profile = {"output_time": 0.0}
         self.energy_log = []
+        # files (md_simulation.py:30-100)
+        self.output_dir = Path(output_dir) if output_dir else None
+        self.dump_format = (dump_format or "xyz").lower()
+        self.write_forces = bool(write_forces)
+        self.write_energies = bool(write_energies)
+        self.dump_interval = int(dump_interval or 0)
+        self.traj_interval = int(traj_interval) if traj_interval is not None else self.dump_interval
+        self.forces_interval = int(forces_interval) if forces_interval is not None else self.dump_interval
+        self.energies_interval = int(energies_interval) if energies_interval is not None else None
+        any_traj = self.traj_interval > 0 and self.dump_format == "xyz"
+        any_forces = self.write_forces and self.forces_interval > 0
+        self.output_enabled = bool(self.output_dir and (any_traj or any_forces or self.write_energies))
+        self._paths = {}
+        self._pending = []
+        if self.output_enabled:
+            self.output_dir.mkdir(parents=True, exist_ok=True)
+            if any_traj:
+                self._paths["traj"] = str(self.output_dir / "traj.xyz")
+                open(self._paths["traj"], "w", encoding="utf-8").close()
+            if self.write_energies:
+                self._paths["energies"] = str(self.output_dir / "energies.csv")
+                with open(self._paths["energies"], "w", encoding="utf-8") as f:
+                    f.write("step,potential,kinetic,total,temperature\n")
+            if any_forces:
+                (self.output_dir / "forces").mkdir(parents=True, exist_ok=True)
+                self._paths["forces_dir"] = str(self.output_dir / "forces")
+
+    # ---- outputs: device -> pinned host by async copies, written later ------
+    def _output_due(self, step_i: int) -> bool:
+        return bool(("traj" in self._paths and step_i % self.traj_interval == 0) or
+                    ("forces_dir" in self._paths and step_i % self.forces_interval == 0))
+
+    def _next_stop(self, step: int) -> int:
+        """Steps from `step` to the next print or output step."""
+        k = self.print_interval - (step % self.print_interval)
+        for iv, key in ((self.traj_interval, "traj"), (self.forces_interval, "forces_dir")):
+            if key in self._paths and iv > 0:
+                k = min(k, iv - (step % iv))
+        return min(k, self.num_steps - step)
+
+    def _stage(self, step_i: int, log_from: int, log_count: int):
+        """Queue the copies for outputs of step_i and the log rows since the last stage."""
+        model = self.model
+        eng = model.engine
+        item = {"step": step_i}
+        stream = torch.cuda.current_stream(self.device)
+        if "traj" in self._paths and step_i % self.traj_interval == 0:
+            x = eng.gather("x")
+            item["x"] = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+            item["x"].copy_(x, non_blocking=True)
+        if "forces_dir" in self._paths and step_i % self.forces_interval == 0:
+            f = eng.gather("f").to(model.molecular.dtype)
+            item["f"] = torch.empty(f.shape, dtype=f.dtype, pin_memory=True)
+            item["f"].copy_(f, non_blocking=True)
+        if "energies" in self._paths or "traj" in self._paths:
+            rows = model.step_log(log_from, log_count)
+            item["log_first"] = log_from
+            item["log"] = torch.empty(rows.shape, dtype=rows.dtype, pin_memory=True)
+            item["log"].copy_(rows, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        item["event"] = ev
+        self._pending.append(item)
+
+    def _write_ready(self, wait: bool = False):
+        t0 = time.perf_counter()
+        mol = self.model.molecular
+        kB = self.model.Integrator.BOLTZMAN
+        n = mol.atom_count
+        types = getattr(mol, "atom_types", None)
+        while self._pending and (wait or self._pending[0]["event"].query()):
+            item = self._pending.pop(0)
+            item["event"].synchronize()
+            step_i = item["step"]
+            log = item.get("log")
+            if log is not None and "energies" in self._paths:
+                with open(self._paths["energies"], "a", encoding="utf-8") as f:
+                    for r, row in enumerate(log.tolist()):
+                        s = item["log_first"] - self._first_log + r + 1
+                        if self.energies_interval is not None and (self.energies_interval <= 0 or
+                                                                   s % self.energies_interval):
+                            continue
+                        pot, kin = row[0] + row[1], row[9]
+                        temp = (2.0 / 3.0) * kin / (n * kB)
+                        f.write(f"{s},{pot:.8f},{kin:.8f},{pot + kin:.8f},{temp:.6f}\n")
+            if "x" in item:
+                pot = log[-1, 0].item() + log[-1, 1].item()
+                lines = [f"{n}\n", f"Step {step_i}, Energy = {pot:.6f}\n"]
+                names = types if types and len(types) == n else ["X"] * n
+                for name, (x, y, z) in zip(names, item["x"].tolist()):
+                    lines.append(f"{name} {x:.6f} {y:.6f} {z:.6f}\n")
+                with open(self._paths["traj"], "a", encoding="utf-8") as f:
+                    f.writelines(lines)
+            if "f" in item:
+                torch.save(item["f"].clone(), os.path.join(self._paths["forces_dir"], f"forces_{step_i:06d}.pt"))
+        self.sim_profile["output_time"] += time.perf_counter() - t0
 
     def run(self, enable_minimize_energy: bool = False):
         if enable_minimize_energy:
@@ -48,8 +158,11 @@ class MDSimulator:
         t0 = time.perf_counter()
         step = 0
         first_log = model.steps_done
+        self._first_log = first_log
+        staged_upto = first_log
         while step < self.num_steps:
-            chunk = min(self.print_interval - (step % self.print_interval), self.num_steps - step)
+            chunk = self._next_stop(step) if self.output_enabled else \
+                min(self.print_interval - (step % self.print_interval), self.num_steps - step)
             if self.store_outputs:
                 for _ in range(chunk):
                     out = model()
@@ -61,6 +174,11 @@ class MDSimulator:
             else:
                 model.run(chunk, graph_steps=self.graph_steps)
                 step += chunk
+            if self.output_enabled and (self._output_due(step) or step % self.print_interval == 0 or
+                                        step == self.num_steps):
+                self._stage(step, staged_upto, model.steps_done - staged_upto)
+                staged_upto = model.steps_done
+                self._write_ready()
             if step % self.print_interval == 0 or step == self.num_steps:
                 t_out = time.perf_counter()
                 row = model.step_log(model.steps_done - 1, 1)[0].cpu()
@@ -75,6 +193,8 @@ class MDSimulator:
                     print(f"Step {step}/{self.num_steps}:Tot_E={pot + kin:.4f} ev, Pot_E = {pot:.4f} ev, "
                           f"Kin_E = {kin:.4f} ev, T = {temp:.4f} K")
                 self.sim_profile["output_time"] += time.perf_counter() - t_out
+        if self.output_enabled:
+            self._write_ready(wait=True)
         torch.cuda.synchronize(self.device)
         self.sim_profile["loop_time"] = time.perf_counter() - t0
         self.first_step_logged = first_log
