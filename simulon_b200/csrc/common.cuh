@@ -27,6 +27,48 @@ int launch_eam_force_tiled(const SimEngine& e, const SimEAMTables& t, const SimI
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Loads of data read once per pass (neighbour-list rows, in-cutoff masks):
+// evict-first in L1 and L2, so the caches keep the gathered neighbour
+// positions instead.
+#ifndef SIM_STREAM_HINT
+#define SIM_STREAM_HINT 1
+#endif
+template <class T>
+__device__ __forceinline__ T ld_stream(const T* p) {
+#if SIM_STREAM_HINT
+    return __ldcs(p);
+#else
+    return __ldg(p);
+#endif
+}
+
+// The FP64 positions and velocities and the skin references are touched
+// once per step by the integrator: streaming loads and stores as well.
+#ifndef SIM_STATE_HINT
+#define SIM_STATE_HINT 1
+#endif
+__device__ __forceinline__ double ld_state(const double* p) {
+#if SIM_STATE_HINT
+    return __ldcs(p);
+#else
+    return *p;
+#endif
+}
+__device__ __forceinline__ int32_t ld_state(const int32_t* p) {
+#if SIM_STATE_HINT
+    return __ldcs(p);
+#else
+    return *p;
+#endif
+}
+__device__ __forceinline__ void st_state(double* p, double v) {
+#if SIM_STATE_HINT
+    __stcs(p, v);
+#else
+    *p = v;
+#endif
+}
+
 // Programmatic dependent launch (sm_90 and later).  A kernel launched by
 // launch_pdl may be scheduled while its predecessor in the stream (or graph)
 // is still finishing: pdl_wait() returns once the predecessor has completed
@@ -262,11 +304,11 @@ __device__ __forceinline__ void second_half_atom(const SimEngine& e, const SimIn
     const double f[3] = {f0, f1, f2};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        double vel = e.v[c * P + i];
+        double vel = ld_state(&e.v[c * P + i]);
         if (p.langevin) vel = __dadd_rn(__dmul_rn(vel, p.damp), __dmul_rn(z[c], rff));
         const double a = __ddiv_rn(f[c], m);
         vel = __dadd_rn(vel, __dmul_rn(__dmul_rn(0.5, a), p.dt));
-        if (store) e.v[c * P + i] = vel;
+        if (store) st_state(&e.v[c * P + i], vel);
         v_out[c] = vel;
         bad |= !isfinite(vel);
     }
@@ -286,10 +328,10 @@ __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimBox
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const double a = __ddiv_rn(f[c], m);
-        const double v0 = v_in ? v_in[c] : e.v[c * P + i];
+        const double v0 = v_in ? v_in[c] : ld_state(&e.v[c * P + i]);
         const double vh = __dadd_rn(v0, __dmul_rn(__dmul_rn(0.5, a), p.dt));
-        xn[c] = __dadd_rn(e.x[c * P + i], __dmul_rn(vh, p.dt));
-        e.v[c * P + i] = vh;
+        xn[c] = __dadd_rn(ld_state(&e.x[c * P + i]), __dmul_rn(vh, p.dt));
+        st_state(&e.v[c * P + i], vh);
         bad |= !isfinite(xn[c]) || !isfinite(vh);
     }
     return place_atom(e, b, i, type, xn);
@@ -306,7 +348,7 @@ __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimInt
 __device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, int64_t i, int type, const double* xn) {
     const int64_t P = e.n_pad;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) e.x[c * P + i] = xn[c];
+    for (int c = 0; c < 3; ++c) st_state(&e.x[c * P + i], xn[c]);
     double s[3];
     cart_to_frac(b, xn[0], xn[1], xn[2], s);
     int4 q;
@@ -316,9 +358,9 @@ __device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, 
     q.w = type;
     reinterpret_cast<int4*>(e.posq)[i] = q;
     // displacement since the last rebuild, minimum image in fractional space
-    const double t0 = (double)(int32_t)((uint32_t)q.x - (uint32_t)e.xref[i]) * 2.3283064365386963e-10;
-    const double t1 = (double)(int32_t)((uint32_t)q.y - (uint32_t)e.xref[P + i]) * 2.3283064365386963e-10;
-    const double t2 = (double)(int32_t)((uint32_t)q.z - (uint32_t)e.xref[2 * P + i]) * 2.3283064365386963e-10;
+    const double t0 = (double)(int32_t)((uint32_t)q.x - (uint32_t)ld_state(&e.xref[i])) * 2.3283064365386963e-10;
+    const double t1 = (double)(int32_t)((uint32_t)q.y - (uint32_t)ld_state(&e.xref[P + i])) * 2.3283064365386963e-10;
+    const double t2 = (double)(int32_t)((uint32_t)q.z - (uint32_t)ld_state(&e.xref[2 * P + i])) * 2.3283064365386963e-10;
     const double d0 = t0 * b.H[0] + t1 * b.H[3] + t2 * b.H[6];
     const double d1 = t0 * b.H[1] + t1 * b.H[4] + t2 * b.H[7];
     const double d2 = t0 * b.H[2] + t1 * b.H[5] + t2 * b.H[8];

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k
             int j[U];
             int4 q[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) j[u] = __ldg(&nbr[(int64_t)(k + u) * P + i]);
+            for (int u = 0; u < U; ++u) j[u] = ld_stream(&nbr[(int64_t)(k + u) * P + i]);
 #pragma unroll
             for (int u = 0; u < U; ++u) q[u] = __ldg(&posq[j[u]]);
             uint32_t bits = 0;
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k
         }
         for (; k < nn; ++k) {
             bool in;
-            rho += density_term<SMEM, ORTHO>(b, qi, __ldg(&posq[__ldg(&nbr[(int64_t)k * P + i])]), rc2, g_i, s_i,
+            rho += density_term<SMEM, ORTHO>(b, qi, __ldg(&posq[ld_stream(&nbr[(int64_t)k * P + i])]), rc2, g_i, s_i,
                                              w, t, in);
             if (k < 32) in_lo |= (uint32_t)in << k;
             else in_hi |= (uint32_t)in << (k - 32);
@@ -155,16 +155,16 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
         if (SINGLE && use_mask) {
             // only the slots pass 1 found inside the cutoff; the next two list
             // entries are fetched while the current pair is gathered and evaluated
-            uint64_t m = e.cut_mask[i];
+            uint64_t m = ld_stream(&e.cut_mask[i]);
             int ka = pop_slot(m), kb = pop_slot(m);
-            int ja = ka >= 0 ? __ldg(&nbr[(int64_t)ka * P + i]) : 0;
-            int jb = kb >= 0 ? __ldg(&nbr[(int64_t)kb * P + i]) : 0;
+            int ja = ka >= 0 ? ld_stream(&nbr[(int64_t)ka * P + i]) : 0;
+            int jb = kb >= 0 ? ld_stream(&nbr[(int64_t)kb * P + i]) : 0;
             while (kb >= 0) {
                 const int j0 = ja, j1 = jb;
                 ka = pop_slot(m);
                 kb = pop_slot(m);
-                if (ka >= 0) ja = __ldg(&nbr[(int64_t)ka * P + i]);
-                if (kb >= 0) jb = __ldg(&nbr[(int64_t)kb * P + i]);
+                if (ka >= 0) ja = ld_stream(&nbr[(int64_t)ka * P + i]);
+                if (kb >= 0) jb = ld_stream(&nbr[(int64_t)kb * P + i]);
                 const int4 q0 = __ldg(&posfp[j0]);
                 const int4 q1 = __ldg(&posfp[j1]);
                 pair_single<ORTHO>(b, pi, q0, rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
@@ -175,13 +175,13 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
         } else if (SINGLE) {
             // the next two list entries are fetched while the current pair is
             // gathered and evaluated, so the list's DRAM latency overlaps work
-            int jn0 = nn > 0 ? __ldg(&nbr[i]) : 0;
-            int jn1 = nn > 1 ? __ldg(&nbr[P + i]) : 0;
+            int jn0 = nn > 0 ? ld_stream(&nbr[i]) : 0;
+            int jn1 = nn > 1 ? ld_stream(&nbr[P + i]) : 0;
             int k = 0;
             for (; k + 2 <= nn; k += 2) {
                 const int j0 = jn0, j1 = jn1;
-                if (k + 2 < nn) jn0 = __ldg(&nbr[(int64_t)(k + 2) * P + i]);
-                if (k + 3 < nn) jn1 = __ldg(&nbr[(int64_t)(k + 3) * P + i]);
+                if (k + 2 < nn) jn0 = ld_stream(&nbr[(int64_t)(k + 2) * P + i]);
+                if (k + 3 < nn) jn1 = ld_stream(&nbr[(int64_t)(k + 3) * P + i]);
                 const int4 q0 = __ldg(&posfp[j0]);
                 const int4 q1 = __ldg(&posfp[j1]);
                 pair_single<ORTHO>(b, pi, q0, rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
@@ -195,9 +195,9 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
             const float4* gd = reinterpret_cast<const float4*>(t.deriv_vd);
             const float2* gp = reinterpret_cast<const float2*>(t.pair_vd);
             ti = posq[i].w;
-            uint64_t m = use_mask ? e.cut_mask[i] : 0;
+            uint64_t m = use_mask ? ld_stream(&e.cut_mask[i]) : 0;
             for (int k = use_mask ? pop_slot(m) : 0; use_mask ? k >= 0 : k < nn; k = use_mask ? pop_slot(m) : k + 1) {
-                const int j = __ldg(&nbr[(int64_t)k * P + i]);
+                const int j = ld_stream(&nbr[(int64_t)k * P + i]);
                 const int4 qj = __ldg(&posfp[j]);
                 float r0, r1, r2;
                 rvec<ORTHO>(b, pi, qj, r0, r1, r2);
