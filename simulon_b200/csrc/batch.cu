@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(BATCH_DENSITY_THREADS, 3) k_bb_density(SimBatc
                 int j[4];
                 int4 q[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) j[u] = __ldg(&nbr[(int64_t)(kk + u) * P + i]);
+                for (int u = 0; u < 4; ++u) j[u] = ld_stream(&nbr[(int64_t)(kk + u) * P + i]);
 #pragma unroll
                 for (int u = 0; u < 4; ++u) q[u] = __ldg(&posq[j[u]]);
                 uint32_t bits = 0;
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(BATCH_DENSITY_THREADS, 3) k_bb_density(SimBatc
             }
             for (; kk < nn; ++kk) {
                 bool in;
-                rho += density_term<true, ORTHO>(b, qi, __ldg(&posq[__ldg(&nbr[(int64_t)kk * P + i])]), rc2, dens,
+                rho += density_term<true, ORTHO>(b, qi, __ldg(&posq[ld_stream(&nbr[(int64_t)kk * P + i])]), rc2, dens,
                                                  s_dens, w, t, in);
                 if (kk < 32) in_lo |= (uint32_t)in << kk;
                 else in_hi |= (uint32_t)in << (kk - 32);
@@ -491,16 +491,16 @@ __global__ void __launch_bounds__(BATCH_FORCE_THREADS, 1) k_bb_force(SimBatch B,
             if (use_mask) {
                 // in-cutoff slots only; the next two list entries are fetched
                 // while the current pair is gathered and evaluated
-                uint64_t m = e.cut_mask[i];
+                uint64_t m = ld_stream(&e.cut_mask[i]);
                 int ka = pop_slot(m), kb = pop_slot(m);
-                int ja = ka >= 0 ? __ldg(&nbr[(int64_t)ka * P + i]) : 0;
-                int jb = kb >= 0 ? __ldg(&nbr[(int64_t)kb * P + i]) : 0;
+                int ja = ka >= 0 ? ld_stream(&nbr[(int64_t)ka * P + i]) : 0;
+                int jb = kb >= 0 ? ld_stream(&nbr[(int64_t)kb * P + i]) : 0;
                 while (kb >= 0) {
                     const int j0 = ja, j1 = jb;
                     ka = pop_slot(m);
                     kb = pop_slot(m);
-                    if (ka >= 0) ja = __ldg(&nbr[(int64_t)ka * P + i]);
-                    if (kb >= 0) jb = __ldg(&nbr[(int64_t)kb * P + i]);
+                    if (ka >= 0) ja = ld_stream(&nbr[(int64_t)ka * P + i]);
+                    if (kb >= 0) jb = ld_stream(&nbr[(int64_t)kb * P + i]);
                     const int4 q0 = __ldg(&posfp[j0]);
                     const int4 q1 = __ldg(&posfp[j1]);
                     pair_single<ORTHO>(b, pi, q0, rc2, fpi, tab_d, tab_p, w, t, fx, fy, fz, acc);
@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(BATCH_FORCE_THREADS, 1) k_bb_force(SimBatch B,
             } else {
                 const int nn = e.nnbr[i];
                 for (int kk = 0; kk < nn; ++kk)
-                    pair_single<ORTHO>(b, pi, __ldg(&posfp[__ldg(&nbr[(int64_t)kk * P + i])]), rc2, fpi, tab_d,
+                    pair_single<ORTHO>(b, pi, __ldg(&posfp[ld_stream(&nbr[(int64_t)kk * P + i])]), rc2, fpi, tab_d,
                                        tab_p, w, t, fx, fy, fz, acc);
             }
             reinterpret_cast<float4*>(e.f32)[i] = make_float4(fx, fy, fz, 0.0f);

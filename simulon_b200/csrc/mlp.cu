@@ -93,7 +93,7 @@ __device__ __forceinline__ int mlp_table(const SimEngine& e, const BoxF& b, int6
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int k = k0 + r * GRP + sub;
-            jj[r] = k < nn ? __ldg(&e.nbr[(int64_t)k * e.n_pad + i]) : -1;
+            jj[r] = k < nn ? ld_stream(&e.nbr[(int64_t)k * e.n_pad + i]) : -1;
         }
 #pragma unroll
         for (int r = 0; r < R; ++r) qq[r] = jj[r] >= 0 ? __ldg(&posq[jj[r]]) : make_int4(0, 0, 0, 0);
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(256) k_eam_atom_energy(SimEngine e, SimEAMTabl
         const int4 qi = posq[i];
         float rho = 0.0f, half = 0.0f;
         for (int k = 0; k < e.nnbr[i]; ++k) {
-            const int4 qj = __ldg(&posq[__ldg(&e.nbr[(int64_t)k * e.n_pad + i])]);
+            const int4 qj = __ldg(&posq[ld_stream(&e.nbr[(int64_t)k * e.n_pad + i])]);
             float r0, r1, r2;
             rvec<false>(b, qi, qj, r0, r1, r2);
             const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
@@ -881,7 +881,7 @@ __global__ void __launch_bounds__(128) k_mlp_ucontract(SimEngine e, const float*
         const float4 ei = er[i];
         int cnt = 0;
         for (int k = 0; k < e.nnbr[i]; ++k) {
-            const int j = __ldg(&e.nbr[(int64_t)k * e.n_pad + i]);
+            const int j = ld_stream(&e.nbr[(int64_t)k * e.n_pad + i]);
             const int4 qj = __ldg(&posq[j]);
             float d0, d1, d2;
             mlp_dvec<ORTHO>(b, qi, qj, d0, d1, d2);
