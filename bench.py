@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "atom-steps/s (EAM-W, 1 B200): plain vs batched vs MLP at stated force RMSE"
 UNIT = "atom-steps/s"
-PASS2_DRAM_BYTES_PER_ATOM = (66975232 + 2780416) / 524288   # k_eam_force<1,1,1>, ncu --set full
+PASS2_DRAM_BYTES_PER_ATOM = (66263040 + 1362176) / 524288   # k_eam_force<1,1,1>, ncu --set full
 A_W, M_W = 3.165, 183.84
 
 

@@ -67,7 +67,8 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k
     const float rc2 = t.cutoff * t.cutoff;
     const bool use_mask = e.cut_mask != nullptr && e.nbr_cap <= 64;
     double acc = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += stride) {
         const int4 qi = posq[i];
         const int ti = qi.w;
         const int nn = e.nnbr[i];

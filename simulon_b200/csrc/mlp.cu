@@ -610,16 +610,13 @@ __global__ void __launch_bounds__(MLP_TILE) k_mlp_fwd(SimMLP m, const float* __r
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" :: "r"(tm));
 }
 
-// TRAIN = false: E_i and dE/dG (scaled by 1/sigma) per atom.
-// TRAIN = true : per-atom loss (E_i - target_i)^2 / n_batch, its gradient
-//                with respect to every weight (added to grads with atomics)
-//                and the loss sum (added to *loss).
-template <bool TRAIN>
-__global__ void __launch_bounds__(MLP_TILE) k_mlp_net(SimMLP m, const float* __restrict__ G, int64_t n,
-                                                      float* __restrict__ e_atom, float* __restrict__ dEdG,
-                                                      const float* __restrict__ target, float inv_batch,
-                                                      float* __restrict__ grads, float* __restrict__ loss,
-                                                      int32_t* status) {
+// Energy regression: per-atom loss (E_i - target_i)^2 / n_batch, its gradient
+// with respect to every weight (added to grads with atomics) and the loss sum
+// (added to *loss).
+__global__ void __launch_bounds__(MLP_TILE) k_mlp_train(SimMLP m, const float* __restrict__ G, int64_t n,
+                                                        const float* __restrict__ target, float inv_batch,
+                                                        float* __restrict__ grads, float* __restrict__ loss,
+                                                        int32_t* status) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     MlpSmem& S = *reinterpret_cast<MlpSmem*>(smem_raw);
     const int t = threadIdx.x, warp = t >> 5;
@@ -695,7 +692,7 @@ __global__ void __launch_bounds__(MLP_TILE) k_mlp_net(SimMLP m, const float* __r
 #pragma unroll
                 for (int q = 0; q < 8; ++q) h[q] = silu(z1[k0 + q] + S.b1[k0 + q]);
                 img_store8(S.a1, t, k0, MLP_H, h);
-                if (TRAIN) img_store8(S.a3, t, k0, MLP_H, h);
+                img_store8(S.a3, t, k0, MLP_H, h);
             }
         }
         async_proxy_fence();
@@ -721,43 +718,36 @@ __global__ void __launch_bounds__(MLP_TILE) k_mlp_net(SimMLP m, const float* __r
         float E = S.b3;
 #pragma unroll
         for (int k = 0; k < MLP_H; ++k) E = fmaf(S.w3[k], silu(z2[k] + S.b2[k]), E);
-        // dL/dE: 1 for forces, 2 (E - target) / n_batch while training
-        float up = 1.0f;
-        if (TRAIN) {
-            const float err = live ? E - target[i] : 0.0f;
-            up = 2.0f * err * inv_batch;
-            const float l = live ? err * err * inv_batch : 0.0f;
-            const float ls = warp_sum_f(l);
+        // dL/dE = 2 (E - target) / n_batch
+        const float err = live ? E - target[i] : 0.0f;
+        const float up = 2.0f * err * inv_batch;
+        {
+            const float ls = warp_sum_f(live ? err * err * inv_batch : 0.0f);
             if ((t & 31) == 0) atomicAdd(loss, ls);
-        } else if (live) {
-            e_atom[i] = E;
         }
-        if (!live) up = 0.0f;
         {
             float d[8];
 #pragma unroll
             for (int k0 = 0; k0 < MLP_H; k0 += 8) {
 #pragma unroll
                 for (int q = 0; q < 8; ++q) d[q] = up * S.w3[k0 + q] * dsilu(z2[k0 + q] + S.b2[k0 + q]);
-                img_store8(TRAIN ? S.a2 : S.a1, t, k0, MLP_H, d);
+                img_store8(S.a2, t, k0, MLP_H, d);
             }
-            if (TRAIN) {
-                // output layer: dw3 = sum up * h2, db3 = sum up
+            // output layer: dw3 = sum up * h2, db3 = sum up
 #pragma unroll 4
-                for (int k = 0; k < MLP_H; ++k) {
-                    const float v = warp_sum_f(up * silu(z2[k] + S.b2[k]));
-                    if ((t & 31) == 0) atomicAdd(&grads[GRAD_W3 + k], v);
-                }
-                const float v = warp_sum_f(up);
-                if ((t & 31) == 0) atomicAdd(&grads[GRAD_B3], v);
+            for (int k = 0; k < MLP_H; ++k) {
+                const float v = warp_sum_f(up * silu(z2[k] + S.b2[k]));
+                if ((t & 31) == 0) atomicAdd(&grads[GRAD_W3 + k], v);
             }
+            const float v = warp_sum_f(up);
+            if ((t & 31) == 0) atomicAdd(&grads[GRAD_B3], v);
         }
         async_proxy_fence();
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
         // D1 = dZ2 W2^T -> tmem columns [64, 128)
-        const __nv_bfloat16* dz2 = TRAIN ? S.a2 : S.a1;
+        const __nv_bfloat16* dz2 = S.a2;
         if (t == 0) {
 #pragma unroll
             for (int s = 0; s < MLP_H / 16; ++s)
@@ -780,78 +770,42 @@ __global__ void __launch_bounds__(MLP_TILE) k_mlp_net(SimMLP m, const float* __r
 #pragma unroll
             for (int k = 0; k < MLP_H; ++k) d1[k] *= dsilu(z1[k] + S.b1[k]);
         }
-        if (TRAIN) {
-            // weight gradients on the CUDA cores from the tile's operands:
-            // thread t owns column n = t & 63 of dW2 (rows k) and of dW1 (rows c),
-            // half the rows each; sums over the tile's 128 atoms
-            float dk[8];
+        // weight gradients on the CUDA cores from the tile's operands:
+        // thread t owns column n = t & 63 of dW2 (rows k) and of dW1 (rows c),
+        // half the rows each; sums over the tile's 128 atoms
+        float dk[8];
 #pragma unroll
-            for (int k0 = 0; k0 < MLP_H; k0 += 8) {
+        for (int k0 = 0; k0 < MLP_H; k0 += 8) {
 #pragma unroll
-                for (int q = 0; q < 8; ++q) dk[q] = d1[k0 + q];
-                img_store8(S.a1, t, k0, MLP_H, dk);        // dZ1 (H1 is kept in a3)
+            for (int q = 0; q < 8; ++q) dk[q] = d1[k0 + q];
+            img_store8(S.a1, t, k0, MLP_H, dk);        // dZ1 (H1 is kept in a3)
+        }
+        __syncthreads();
+        const int col = t & 63, half = t >> 6;
+        // dW2[k][col] = sum_r H1[r][k] dZ2[r][col]; db2[col] = sum_r dZ2[r][col]
+        for (int k = half * 32; k < half * 32 + 32; ++k) {
+            float acc = 0.0f;
+            for (int r = 0; r < MLP_TILE; ++r)
+                acc = fmaf(__bfloat162float(S.a3[img_off(r, k, MLP_H)]),
+                           __bfloat162float(S.a2[img_off(r, col, MLP_H)]), acc);
+            atomicAdd(&grads[GRAD_W2 + k * MLP_H + col], acc);
+        }
+        // dW1[c][col] = sum_r G[r][c] dZ1[r][col]; db1, db2
+        for (int c = half * 8; c < half * 8 + 8; ++c) {
+            float acc = 0.0f;
+            for (int r = 0; r < MLP_TILE; ++r)
+                acc = fmaf(__bfloat162float(S.a0[img_off(r, c, MLP_D)]),
+                           __bfloat162float(S.a1[img_off(r, col, MLP_H)]), acc);
+            atomicAdd(&grads[GRAD_W1 + c * MLP_H + col], acc);
+        }
+        if (half == 0) {
+            float a = 0.0f, bsum = 0.0f;
+            for (int r = 0; r < MLP_TILE; ++r) {
+                a += __bfloat162float(S.a1[img_off(r, col, MLP_H)]);
+                bsum += __bfloat162float(S.a2[img_off(r, col, MLP_H)]);
             }
-            __syncthreads();
-            const int col = t & 63, half = t >> 6;
-            // dW2[k][col] = sum_r H1[r][k] dZ2[r][col]; db2[col] = sum_r dZ2[r][col]
-            for (int k = half * 32; k < half * 32 + 32; ++k) {
-                float acc = 0.0f;
-                for (int r = 0; r < MLP_TILE; ++r)
-                    acc = fmaf(__bfloat162float(S.a3[img_off(r, k, MLP_H)]),
-                               __bfloat162float(S.a2[img_off(r, col, MLP_H)]), acc);
-                atomicAdd(&grads[GRAD_W2 + k * MLP_H + col], acc);
-            }
-            // dW1[c][col] = sum_r G[r][c] dZ1[r][col]; db1, db2
-            for (int c = half * 8; c < half * 8 + 8; ++c) {
-                float acc = 0.0f;
-                for (int r = 0; r < MLP_TILE; ++r)
-                    acc = fmaf(__bfloat162float(S.a0[img_off(r, c, MLP_D)]),
-                               __bfloat162float(S.a1[img_off(r, col, MLP_H)]), acc);
-                atomicAdd(&grads[GRAD_W1 + c * MLP_H + col], acc);
-            }
-            if (half == 0) {
-                float a = 0.0f, bsum = 0.0f;
-                for (int r = 0; r < MLP_TILE; ++r) {
-                    a += __bfloat162float(S.a1[img_off(r, col, MLP_H)]);
-                    bsum += __bfloat162float(S.a2[img_off(r, col, MLP_H)]);
-                }
-                atomicAdd(&grads[GRAD_B1 + col], a);
-                atomicAdd(&grads[GRAD_B2 + col], bsum);
-            }
-        } else {
-            float dk[8];
-#pragma unroll
-            for (int k0 = 0; k0 < MLP_H; k0 += 8) {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) dk[q] = d1[k0 + q];
-                img_store8(S.a2, t, k0, MLP_H, dk);
-            }
-            async_proxy_fence();
-            tc_fence_before();
-            __syncthreads();
-            tc_fence_after();
-            // dG = dZ1 W1^T -> tmem columns [64, 80)
-            if (t == 0) {
-#pragma unroll
-                for (int s = 0; s < MLP_H / 16; ++s)
-                    mma_bf16(tm + 64, smem_desc(S.a2 + s * 2 * 64, MLP_H), smem_desc(S.w1 + s * 2 * 64, MLP_H),
-                             mma_idesc(128, MLP_D), s > 0);
-                mma_commit(&S.bar);
-            }
-            failed = __syncthreads_or(!mbar_wait(&S.bar, phase));
-            phase ^= 1;
-            if (failed) break;
-            tc_fence_after();
-            float gv[MLP_D];
-            tmem_ld16(tm + lane_base + 64, gv);
-            tmem_wait_ld();
-            if (live) {
-                float4* out = reinterpret_cast<float4*>(dEdG + i * MLP_D);
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    out[q] = make_float4(gv[4 * q] * S.isg[4 * q], gv[4 * q + 1] * S.isg[4 * q + 1],
-                                         gv[4 * q + 2] * S.isg[4 * q + 2], gv[4 * q + 3] * S.isg[4 * q + 3]);
-            }
+            atomicAdd(&grads[GRAD_B1 + col], a);
+            atomicAdd(&grads[GRAD_B2 + col], bsum);
         }
         tc_fence_before();
         __syncthreads();
@@ -1254,7 +1208,7 @@ static void mlp_set_attributes() {
     static bool done = false;   // the first call happens before any stream capture
     if (done) return;
     cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_fwd_smem());
-    cudaFuncSetAttribute(k_mlp_net<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
+    cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
     cudaGetLastError();
     done = true;
 }
@@ -1383,9 +1337,8 @@ extern "C" int sim_mlp_train_grads(const SimMLP* m, const float* G, const float*
     cudaError_t err = cudaMemsetAsync(grads, 0, sizeof(float) * SIM_MLP_PARAMS, st);
     if (err == cudaSuccess) err = cudaMemsetAsync(loss, 0, sizeof(float), st);
     if (err != cudaSuccess) { set_cuda_error(err, "sim_mlp_train_grads: zero"); return SIM_ERR_CUDA; }
-    const int g = mlp_grid((const void*)k_mlp_net<true>, (n + MLP_TILE - 1) / MLP_TILE, sizeof(MlpSmem), 128);
-    k_mlp_net<true><<<g, MLP_TILE, sizeof(MlpSmem), st>>>(*m, G, n, nullptr, nullptr, target, 1.0f / (float)n, grads,
-                                                         loss, status);
+    const int g = mlp_grid((const void*)k_mlp_train, (n + MLP_TILE - 1) / MLP_TILE, sizeof(MlpSmem), 128);
+    k_mlp_train<<<g, MLP_TILE, sizeof(MlpSmem), st>>>(*m, G, n, target, 1.0f / (float)n, grads, loss, status);
     return launch_status("sim_mlp_train_grads");
 }
 
