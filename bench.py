@@ -214,13 +214,14 @@ def run_reference(args):
 # ------------------------------------------------------------------ GPU arm
 def launches_for(steps: int, graph_steps: int) -> int:
     """Kernels of ours launched by BaseModel.run(steps): per run of k > 1 steps,
-    the first half-step and its IF-node condition, then per step EAM pass 1,
-    pass 2 (fused with the second half and the next first half) and the step
-    log, plus the IF-node condition between steps (4k + 1); a single step is
-    first half, condition, pass 1, pass 2 + second half, log (5).  Each
-    triggered rebuild adds the 10 kernels of the IF body."""
+    the first half-step and its IF-node condition, then per step EAM pass 1
+    and pass 2 (fused with the second half and the next first half; its last
+    block writes the step log row and sets the next IF node's value), the last
+    step's pass 2 finishing without the drift and followed by its log kernel
+    (2k + 3); a single step is first half, condition, pass 1, pass 2 + second
+    half, log (5).  Each triggered rebuild adds the 10 kernels of the IF body."""
     full, rest = divmod(int(steps), int(graph_steps))
-    per = lambda k: 0 if k == 0 else (5 if k == 1 else 4 * k + 1)
+    per = lambda k: 0 if k == 0 else (5 if k == 1 else 2 * k + 3)
     return full * per(int(graph_steps)) + per(rest)
 
 

@@ -322,6 +322,19 @@ int sim_eam_force_integrate(const SimEngine* e, const SimEAMTables* t, const Sim
  * Not available with neighbour tiles (nbr16 set): SIM_ERR_ARG. */
 int sim_eam_force_integrate_drift(const SimEngine* e, const SimEAMTables* t, const SimIntegrator* p,
                                   void* stream);
+/* One whole MD step of the drift-fused form ended on the device: EAM pass 1,
+ * then pass 2 as sim_eam_force_integrate_drift, whose last block also appends
+ * the step's log row (as sim_log_step on &step_ctr[1]) and decides the
+ * conditional rebuild (as sim_rebuild_if_needed): while `stream` is being
+ * captured, an IF node holding the rebuild follows pass 2, which sets the
+ * node's value itself (no separate log or condition kernel in the graph);
+ * otherwise the flag-gated rebuild is launched after it.  Same results, bit
+ * for bit, as sim_eam_density + sim_eam_force_integrate_drift + sim_log_step +
+ * sim_rebuild_if_needed.  Replaces one pass of BaseModel.forward's step
+ * (md_model.py:107-139: first_half with its list update, sum_bone,
+ * second_half) plus the step's energy record.  n_extra <= 32. */
+int sim_eam_step_drift(const SimEngine* e, const SimEAMTables* t, const SimIntegrator* p, const double* extra,
+                       int32_t n_extra, double* log, int32_t log_capacity, void* stream);
 
 /* sim_eam_forces without caller-allocated scratch.  No counterpart in the
  * reference (which allocates through PyTorch on every call); it exists for

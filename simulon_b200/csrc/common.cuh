@@ -16,6 +16,13 @@ void prepare_capture_stream();           // side stream used to capture IF-node 
 typedef int (*BodyFn)(const void* ctx, cudaStream_t s);
 int  launch_if_flag(cudaStream_t st, const int32_t* flag, BodyFn body, BodyFn eager, const void* ctx,
                     const char* what);       // IF node on *flag while capturing, else eager()
+// cond(ctx, s, h) launches work that sets the IF node's value through *h
+// (cudaGraphSetConditional), or the same work without it when h is null
+typedef int (*CondFn)(const void* ctx, cudaStream_t s, const cudaGraphConditionalHandle* h);
+int  launch_if_cond(cudaStream_t st, CondFn cond, BodyFn body, BodyFn eager, const void* ctx, const char* what);
+// the engine's rebuild as an IF-node body (ungated) and eagerly (gated on flags[0]); ctx is the SimEngine
+int  rebuild_body(const void* ctx, cudaStream_t s);
+int  rebuild_eager(const void* ctx, cudaStream_t s);
 // Persistent grid: resident blocks per SM (cached occupancy query) x SM count,
 // capped by the number of atom tiles.
 int persistent_grid(const void* fn, int threads, size_t smem, int64_t n);

@@ -121,9 +121,22 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k
 // step counter (step_ctr[0] = step + 1, step_ctr[1] = step for the step log).
 // Pass 2 reads only posfp (pass 1's copy of the positions), so atoms can move
 // while other threads still gather their neighbours.
+// What the last block of a drift-fused pass 2 (INTEG 2) does to end the MD
+// step on the device when sim_eam_step_drift launched it: append the step's
+// log row (as k_log_step on step_ctr[1]) and, inside a captured graph, set
+// the value of the conditional rebuild's IF node from the skin/2 trigger (as
+// k_set_rebuild_condition).
+struct StepEnd {
+    const double* extra;
+    double* log;                        // null: no log row
+    int n_extra, cap;
+    cudaGraphConditionalHandle h;
+    int set_cond;                       // 0: no IF node (eager launch)
+};
+
 template <bool SINGLE, int INTEG, bool ORTHO>
 __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam_force(SimEngine e, SimEAMTables t, SimIntegrator ip,
-                                                                    Window w) {
+                                                                    Window w, StepEnd end) {
     extern __shared__ float4 s_tab4[];
     pdl_trigger();
     float4* tab_d = s_tab4;
@@ -242,9 +255,24 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
         for (int k = 0; k < 15; ++k) vals[k] = k < 8 ? 0.5 * (double)acc[k] : (double)acc[k];
         block_partials<15>(vals, e.partials, SIM_RED_EPOT_PAIR);
         const bool last = last_block_finalize<15>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
-        if (INTEG == 2 && last && threadIdx.x == 0) {
-            ip.step_ctr[1] = step;
-            ip.step_ctr[0] = step + 1;
+        if (INTEG == 2 && last) {     // uniform across the block
+            if (threadIdx.x == 0) {
+                ip.step_ctr[1] = step;
+                ip.step_ctr[0] = step + 1;
+            }
+            if (end.log || end.set_cond) {
+                // every block's trigger and status writes preceded its fence
+                // and counter increment; this block's red_out rows precede the barrier
+                __syncthreads();
+                const int k = threadIdx.x;
+                if (end.log) {
+                    double* row = end.log + (size_t)(step % (uint64_t)end.cap) * (SIM_RED_SLOTS + end.n_extra + 1);
+                    if (k < SIM_RED_SLOTS) row[k] = __ldcg(&e.red_out[k]);
+                    else if (k < SIM_RED_SLOTS + end.n_extra) row[k] = end.extra[k - SIM_RED_SLOTS];
+                    else if (k == SIM_RED_SLOTS + end.n_extra) row[k] = (double)__ldcg(&e.flags[1]);
+                }
+                if (end.set_cond && k == 0) cudaGraphSetConditional(end.h, __ldcg(&e.flags[0]) != 0 ? 1u : 0u);
+            }
         }
     } else {
         double vals[8];
@@ -343,20 +371,22 @@ extern "C" int sim_eam_density(const SimEngine* ep, const SimEAMTables* tp, void
 }
 
 template <bool SINGLE, int INTEG, bool ORTHO>
-static int launch_force(const SimEngine& e, const SimEAMTables& t, const SimIntegrator& ip, cudaStream_t st) {
+static int launch_force(const SimEngine& e, const SimEAMTables& t, const SimIntegrator& ip, const StepEnd& end,
+                        cudaStream_t st) {
     const size_t smem = SINGLE ? smem_pass2(t) : 0;
     const int threads = force_threads(e);
     if (threads < 0) return SIM_ERR_ARG;
     const int g = persistent_grid((const void*)k_eam_force<SINGLE, INTEG, ORTHO>, threads, smem, e.n);
     if (g > e.n_blocks_max) return SIM_ERR_ARG;
     const cudaError_t err = launch_pdl(k_eam_force<SINGLE, INTEG, ORTHO>, dim3(g), dim3(threads), smem, st, e, t, ip,
-                                       table_window(t));
+                                       table_window(t), end);
     if (err != cudaSuccess) { set_cuda_error(err, "sim_eam_force: launch"); return SIM_ERR_CUDA; }
     return SIM_OK;
 }
 
 template <int INTEG>
-static int launch_eam_force(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip, void* stream) {
+static int launch_eam_force(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip, void* stream,
+                            const StepEnd& end = StepEnd{}) {
     if (!ep || !tp || ep->n <= 0 || !ep->posfp || !valid_tables(*tp)) return SIM_ERR_ARG;
     const SimEngine& e = *ep;
     const SimEAMTables& t = *tp;
@@ -377,11 +407,11 @@ static int launch_eam_force(const SimEngine* ep, const SimEAMTables* tp, const S
     if (tiled)
         rc = launch_eam_force_tiled(e, t, INTEG ? &integ : nullptr, st);
     else if (single)
-        rc = e.box_orthogonal ? launch_force<true, INTEG, true>(e, t, integ, st)
-                              : launch_force<true, INTEG, false>(e, t, integ, st);
+        rc = e.box_orthogonal ? launch_force<true, INTEG, true>(e, t, integ, end, st)
+                              : launch_force<true, INTEG, false>(e, t, integ, end, st);
     else
-        rc = e.box_orthogonal ? launch_force<false, INTEG, true>(e, t, integ, st)
-                              : launch_force<false, INTEG, false>(e, t, integ, st);
+        rc = e.box_orthogonal ? launch_force<false, INTEG, true>(e, t, integ, end, st)
+                              : launch_force<false, INTEG, false>(e, t, integ, end, st);
     if (rc != SIM_OK) return rc;
     return launch_status(INTEG == 2 ? "sim_eam_force_integrate_drift"
                                     : (INTEG ? "sim_eam_force_integrate" : "sim_eam_force"));
@@ -399,6 +429,36 @@ extern "C" int sim_eam_force_integrate(const SimEngine* ep, const SimEAMTables* 
 extern "C" int sim_eam_force_integrate_drift(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip,
                                              void* stream) {
     return launch_eam_force<2>(ep, tp, ip, stream);
+}
+
+namespace {
+struct StepCtx {
+    const SimEngine* e;
+    const SimEAMTables* t;
+    const SimIntegrator* ip;
+    StepEnd end;
+};
+int step_pass2(const void* ctx, cudaStream_t st, const cudaGraphConditionalHandle* h) {
+    const StepCtx& c = *static_cast<const StepCtx*>(ctx);
+    StepEnd end = c.end;
+    end.set_cond = h != nullptr;
+    if (h) end.h = *h;
+    return launch_eam_force<2>(c.e, c.t, c.ip, st, end);
+}
+int step_rebuild_body(const void* ctx, cudaStream_t s) { return rebuild_body(static_cast<const StepCtx*>(ctx)->e, s); }
+int step_rebuild_eager(const void* ctx, cudaStream_t s) { return rebuild_eager(static_cast<const StepCtx*>(ctx)->e, s); }
+}  // namespace
+
+extern "C" int sim_eam_step_drift(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip,
+                                  const double* extra, int32_t n_extra, double* log, int32_t log_capacity,
+                                  void* stream) {
+    if (!ep || !ep->box || !log || log_capacity <= 0 || n_extra < 0 || n_extra > 32 || (n_extra > 0 && !extra))
+        return SIM_ERR_ARG;
+    int rc = sim_eam_density(ep, tp, stream);
+    if (rc != SIM_OK) return rc;
+    StepCtx c{ep, tp, ip, StepEnd{extra, log, (int)n_extra, (int)log_capacity, 0, 0}};
+    return launch_if_cond((cudaStream_t)stream, step_pass2, step_rebuild_body, step_rebuild_eager, &c,
+                          "sim_eam_step_drift");
 }
 
 extern "C" int sim_eam_forces(const SimEngine* ep, const SimEAMTables* tp, void* stream) {

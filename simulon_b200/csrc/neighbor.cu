@@ -569,25 +569,17 @@ void simb200::prepare_capture_stream() {
     if (!g_body_stream) cudaStreamCreateWithFlags(&g_body_stream, cudaStreamNonBlocking);
 }
 
-// While `st` is being captured: a one-thread kernel turns *flag into the value
-// of an IF node whose body is captured from body(ctx, body_stream); otherwise
-// run eager(ctx, st), which tests the flag on the device itself.
-int simb200::launch_if_flag(cudaStream_t st, const int32_t* flag, BodyFn body, BodyFn eager, const void* ctx,
-                            const char* what) {
+// While `st` is being captured: an IF node on handle h follows the launches
+// captured so far (the kernel that sets h among them), with its body captured
+// from body(ctx, body_stream).
+static int add_if_node(cudaStream_t st, cudaGraphConditionalHandle h, BodyFn body, const void* ctx,
+                       const char* what) {
     char msg[160];
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaGraph_t graph = nullptr;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
     cudaError_t err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
-    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: capture info", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
-    if (cs != cudaStreamCaptureStatusActive || !g_body_stream) return eager(ctx, st);
-    cudaGraphConditionalHandle h;
-    err = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
-    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: handle", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
-    err = launch_pdl(k_set_rebuild_condition, dim3(1), dim3(1), 0, st, h, flag);
-    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: condition kernel", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
-    err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
     if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: capture info 2", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
@@ -609,8 +601,72 @@ int simb200::launch_if_flag(cudaStream_t st, const int32_t* flag, BodyFn body, B
     return rc;
 }
 
-static int rebuild_body(const void* ctx, cudaStream_t s) { return sim_rebuild((const SimEngine*)ctx, 0, s); }
-static int rebuild_eager(const void* ctx, cudaStream_t s) { return sim_rebuild((const SimEngine*)ctx, 1, s); }
+// The graph `st` is being captured into, or null when it is not captured (or
+// no body stream exists yet); *failed reports an error of the query.
+static cudaGraph_t capturing_graph(cudaStream_t st, const char* what, bool* failed) {
+    char msg[160];
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    *failed = false;
+    cudaError_t err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
+    if (err != cudaSuccess) {
+        snprintf(msg, sizeof(msg), "%s: capture info", what);
+        set_cuda_error(err, msg);
+        *failed = true;
+        return nullptr;
+    }
+    return cs == cudaStreamCaptureStatusActive && g_body_stream ? graph : nullptr;
+}
+
+static int new_handle(cudaGraph_t graph, cudaGraphConditionalHandle* h, const char* what) {
+    char msg[160];
+    const cudaError_t err = cudaGraphConditionalHandleCreate(h, graph, 0, cudaGraphCondAssignDefault);
+    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: handle", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
+    return SIM_OK;
+}
+
+// While `st` is being captured: a one-thread kernel turns *flag into the value
+// of an IF node whose body is captured from body(ctx, body_stream); otherwise
+// run eager(ctx, st), which tests the flag on the device itself.
+int simb200::launch_if_flag(cudaStream_t st, const int32_t* flag, BodyFn body, BodyFn eager, const void* ctx,
+                            const char* what) {
+    char msg[160];
+    bool failed;
+    cudaGraph_t graph = capturing_graph(st, what, &failed);
+    if (failed) return SIM_ERR_CUDA;
+    if (!graph) return eager(ctx, st);
+    cudaGraphConditionalHandle h;
+    if (new_handle(graph, &h, what) != SIM_OK) return SIM_ERR_CUDA;
+    const cudaError_t err = launch_pdl(k_set_rebuild_condition, dim3(1), dim3(1), 0, st, h, flag);
+    if (err != cudaSuccess) { snprintf(msg, sizeof(msg), "%s: condition kernel", what); set_cuda_error(err, msg); return SIM_ERR_CUDA; }
+    return add_if_node(st, h, body, ctx, what);
+}
+
+// As launch_if_flag, with the IF node's value set by a kernel of the caller's:
+// while `st` is being captured, cond(ctx, st, &h) launches a kernel that calls
+// cudaGraphSetConditional(h, ...) and the IF node follows it; otherwise
+// cond(ctx, st, nullptr) launches the same work without a handle and
+// eager(ctx, st) follows.
+int simb200::launch_if_cond(cudaStream_t st, CondFn cond, BodyFn body, BodyFn eager, const void* ctx,
+                            const char* what) {
+    bool failed;
+    cudaGraph_t graph = capturing_graph(st, what, &failed);
+    if (failed) return SIM_ERR_CUDA;
+    if (!graph) {
+        const int rc = cond(ctx, st, nullptr);
+        return rc != SIM_OK ? rc : eager(ctx, st);
+    }
+    cudaGraphConditionalHandle h;
+    if (new_handle(graph, &h, what) != SIM_OK) return SIM_ERR_CUDA;
+    const int rc = cond(ctx, st, &h);
+    if (rc != SIM_OK) return rc;
+    return add_if_node(st, h, body, ctx, what);
+}
+
+int simb200::rebuild_body(const void* ctx, cudaStream_t s) { return sim_rebuild((const SimEngine*)ctx, 0, s); }
+int simb200::rebuild_eager(const void* ctx, cudaStream_t s) { return sim_rebuild((const SimEngine*)ctx, 1, s); }
 
 extern "C" int sim_rebuild_if_needed(const SimEngine* ep, void* stream) {
     if (!ep || !ep->box || ep->n <= 0) return SIM_ERR_ARG;

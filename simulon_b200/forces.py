@@ -96,6 +96,11 @@ class EAMForceCUDAExt(BackboneInterface):
         in one pass over the atoms."""
         self.molecular.engine.eam_forces_integrate_drift(self.tables, integrator.params)
 
+    def step_and_drift(self, integrator):
+        """compute_finish_and_drift, the step's log row and the conditional
+        list rebuild, with the last two decided inside the force pass."""
+        self.molecular.engine.eam_step_drift(self.tables, integrator.params)
+
     def forward(self):
         self.compute()
         red = self.molecular.engine.red_out

@@ -103,9 +103,12 @@ class BaseModel(nn.Module):
         self.Integrator.first_half()
         for s in range(k):
             if s < k - 1:
-                bone.compute_finish_and_drift(self.Integrator)
-                self.engine.log_step(after_drift=True)
-                self.engine.rebuild_if_needed()
+                if hasattr(bone, "step_and_drift"):
+                    bone.step_and_drift(self.Integrator)   # log row and rebuild decision inside pass 2
+                else:
+                    bone.compute_finish_and_drift(self.Integrator)
+                    self.engine.log_step(after_drift=True)
+                    self.engine.rebuild_if_needed()
             else:
                 bone.compute_and_finish(self.Integrator)
                 self.engine.log_step()

@@ -307,9 +307,11 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
     from simulon_b200.engine import integrator_params
     # (graph?, conditional IF-node rebuild?, second half fused into EAM pass 2?);
     # fused == "drift": the next step's first half is fused in as well;
-    # fused == "sf": standalone forces, then sim_integrate_second_first
+    # fused == "sf": standalone forces, then sim_integrate_second_first;
+    # fused == "step": sim_eam_step_drift (log row and rebuild decision in pass 2)
     modes = [(False, False, False), (True, False, False), (True, True, False), (True, True, True), (False, True, True),
-             (False, True, "drift"), (True, True, "drift"), (False, True, "sf"), (True, True, "sf")]
+             (False, True, "drift"), (True, True, "drift"), (False, True, "sf"), (True, True, "sf"),
+             (False, True, "step"), (True, True, "step")]
     for use_graph, cond, fused in modes:
         eng, tables, parser = _eam_engine(sb, fsw_path, x, np.diag([L] * 3), v)
         # an NVT integrator exercises the noise and triggers rebuilds
@@ -320,7 +322,9 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
             eng.integrate_first(integ, 0)
             eng.rebuild_if_needed()
             for s in range(k):
-                if s < k - 1:
+                if s < k - 1 and fused == "step":
+                    eng.eam_step_drift(tables, integ)
+                elif s < k - 1:
                     if fused == "sf":
                         eng.eam_forces(tables)
                         eng.integrate_second_first(integ, 0)
@@ -353,7 +357,7 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
             s.wait_stream(torch.cuda.current_stream())
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=s):
-                if fused in ("drift", "sf"):
+                if fused in ("drift", "sf", "step"):
                     drift_steps(20)
                 else:
                     for _ in range(20):
@@ -362,7 +366,7 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
             torch.cuda.current_stream().wait_stream(s)
             for _ in range(steps // 20):
                 g.replay()
-        elif fused in ("drift", "sf"):
+        elif fused in ("drift", "sf", "step"):
             for _ in range(steps // 20):
                 drift_steps(20)
         else:
@@ -372,7 +376,7 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
         torch.cuda.synchronize()
         res.append((eng.gather("x").cpu(), eng.gather("v").cpu(), int(eng.flags[3].item()),
                     eng.red_out.cpu().numpy(), eng.log[:steps, :_lib_red_slots()].cpu().numpy(),
-                    eng.step_ctr.cpu().numpy()))
+                    eng.step_ctr.cpu().numpy(), eng.log[:steps].cpu().numpy()))
     for r in res[1:]:
         assert torch.equal(res[0][0], r[0]) and torch.equal(res[0][1], r[1])
         assert r[2] == res[0][2]
@@ -381,6 +385,11 @@ def test_graph_run_matches_eager_steps(sb, fsw_path):
         np.testing.assert_allclose(r[4][:, :9], res[0][4][:, :9], rtol=1e-6, atol=1e-9)
         np.testing.assert_allclose(r[3][9], res[0][3][9], rtol=1e-6)   # kinetic energy (FP32 per-thread partials)
     assert res[0][2] >= 2      # the load rebuild plus at least one triggered
+    # the step entry point runs the drift path's kernels: whole log rows
+    # (reductions, extra columns, status) equal bit for bit, eager and graphed
+    drift = res[modes.index((True, True, "drift"))][6]
+    for m in ((False, True, "step"), (True, True, "step")):
+        np.testing.assert_array_equal(res[modes.index(m)][6], drift)
 
 
 def test_langevin_noise_matches_oracle_philox(sb, fsw_path):
