@@ -187,27 +187,18 @@ __global__ void k_bb_scatter(SimBatch B, int only_flagged) {
     }
 }
 
-// In-cell order by original index (reruns are bitwise reproducible); counts
-// are cleared for the next rebuild.
+// In-cell order by original index (reruns are bitwise reproducible), one
+// warp per cell; counts are cleared for the next rebuild.
 __global__ void k_bb_sort_cells(SimBatch B, int only_flagged) {
     const SimEngine& e = B.e;
     const WorkList W = work_list(B);
     const int total = W.nf ? W.cells[W.nf] : 0;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int warps = (int)(gridDim.x * blockDim.x) >> 5;
+    for (int t = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); t < total; t += warps) {
         const int f = work_find(W.cells, W.nf, t);
         const int c = B.rep[W.ids[f]].cell_off + (t - W.cells[f]);
-        e.cell_count[c] = 0;
-        const int b0 = e.cell_start[c], b1 = e.cell_start[c + 1];
-        for (int a = b0 + 1; a < b1; ++a) {
-            const int key = e.perm[a];
-            const int ko = e.orig[key];
-            int p = a - 1;
-            while (p >= b0 && e.orig[e.perm[p]] > ko) {
-                e.perm[p + 1] = e.perm[p];
-                --p;
-            }
-            e.perm[p + 1] = key;
-        }
+        if ((threadIdx.x & 31) == 0) e.cell_count[c] = 0;
+        warp_sort_cell(e.perm, e.orig, e.cell_start[c], e.cell_start[c + 1]);
     }
 }
 
@@ -285,6 +276,24 @@ __global__ void __launch_bounds__(BATCH_ELL_WARPS * 32) k_bb_build_ell(SimBatch 
     const int warp = threadIdx.x >> 5;
     const WorkList W = work_list(B);
     const int total = W.nf ? W.cells[W.nf] : 0;
+    const int64_t n_warps = (int64_t)gridDim.x * BATCH_ELL_WARPS;
+    const int64_t flagged = W.nf ? (int64_t)W.chunks[W.nf] << 5 : 0;
+    if (flagged <= n_warps) {
+        // few atoms to rebuild (one wave of warps): one warp per row, so a
+        // small replica's rows are not built one after another per cell
+        // (rows equal ell_cell_warp's)
+        int64_t m;
+        int k;
+        for (int64_t t = blockIdx.x * BATCH_ELL_WARPS + warp; work_slot(B, W, t, m, k); t += n_warps) {
+            const SimRep& R = B.rep[k];
+            if (m - R.off >= R.n) continue;   // padding (uniform across the warp)
+            const int32_t* rank = e.cell_rank + 2 * R.cell_off;
+            const CellGrid g{&R.box, R.ncell[0], R.ncell[1], R.ncell[2], rank, e.cell_start + R.cell_off};
+            const int lin = rank[R.n_cells + (e.cell_of[m] - R.cell_off)];
+            ell_row_warp(posq, m, lin, g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags, keys[warp]);
+        }
+        return;
+    }
     for (int t = blockIdx.x * BATCH_ELL_WARPS + warp; t < total; t += gridDim.x * BATCH_ELL_WARPS) {
         const int f = work_find(W.cells, W.nf, t);
         const SimRep& R = B.rep[W.ids[f]];
@@ -322,7 +331,7 @@ static int batch_rebuild(const SimBatch& B, int only_flagged, cudaStream_t st) {
     k_bb_bin<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
     k_bb_scan<<<B.n_rep, 1024, 0, st>>>(B, only_flagged);
     k_bb_scatter<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
-    k_bb_sort_cells<<<grid_slots(B.n_cell_entries), SIM_THREADS, 0, st>>>(B, only_flagged);
+    k_bb_sort_cells<<<grid_slots((int64_t)B.n_cell_entries * 32), SIM_THREADS, 0, st>>>(B, only_flagged);
     k_bb_permute<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
     k_bb_commit<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
     k_bb_slot_cells<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);

@@ -19,6 +19,42 @@ __device__ __forceinline__ int stencil_cell(int c, int k, int n) {
     return k;   // n <= 2: enumerate every cell once
 }
 
+// Sort the slots perm[b0, b1) of one cell by their original index orig[perm[.]]
+// (unique keys), with the 32 lanes of one warp: a cell of up to 32 atoms by
+// rank -- each lane counts the smaller keys through shuffles, so no chain of
+// dependent global loads -- a longer cell by lane 0's insertion sort.  Every
+// lane of the warp must call this with the same b0, b1.
+__device__ __forceinline__ void warp_sort_cell(int32_t* perm, const int32_t* orig, int b0, int b1) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int n = b1 - b0;
+    if (n <= 1) return;
+    if (n <= 32) {
+        const bool on = lane < n;
+        const int32_t v = on ? perm[b0 + lane] : 0;
+        const int32_t key = on ? orig[v] : 0;
+        int rank = 0;
+        for (int s = 0; s < n; ++s) rank += __shfl_sync(FULL, key, s) < key ? 1 : 0;
+        __syncwarp();
+        if (on) perm[b0 + rank] = v;
+        __syncwarp();
+        return;
+    }
+    if (lane == 0) {
+        for (int a = b0 + 1; a < b1; ++a) {
+            const int32_t v = perm[a];
+            const int32_t ko = orig[v];
+            int p = a - 1;
+            while (p >= b0 && orig[perm[p]] > ko) {
+                perm[p + 1] = perm[p];
+                --p;
+            }
+            perm[p + 1] = v;
+        }
+    }
+    __syncwarp();
+}
+
 #define ELL_SORT_MAX 128    // rows up to this length are sorted by distance
 #define ELL_CELL_CAND 384   // candidates of one cell's stencil kept in shared memory
 

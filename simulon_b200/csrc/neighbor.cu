@@ -206,19 +206,9 @@ __global__ void k_scatter(SimEngine e, const int32_t* gate) {
 // In-cell order by original index: reruns are bitwise reproducible.
 __global__ void k_sort_cells(SimEngine e, const int32_t* gate) {
     if (gate && __ldg(gate) == 0) return;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < e.n_cells; c += gridDim.x * blockDim.x) {
-        int b0 = e.cell_start[c], b1 = e.cell_start[c + 1];
-        for (int a = b0 + 1; a < b1; ++a) {
-            int key = e.perm[a];
-            int ko = e.orig[key];
-            int p = a - 1;
-            while (p >= b0 && e.orig[e.perm[p]] > ko) {
-                e.perm[p + 1] = e.perm[p];
-                --p;
-            }
-            e.perm[p + 1] = key;
-        }
-    }
+    const int warps = (int)(gridDim.x * blockDim.x) >> 5;
+    for (int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); c < e.n_cells; c += warps)
+        warp_sort_cell(e.perm, e.orig, e.cell_start[c], e.cell_start[c + 1]);
 }
 
 __global__ void k_permute(SimEngine e, const int32_t* gate) {
@@ -538,7 +528,7 @@ extern "C" int sim_rebuild(const SimEngine* ep, int32_t only_if_flagged, void* s
     k_scan_apply<<<n_tiles, SCAN_TILE / 4, 0, st>>>(e.cell_count, e.n_cells, e.cell_start, e.cell_count, tile_off,
                                                     gate);
     k_scatter<<<g, SIM_THREADS, 0, st>>>(e, gate);
-    k_sort_cells<<<grid_for(e.n_cells), SIM_THREADS, 0, st>>>(e, gate);
+    k_sort_cells<<<grid_for((int64_t)e.n_cells * 32), SIM_THREADS, 0, st>>>(e, gate);
     k_permute<<<g, SIM_THREADS, 0, st>>>(e, gate);
     k_commit<<<g, SIM_THREADS, 0, st>>>(e, gate);
     // the scatter left cell_count == counts; zero them for the next rebuild
