@@ -131,6 +131,42 @@ def test_batch_rebuilds_only_moving_replicas(sb, fsw):
     assert T[0] < 1e-6 and T[1] > 300.0
 
 
+def test_batch_small_rebuild_rows_equal_full_rebuild(sb, fsw):
+    """A rebuild of few atoms (they fit in one wave of the list kernel's warps)
+    builds one row per warp; a rebuild of every replica builds the rows of a
+    cell with one warp.  From the same positions both give the same slots and
+    the same rows, bit for bit."""
+    from simulon_b200.batch import BatchedEngine, Replica
+    parser, tables = fsw
+    reps = []
+    for k, n in enumerate((7, 7, 7, 7, 5)):
+        x, L = oin.bcc_lattice(n)
+        x = oin.jitter(x, 0.06, 120 + k)
+        v = oin.maxwell_boltzmann(np.full(len(x), oin.W_MASS), 600.0, 130 + k)
+        reps.append(Replica(positions=x, H=np.diag([L] * 3), velocities=v, temperature=600.0))
+    be = BatchedEngine(reps, oin.W_MASS, parser.cutoff, 0.5, device=DEV)
+    be.run(tables, be.integrator(0.002, langevin=False), 20, graph_steps=20)   # off the loaded lattice
+    torch.cuda.synchronize()
+    small = len(reps) - 1
+    o, ns = int(be.plan.off[small]), int(be.plan.n_slots[small])
+    n_warps = 4 * min(-(-int(be.plan.n_cell_entries) // 4), 148 * 64)
+    assert ns <= n_warps < sum(int(s) for s in be.plan.n_slots)   # one warp per row; a full rebuild per cell
+    before = be.rebuild_counts().copy()
+    be.rep_flags.zero_()
+    be.rep_flags[small] = 1
+    be.rebuild(only_flagged=True)
+    torch.cuda.synchronize()
+    assert (be.rebuild_counts() - before).tolist() == [0] * small + [1]
+    orig1, n1, rows1 = be.orig[o:o + ns].clone(), be.nnbr[o:o + ns].clone(), be.nbr[:, o:o + ns].clone()
+    be.rebuild(only_flagged=False)
+    torch.cuda.synchronize()
+    assert be.status() == 0
+    assert torch.equal(be.orig[o:o + ns], orig1)
+    assert torch.equal(be.nnbr[o:o + ns], n1) and int(n1.max()) > 0
+    filled = torch.arange(rows1.shape[0], device=DEV)[:, None] < n1[None, :].long()
+    assert torch.equal(be.nbr[:, o:o + ns][filled], rows1[filled])
+
+
 def test_batch_grips_follow_the_opening(sb, fsw):
     from simulon_b200.batch import BatchedEngine, crack_slab
     parser, tables = fsw
