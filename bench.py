@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--no-mlp", action="store_true", help="skip the MLP-surrogate form")
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the built-in launch shapes (profiling runs: fewer launches before the timed ones)")
-    p.add_argument("--forms", default="plain,lj,mlp,batched",
+    p.add_argument("--forms", default="plain,lj,mlp,batched,variants",
                    help="forms to run (profiling runs: e.g. --forms mlp prints only the mlp object)")
     p.add_argument("--lj-n", type=int, default=63, help="FCC cells per side of the LJ form (atoms = 4 n^3)")
     p.add_argument("--batch-replicas", type=int, default=48)
@@ -254,6 +254,8 @@ def run_b200(args):
             line["mlp"] = mlp_form(args, sb, pot, dev, world)
         if "batched" in forms and not args.no_batched:
             line["batched"] = batched_form(args, sb, pot, dev, world, rank, barrier)
+        if "variants" in forms:
+            line["eam_variants"] = eam_variants_form(args, sb, pot, dev, world)
         if world > 1:
             dist.destroy_process_group()
         if rank == 0:
@@ -370,6 +372,8 @@ def run_b200(args):
         line["mlp"] = mlp_form(args, sb, pot, dev, world)
     if not args.no_batched and "batched" in forms:
         line["batched"] = batched_form(args, sb, pot, dev, world, rank, barrier)
+    if "variants" in forms:
+        line["eam_variants"] = eam_variants_form(args, sb, pot, dev, world)
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
@@ -442,6 +446,71 @@ def batched_form(args, sb, pot, dev, world, rank, barrier):
                                    "precrack L_x/4, 3-layer grips opening 1e-4 A/step, T 50-1200 K Langevin "
                                    f"gamma 10/ps, dt 1 fs, skin {args.batch_skin} A",
                        "parallelism": f"LPT over {world} rank(s)", "graph_steps": G}}
+
+
+def eam_variants_form(args, sb, pot, dev, world):
+    """The other EAM-W bulk cases of the plain form, 2 n^3 = 1,024,000 atoms:
+    NVE in a triclinic box (rows (L,0,0), (0.02 L, L, 0), (0,0,L), the BCC
+    sites sheared with it) and Berendsen NPT at P0 = 0 bar with a 300 K
+    Langevin thermostat (gamma 10/ps, tau_p 1 ps, orthogonal box); both from
+    300 K Maxwell-Boltzmann velocities, dt 2 fs, each timed like the plain
+    line (CUDA events around BaseModel.run, graphs of 20 steps)."""
+    import torch
+    import torch.distributed as dist
+    x, L = bcc(args.n)
+    N = len(x)
+    v = mb_velocities(N, 300.0, 3000 + int(os.environ.get("RANK", "0")))
+    parser = sb.EAMParser(pot)
+    out = {}
+    for name in ("triclinic_nve", "berendsen_npt"):
+        if name == "triclinic_nve":
+            H = np.array([[L, 0.0, 0.0], [0.02 * L, L, 0.0], [0.0, 0.0, L]])
+            xs = (x / L) @ H
+            mol = sb.AtomFileReader.from_arrays(["W"] * N, xs, L, parser.cutoff, device=dev, skin_thickness=0.5,
+                                                is_fs=True, box_vectors=H)
+        else:
+            mol = sb.AtomFileReader.from_arrays(["W"] * N, x, L, parser.cutoff, device=dev, skin_thickness=0.5,
+                                                is_fs=True)
+        mol.atom_velocities = torch.tensor(v, device=dev)
+        ff = sb.EAMForceCUDAExt(parser, mol)
+        if name == "triclinic_nve":
+            integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NVE")
+            baro = None
+        else:
+            integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NPT", temperature=(300.0, 300.0), gamma=10.0, seed=5)
+            baro = sb.BerendsenBarostat(mol, 0.0, 1.0)
+        model = sb.BaseModel(sb.SumBackboneInterface([ff], mol), integ, mol, barostat=baro)
+        eng = mol.engine
+        model.run(max(args.warmup, args.graph_steps), graph_steps=args.graph_steps)
+        torch.cuda.synchronize()
+        rb0 = int(eng.flags[3].item())
+        V0 = abs(float(np.linalg.det(eng.box_matrix())))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record()
+        outs = model.run(args.steps, graph_steps=args.graph_steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        row = {"value": world * N * args.steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.steps,
+               "status": eng.status(), "rebuilds_in_timed": int(eng.flags[3].item()) - rb0,
+               "temperature_k": float(outs["temperature"])}
+        if baro is not None:
+            row["pressure_bar"] = float(baro.pressure())
+            row["volume_change"] = abs(float(np.linalg.det(eng.box_matrix()))) / V0 - 1.0
+        out[name] = row
+        del model, ff, integ, mol, eng
+        torch.cuda.empty_cache()
+    out["config"] = {"workload": f"EAM-W bulk BCC 2*{args.n}^3 = {N:,} atoms per GPU, synthetic FS W, dt 2 fs, "
+                                 "skin 0.5 A: triclinic NVE (xy tilt 0.02) and Berendsen NPT (P0 0 bar, tau_p 1 ps, "
+                                 "Langevin 300 K)", "scaling": "weak", "parallelism": f"replicas x{world}"}
+    return out
 
 
 def lj_form(args, sb, dev, world):
