@@ -471,7 +471,6 @@ def eam_variants_form(args, sb, pot, dev, world):
         else:
             mol = sb.AtomFileReader.from_arrays(["W"] * N, x, L, parser.cutoff, device=dev, skin_thickness=0.5,
                                                 is_fs=True)
-        mol.atom_velocities = torch.tensor(v, device=dev)
         ff = sb.EAMForceCUDAExt(parser, mol)
         if name == "triclinic_nve":
             integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NVE")
@@ -479,6 +478,7 @@ def eam_variants_form(args, sb, pot, dev, world):
         else:
             integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NPT", temperature=(300.0, 300.0), gamma=10.0, seed=5)
             baro = sb.BerendsenBarostat(mol, 0.0, 1.0)
+        mol.atom_velocities = torch.tensor(v, device=dev)   # the seeded draw, after the integrator's own
         model = sb.BaseModel(sb.SumBackboneInterface([ff], mol), integ, mol, barostat=baro)
         eng = mol.engine
         model.run(max(args.warmup, args.graph_steps), graph_steps=args.graph_steps)

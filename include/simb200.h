@@ -384,6 +384,18 @@ int sim_integrate_second_first(const SimEngine* e, const SimIntegrator* p, int32
  * P (bar) and mu on the device in FP64, scales box, coordinates (mu^power),
  * velocities; writes pressure_out[0] = P (bar), pressure_out[1] = mu. */
 int sim_berendsen(const SimEngine* e, const SimBerendsen* p, double* pressure_out, void* stream);
+/* sim_berendsen in two parts, so that a run of NPT steps passes over the atoms
+ * once less per step.  sim_berendsen_mu: the controller alone (P, mu, the box
+ * scaled by mu; pressure_out as sim_berendsen) -- BerendsenBarostat.step's
+ * pressure, mu and box scale (barostat.py:44-61).  sim_berendsen_scale_first: the atoms'
+ * part of that update (coordinates x mu^power, velocities x mu, the skin
+ * reference reset; barostat.py:63-68; mu = mu_in[1] from sim_berendsen_mu)
+ * fused with the NEXT step's first half (as sim_integrate_first,
+ * integrator.py:91-99), bit for bit sim_berendsen followed by
+ * sim_integrate_first. */
+int sim_berendsen_mu(const SimEngine* e, const SimBerendsen* p, double* pressure_out, void* stream);
+int sim_berendsen_scale_first(const SimEngine* e, const SimBerendsen* p, const double* mu_in,
+                              const SimIntegrator* integ, int32_t force_precision, void* stream);
 
 /* AnisotropicNPTBarostat.step (barostat.py:137-208) on the device in FP64:
  * axis pressures from the kinetic and virial tensors in red_out projected on

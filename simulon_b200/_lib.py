@@ -163,6 +163,8 @@ SIGNATURES = {
     "sim_integrate_second": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_integrate_second_first": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_berendsen": [_P(SimEngine), _P(SimBerendsen), c_p, c_p],
+    "sim_berendsen_mu": [_P(SimEngine), _P(SimBerendsen), c_p, c_p],
+    "sim_berendsen_scale_first": [_P(SimEngine), _P(SimBerendsen), c_p, _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_aniso_npt": [_P(SimEngine), _P(SimAniso), c_p, c_p],
     "sim_box_scale": [_P(SimEngine), _P(SimBoxScale), c_p, c_p],
     "sim_indenter_add": [_P(SimEngine), _P(SimIndenter), ctypes.c_int32, c_p],

@@ -49,6 +49,20 @@ class BerendsenBarostat:
         eng.berendsen(self.params(dt))
         return eng.extra[0]
 
+    def controller(self, dt: float):
+        """step() without the atoms' scaling, which the next step's first half
+        applies (deferred_first_half); for runs of several steps."""
+        self.molecular.engine.berendsen_mu(self.params(dt))
+        return self.molecular.engine.extra[0]
+
+    def deferred_first_half(self, integrator):
+        """The atoms' scaling of the last controller() call, then
+        integrator.first_half() (kick, drift, skin/2 trigger, conditional
+        rebuild), with the scaling and the half-step in one pass."""
+        eng = self.molecular.engine
+        eng.berendsen_scale_first(self.params(integrator.dt), integrator.params, integrator.force_precision)
+        eng.rebuild_if_needed()
+
     def pressure(self) -> torch.Tensor:
         """Pressure (bar) of the last step (device scalar)."""
         return self.molecular.engine.extra[0]

@@ -324,11 +324,13 @@ __device__ __forceinline__ void second_half_atom(const SimEngine& e, const SimIn
 // First half of velocity Verlet for atom i (integrator.py:91-99): v += F/m dt/2,
 // x += v dt, refresh the fixed-point code in posq, and report whether the atom
 // moved more than skin/2 from its position at the last rebuild
-// (reader.py:136-163).  v_in: the velocity to kick (read from e.v when NULL).
+// (reader.py:136-163).  v_in / x_in: the velocity to kick and the position to
+// drift (read from e.v / e.x when NULL).
 __device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, int64_t i, int type, const double* xn);
 
 __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimBox& b, const SimIntegrator& p, int64_t i,
-                                                int type, const double* f, const double* v_in, bool& bad) {
+                                                int type, const double* f, const double* v_in, bool& bad,
+                                                const double* x_in = nullptr) {
     const int64_t P = e.n_pad;
     const double m = e.mass[type];
     double xn[3];
@@ -337,7 +339,7 @@ __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimBox
         const double a = __ddiv_rn(f[c], m);
         const double v0 = v_in ? v_in[c] : ld_state(&e.v[c * P + i]);
         const double vh = __dadd_rn(v0, __dmul_rn(__dmul_rn(0.5, a), p.dt));
-        xn[c] = __dadd_rn(ld_state(&e.x[c * P + i]), __dmul_rn(vh, p.dt));
+        xn[c] = __dadd_rn(x_in ? x_in[c] : ld_state(&e.x[c * P + i]), __dmul_rn(vh, p.dt));
         st_state(&e.v[c * P + i], vh);
         bad |= !isfinite(xn[c]) || !isfinite(vh);
     }

@@ -391,6 +391,45 @@ __global__ void __launch_bounds__(SIM_THREADS) k_berendsen_scale(SimEngine e, Si
     }
 }
 
+// The atoms' part of the previous step's Berendsen update (as k_berendsen_scale,
+// with the mu that k_berendsen_mu left in mu_p[1] after scaling the box)
+// followed by this step's first half (as k_first_half), in one pass: the same
+// operations in the same order as the two launches, so the same bits.  The
+// fixed-point code of the scaled position is needed only as the new skin
+// reference; posq gets the drifted position's.
+__global__ void __launch_bounds__(SIM_THREADS) k_berendsen_scale_first(SimEngine e, SimBerendsen bp,
+                                                                       const double* mu_p, SimIntegrator p, int prec) {
+    pdl_trigger();
+    pdl_wait();
+    const int64_t P = e.n_pad;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool trigger = false, bad = false;
+    if (i == 0 && p.step_ctr) *p.step_ctr += 1;
+    if (i < e.n) {
+        const SimBox& b = *e.box;
+        const double mu = mu_p[1];
+        double xs[3], vs[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double xc = ld_state(&e.x[c * P + i]);
+            for (int k = 0; k < bp.coordinate_scale_power; ++k) xc = __dmul_rn(xc, mu);
+            xs[c] = xc;
+            vs[c] = __dmul_rn(ld_state(&e.v[c * P + i]), mu);
+        }
+        if (bp.reset_reference) {
+            double s[3];
+            cart_to_frac(b, xs[0], xs[1], xs[2], s);
+            e.xref[i] = (int32_t)to_fixed(s[0]);
+            e.xref[P + i] = (int32_t)to_fixed(s[1]);
+            e.xref[2 * P + i] = (int32_t)to_fixed(s[2]);
+        }
+        const double f[3] = {load_force(e, prec, i, 0), load_force(e, prec, i, 1), load_force(e, prec, i, 2)};
+        trigger = first_half_atom(e, b, p, i, e.posq[4 * i + 3], f, vs, bad, xs);
+    }
+    if (__any_sync(0xffffffffu, trigger) && (threadIdx.x & 31) == 0) e.flags[0] = 1;
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+}
+
 // ---- load / gather ------------------------------------------------------------
 __global__ void k_load(SimEngine e, const double* __restrict__ xr, const double* __restrict__ vr,
                        const int32_t* __restrict__ types) {
@@ -500,6 +539,22 @@ extern "C" int sim_berendsen(const SimEngine* ep, const SimBerendsen* p, double*
     k_berendsen_mu<<<1, 1, 0, st>>>(*ep, *p, pressure_out);
     k_berendsen_scale<<<(int)ceil_div(ep->n, SIM_THREADS), SIM_THREADS, 0, st>>>(*ep, *p, pressure_out);
     return launch_status("sim_berendsen");
+}
+
+extern "C" int sim_berendsen_mu(const SimEngine* ep, const SimBerendsen* p, double* pressure_out, void* stream) {
+    if (!ep || !p || !pressure_out || p->tau <= 0.0) return SIM_ERR_ARG;
+    k_berendsen_mu<<<1, 1, 0, (cudaStream_t)stream>>>(*ep, *p, pressure_out);
+    return launch_status("sim_berendsen_mu");
+}
+
+extern "C" int sim_berendsen_scale_first(const SimEngine* ep, const SimBerendsen* bp, const double* mu_in,
+                                         const SimIntegrator* p, int32_t force_precision, void* stream) {
+    if (!ep || !bp || !mu_in || !p || ep->n <= 0 || (force_precision == 1 && !ep->f64)) return SIM_ERR_ARG;
+    const cudaError_t err = launch_pdl(k_berendsen_scale_first, dim3((unsigned)ceil_div(ep->n, SIM_THREADS)),
+                                       dim3(SIM_THREADS), 0, (cudaStream_t)stream, *ep, *bp, mu_in, *p,
+                                       force_precision);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_berendsen_scale_first: launch"); return SIM_ERR_CUDA; }
+    return launch_status("sim_berendsen_scale_first");
 }
 
 extern "C" int sim_engine_load(const SimEngine* ep, const double* x_rows, const double* v_rows, const int32_t* types,

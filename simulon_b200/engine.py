@@ -386,6 +386,16 @@ class MDEngine:
     def berendsen(self, params):
         _lib.call("sim_berendsen", self.st_ref, params.ref, _lib.ptr(self.extra), self.stream)
 
+    def berendsen_mu(self, params):
+        """The Berendsen controller alone (pressure, mu, box scaled); the atoms
+        follow in berendsen_scale_first at the next step."""
+        _lib.call("sim_berendsen_mu", self.st_ref, params.ref, _lib.ptr(self.extra), self.stream)
+
+    def berendsen_scale_first(self, params, integ, precision: int):
+        """The atoms' part of the last berendsen_mu and this step's first half in one pass."""
+        _lib.call("sim_berendsen_scale_first", self.st_ref, params.ref, _lib.ptr(self.extra), integ.ref,
+                  int(precision), self.stream)
+
     def log_step(self, after_drift: bool = False):
         """Record this step's reductions in the device log (after_drift: the step
         was finished by eam_forces_integrate_drift, whose index is step_ctr[1])."""

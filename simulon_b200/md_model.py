@@ -74,14 +74,17 @@ class BaseModel(nn.Module):
         self._graphs = {}
 
     # one step, launches only (no host sync)
-    def _step_launches(self):
-        self.Integrator.first_half()
+    def _forces_and_second_half(self):
         fused = getattr(self.sum_bone.backbones[0], "compute_and_finish", None) if self.sum_bone.single else None
         if fused is not None and hasattr(self.Integrator, "params"):
             fused(self.Integrator)        # EAM: second half fused into pass 2
         else:
             self.sum_bone.compute()
             self.Integrator.second_half()
+
+    def _step_launches(self):
+        self.Integrator.first_half()
+        self._forces_and_second_half()
         if self.barostat is not None:
             self.barostat.step(self.Integrator.dt)
         self.engine.log_step()
@@ -94,7 +97,23 @@ class BaseModel(nn.Module):
     def _launch_steps(self, k: int):
         """k steps, launches only.  For EAM without a barostat the first half of
         step s+1 runs inside step s's force pass (same arithmetic, one pass over
-        the atoms fewer per step); the last step ends with full-step velocities."""
+        the atoms fewer per step); the last step ends with full-step velocities.
+        With a Berendsen barostat the atoms' scaling of step s runs inside step
+        s+1's first half; the last step scales them itself."""
+        if k > 1 and not self._drift_fusable() and callable(getattr(self.barostat, "deferred_first_half", None)) \
+                and hasattr(self.Integrator, "params"):
+            for s in range(k):
+                if s == 0:
+                    self.Integrator.first_half()
+                else:
+                    self.barostat.deferred_first_half(self.Integrator)
+                self._forces_and_second_half()
+                if s < k - 1:
+                    self.barostat.controller(self.Integrator.dt)
+                else:
+                    self.barostat.step(self.Integrator.dt)
+                self.engine.log_step()
+            return
         if k <= 1 or not self._drift_fusable():
             for _ in range(k):
                 self._step_launches()

@@ -294,6 +294,45 @@ def test_md_eam_matches_reference_trajectory(sb, fsw_path, tmp_path, ens):
     np.testing.assert_allclose(mol.coordinates.cpu().numpy(), g["x"], atol=5e-4)
 
 
+def test_npt_runs_equal_per_step_calls(sb, fsw_path):
+    """Berendsen NPT: BaseModel.run folds each step's atom scaling into the next
+    step's first half (sim_berendsen_scale_first); per-step calls scale
+    separately (sim_berendsen).  Same positions, velocities, box and log rows,
+    bit for bit, graphed and eager."""
+    x, L = oin.bcc_lattice(8)
+    x = oin.jitter(x, 0.05, 61)
+    v = oin.maxwell_boltzmann(np.full(len(x), oin.W_MASS), 600.0, 62)
+    parser = sb.EAMParser(fsw_path)
+    res = []
+    for mode in ("calls", "graph", "eager"):
+        mol = sb.AtomFileReader.from_arrays(["W"] * len(x), x, L, parser.cutoff, device=DEV, skin_thickness=0.5,
+                                            is_fs=True)
+        integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NPT", temperature=(600.0, 600.0), gamma=10.0, seed=3)
+        mol.atom_velocities = torch.tensor(v, device=DEV)   # after the integrator's own Maxwell-Boltzmann draw
+        baro = sb.BerendsenBarostat(mol, 0.0, 1.0)
+        model = sb.BaseModel(sb.SumBackboneInterface([sb.EAMForceCUDAExt(parser, mol)], mol), integ, mol,
+                             barostat=baro)
+        if mode == "calls":
+            for _ in range(60):
+                model()
+        elif mode == "graph":
+            model.run(60, graph_steps=20)
+        else:
+            for _ in range(4):
+                model.run(15, graph_steps=20)      # below graph_steps: eager launches
+        torch.cuda.synchronize()
+        eng = mol.engine
+        assert eng.status() == 0
+        res.append((eng.gather("x").cpu(), eng.gather("v").cpu(), eng.box_matrix(), eng.log[:60].cpu().numpy(),
+                    int(eng.flags[3])))
+    assert abs(np.linalg.det(res[0][2]) / L ** 3 - 1.0) > 1e-6      # the box did move
+    for r in res[1:]:
+        assert torch.equal(r[0], res[0][0]) and torch.equal(r[1], res[0][1])
+        np.testing.assert_array_equal(r[2], res[0][2])
+        np.testing.assert_array_equal(r[3], res[0][3])
+        assert r[4] == res[0][4]
+
+
 def _lib_red_slots():
     from simulon_b200 import _lib
     return _lib.RED_SLOTS
