@@ -363,6 +363,15 @@ int sim_eam_forces_static(const SimEngine* e, const SimEAMTables* t, void* strea
 /* LJ forces; precision 0 = FP32 pair arithmetic, 1 = FP64 (positions read
  * from e->x, forces to e->f64).  Scalar virial = sum F*r (lennard_jones_force.py:93). */
 int sim_lj_forces(const SimEngine* e, const SimLJParams* p, int32_t precision, void* stream);
+/* FP32-pair LJ forces (as sim_lj_forces, precision 0) with the integrator
+ * fused into the same pass over the atoms, like the EAM force pass: mode 1
+ * adds the second half of the step (as sim_integrate_second,
+ * integrator.py:102-124); mode 2 adds the next step's first half as well
+ * (as sim_integrate_first, integrator.py:91-99: kick with the new forces,
+ * drift, posq refresh, skin/2 trigger), advancing p->step_ctr[0] and setting
+ * step_ctr[1] to this step like sim_eam_force_integrate_drift. */
+int sim_lj_forces_integrate(const SimEngine* e, const SimLJParams* p, const SimIntegrator* integ, int32_t mode,
+                            void* stream);
 
 /* first_half: v += 0.5 a dt; x += v dt; refresh posq; skin/2 trigger -> flags[0].
  * force_precision: 0 reads f32, 1 reads f64. */

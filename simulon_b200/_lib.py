@@ -159,6 +159,7 @@ SIGNATURES = {
     "sim_eam_step_drift": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), c_p, ctypes.c_int32, c_p,
                            ctypes.c_int32, c_p],
     "sim_lj_forces": [_P(SimEngine), _P(SimLJParams), ctypes.c_int32, c_p],
+    "sim_lj_forces_integrate": [_P(SimEngine), _P(SimLJParams), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_integrate_first": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_integrate_second": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_integrate_second_first": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],

@@ -8,67 +8,139 @@
 // quintic-switch ("is_switch") modes, cutoff mask r < rc, scalar virial
 // sum F r and tensor sum f (x) r.
 #include "common.cuh"
+#include "eam_device.cuh"
 
 namespace simb200 {
 
-// LJ (engine).  FP32 variant on fixed-point displacements.
-__global__ void __launch_bounds__(SIM_THREADS) k_lj_f32(SimEngine e, SimLJParams p) {
-    const SimBox& b = *e.box;
+#ifndef LJ_MIN_BLOCKS
+#define LJ_MIN_BLOCKS 4   // 4 x 256 threads per SM (<= 64 registers)
+#endif
+
+// Per-pair constants of one type pair, as FP32 (the FP32 path's own rounding).
+struct LJConst {
+    float sig, c4, c24, urc, frc;
+};
+__device__ __forceinline__ LJConst lj_const(const SimLJParams& p, int tt) {
+    return LJConst{(float)p.sigma[tt], (float)p.c4eps[tt], (float)p.c24eps[tt], p.u_rc ? (float)p.u_rc[tt] : 0.0f,
+                   p.f_rc ? (float)p.f_rc[tt] : 0.0f};
+}
+
+// One pair (r = x_i - x_j) into atom i's force and the thread's sums
+// a[0] energy, a[1] scalar virial, a[2..7] virial tensor (xx yy zz xy xz yz).
+__device__ __forceinline__ void lj_pair(const SimLJParams& p, const LJConst& c, float rc, float rc2, float rs,
+                                        float r0, float r1, float r2, float& fx, float& fy, float& fz,
+                                        float (&a)[15]) {
+    const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
+    if (!(d2 < rc2)) return;
+    const float inv_r2 = 1.0f / d2;
+    const float sr2 = c.sig * c.sig * inv_r2;
+    const float sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6;
+    float U = c.c4 * (sr12 - sr6);
+    float Fr = c.c24 * (2.0f * sr12 - sr6) * inv_r2;   // |F|/r
+    if (p.mode != SIM_LJ_RAW) {
+        const float r = sqrtf(d2);
+        if (p.mode == SIM_LJ_SHIFT) {
+            U = U - c.urc + (r - rc) * c.frc;
+            Fr = Fr - c.frc / r;
+        } else if (r > rs) {
+            const float x = (r - rs) / (rc - rs);
+            const float x2 = x * x, x3 = x2 * x;
+            const float S = 1.0f - 10.0f * x3 + 15.0f * x3 * x - 6.0f * x3 * x2;
+            const float dS = (-30.0f * x2 + 60.0f * x3 - 30.0f * x3 * x) / (rc - rs);
+            Fr = Fr * S - U * dS / r;
+            U = U * S;
+        }
+    }
+    const float ax = Fr * r0, ay = Fr * r1, az = Fr * r2;
+    fx += ax; fy += ay; fz += az;
+    a[0] += U;
+    a[1] = fmaf(Fr, d2, a[1]);
+    a[2] = fmaf(ax, r0, a[2]); a[3] = fmaf(ay, r1, a[3]); a[4] = fmaf(az, r2, a[4]);
+    a[5] = fmaf(ax, r1, a[5]); a[6] = fmaf(ax, r2, a[6]); a[7] = fmaf(ay, r2, a[7]);
+}
+
+// LJ (engine), FP32 pair arithmetic on fixed-point displacements.  Persistent
+// grid; the box terms, and with one element type the pair constants, sit in
+// registers; list entries are gathered four at a time.  INTEG 1 / 2: the
+// integrator epilogue of the EAM force pass on atom i's finished force --
+// second half of the step (Langevin O-step, half kick, K and K tensor), and
+// with 2 also the next step's first half (kick, drift, posq refresh, skin/2
+// trigger; step_ctr[0] advanced, step_ctr[1] = this step).
+template <bool ORTHO, bool SINGLE, int INTEG>
+__global__ void __launch_bounds__(SIM_THREADS, LJ_MIN_BLOCKS) k_lj_f32(SimEngine e, SimLJParams p, SimIntegrator ip) {
+    pdl_trigger();
+    pdl_wait();   // positions, box and list come from earlier kernels
+    const BoxF b(*e.box);
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
+    const int32_t* __restrict__ nbr = e.nbr;
     const int64_t P = e.n_pad;
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const float rc = (float)p.rc, rc2 = rc * rc, rs = (float)p.rs;
-    double vals[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (i < e.n) {
+    const LJConst c1 = SINGLE ? lj_const(p, 0) : LJConst{0.f, 0.f, 0.f, 0.f, 0.f};
+    float acc[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};   // as k_eam_force's
+    bool bad = false, trig = false;
+    const uint64_t step = INTEG && ip.step_ctr ? *ip.step_ctr : 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += stride) {
         const int4 qi = posq[i];
         const int ti = qi.w;
         const int nn = e.nnbr[i];
-        float fx = 0.f, fy = 0.f, fz = 0.f, ep = 0.f, vir = 0.f;
-        float wxx = 0.f, wyy = 0.f, wzz = 0.f, wxy = 0.f, wxz = 0.f, wyz = 0.f;
-        for (int k = 0; k < nn; ++k) {
-            const int j = __ldg(&e.nbr[(int64_t)k * P + i]);
-            const int4 qj = posq[j];
-            float r0, r1, r2;
-            pair_vector(b, qi, qj, r0, r1, r2);
-            const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
-            if (d2 < rc2) {
-                const int tt = ti * p.n_types + qj.w;
-                const float sig = (float)p.sigma[tt];
-                const float inv_r2 = 1.0f / d2;
-                const float sr2 = sig * sig * inv_r2;
-                const float sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6;
-                float U = (float)p.c4eps[tt] * (sr12 - sr6);
-                float Fr = (float)p.c24eps[tt] * (2.0f * sr12 - sr6) * inv_r2;   // |F|/r
-                if (p.mode != SIM_LJ_RAW) {
-                    const float r = sqrtf(d2);
-                    if (p.mode == SIM_LJ_SHIFT) {
-                        U = U - (float)p.u_rc[tt] + (r - rc) * (float)p.f_rc[tt];
-                        Fr = Fr - (float)p.f_rc[tt] / r;
-                    } else if (r > rs) {
-                        const float x = (r - rs) / (rc - rs);
-                        const float x2 = x * x, x3 = x2 * x;
-                        const float S = 1.0f - 10.0f * x3 + 15.0f * x3 * x - 6.0f * x3 * x2;
-                        const float dS = (-30.0f * x2 + 60.0f * x3 - 30.0f * x3 * x) / (rc - rs);
-                        Fr = Fr * S - U * dS / r;
-                        U = U * S;
-                    }
-                }
-                const float ax = Fr * r0, ay = Fr * r1, az = Fr * r2;
-                fx += ax; fy += ay; fz += az;
-                ep += U;
-                vir = fmaf(Fr, d2, vir);
-                wxx = fmaf(ax, r0, wxx); wyy = fmaf(ay, r1, wyy); wzz = fmaf(az, r2, wzz);
-                wxy = fmaf(ax, r1, wxy); wxz = fmaf(ax, r2, wxz); wyz = fmaf(ay, r2, wyz);
+        float fx = 0.f, fy = 0.f, fz = 0.f;
+        int k = 0;
+        for (; k + 4 <= nn; k += 4) {
+            int j[4];
+            int4 q[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) j[u] = ld_stream(&nbr[(int64_t)(k + u) * P + i]);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) q[u] = __ldg(&posq[j[u]]);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                float r0, r1, r2;
+                rvec<ORTHO>(b, qi, q[u], r0, r1, r2);
+                lj_pair(p, SINGLE ? c1 : lj_const(p, ti * p.n_types + q[u].w), rc, rc2, rs, r0, r1, r2, fx, fy, fz,
+                        acc);
             }
         }
+        for (; k < nn; ++k) {
+            const int4 qj = __ldg(&posq[ld_stream(&nbr[(int64_t)k * P + i])]);
+            float r0, r1, r2;
+            rvec<ORTHO>(b, qi, qj, r0, r1, r2);
+            lj_pair(p, SINGLE ? c1 : lj_const(p, ti * p.n_types + qj.w), rc, rc2, rs, r0, r1, r2, fx, fy, fz, acc);
+        }
         reinterpret_cast<float4*>(e.f32)[i] = make_float4(fx, fy, fz, 0.0f);
-        vals[0] = 0.5 * (double)ep; vals[1] = 0.5 * (double)vir;
-        vals[2] = 0.5 * (double)wxx; vals[3] = 0.5 * (double)wyy; vals[4] = 0.5 * (double)wzz;
-        vals[5] = 0.5 * (double)wxy; vals[6] = 0.5 * (double)wxz; vals[7] = 0.5 * (double)wyz;
-        if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+        bad |= !(isfinite(fx) && isfinite(fy) && isfinite(fz));
+        if (INTEG) {
+            double v[3];
+            second_half_atom(e, ip, i, ti, step, (double)fx, (double)fy, (double)fz, v, bad, INTEG == 1);
+            const double m = e.mass[ti];
+            acc[8] += (float)(0.5 * m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+            acc[9] += (float)(m * v[0] * v[0]); acc[10] += (float)(m * v[1] * v[1]); acc[11] += (float)(m * v[2] * v[2]);
+            acc[12] += (float)(m * v[0] * v[1]); acc[13] += (float)(m * v[0] * v[2]); acc[14] += (float)(m * v[1] * v[2]);
+            if (INTEG == 2) {
+                const double f[3] = {(double)fx, (double)fy, (double)fz};
+                trig |= first_half_atom(e, ip, i, ti, f, v, bad);
+            }
+        }
     }
-    block_partials<8>(vals, e.partials, SIM_RED_EPOT_PAIR);
-    last_block_finalize<8>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+    if (INTEG == 2 && __any_sync(0xffffffffu, trig) && (threadIdx.x & 31) == 0) e.flags[0] = 1;
+    if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+    if (INTEG) {
+        double vals[15];
+#pragma unroll
+        for (int s = 0; s < 15; ++s) vals[s] = s < 8 ? 0.5 * (double)acc[s] : (double)acc[s];
+        block_partials<15>(vals, e.partials, SIM_RED_EPOT_PAIR);
+        const bool last = last_block_finalize<15>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+        if (INTEG == 2 && last && threadIdx.x == 0) {
+            ip.step_ctr[1] = step;
+            ip.step_ctr[0] = step + 1;
+        }
+    } else {
+        double vals[8];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) vals[s] = 0.5 * (double)acc[s];
+        block_partials<8>(vals, e.partials, SIM_RED_EPOT_PAIR);
+        last_block_finalize<8>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+    }
 }
 
 // FP64 variant: positions from e.x, minimum image and pair arithmetic in the
@@ -140,19 +212,47 @@ __global__ void k_zero_slot(double* out, int slot) { out[slot] = 0.0; }
 
 using namespace simb200;
 
+template <bool ORTHO, bool SINGLE, int INTEG>
+static int launch_lj_f32(const SimEngine& e, const SimLJParams& p, const SimIntegrator& ip, cudaStream_t st) {
+    const int g = persistent_grid((const void*)k_lj_f32<ORTHO, SINGLE, INTEG>, SIM_THREADS, 0, e.n);
+    if (g > e.n_blocks_max) return SIM_ERR_ARG;
+    const cudaError_t err = launch_pdl(k_lj_f32<ORTHO, SINGLE, INTEG>, dim3(g), dim3(SIM_THREADS), 0, st, e, p, ip);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_lj_forces: launch"); return SIM_ERR_CUDA; }
+    return SIM_OK;
+}
+
+template <int INTEG>
+static int lj_f32(const SimEngine& e, const SimLJParams& p, const SimIntegrator& ip, cudaStream_t st) {
+    const bool single = p.n_types == 1;
+    if (e.box_orthogonal)
+        return single ? launch_lj_f32<true, true, INTEG>(e, p, ip, st) : launch_lj_f32<true, false, INTEG>(e, p, ip, st);
+    return single ? launch_lj_f32<false, true, INTEG>(e, p, ip, st) : launch_lj_f32<false, false, INTEG>(e, p, ip, st);
+}
+
 extern "C" int sim_lj_forces(const SimEngine* ep, const SimLJParams* pp, int32_t precision, void* stream) {
     if (!ep || !pp || ep->n <= 0) return SIM_ERR_ARG;
     const SimEngine& e = *ep;
     cudaStream_t st = (cudaStream_t)stream;
     const int blocks = (int)ceil_div(e.n, SIM_THREADS);
-    if (blocks > e.n_blocks_max) return SIM_ERR_ARG;
     k_zero_slot<<<1, 1, 0, st>>>(e.red_out, SIM_RED_EPOT_EMBED);
     if (precision == 1) {
-        if (!e.f64) return SIM_ERR_ARG;
+        if (!e.f64 || blocks > e.n_blocks_max) return SIM_ERR_ARG;
         k_lj_f64<<<blocks, SIM_THREADS, 0, st>>>(e, *pp);
     } else {
-        k_lj_f32<<<blocks, SIM_THREADS, 0, st>>>(e, *pp);
+        const int rc = lj_f32<0>(e, *pp, SimIntegrator{}, st);
+        if (rc != SIM_OK) return rc;
     }
     return launch_status("sim_lj_forces");
+}
+
+extern "C" int sim_lj_forces_integrate(const SimEngine* ep, const SimLJParams* pp, const SimIntegrator* ip,
+                                       int32_t mode, void* stream) {
+    if (!ep || !pp || !ip || ep->n <= 0 || (mode != 1 && mode != 2) || !ip->step_ctr) return SIM_ERR_ARG;
+    if (ip->langevin && !ip->rff) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    k_zero_slot<<<1, 1, 0, st>>>(ep->red_out, SIM_RED_EPOT_EMBED);
+    const int rc = mode == 1 ? lj_f32<1>(*ep, *pp, *ip, st) : lj_f32<2>(*ep, *pp, *ip, st);
+    if (rc != SIM_OK) return rc;
+    return launch_status(mode == 1 ? "sim_lj_forces_integrate" : "sim_lj_forces_integrate (drift)");
 }
 

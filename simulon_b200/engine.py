@@ -373,6 +373,13 @@ class MDEngine:
         self._last_force_precision = int(precision)
         self.forces_valid = True
 
+    def lj_forces_integrate(self, params, integ, mode: int):
+        """FP32-pair LJ forces with the integrator's second half (mode 1), and
+        also the next step's first half (mode 2), in the same pass."""
+        _lib.call("sim_lj_forces_integrate", self.st_ref, params.ref, integ.ref, int(mode), self.stream)
+        self._last_force_precision = 0
+        self.forces_valid = True
+
     def integrate_first(self, integ, precision: int):
         _lib.call("sim_integrate_first", self.st_ref, integ.ref, int(precision), self.stream)
 

@@ -181,6 +181,26 @@ class LennardJonesForce(BackboneInterface):
     def compute(self):
         self.molecular.engine.lj_forces(self.params, self.force_precision)
 
+    def compute_and_finish(self, integrator):
+        """Forces plus the integrator's second half (one pass over the atoms for
+        FP32 pairs; the FP64 path runs the two separately)."""
+        eng = self.molecular.engine
+        if self.force_precision == 0:
+            eng.lj_forces_integrate(self.params, integrator.params, 1)
+        else:
+            eng.lj_forces(self.params, 1)
+            eng.integrate_second(integrator.params, 1)
+
+    def compute_finish_and_drift(self, integrator):
+        """Forces, the integrator's second half and the next step's first half
+        (one pass for FP32 pairs; FP64: forces, then sim_integrate_second_first)."""
+        eng = self.molecular.engine
+        if self.force_precision == 0:
+            eng.lj_forces_integrate(self.params, integrator.params, 2)
+        else:
+            eng.lj_forces(self.params, 1)
+            eng.integrate_second_first(integrator.params, 1)
+
     def forward(self):
         self.compute()
         return _force_outputs(self.molecular)

@@ -241,6 +241,51 @@ def test_lj_fp32_pairs_match_reference(sb, tmp_path, mode):
     assert np.sqrt(((f - g["forces"]) ** 2).mean()) < 2e-6
 
 
+@pytest.mark.parametrize("mode", ["raw", "switch"])
+def test_lj_fused_integrator_equals_separate_kernels(sb, tmp_path, mode):
+    """FP32 LJ with the integrator in the force pass (second half; second half
+    plus the next first half) against the separate force and integrator
+    kernels: positions and velocities bit for bit after 40 Langevin steps,
+    triggered rebuilds included; energies and virials to FP32 sum order."""
+    from simulon_b200.engine import integrator_params
+    x, L = oin.fcc_lattice(6)
+    x = oin.jitter(x, 0.05, 91)
+    res = []
+    for fused in ("separate", "second", "drift"):
+        mol, ff = _lj_system(sb, tmp_path, x, L, mode, torch.float32)
+        eng = mol.engine
+        eng.set_velocities(torch.tensor(oin.maxwell_boltzmann(np.full(len(x), 39.948), 300.0, 92), device=DEV))
+        ip = integrator_params(eng, 0.004, langevin=True, temperature=300.0, gamma=10.0, seed=9)
+        ff.compute()
+        if fused == "drift":
+            eng.integrate_first(ip, 0)
+            eng.rebuild_if_needed()
+            for s in range(40):
+                if s < 39:
+                    eng.lj_forces_integrate(ff.params, ip, 2)
+                    eng.rebuild_if_needed()
+                else:
+                    eng.lj_forces_integrate(ff.params, ip, 1)
+        else:
+            for _ in range(40):
+                eng.integrate_first(ip, 0)
+                eng.rebuild_if_needed()
+                if fused == "second":
+                    eng.lj_forces_integrate(ff.params, ip, 1)
+                else:
+                    eng.lj_forces(ff.params, 0)
+                    eng.integrate_second(ip, 0)
+        torch.cuda.synchronize()
+        assert eng.status() == 0
+        res.append((eng.gather("x").cpu(), eng.gather("v").cpu(), int(eng.flags[3]), eng.red_out.cpu().numpy(),
+                    int(eng.step_ctr[0])))
+    assert res[0][2] >= 2     # the load rebuild plus at least one triggered
+    for r in res[1:]:
+        assert torch.equal(r[0], res[0][0]) and torch.equal(r[1], res[0][1])
+        assert r[2] == res[0][2] and r[4] == res[0][4]
+        np.testing.assert_allclose(r[3][1:10], res[0][3][1:10], rtol=1e-5, atol=1e-6)
+
+
 # ---------------------------------------------------------------- MD
 @pytest.mark.parametrize("ens", ["nve", "nvt"])
 def test_md_lj_fp64_matches_reference_trajectory(sb, tmp_path, ens):
