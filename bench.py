@@ -212,6 +212,13 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ GPU arm
+def eng_state_bytes(eng) -> int:
+    """Device bytes a step touches: the engine's per-slot arrays and its list."""
+    import torch
+    return sum(t.numel() * t.element_size() for t in (eng.x, eng.v, eng.posq, eng.posfp, eng.xref, eng.f32, eng.nbr,
+                                                       eng.nnbr) if isinstance(t, torch.Tensor))
+
+
 def launches_for(steps: int, graph_steps: int) -> int:
     """Kernels of ours launched by BaseModel.run(steps): per run of k > 1 steps,
     the first half-step and its IF-node condition, then per step EAM pass 1
@@ -347,7 +354,9 @@ def run_b200(args):
             "config": {"workload": f"EAM-W bulk BCC 2*{args.n}^3 = {N:,} atoms per GPU, synthetic FS W (eam/fs "
                                    "tables 5000 pts), NVE from 300 K MB velocities, dt 2 fs, skin 0.5 A",
                        "form": "plain", "atoms_per_gpu": N, "graph_steps": G,
-                       "l2": "state ~0.4 GB > 126 MB L2 (no flush needed)",
+                       "l2": (f"state ~{eng_state_bytes(eng) / 1e9:.2f} GB > 126 MB L2 (no flush needed)"
+                              if eng_state_bytes(eng) > 126e6 else
+                              f"state ~{eng_state_bytes(eng) / 1e6:.0f} MB fits the 126 MB L2 (small case: L2-resident)"),
                        "neighbors_mean": nbar, "neighbor_capacity": nbr["cap"], "rebuilds_in_timed": rebuilds,
                        "launch_shapes": {"density_threads": shapes["density_threads"],
                                          "force_threads": shapes["force_threads"], "autotune_ms": shapes["ms"]},
