@@ -257,6 +257,12 @@ __global__ void __launch_bounds__(128) k_mlp_force(SimEngine e, const float* __r
         float sd[8];   // coefficients of S': (m + 1) s_(m+1)
 #pragma unroll
         for (int m = 0; m < 8; ++m) sd[m] = (float)(m + 1) * s[m + 1];
+        // S and S' by one Horner recurrence on FP32x2 pairs {S, S'}: coefficient
+        // pairs {s_m, sd_(m-1)}; each lane rounds as the scalar fmaf
+        float2 ssd[8];
+#pragma unroll
+        for (int m = 1; m <= 7; ++m) ssd[m] = make_float2(s[m], sd[m - 1]);
+        ssd[0] = make_float2(s[8], sd[7]);
         const int cnt = mlp_table<ORTHO, true, GRP>(e, b, i, live, g, sub, T, gr, nullptr, over);
         float fx = 0.f, fy = 0.f, fz = 0.f;
         for (int a = sub; a < cnt; a += GRP) {
@@ -265,13 +271,11 @@ __global__ void __launch_bounds__(128) k_mlp_force(SimEngine e, const float* __r
             for (int c = 0; c < cnt; ++c) {
                 const float4 uc = T.u[c][g];
                 const float x = fmaf(ua.z, uc.z, fmaf(ua.y, uc.y, ua.x * uc.x));
-                float S = s[8], Sp = sd[7];
+                const float2 xx = make_float2(x, x);
+                float2 h = ssd[0];
 #pragma unroll
-                for (int m = 7; m >= 1; --m) {
-                    S = fmaf(S, x, s[m]);
-                    Sp = fmaf(Sp, x, sd[m - 1]);
-                }
-                S = fmaf(S, x, s[0]);
+                for (int m = 7; m >= 1; --m) h = __ffma2_rn(h, xx, ssd[m]);
+                const float S = fmaf(h.x, x, s[0]), Sp = h.y;
                 if (c != a) {
                     const float t1 = Sp * uc.w;
                     Ax = fmaf(t1, uc.x, Ax); Ay = fmaf(t1, uc.y, Ay); Az = fmaf(t1, uc.z, Az);
