@@ -337,7 +337,7 @@ static int density_threads(const SimEngine& e) {
 }
 static int force_threads(const SimEngine& e) {
     const int t = e.launch[1];
-    return t == 0 ? EAM_FORCE_THREADS : (t == 256 || t == 512 || t == 1024) && t <= EAM_FORCE_THREADS ? t : -1;
+    return t == 0 ? EAM_FORCE_THREADS : (t == 256 || t == 512 || t == EAM_FORCE_THREADS) && t <= EAM_FORCE_THREADS ? t : -1;
 }
 
 template <bool SMEM, bool ORTHO>
@@ -476,7 +476,7 @@ extern "C" int sim_autotune_eam(const SimEngine* ep, const SimEAMTables* tp, int
     }
     cudaStream_t st = (cudaStream_t)stream;
     SimEngine e = *ep;
-    const int d_cand[3] = {128, 256, 512}, f_cand[3] = {256, 512, 1024};
+    const int d_cand[3] = {128, 256, 512}, f_cand[3] = {256, 512, EAM_FORCE_THREADS};
     for (int k = 0; k < 3; ++k) {
         e.launch[0] = d_cand[k];
         int rc = SIM_OK;
