@@ -286,6 +286,38 @@ def test_lj_fused_integrator_equals_separate_kernels(sb, tmp_path, mode):
         np.testing.assert_allclose(r[3][1:10], res[0][3][1:10], rtol=1e-5, atol=1e-6)
 
 
+@pytest.mark.parametrize("tri", [False, True])
+def test_lj_fp32_two_types_matches_fp64(sb, tri):
+    """FP32-pair LJ for an Ar/Ne mixture (per type-pair constants read per
+    pair) in an orthogonal and a triclinic box, against the FP64 path on the
+    same positions: force RMSE < 5e-6 eV/A, energy and virial tensor within
+    FP32 round-off."""
+    x, L = oin.fcc_lattice(5)
+    x = oin.jitter(x, 0.05, 93)
+    H = oin.triclinic_box(L) if tri else np.diag([L] * 3)
+    if tri:
+        x = (x / L) @ H
+    sym = ["Ne" if k % 3 == 0 else "Ar" for k in range(len(x))]
+    par = {"[0 0]": {"epsilon": 0.00307, "sigma": 2.78}, "[0 1]": {"epsilon": 0.00565, "sigma": 3.09},
+           "[1 1]": {"epsilon": 0.0104, "sigma": 3.405}}
+    out = []
+    for dt in (torch.float32, torch.float64):
+        torch.set_default_dtype(dt)
+        try:
+            mol = sb.AtomFileReader.from_arrays(sym, x, L, 7.0, device=DEV, parameter=par, skin_thickness=0.5,
+                                                box_vectors=H if tri else None)
+            ff = sb.LennardJonesForce(mol)
+        finally:
+            torch.set_default_dtype(torch.float32)
+        assert mol.engine.n_types == 2 and bool(mol.engine.st.box_orthogonal) == (not tri)
+        o = ff()
+        out.append((o["forces"].double().cpu().numpy(), float(o["energy"]), o["virial_tensor"].double().cpu().numpy()))
+    rmse = float(np.sqrt(((out[0][0] - out[1][0]) ** 2).mean()))
+    assert rmse < 5e-6, rmse
+    assert abs(out[0][1] - out[1][1]) < 2e-6 * abs(out[1][1]) + 1e-6
+    np.testing.assert_allclose(out[0][2], out[1][2], rtol=1e-5, atol=1e-4)
+
+
 # ---------------------------------------------------------------- MD
 @pytest.mark.parametrize("ens", ["nve", "nvt"])
 def test_md_lj_fp64_matches_reference_trajectory(sb, tmp_path, ens):
