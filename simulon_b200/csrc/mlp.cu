@@ -157,6 +157,23 @@ __device__ __forceinline__ float grp_sum(float v) {
     return v;
 }
 
+// The eight angular terms of one pair (raw powers of 1 +- cos; the 2^(1-z)
+// after the reduction) into d[8..15].
+__device__ __forceinline__ void angular_terms(const float4& ua, const float4& uc, float* d) {
+    const float cs = fmaf(ua.z, uc.z, fmaf(ua.y, uc.y, ua.x * uc.x));
+    const float rad = ua.w * uc.w;
+    const float p1 = 1.0f + cs, m1 = 1.0f - cs;
+    const float p2 = p1 * p1, m2 = m1 * m1, p4 = p2 * p2, m4 = m2 * m2;
+    d[8] = fmaf(p1, rad, d[8]);
+    d[9] = fmaf(m1, rad, d[9]);
+    d[10] = fmaf(p2, rad, d[10]);
+    d[11] = fmaf(m2, rad, d[11]);
+    d[12] = fmaf(p4, rad, d[12]);
+    d[13] = fmaf(m4, rad, d[13]);
+    d[14] = fmaf(p4 * p4, rad, d[14]);
+    d[15] = fmaf(m4 * m4, rad, d[15]);
+}
+
 template <bool ORTHO, int GRP>
 __global__ void __launch_bounds__(128) k_mlp_desc(SimEngine e, float* __restrict__ G) {
     constexpr int APB = 128 / GRP;
@@ -174,26 +191,23 @@ __global__ void __launch_bounds__(128) k_mlp_desc(SimEngine e, float* __restrict
         for (int q = 0; q < MLP_D; ++q) d[q] = 0.0f;
         const int cnt = mlp_table<ORTHO, false, GRP>(e, b, i, live, g, sub, T, nullptr, d, over);
         // angular: raw powers (1 +- c)^z summed over a < c; the 2^(1-z) after the
-        // reduction.  Lane sub takes a = sub and 2 GRP - 1 - sub of every block of
-        // 2 GRP (a long and a short row of the triangle: the lanes' pair counts balance)
-        for (int k = 0; k < 2 * ((cnt + 2 * GRP - 1) / (2 * GRP)); ++k) {
-            const int a = (k >> 1) * 2 * GRP + ((k & 1) ? 2 * GRP - 1 - sub : sub);
-            if (a >= cnt) continue;
-            const float4 ua = T.u[a][g];
-            for (int c = a + 1; c < cnt; ++c) {
+        // reduction.  Lane sub takes rows a0 = sub and a1 = 2 GRP - 1 - sub of
+        // every block of 2 GRP (a long and a short row of the triangle: the
+        // lanes' pair counts balance) and walks them together: c in (a0, a1]
+        // pairs with a0 alone, c > a1 with both, one table load of u_c serving
+        // the two pairs.
+        for (int blk = 0; blk < (cnt + 2 * GRP - 1) / (2 * GRP); ++blk) {
+            const int a0 = blk * 2 * GRP + sub, a1 = blk * 2 * GRP + 2 * GRP - 1 - sub;
+            if (a0 >= cnt) continue;
+            const float4 ua0 = T.u[a0][g];
+            const int c1 = a1 < cnt ? a1 : cnt - 1;
+            for (int c = a0 + 1; c <= c1; ++c) angular_terms(ua0, T.u[c][g], d);
+            if (a1 >= cnt) continue;
+            const float4 ua1 = T.u[a1][g];
+            for (int c = a1 + 1; c < cnt; ++c) {
                 const float4 uc = T.u[c][g];
-                const float cs = fmaf(ua.z, uc.z, fmaf(ua.y, uc.y, ua.x * uc.x));
-                const float rad = ua.w * uc.w;
-                const float p1 = 1.0f + cs, m1 = 1.0f - cs;
-                const float p2 = p1 * p1, m2 = m1 * m1, p4 = p2 * p2, m4 = m2 * m2;
-                d[8] = fmaf(p1, rad, d[8]);
-                d[9] = fmaf(m1, rad, d[9]);
-                d[10] = fmaf(p2, rad, d[10]);
-                d[11] = fmaf(m2, rad, d[11]);
-                d[12] = fmaf(p4, rad, d[12]);
-                d[13] = fmaf(m4, rad, d[13]);
-                d[14] = fmaf(p4 * p4, rad, d[14]);
-                d[15] = fmaf(m4 * m4, rad, d[15]);
+                angular_terms(ua0, uc, d);
+                angular_terms(ua1, uc, d);
             }
         }
 #pragma unroll
