@@ -235,6 +235,41 @@ __global__ void __launch_bounds__(128) k_mlp_desc(SimEngine e, float* __restrict
 // (each ordered pair evaluated by the lane owning a).  Atom j_a receives
 // -g_a, atom i +sum_a g_a, by float4 atomics (the summation order, and so
 // the last bits, vary from run to run).
+// Sums over c of one row a of the force kernel: A_a (vector), B_a, C_a.
+struct MlpRowSums {
+    float Ax = 0.f, Ay = 0.f, Az = 0.f, B = 0.f, C = 0.f;
+};
+
+// Pair (a, c): S and S' of cos_ac by one Horner recurrence on FP32x2 pairs
+// {S, S'} (coefficient pairs ssd, each lane rounding as the scalar fmaf),
+// added to the row sums unless c is a itself.
+__device__ __forceinline__ void force_pair(const float4& ua, const float4& uc, bool other, const float2 (&ssd)[8],
+                                           float s0, MlpRowSums& r) {
+    const float x = fmaf(ua.z, uc.z, fmaf(ua.y, uc.y, ua.x * uc.x));
+    const float2 xx = make_float2(x, x);
+    float2 h = ssd[0];
+#pragma unroll
+    for (int m = 7; m >= 1; --m) h = __ffma2_rn(h, xx, ssd[m]);
+    const float S = fmaf(h.x, x, s0), Sp = h.y;
+    if (other) {
+        const float t1 = Sp * uc.w;
+        r.Ax = fmaf(t1, uc.x, r.Ax); r.Ay = fmaf(t1, uc.y, r.Ay); r.Az = fmaf(t1, uc.z, r.Az);
+        r.B = fmaf(t1, x, r.B);
+        r.C = fmaf(S, uc.w, r.C);
+    }
+}
+
+// Row a finished: g_a to neighbour j_a (-g_a) and to the atom's own sum.
+template <class Table>
+__device__ __forceinline__ void force_row(const Table& T, int a, int g, const float4& ua, const MlpRowSums& r,
+                                          float4* f, float& fx, float& fy, float& fz) {
+    const float2 wa = T.w[a][g];
+    const float k = T.srad[a][g] - wa.y * r.B + wa.x * r.C;
+    const float gx = fmaf(wa.y, r.Ax, k * ua.x), gy = fmaf(wa.y, r.Ay, k * ua.y), gz = fmaf(wa.y, r.Az, k * ua.z);
+    atomicAdd(&f[T.j[a][g]], make_float4(-gx, -gy, -gz, 0.0f));
+    fx += gx; fy += gy; fz += gz;
+}
+
 template <bool ORTHO, int GRP>
 __global__ void __launch_bounds__(128) k_mlp_force(SimEngine e, const float* __restrict__ dEdG) {
     constexpr int APB = 128 / GRP;
@@ -279,29 +314,21 @@ __global__ void __launch_bounds__(128) k_mlp_force(SimEngine e, const float* __r
         ssd[0] = make_float2(s[8], sd[7]);
         const int cnt = mlp_table<ORTHO, true, GRP>(e, b, i, live, g, sub, T, gr, nullptr, over);
         float fx = 0.f, fy = 0.f, fz = 0.f;
-        for (int a = sub; a < cnt; a += GRP) {
+        // rows a and a + GRP of the lane together: one table load of u_c
+        // serves both rows' pairs
+        for (int a = sub; a < cnt; a += 2 * GRP) {
+            const int a2 = a + GRP;
+            const bool two = a2 < cnt;
             const float4 ua = T.u[a][g];
-            float Ax = 0.f, Ay = 0.f, Az = 0.f, B = 0.f, C = 0.f;
+            const float4 ub = T.u[two ? a2 : a][g];
+            MlpRowSums ra, rb;
             for (int c = 0; c < cnt; ++c) {
                 const float4 uc = T.u[c][g];
-                const float x = fmaf(ua.z, uc.z, fmaf(ua.y, uc.y, ua.x * uc.x));
-                const float2 xx = make_float2(x, x);
-                float2 h = ssd[0];
-#pragma unroll
-                for (int m = 7; m >= 1; --m) h = __ffma2_rn(h, xx, ssd[m]);
-                const float S = fmaf(h.x, x, s[0]), Sp = h.y;
-                if (c != a) {
-                    const float t1 = Sp * uc.w;
-                    Ax = fmaf(t1, uc.x, Ax); Ay = fmaf(t1, uc.y, Ay); Az = fmaf(t1, uc.z, Az);
-                    B = fmaf(t1, x, B);
-                    C = fmaf(S, uc.w, C);
-                }
+                force_pair(ua, uc, c != a, ssd, s[0], ra);
+                if (two) force_pair(ub, uc, c != a2, ssd, s[0], rb);
             }
-            const float2 wa = T.w[a][g];
-            const float k = T.srad[a][g] - wa.y * B + wa.x * C;
-            const float gx = fmaf(wa.y, Ax, k * ua.x), gy = fmaf(wa.y, Ay, k * ua.y), gz = fmaf(wa.y, Az, k * ua.z);
-            atomicAdd(&f[T.j[a][g]], make_float4(-gx, -gy, -gz, 0.0f));
-            fx += gx; fy += gy; fz += gz;
+            force_row(T, a, g, ua, ra, f, fx, fy, fz);
+            if (two) force_row(T, a2, g, ub, rb, f, fx, fy, fz);
         }
         fx = grp_sum<GRP>(fx); fy = grp_sum<GRP>(fy); fz = grp_sum<GRP>(fz);
         if (live && sub == 0) atomicAdd(&f[i], make_float4(fx, fy, fz, 0.0f));
