@@ -430,8 +430,16 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// logistic sigmoid with the fast divide (1 + exp(-z) above 2^126 gives 0)
-__device__ __forceinline__ float sigm(float z) { return __fdividef(1.0f, 1.0f + __expf(-z)); }
+// logistic sigmoid as 1/2 + tanh(z/2)/2 on the hardware tanh approximation
+// (tanh.approx.f32: one MUFU operation instead of an exponential and a
+// reciprocal; its relative error, about 2^-11, is below the BF16 rounding of
+// the activations that feed the next layer; saturates to 0 and 1)
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sigm(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
 __device__ __forceinline__ float silu(float z) { return z * sigm(z); }
 __device__ __forceinline__ float dsilu(float z) {
     const float s = sigm(z);
