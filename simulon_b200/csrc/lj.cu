@@ -145,61 +145,95 @@ __global__ void __launch_bounds__(SIM_THREADS, LJ_MIN_BLOCKS) k_lj_f32(SimEngine
 
 // FP64 variant: positions from e.x, minimum image and pair arithmetic in the
 // reference's order (lennard_jones_force.py:35-79), forces to e.f64.
+// Persistent grid; with one element type the pair constants sit in
+// registers; the positions of two list entries are gathered together.  The
+// arithmetic of each pair and the order of the sums are those of one
+// pair at a time.
+struct LJConst64 {
+    double sig, c4, c24, urc, frc;
+};
+__device__ __forceinline__ LJConst64 lj_const64(const SimLJParams& p, int tt) {
+    return LJConst64{p.sigma[tt], p.c4eps[tt], p.c24eps[tt], p.u_rc ? p.u_rc[tt] : 0.0, p.f_rc ? p.f_rc[tt] : 0.0};
+}
+
+// One pair: r = x_i - x_j (raw difference, then the minimum image) into atom
+// i's force and per-atom sums a[0] energy, a[1] scalar virial, a[2..7]
+// virial tensor (xx yy zz xy xz yz).
+__device__ __forceinline__ void lj_pair_f64(const SimBox& b, const SimLJParams& p, const LJConst64& c, double rc,
+                                            double rs, double r0, double r1, double r2, double& fx, double& fy,
+                                            double& fz, double (&a)[8]) {
+    min_image_f64(b, r0, r1, r2);
+    double d2 = norm2_f64(r0, r1, r2);
+    d2 = d2 < 1e-24 ? 1e-24 : d2;
+    const double r = __dsqrt_rn(d2);
+    if (!(r < rc)) return;
+    const double inv_r = __drcp_rn(r);
+    const double sr = __dmul_rn(c.sig, inv_r);
+    const double sr6 = pow(sr, 6.0);
+    const double sr12 = __dmul_rn(sr6, sr6);
+    double U = __dmul_rn(c.c4, __dsub_rn(sr12, sr6));
+    double F = __dmul_rn(__dmul_rn(c.c24, inv_r), __dsub_rn(__dmul_rn(2.0, sr12), sr6));
+    if (p.mode == SIM_LJ_SHIFT) {
+        U = __dadd_rn(__dsub_rn(U, c.urc), __dmul_rn(__dsub_rn(r, rc), c.frc));
+        F = __dsub_rn(F, c.frc);
+    } else if (p.mode == SIM_LJ_SWITCH) {
+        double x = __ddiv_rn(__dsub_rn(r, rs), __dsub_rn(rc, rs));
+        x = x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x);
+        const double S_poly = __dsub_rn(__dadd_rn(__dsub_rn(1.0, __dmul_rn(10.0, pow(x, 3.0))),
+                                                  __dmul_rn(15.0, pow(x, 4.0))),
+                                        __dmul_rn(6.0, pow(x, 5.0)));
+        const double dS_poly = __ddiv_rn(__dsub_rn(__dadd_rn(__dmul_rn(-30.0, pow(x, 2.0)), __dmul_rn(60.0, pow(x, 3.0))),
+                                                   __dmul_rn(30.0, pow(x, 4.0))),
+                                         __dsub_rn(rc, rs));
+        const bool mid = (r > rs) && (r < rc);
+        const double S = r <= rs ? 1.0 : (mid ? S_poly : 0.0);
+        const double dS = mid ? dS_poly : 0.0;
+        F = __dsub_rn(__dmul_rn(F, S), __dmul_rn(U, dS));
+        U = __dmul_rn(U, S);
+    }
+    const double ex = __dmul_rn(r0, inv_r), ey = __dmul_rn(r1, inv_r), ez = __dmul_rn(r2, inv_r);
+    const double ax = __dmul_rn(F, ex), ay = __dmul_rn(F, ey), az = __dmul_rn(F, ez);
+    fx += ax; fy += ay; fz += az;
+    a[0] += U;
+    a[1] += __dmul_rn(F, r);
+    a[2] += ax * r0; a[3] += ay * r1; a[4] += az * r2; a[5] += ax * r1; a[6] += ax * r2; a[7] += ay * r2;
+}
+
+template <bool SINGLE>
 __global__ void __launch_bounds__(SIM_THREADS) k_lj_f64(SimEngine e, SimLJParams p) {
+    pdl_trigger();
+    pdl_wait();   // positions, box and list come from earlier kernels
     const SimBox& b = *e.box;
     const int64_t P = e.n_pad;
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const double rc = p.rc, rs = p.rs;
+    const LJConst64 c1 = SINGLE ? lj_const64(p, 0) : LJConst64{0, 0, 0, 0, 0};
     double vals[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (i < e.n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += stride) {
         const double xi0 = e.x[i], xi1 = e.x[P + i], xi2 = e.x[2 * P + i];
         const int ti = e.posq[4 * i + 3];
         const int nn = e.nnbr[i];
-        double fx = 0, fy = 0, fz = 0, ep = 0, vir = 0, wxx = 0, wyy = 0, wzz = 0, wxy = 0, wxz = 0, wyz = 0;
-        for (int k = 0; k < nn; ++k) {
-            const int j = __ldg(&e.nbr[(int64_t)k * P + i]);
-            double r0 = __dsub_rn(xi0, e.x[j]), r1 = __dsub_rn(xi1, e.x[P + j]), r2 = __dsub_rn(xi2, e.x[2 * P + j]);
-            min_image_f64(b, r0, r1, r2);
-            double d2 = norm2_f64(r0, r1, r2);
-            d2 = d2 < 1e-24 ? 1e-24 : d2;
-            const double r = __dsqrt_rn(d2);
-            if (!(r < rc)) continue;
-            const int tt = ti * p.n_types + e.posq[4 * j + 3];
-            const double inv_r = __drcp_rn(r);
-            const double sr = __dmul_rn(p.sigma[tt], inv_r);
-            const double sr6 = pow(sr, 6.0);
-            const double sr12 = __dmul_rn(sr6, sr6);
-            double U = __dmul_rn(p.c4eps[tt], __dsub_rn(sr12, sr6));
-            double F = __dmul_rn(__dmul_rn(p.c24eps[tt], inv_r), __dsub_rn(__dmul_rn(2.0, sr12), sr6));
-            if (p.mode == SIM_LJ_SHIFT) {
-                U = __dadd_rn(__dsub_rn(U, p.u_rc[tt]), __dmul_rn(__dsub_rn(r, rc), p.f_rc[tt]));
-                F = __dsub_rn(F, p.f_rc[tt]);
-            } else if (p.mode == SIM_LJ_SWITCH) {
-                double x = __ddiv_rn(__dsub_rn(r, rs), __dsub_rn(rc, rs));
-                x = x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x);
-                const double S_poly = __dsub_rn(__dadd_rn(__dsub_rn(1.0, __dmul_rn(10.0, pow(x, 3.0))),
-                                                          __dmul_rn(15.0, pow(x, 4.0))),
-                                                __dmul_rn(6.0, pow(x, 5.0)));
-                const double dS_poly = __ddiv_rn(__dsub_rn(__dadd_rn(__dmul_rn(-30.0, pow(x, 2.0)), __dmul_rn(60.0, pow(x, 3.0))),
-                                                           __dmul_rn(30.0, pow(x, 4.0))),
-                                                 __dsub_rn(rc, rs));
-                const bool mid = (r > rs) && (r < rc);
-                const double S = r <= rs ? 1.0 : (mid ? S_poly : 0.0);
-                const double dS = mid ? dS_poly : 0.0;
-                F = __dsub_rn(__dmul_rn(F, S), __dmul_rn(U, dS));
-                U = __dmul_rn(U, S);
-            }
-            const double ex = __dmul_rn(r0, inv_r), ey = __dmul_rn(r1, inv_r), ez = __dmul_rn(r2, inv_r);
-            const double ax = __dmul_rn(F, ex), ay = __dmul_rn(F, ey), az = __dmul_rn(F, ez);
-            fx += ax; fy += ay; fz += az;
-            ep += U;
-            vir += __dmul_rn(F, r);
-            wxx += ax * r0; wyy += ay * r1; wzz += az * r2; wxy += ax * r1; wxz += ax * r2; wyz += ay * r2;
+        double fx = 0, fy = 0, fz = 0;
+        double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        int k = 0;
+        for (; k + 2 <= nn; k += 2) {
+            const int j0 = ld_stream(&e.nbr[(int64_t)k * P + i]), j1 = ld_stream(&e.nbr[(int64_t)(k + 1) * P + i]);
+            const double x00 = __ldg(&e.x[j0]), x01 = __ldg(&e.x[P + j0]), x02 = __ldg(&e.x[2 * P + j0]);
+            const double x10 = __ldg(&e.x[j1]), x11 = __ldg(&e.x[P + j1]), x12 = __ldg(&e.x[2 * P + j1]);
+            const LJConst64 ca = SINGLE ? c1 : lj_const64(p, ti * p.n_types + e.posq[4 * j0 + 3]);
+            lj_pair_f64(b, p, ca, rc, rs, __dsub_rn(xi0, x00), __dsub_rn(xi1, x01), __dsub_rn(xi2, x02), fx, fy, fz, a);
+            const LJConst64 cb = SINGLE ? c1 : lj_const64(p, ti * p.n_types + e.posq[4 * j1 + 3]);
+            lj_pair_f64(b, p, cb, rc, rs, __dsub_rn(xi0, x10), __dsub_rn(xi1, x11), __dsub_rn(xi2, x12), fx, fy, fz, a);
+        }
+        if (k < nn) {
+            const int j = ld_stream(&e.nbr[(int64_t)k * P + i]);
+            const LJConst64 cc = SINGLE ? c1 : lj_const64(p, ti * p.n_types + e.posq[4 * j + 3]);
+            lj_pair_f64(b, p, cc, rc, rs, __dsub_rn(xi0, __ldg(&e.x[j])), __dsub_rn(xi1, __ldg(&e.x[P + j])),
+                        __dsub_rn(xi2, __ldg(&e.x[2 * P + j])), fx, fy, fz, a);
         }
         e.f64[i] = fx; e.f64[P + i] = fy; e.f64[2 * P + i] = fz;
-        vals[0] = 0.5 * ep; vals[1] = 0.5 * vir;
-        vals[2] = 0.5 * wxx; vals[3] = 0.5 * wyy; vals[4] = 0.5 * wzz;
-        vals[5] = 0.5 * wxy; vals[6] = 0.5 * wxz; vals[7] = 0.5 * wyz;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) vals[s] += 0.5 * a[s];
         if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
     }
     block_partials<8>(vals, e.partials, SIM_RED_EPOT_PAIR);
@@ -236,8 +270,13 @@ extern "C" int sim_lj_forces(const SimEngine* ep, const SimLJParams* pp, int32_t
     const int blocks = (int)ceil_div(e.n, SIM_THREADS);
     k_zero_slot<<<1, 1, 0, st>>>(e.red_out, SIM_RED_EPOT_EMBED);
     if (precision == 1) {
-        if (!e.f64 || blocks > e.n_blocks_max) return SIM_ERR_ARG;
-        k_lj_f64<<<blocks, SIM_THREADS, 0, st>>>(e, *pp);
+        if (!e.f64) return SIM_ERR_ARG;
+        const void* fn = pp->n_types == 1 ? (const void*)k_lj_f64<true> : (const void*)k_lj_f64<false>;
+        const int g = persistent_grid(fn, SIM_THREADS, 0, e.n);
+        if (g > e.n_blocks_max) return SIM_ERR_ARG;
+        const cudaError_t err = pp->n_types == 1 ? launch_pdl(k_lj_f64<true>, dim3(g), dim3(SIM_THREADS), 0, st, e, *pp)
+                                                 : launch_pdl(k_lj_f64<false>, dim3(g), dim3(SIM_THREADS), 0, st, e, *pp);
+        if (err != cudaSuccess) { set_cuda_error(err, "sim_lj_forces: launch"); return SIM_ERR_CUDA; }
     } else {
         const int rc = lj_f32<0>(e, *pp, SimIntegrator{}, st);
         if (rc != SIM_OK) return rc;
