@@ -52,6 +52,16 @@ def test_argument_errors_are_reported_without_gpu(lib):
     assert lib.sim_rebuild(None, 0, None) == _lib.SIM_ERR_ARG
     assert lib.sim_legacy_density_pass(None, None, None, None, 0, None, 1, 1.0, 1, None, None) == _lib.SIM_ERR_ARG
     assert lib.sim_legacy_density_pass(None, None, None, None, 0, None, 1, 1.0, 8, None, None) == _lib.SIM_OK
+    # the fused step, LJ and Berendsen entry points check their arguments before any device work
+    assert lib.sim_eam_step_drift(None, None, None, None, 0, None, 0, None) == _lib.SIM_ERR_ARG
+    assert lib.sim_lj_forces_integrate(None, None, None, 1, None) == _lib.SIM_ERR_ARG
+    assert lib.sim_berendsen_mu(None, None, None, None) == _lib.SIM_ERR_ARG
+    assert lib.sim_berendsen_scale_first(None, None, None, None, 0, None) == _lib.SIM_ERR_ARG
+    e, p, ip = _lib.SimEngine(), _lib.SimLJParams(), _lib.SimIntegrator()
+    e.n = 10
+    for mode in (0, 3):   # only 1 (second half) and 2 (with the next first half)
+        assert lib.sim_lj_forces_integrate(ctypes.byref(e), ctypes.byref(p), ctypes.byref(ip), mode, None) == \
+            _lib.SIM_ERR_ARG
     with pytest.raises(_lib.SimError):
         _lib.check(_lib.SIM_ERR_ARG, "probe")
 
