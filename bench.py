@@ -263,6 +263,8 @@ def run_b200(args):
             line["batched"] = batched_form(args, sb, pot, dev, world, rank, barrier)
         if "variants" in forms:
             line["eam_variants"] = eam_variants_form(args, sb, pot, dev, world)
+        if "mechanics" in forms and world == 1:
+            line["mechanics"] = mechanics_form(args, sb, pot, dev, world)
         if world > 1:
             dist.destroy_process_group()
         if rank == 0:
@@ -383,6 +385,8 @@ def run_b200(args):
         line["batched"] = batched_form(args, sb, pot, dev, world, rank, barrier)
     if "variants" in forms:
         line["eam_variants"] = eam_variants_form(args, sb, pot, dev, world)
+    if "mechanics" in forms and world == 1:
+        line["mechanics"] = mechanics_form(args, sb, pot, dev, world)
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
@@ -519,6 +523,86 @@ def eam_variants_form(args, sb, pot, dev, world):
     out["config"] = {"workload": f"EAM-W bulk BCC 2*{args.n}^3 = {N:,} atoms per GPU, synthetic FS W, dt 2 fs, "
                                  "skin 0.5 A: triclinic NVE (xy tilt 0.02) and Berendsen NPT (P0 0 bar, tau_p 1 ps, "
                                  "Langevin 300 K)", "scaling": "weak", "parallelism": f"replicas x{world}"}
+    return out
+
+
+def mechanics_form(args, sb, pot, dev, world):
+    """The tensile and indentation callers of the EAM-W force path at 2 n^3
+    atoms (BCC W, synthetic FS potential, dt 2 fs, 300 K Maxwell-Boltzmann
+    velocities): (1) uniaxial tension along x at 0.1 / ps with the anisotropic
+    NPT barostat holding y and z at 0 bar (core/mechanics/loading.py:6-81,
+    core/barostat.py:78-208), one loader.step + model() per step as the
+    reference's loop does (eager launches); (2) a spherical indenter (radius
+    20 A, stiffness 0.05 eV/A^3) on the top layer as a second backbone
+    (core/mechanics/indenter.py:7-68), its centre lowered 0.04 A between
+    20-step graph replays.  Each timed with CUDA events like the plain line."""
+    import torch
+    from simulon_b200.barostat import AnisotropicNPTBarostat
+    from simulon_b200.mechanics import SphericalIndenterForce, UniaxialTensileLoader
+    x, L = bcc(args.n)
+    N = len(x)
+    v = mb_velocities(N, 300.0, 4000 + int(os.environ.get("RANK", "0")))
+    parser = sb.EAMParser(pot)
+    out = {}
+    for name in ("tensile", "indentation"):
+        mol = sb.AtomFileReader.from_arrays(["W"] * N, x, L, parser.cutoff, device=dev, skin_thickness=0.5,
+                                            is_fs=True)
+        integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NVE")
+        mol.atom_velocities = torch.tensor(v, device=dev)
+        ff = sb.EAMForceCUDAExt(parser, mol)
+        eng = mol.engine
+        if name == "tensile":
+            baro = AnisotropicNPTBarostat(mol, [0.0, 0.0, 0.0], temperature_k=300.0, control_axes=(False, True, True))
+            loader = UniaxialTensileLoader(mol, axis=0, strain_rate=0.1)
+            model = sb.BaseModel(sb.SumBackboneInterface([ff], mol), integ, mol, barostat=baro)
+
+            def steps(k):
+                o = None
+                for _ in range(k):
+                    loader.step(0.002)
+                    o = model()
+                return o
+        else:
+            top = float(x[:, 2].max())
+            center = np.array([0.5 * L, 0.5 * L, top + 20.0 - 1.0])
+            ind = SphericalIndenterForce(mol, radius=20.0, stiffness=0.05, center=center)
+            model = sb.BaseModel(sb.SumBackboneInterface([ff, ind], mol), integ, mol)
+            depth = [0.0]
+
+            def steps(k):
+                o = None
+                for _ in range(k // args.graph_steps):
+                    depth[0] += 0.04
+                    ind.set_center(center - np.array([0.0, 0.0, depth[0]]))
+                    o = model.run(args.graph_steps, graph_steps=args.graph_steps)
+                return o
+        steps(max(args.warmup, args.graph_steps))
+        torch.cuda.synchronize()
+        rb0 = int(eng.flags[3].item())
+        K = (args.steps // args.graph_steps) * args.graph_steps
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        o = steps(K)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        row = {"value": N * K / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K, "steps": K, "status": eng.status(),
+               "rebuilds_in_timed": int(eng.flags[3].item()) - rb0, "temperature_k": float(o["temperature"])}
+        if name == "tensile":
+            row["engineering_strain"] = float(loader.total_engineering_strain)
+            row["forced_rebuilds"] = int(loader.forced_rebuilds)
+            row["pressure_bar"] = [float(p) for p in o["pressure"].reshape(-1)[:3]]
+        else:
+            row["force_on_indenter_ev_per_a"] = [float(f) for f in ind.force_on_indenter]
+            row["contact_atoms"] = int(ind.contact_atoms)
+        out[name] = row
+        del model, ff, integ, mol, eng
+        torch.cuda.empty_cache()
+    out["config"] = {"workload": f"EAM-W BCC 2*{args.n}^3 = {N:,} atoms, synthetic FS W, dt 2 fs, 300 K: uniaxial "
+                                 "tension 0.1/ps along x with anisotropic NPT at 0 bar on y, z (eager per-step loop); "
+                                 "spherical indenter r 20 A, k 0.05 eV/A^3, lowered 0.04 A per 20-step graph",
+                     "parallelism": "replicas x1"}
     return out
 
 
