@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--no-mlp", action="store_true", help="skip the MLP-surrogate form")
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the built-in launch shapes (profiling runs: fewer launches before the timed ones)")
-    p.add_argument("--forms", default="plain,lj,mlp,batched,variants",
+    p.add_argument("--forms", default="plain,lj,mlp,batched,variants,mechanics",
                    help="forms to run (profiling runs: e.g. --forms mlp prints only the mlp object)")
     p.add_argument("--lj-n", type=int, default=63, help="FCC cells per side of the LJ form (atoms = 4 n^3)")
     p.add_argument("--batch-replicas", type=int, default=48)
