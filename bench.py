@@ -599,9 +599,37 @@ def mechanics_form(args, sb, pot, dev, world):
         out[name] = row
         del model, ff, integ, mol, eng
         torch.cuda.empty_cache()
+    # (3) the simulator's output path (core/md_simulation.py:125-168): NVE run
+    # through MDSimulator writing traj.xyz and energies.csv every 100 steps
+    # from pinned asynchronous copies while the next steps run
+    mol = sb.AtomFileReader.from_arrays(["W"] * N, x, L, parser.cutoff, device=dev, skin_thickness=0.5, is_fs=True)
+    integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NVE")
+    mol.atom_velocities = torch.tensor(v, device=dev)
+    ff = sb.EAMForceCUDAExt(parser, mol)
+    model = sb.BaseModel(sb.SumBackboneInterface([ff], mol), integ, mol)
+    model.run(max(args.warmup, args.graph_steps), graph_steps=args.graph_steps)
+    K = max(100, (args.steps // 100) * 100)
+    with tempfile.TemporaryDirectory() as tmp:
+        sim = sb.MDSimulator(model, num_steps=K, print_interval=100, store_outputs=False, verbose=False,
+                             graph_steps=args.graph_steps, output_dir=tmp, traj_interval=100, write_energies=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        sim.run()
+        e1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        ms = e0.elapsed_time(e1)
+        size = sum(os.path.getsize(os.path.join(tmp, f)) for f in os.listdir(tmp))
+    out["simulator_output"] = {"value": N * K / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K, "steps": K,
+                               "wall_s": wall, "bytes_written": size, "status": mol.engine.status()}
+    del sim, model, ff, integ, mol
+    torch.cuda.empty_cache()
     out["config"] = {"workload": f"EAM-W BCC 2*{args.n}^3 = {N:,} atoms, synthetic FS W, dt 2 fs, 300 K: uniaxial "
                                  "tension 0.1/ps along x with anisotropic NPT at 0 bar on y, z (eager per-step loop); "
-                                 "spherical indenter r 20 A, k 0.05 eV/A^3, lowered 0.04 A per 20-step graph",
+                                 "spherical indenter r 20 A, k 0.05 eV/A^3, lowered 0.04 A per 20-step graph; "
+                                 "MDSimulator NVE writing traj.xyz and energies.csv every 100 steps",
                      "parallelism": "replicas x1"}
     return out
 

@@ -435,6 +435,17 @@ int sim_scatter_original_f64(const SimEngine* e, const double* rows, double* dst
 int sim_log_step(const SimEngine* e, const uint64_t* step_ctr, const double* extra, int32_t n_extra,
                  double* log, int32_t capacity, void* stream);
 
+/* Host helper of the simulator's trajectory file (no device work): rows
+ * "<symbols[type[i]]> <x> <y> <z>\n" for i < n with the coordinates in fixed
+ * notation, six decimals, digits as Python's format(v, ".6f") (correctly
+ * rounded, ties to even; NaN as "nan") -- the rows that
+ * MDSimulator._dump_step_outputs writes (core/md_simulation.py:125-168).
+ * type may be NULL (all symbols[0]).  Writes into out[0, cap) and returns the
+ * byte count, or -1 for a bad argument or a buffer that may be too small
+ * (cap below n * (longest symbol + 196) always suffices). */
+int64_t sim_format_xyz_rows(const double* xyz, const int32_t* type, int64_t n, const char* const* symbols,
+                            int32_t n_symbols, char* out, int64_t cap);
+
 /* Un-permute: out_rows[orig[k]*3 + c] = src[c*n_pad + k] (FP64 or FP32 source). */
 int sim_gather_original_f64(const SimEngine* e, const double* src_soa, double* out_rows, void* stream);
 int sim_gather_original_f32(const SimEngine* e, const float* src_soa, double* out_rows, void* stream);

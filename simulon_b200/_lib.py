@@ -174,6 +174,7 @@ SIGNATURES = {
     "sim_gather_original_f32": [_P(SimEngine), c_p, c_p, c_p],
     "sim_scatter_original_f64": [_P(SimEngine), c_p, c_p, c_p],
     "sim_log_step": [_P(SimEngine), c_p, c_p, ctypes.c_int32, c_p, ctypes.c_int32, c_p],
+    "sim_format_xyz_rows": [c_p, c_p, ctypes.c_int64, c_p, ctypes.c_int32, c_p, ctypes.c_int64],
     "sim_engine_half_count": [_P(SimEngine), ctypes.c_double, c_p, c_p],
     "sim_engine_half_fill": [_P(SimEngine), ctypes.c_double, c_p, c_p, c_p, c_p, c_p],
     "sim_scan_i64": [c_p, ctypes.c_int64, c_p, c_p],
@@ -209,7 +210,7 @@ SIGNATURES = {
 }
 STRUCTS = (SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator, SimBerendsen, SimRep, SimBatch, SimMLP,
            SimAniso, SimBoxScale, SimIndenter, SimCrack)
-_RESTYPES = {"sim_last_cuda_error": ctypes.c_char_p}
+_RESTYPES = {"sim_last_cuda_error": ctypes.c_char_p, "sim_format_xyz_rows": ctypes.c_int64}
 
 _lib = None
 

@@ -15,16 +15,25 @@ Energy = E", "type x y z"), ``energies.csv`` (step, potential, kinetic, total,
 temperature; every step or every ``energies_interval``) and
 ``forces/forces_<step>.pt``.  The run stays in CUDA graphs up to each
 output step; positions, forces and the step log rows go to pinned host
-buffers by asynchronous copies, and the files are written while the device
-runs on (no synchronisation per output step).
+buffers by asynchronous copies, and a background thread writes the files
+(trajectory rows formatted by the library, sim_format_xyz_rows) while the
+device runs on (no synchronisation per output step).
 """
 from __future__ import annotations
 
+import ctypes
 import os
 import time
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
+import numpy as np
 import torch
+
+from . import _lib
+
+
+XYZ_THREADS = min(8, os.cpu_count() or 1)   # threads formatting one trajectory frame
 
 
 class MDSimulator:
@@ -63,6 +72,9 @@ class MDSimulator:
         self.output_enabled = bool(self.output_dir and (any_traj or any_forces or self.write_energies))
         self._paths = {}
         self._pending = []
+        self._writer = None      # one background thread writes the files in step order
+        self._formatters = None  # threads formatting the blocks of one trajectory frame
+        self._jobs = []
         if self.output_enabled:
             self.output_dir.mkdir(parents=True, exist_ok=True)
             if any_traj:
@@ -113,38 +125,85 @@ class MDSimulator:
         item["event"] = ev
         self._pending.append(item)
 
-    def _write_ready(self, wait: bool = False):
+    def _xyz_table(self):
+        """Per-atom type indices and the symbol table for sim_format_xyz_rows."""
+        if not hasattr(self, "_xyz_types"):
+            mol = self.model.molecular
+            names = getattr(mol, "atom_types", None)
+            names = list(names) if names is not None and len(names) == mol.atom_count else ["X"] * mol.atom_count
+            symbols = sorted(set(names))
+            index = {sym: k for k, sym in enumerate(symbols)}
+            self._xyz_types = np.array([index[sym] for sym in names], dtype=np.int32)
+            self._xyz_symbols = (ctypes.c_char_p * len(symbols))(*[sym.encode() for sym in symbols])
+            self._xyz_width = max(len(sym) for sym in symbols) + 196
+        return self._xyz_types, self._xyz_symbols, self._xyz_width
+
+    def _write_item(self, item, n, kB):
+        """Append one staged output step to the files (runs on the writer thread;
+        the library's row formatter releases the GIL while it works)."""
         t0 = time.perf_counter()
+        step_i = item["step"]
+        log = item.get("log")
+        if log is not None and "energies" in self._paths:
+            with open(self._paths["energies"], "a", encoding="utf-8") as f:
+                for r, row in enumerate(log.tolist()):
+                    s = item["log_first"] - self._first_log + r + 1
+                    if self.energies_interval is not None and (self.energies_interval <= 0 or
+                                                               s % self.energies_interval):
+                        continue
+                    pot, kin = row[0] + row[1], row[9]
+                    temp = (2.0 / 3.0) * kin / (n * kB)
+                    f.write(f"{s},{pot:.8f},{kin:.8f},{pot + kin:.8f},{temp:.6f}\n")
+        if "x" in item:
+            pot = log[-1, 0].item() + log[-1, 1].item()
+            types, symbols, width = self._xyz_table()
+            xyz = item["x"].numpy()
+            lib = _lib.load()
+            # row blocks formatted on parallel threads (the call releases the GIL)
+            bounds = np.linspace(0, n, min(XYZ_THREADS, max(1, n // 4096)) + 1).astype(np.int64)
+
+            def block(k):
+                a, b = int(bounds[k]), int(bounds[k + 1])
+                buf = np.empty(max(1, (b - a) * width), dtype=np.uint8)
+                nb = lib.sim_format_xyz_rows(xyz[a:].ctypes.data, types[a:].ctypes.data, b - a, symbols,
+                                             len(symbols), buf.ctypes.data, buf.size)
+                if nb < 0:
+                    raise RuntimeError("sim_format_xyz_rows: bad arguments or buffer")
+                return memoryview(buf)[:nb]
+            if self._formatters is None:
+                self._formatters = ThreadPoolExecutor(max_workers=XYZ_THREADS)
+            parts = list(self._formatters.map(block, range(len(bounds) - 1)))
+            with open(self._paths["traj"], "ab") as f:
+                f.write(f"{n}\nStep {step_i}, Energy = {pot:.6f}\n".encode())
+                for part in parts:
+                    f.write(part)
+        if "f" in item:
+            torch.save(item["f"].clone(), os.path.join(self._paths["forces_dir"], f"forces_{step_i:06d}.pt"))
+        self.sim_profile["output_time"] += time.perf_counter() - t0
+
+    def _write_ready(self, wait: bool = False):
+        """Hand every staged output whose copies have landed to the writer
+        thread; with wait, also the rest, and wait until all files are written."""
         mol = self.model.molecular
         kB = self.model.Integrator.BOLTZMAN
         n = mol.atom_count
-        types = getattr(mol, "atom_types", None)
+        if self._writer is None:
+            self._writer = ThreadPoolExecutor(max_workers=1)
         while self._pending and (wait or self._pending[0]["event"].query()):
             item = self._pending.pop(0)
             item["event"].synchronize()
-            step_i = item["step"]
-            log = item.get("log")
-            if log is not None and "energies" in self._paths:
-                with open(self._paths["energies"], "a", encoding="utf-8") as f:
-                    for r, row in enumerate(log.tolist()):
-                        s = item["log_first"] - self._first_log + r + 1
-                        if self.energies_interval is not None and (self.energies_interval <= 0 or
-                                                                   s % self.energies_interval):
-                            continue
-                        pot, kin = row[0] + row[1], row[9]
-                        temp = (2.0 / 3.0) * kin / (n * kB)
-                        f.write(f"{s},{pot:.8f},{kin:.8f},{pot + kin:.8f},{temp:.6f}\n")
-            if "x" in item:
-                pot = log[-1, 0].item() + log[-1, 1].item()
-                lines = [f"{n}\n", f"Step {step_i}, Energy = {pot:.6f}\n"]
-                names = types if types and len(types) == n else ["X"] * n
-                for name, (x, y, z) in zip(names, item["x"].tolist()):
-                    lines.append(f"{name} {x:.6f} {y:.6f} {z:.6f}\n")
-                with open(self._paths["traj"], "a", encoding="utf-8") as f:
-                    f.writelines(lines)
-            if "f" in item:
-                torch.save(item["f"].clone(), os.path.join(self._paths["forces_dir"], f"forces_{step_i:06d}.pt"))
-        self.sim_profile["output_time"] += time.perf_counter() - t0
+            self._jobs.append(self._writer.submit(self._write_item, item, n, kB))
+        if wait:
+            jobs, self._jobs = self._jobs, []
+            for job in jobs:
+                job.result()            # re-raises a failed write here
+            self._writer.shutdown()
+            self._writer = None
+            if self._formatters is not None:
+                self._formatters.shutdown()
+                self._formatters = None
+        else:
+            self._jobs = [j for j in self._jobs if not j.done() or j.exception() is not None]
 
     def run(self, enable_minimize_energy: bool = False):
         if enable_minimize_energy:

@@ -27,7 +27,7 @@ def lib():
 def declared_symbols():
     src = open(os.path.join(ROOT, "include", "simb200.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(sim_\w+)\s*\(", src, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int64_t|int|const char\*)\s+(sim_\w+)\s*\(", src, flags=re.M)))
 
 
 def test_library_exports_every_declared_symbol(lib):
@@ -64,6 +64,27 @@ def test_argument_errors_are_reported_without_gpu(lib):
             _lib.SIM_ERR_ARG
     with pytest.raises(_lib.SimError):
         _lib.check(_lib.SIM_ERR_ARG, "probe")
+
+
+def test_xyz_rows_match_python_formatting(lib):
+    """The trajectory row formatter (host code of the library) against
+    Python's f"{v:.6f}": random magnitudes, exact ties (ties to even),
+    signed zeros, tiny and subnormal values, large values and non-finite ones."""
+    rng = np.random.default_rng(5)
+    edge = [0.0, -0.0, 0.0078125, -0.0078125, 0.0234375, 1.0000005, 2.5e-7, -2.5e-7, 4.9999995e-7, 123456.0000005,
+            1e-300, -1e-300, 5e-324, 1.5, 2.0 ** 39 + 0.1, 2.0 ** 40 + 0.5, 1e15, -1e15, float("inf"),
+            float("-inf"), float("nan"), -float("nan"), 999999.9999995, -0.0000005]
+    vals = np.concatenate([rng.normal(0, 50, 3000), rng.uniform(-1e6, 1e6, 600), rng.normal(0, 1e-5, 600),
+                           np.ldexp(rng.integers(-2 ** 20, 2 ** 20, 600).astype(np.float64), -20), edge])
+    vals = np.concatenate([vals, np.zeros((-len(vals)) % 3)])
+    xyz = np.ascontiguousarray(vals.reshape(-1, 3))
+    types = (np.arange(len(xyz)) % 2).astype(np.int32)
+    syms = (ctypes.c_char_p * 2)(b"W", b"Ar")
+    buf = np.empty(len(xyz) * 220, np.uint8)
+    nb = lib.sim_format_xyz_rows(xyz.ctypes.data, types.ctypes.data, len(xyz), syms, 2, buf.ctypes.data, buf.size)
+    want = "".join(f"{('W', 'Ar')[t]} {x:.6f} {y:.6f} {z:.6f}\n" for t, (x, y, z) in zip(types, xyz.tolist()))
+    assert nb == len(want.encode()) and bytes(buf[:nb]).decode() == want
+    assert lib.sim_format_xyz_rows(xyz.ctypes.data, None, len(xyz), syms, 2, buf.ctypes.data, 100) == -1
 
 
 def test_cell_grid_and_morton_order():
