@@ -322,6 +322,18 @@ int sim_eam_force_integrate(const SimEngine* e, const SimEAMTables* t, const Sim
  * Not available with neighbour tiles (nbr16 set): SIM_ERR_ARG. */
 int sim_eam_force_integrate_drift(const SimEngine* e, const SimEAMTables* t, const SimIntegrator* p,
                                   void* stream);
+/* EAM pass 2 as sim_eam_force_integrate (mode 1) or
+ * sim_eam_force_integrate_drift (mode 2) with the spherical indenter of
+ * sim_indenter_add added to each atom's force before the integrator epilogue
+ * (indenter.py:40-68, the force field and the indenter summed as
+ * SumBackboneInterface sums them, md_model.py:33-52): bit for bit the
+ * positions and velocities of sim_eam_force + sim_indenter_add +
+ * sim_integrate_second (+ sim_integrate_first), with ind->out written as
+ * sim_indenter_add writes it and its energy and virial added to red_out.
+ * One element type, untiled kernels (else SIM_ERR_ARG); needs 2 x the
+ * persistent grid in n_blocks_max (a second set of block partials). */
+int sim_eam_force_integrate_indenter(const SimEngine* e, const SimEAMTables* t, const SimIntegrator* p,
+                                     const SimIndenter* ind, int32_t mode, void* stream);
 /* One whole MD step of the drift-fused form ended on the device: EAM pass 1,
  * then pass 2 as sim_eam_force_integrate_drift, whose last block also appends
  * the step's log row (as sim_log_step on &step_ctr[1]) and decides the

@@ -156,6 +156,8 @@ SIGNATURES = {
     "sim_eam_force": [_P(SimEngine), _P(SimEAMTables), c_p],
     "sim_eam_force_integrate": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), c_p],
     "sim_eam_force_integrate_drift": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), c_p],
+    "sim_eam_force_integrate_indenter": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), _P(SimIndenter),
+                                         ctypes.c_int32, c_p],
     "sim_eam_step_drift": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), c_p, ctypes.c_int32, c_p,
                            ctypes.c_int32, c_p],
     "sim_lj_forces": [_P(SimEngine), _P(SimLJParams), ctypes.c_int32, c_p],

@@ -198,7 +198,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Block-reduce `vals[0..NV)` (FP64) and store one row of `partials` per block.
 // Deterministic: fixed shuffle tree, fixed warp order.
 template <int NV>
-__device__ __forceinline__ void block_partials(double (&vals)[NV], double* partials, int slot0) {
+__device__ __forceinline__ void block_partials(double (&vals)[NV], double* partials, int slot0,
+                                               int stride = SIM_RED_SLOTS) {
     __shared__ double red[NV][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -210,34 +211,22 @@ __device__ __forceinline__ void block_partials(double (&vals)[NV], double* parti
     if (threadIdx.x < NV) {
         double s = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
-        partials[(size_t)blockIdx.x * SIM_RED_SLOTS + slot0 + threadIdx.x] = s;
+        partials[(size_t)blockIdx.x * stride + slot0 + threadIdx.x] = s;
     }
 }
 
-// The last block to finish sums all partial rows for slots [slot0, slot0+NV)
-// and resets the counter (so a captured graph can replay).  Warp k sums slot
-// k: lane l adds rows l, l+32, ... with Kahan compensation, then the 32
-// compensated sums combine in a fixed tree (TwoSum of the sums, the
-// compensations added): the order depends only on the grid size.  Must be
-// called by every thread of every block (blockDim.x a multiple of 32).
+// The sums over the grid's blocks of partial slots [slot0, slot0+NV) (rows of
+// `stride` doubles) into out[out0 + k], by the calling block: warp k sums
+// slot k, lane l adding rows l, l+32, ... with Kahan compensation, then the
+// 32 compensated sums combine in a fixed tree (TwoSum of the sums, the
+// compensations added): the order depends only on the grid size.
 template <int NV>
-__device__ __forceinline__ bool last_block_finalize(double* partials, uint32_t* counter,
-                                                    double* out, int slot0) {
-    __shared__ bool is_last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t done = atomicAdd(counter, 1u);
-        is_last = (done == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!is_last) return false;
-    __threadfence();
+__device__ __forceinline__ void partial_sums(const double* partials, int slot0, int stride, double* out, int out0) {
     const int lane = threadIdx.x & 31, nw = (int)(blockDim.x >> 5);
     for (int k = (int)(threadIdx.x >> 5); k < NV; k += nw) {
         double s = 0.0, c = 0.0;   // value s - c
         for (unsigned b = lane; b < gridDim.x; b += 32) {
-            const double y = __ldcg(&partials[(size_t)b * SIM_RED_SLOTS + slot0 + k]) - c;
+            const double y = __ldcg(&partials[(size_t)b * stride + slot0 + k]) - c;
             const double t = s + y;
             c = (t - s) - y;
             s = t;
@@ -251,8 +240,30 @@ __device__ __forceinline__ bool last_block_finalize(double* partials, uint32_t* 
             c = c + c2 - err;
             s = t;
         }
-        if (lane == 0) out[slot0 + k] = s - c;
+        if (lane == 0) out[out0 + k] = s - c;
     }
+}
+
+// The last block to finish sums all partial rows for slots [slot0, slot0+NV)
+// and resets the counter (so a captured graph can replay).  Warp k sums slot
+// k: lane l adds rows l, l+32, ... with Kahan compensation, then the 32
+// compensated sums combine in a fixed tree (TwoSum of the sums, the
+// compensations added): the order depends only on the grid size.  Must be
+// called by every thread of every block (blockDim.x a multiple of 32).
+template <int NV>
+__device__ __forceinline__ bool last_block_finalize(double* partials, uint32_t* counter,
+                                                    double* out, int slot0, int stride = SIM_RED_SLOTS) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t done = atomicAdd(counter, 1u);
+        is_last = (done == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    partial_sums<NV>(partials, slot0, stride, out, slot0);
     if (threadIdx.x == 0) *counter = 0u;
     return true;
 }

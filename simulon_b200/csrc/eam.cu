@@ -134,9 +134,14 @@ struct StepEnd {
     int set_cond;                       // 0: no IF node (eager launch)
 };
 
-template <bool SINGLE, int INTEG, bool ORTHO>
+// IND (with INTEG 1 or 2): the spherical indenter of sim_indenter_add is added
+// to atom i's force before the integrator epilogue (the same FP32 addition as
+// k_indenter's, so the same trajectory), its 11 FP64 sums going to a second
+// set of block partials (rows gridDim.x .. 2 gridDim.x - 1) that the last block
+// finishes into ind.out and folds into red_out as k_indenter does.
+template <bool SINGLE, int INTEG, bool ORTHO, bool IND = false>
 __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam_force(SimEngine e, SimEAMTables t, SimIntegrator ip,
-                                                                    Window w, StepEnd end) {
+                                                                    Window w, StepEnd end, SimIndenter ind) {
     extern __shared__ float4 s_tab4[];
     pdl_trigger();
     float4* tab_d = s_tab4;
@@ -160,6 +165,7 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
     float acc[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     bool bad = false, trig = false;
     const uint64_t step = INTEG && ip.step_ctr ? *ip.step_ctr : 0;
+    double iv[IND ? 11 : 1] = {0};     // indenter: energy, force (3), contacts, virial xx yy zz xy xz yz
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
         const int4 pi = posfp[i];
         const float fpi = __int_as_float(pi.w);
@@ -232,6 +238,23 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
                            fx, fy, fz, acc);
             }
         }
+        if (IND) {   // as k_indenter (indenter.py:40-68), on the positions of this step
+            const int64_t P = e.n_pad;
+            const double x0 = e.x[i], x1 = e.x[P + i], x2 = e.x[2 * P + i];
+            const double d0 = x0 - ind.center[0], d1 = x1 - ind.center[1], d2 = x2 - ind.center[2];
+            const double d = fmax(sqrt(d0 * d0 + d1 * d1 + d2 * d2), 1e-12);
+            const double pen = ind.radius - d;
+            if (pen > 0.0) {
+                const double k = ind.stiffness * pen * pen;
+                const double f0 = k * (d0 / d), f1 = k * (d1 / d), f2 = k * (d2 / d);
+                fx += (float)f0; fy += (float)f1; fz += (float)f2;
+                iv[0] += ind.stiffness / 3.0 * pen * pen * pen;
+                iv[1] += f0; iv[2] += f1; iv[3] += f2;
+                iv[4] += 1.0;
+                iv[5] += f0 * x0; iv[6] += f1 * x1; iv[7] += f2 * x2;
+                iv[8] += f0 * x1; iv[9] += f0 * x2; iv[10] += f1 * x2;
+            }
+        }
         reinterpret_cast<float4*>(e.f32)[i] = make_float4(fx, fy, fz, 0.0f);
         bad |= !(isfinite(fx) && isfinite(fy) && isfinite(fz));
         if (INTEG) {
@@ -254,7 +277,21 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
 #pragma unroll
         for (int k = 0; k < 15; ++k) vals[k] = k < 8 ? 0.5 * (double)acc[k] : (double)acc[k];
         block_partials<15>(vals, e.partials, SIM_RED_EPOT_PAIR);
+        double* ipart = e.partials + (size_t)gridDim.x * SIM_RED_SLOTS;
+        if (IND) block_partials<IND ? 11 : 1>(iv, ipart, 0);
         const bool last = last_block_finalize<15>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+        if (IND && last) {            // uniform across the block
+            __syncthreads();
+            partial_sums<11>(ipart, 0, SIM_RED_SLOTS, ind.out, 0);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double* r = e.red_out;
+                r[SIM_RED_EPOT_PAIR] += ind.out[0];
+                r[SIM_RED_VIRIAL] += ind.out[5] + ind.out[6] + ind.out[7];
+                for (int k = 0; k < 6; ++k) r[SIM_RED_W_XX + k] += ind.out[5 + k];
+                for (int k = 1; k < 4; ++k) ind.out[k] = -ind.out[k];   // force on the indenter
+            }
+        }
         if (INTEG == 2 && last) {     // uniform across the block
             if (threadIdx.x == 0) {
                 ip.step_ctr[1] = step;
@@ -320,6 +357,10 @@ static void eam_set_attributes() {
         allow_smem(k_eam_force<true, 0, false>);
         allow_smem(k_eam_force<true, 1, false>);
         allow_smem(k_eam_force<true, 2, false>);
+        allow_smem(k_eam_force<true, 1, true, true>);
+        allow_smem(k_eam_force<true, 2, true, true>);
+        allow_smem(k_eam_force<true, 1, false, true>);
+        allow_smem(k_eam_force<true, 2, false, true>);
         done = true;
     }
 }
@@ -370,16 +411,16 @@ extern "C" int sim_eam_density(const SimEngine* ep, const SimEAMTables* tp, void
     return launch_status("sim_eam_density");
 }
 
-template <bool SINGLE, int INTEG, bool ORTHO>
+template <bool SINGLE, int INTEG, bool ORTHO, bool IND = false>
 static int launch_force(const SimEngine& e, const SimEAMTables& t, const SimIntegrator& ip, const StepEnd& end,
-                        cudaStream_t st) {
+                        cudaStream_t st, const SimIndenter& ind = SimIndenter{}) {
     const size_t smem = SINGLE ? smem_pass2(t) : 0;
     const int threads = force_threads(e);
     if (threads < 0) return SIM_ERR_ARG;
-    const int g = persistent_grid((const void*)k_eam_force<SINGLE, INTEG, ORTHO>, threads, smem, e.n);
-    if (g > e.n_blocks_max) return SIM_ERR_ARG;
-    const cudaError_t err = launch_pdl(k_eam_force<SINGLE, INTEG, ORTHO>, dim3(g), dim3(threads), smem, st, e, t, ip,
-                                       table_window(t), end);
+    const int g = persistent_grid((const void*)k_eam_force<SINGLE, INTEG, ORTHO, IND>, threads, smem, e.n);
+    if (g * (IND ? 2 : 1) > e.n_blocks_max) return SIM_ERR_ARG;   // IND: a second set of block partials
+    const cudaError_t err = launch_pdl(k_eam_force<SINGLE, INTEG, ORTHO, IND>, dim3(g), dim3(threads), smem, st, e, t,
+                                       ip, table_window(t), end, ind);
     if (err != cudaSuccess) { set_cuda_error(err, "sim_eam_force: launch"); return SIM_ERR_CUDA; }
     return SIM_OK;
 }
@@ -459,6 +500,32 @@ extern "C" int sim_eam_step_drift(const SimEngine* ep, const SimEAMTables* tp, c
     StepCtx c{ep, tp, ip, StepEnd{extra, log, (int)n_extra, (int)log_capacity, 0, 0}};
     return launch_if_cond((cudaStream_t)stream, step_pass2, step_rebuild_body, step_rebuild_eager, &c,
                           "sim_eam_step_drift");
+}
+
+extern "C" int sim_eam_force_integrate_indenter(const SimEngine* ep, const SimEAMTables* tp,
+                                                const SimIntegrator* ip, const SimIndenter* ind, int32_t mode,
+                                                void* stream) {
+    if (!ep || !tp || !ip || !ind || ep->n <= 0 || !ep->posfp || !valid_tables(*tp) || (mode != 1 && mode != 2))
+        return SIM_ERR_ARG;
+    if (!ind->center || !ind->out || !(ind->radius >= 0.0) || !ip->step_ctr || (ip->langevin && !ip->rff))
+        return SIM_ERR_ARG;
+    const SimEngine& e = *ep;
+    const SimEAMTables& t = *tp;
+    if (t.n_types != 1 || smem_pass2(t) > kSmemLimit || tiled_eam_usable(e, t)) {
+        set_error_text("sim_eam_force_integrate_indenter: one element type, untiled kernels only");
+        return SIM_ERR_ARG;
+    }
+    eam_set_attributes();
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if (mode == 1)
+        rc = e.box_orthogonal ? launch_force<true, 1, true, true>(e, t, *ip, StepEnd{}, st, *ind)
+                              : launch_force<true, 1, false, true>(e, t, *ip, StepEnd{}, st, *ind);
+    else
+        rc = e.box_orthogonal ? launch_force<true, 2, true, true>(e, t, *ip, StepEnd{}, st, *ind)
+                              : launch_force<true, 2, false, true>(e, t, *ip, StepEnd{}, st, *ind);
+    if (rc != SIM_OK) return rc;
+    return launch_status("sim_eam_force_integrate_indenter");
 }
 
 extern "C" int sim_eam_forces(const SimEngine* ep, const SimEAMTables* tp, void* stream) {

@@ -354,6 +354,16 @@ class MDEngine:
         self._last_force_precision = 0
         self.forces_valid = True
 
+    def eam_forces_integrate_indenter(self, tables, integ, indenter_ref, mode: int):
+        """EAM pass 1, then pass 2 with a spherical indenter's force added before
+        the integrator epilogue: mode 1 the second half-step, mode 2 also the
+        next step's first half."""
+        _lib.call("sim_eam_density", self.st_ref, tables.ref, self.stream)
+        _lib.call("sim_eam_force_integrate_indenter", self.st_ref, tables.ref, integ.ref, indenter_ref, int(mode),
+                  self.stream)
+        self._last_force_precision = 0
+        self.forces_valid = True
+
     def eam_step_drift(self, tables, integ):
         """eam_forces_integrate_drift + log_step(after_drift=True) +
         rebuild_if_needed, with the log row and the rebuild decision made by

@@ -96,6 +96,11 @@ class EAMForceCUDAExt(BackboneInterface):
         in one pass over the atoms."""
         self.molecular.engine.eam_forces_integrate_drift(self.tables, integrator.params)
 
+    def compute_finish_with_indenter(self, integrator, indenter, mode: int):
+        """Forces with a SphericalIndenterForce added in the same pass, and the
+        integrator's second half (mode 1) or both half-steps (mode 2)."""
+        self.molecular.engine.eam_forces_integrate_indenter(self.tables, integrator.params, indenter._ref, mode)
+
     def step_and_drift(self, integrator):
         """compute_finish_and_drift, the step's log row and the conditional
         list rebuild, with the last two decided inside the force pass."""

@@ -74,7 +74,21 @@ class BaseModel(nn.Module):
         self._graphs = {}
 
     # one step, launches only (no host sync)
+    def _indenter_fused(self):
+        """(EAM backbone, indenter) when the pair can run as one force pass with
+        the integrator fused (one element type, FP32 pairs, no barostat)."""
+        bb = self.sum_bone.backbones
+        if (self.barostat is not None or len(bb) != 2 or not hasattr(bb[0], "compute_finish_with_indenter")
+                or not hasattr(bb[1], "add_to_engine") or not hasattr(self.Integrator, "params")
+                or self.engine.use_tiles or getattr(bb[0], "E", 0) != 1 or bb[0].force_precision != 0):
+            return None
+        return bb[0], bb[1]
+
     def _forces_and_second_half(self):
+        pair = self._indenter_fused()
+        if pair is not None:
+            pair[0].compute_finish_with_indenter(self.Integrator, pair[1], 1)
+            return
         fused = getattr(self.sum_bone.backbones[0], "compute_and_finish", None) if self.sum_bone.single else None
         if fused is not None and hasattr(self.Integrator, "params"):
             fused(self.Integrator)        # EAM: second half fused into pass 2
@@ -113,6 +127,16 @@ class BaseModel(nn.Module):
                 else:
                     self.barostat.step(self.Integrator.dt)
                 self.engine.log_step()
+            return
+        pair = self._indenter_fused() if k > 1 else None
+        if pair is not None:     # EAM + indenter: the indenter inside the drift-fused force pass
+            eam, ind = pair
+            self.Integrator.first_half()
+            for s in range(k):
+                eam.compute_finish_with_indenter(self.Integrator, ind, 2 if s < k - 1 else 1)
+                self.engine.log_step(after_drift=s < k - 1)
+                if s < k - 1:
+                    self.engine.rebuild_if_needed()
             return
         if k <= 1 or not self._drift_fusable():
             for _ in range(k):

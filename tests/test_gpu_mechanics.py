@@ -166,7 +166,8 @@ def test_indenter_backbone_matches_reference(sb, tmp_path):
 def test_indenter_alone_and_with_eam_in_graphs(sb, tmp_path):
     """The indenter as the only backbone (forces against the FP64
     restatement), and EAM + indenter stepped eagerly and through CUDA graphs
-    with the centre changed between replays: identical states."""
+    with the centre changed between replays (the indenter inside EAM pass 2)
+    and by the separate kernels: identical states."""
     from oracle.integrator import indenter
     from simulon_b200.mechanics import SphericalIndenterForce
     x, L = oin.bcc_lattice(6)
@@ -188,22 +189,39 @@ def test_indenter_alone_and_with_eam_in_graphs(sb, tmp_path):
     pot = oi.write_fs_w_setfl(str(tmp_path / "W.eam.fs"))
     parser = sb.EAMParser(pot)
     res = []
-    for graph in (False, True):
-        p = oi.write_xyz(str(tmp_path / f"w{int(graph)}.xyz"), x, "W")
+    # eager model steps and graph runs (both with the indenter inside EAM pass
+    # 2), and the separate kernels: force field, indenter, integrator halves
+    for mode in ("eager", "graph", "separate"):
+        p = oi.write_xyz(str(tmp_path / f"w_{mode}.xyz"), x, "W")
         mol = sb.AtomFileReader(p, L, parser.cutoff, device=DEV, skin_thickness=0.5, is_fs=True)
         mol.atom_velocities = torch.tensor(oi.maxwell_boltzmann(np.full(len(x), oi.W_MASS), 300.0, 4), device=DEV)
         integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NVE")
         ind = SphericalIndenterForce(mol, radius=3.0, stiffness=1.0, center=c)
-        model = sb.BaseModel(sb.SumBackboneInterface([sb.EAMForceCUDAExt(parser, mol), ind], mol), integ, mol)
+        ff = sb.EAMForceCUDAExt(parser, mol)
+        model = sb.BaseModel(sb.SumBackboneInterface([ff, ind], mol), integ, mol)
+        eng = mol.engine
+        if mode == "separate":
+            model.sum_bone.compute()
         for chunk in range(4):
             ind.set_center(c - np.array([0.0, 0.0, 0.1 * chunk]))
-            if graph:
+            if mode == "graph":
                 model.run(5, graph_steps=5)
-            else:
+            elif mode == "eager":
                 for _ in range(5):
                     model()
+            else:
+                for _ in range(5):
+                    eng.integrate_first(integ.params, 0)
+                    eng.rebuild_if_needed()
+                    eng.eam_forces(ff.tables)
+                    ind.add_to_engine(0)
+                    eng.integrate_second(integ.params, 0)
+                    eng.log_step()
         torch.cuda.synchronize()
-        res.append((mol.coordinates.cpu(), mol.atom_velocities.cpu(), ind.out.cpu()))
-        assert mol.engine.status() == 0
+        res.append((mol.coordinates.cpu(), mol.atom_velocities.cpu(), ind.out.cpu(), eng.red_out.cpu()))
+        assert eng.status() == 0
     assert torch.equal(res[0][0], res[1][0]) and torch.equal(res[0][1], res[1][1])
     assert torch.equal(res[0][2], res[1][2]) and res[0][2][4] > 0
+    assert torch.equal(res[0][0], res[2][0]) and torch.equal(res[0][1], res[2][1])
+    np.testing.assert_allclose(res[0][2].numpy(), res[2][2].numpy(), rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(res[0][3].numpy()[:10], res[2][3].numpy()[:10], rtol=1e-6, atol=1e-6)
