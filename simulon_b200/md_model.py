@@ -112,8 +112,10 @@ class BaseModel(nn.Module):
         """k steps, launches only.  For EAM without a barostat the first half of
         step s+1 runs inside step s's force pass (same arithmetic, one pass over
         the atoms fewer per step); the last step ends with full-step velocities.
-        With a Berendsen barostat the atoms' scaling of step s runs inside step
-        s+1's first half; the last step scales them itself."""
+        With a spherical indenter as EAM's second backbone, the indenter's force
+        is added inside that pass.  With a Berendsen barostat the atoms'
+        scaling of step s runs inside step s+1's first half; the last step
+        scales them itself."""
         if k > 1 and not self._drift_fusable() and callable(getattr(self.barostat, "deferred_first_half", None)) \
                 and hasattr(self.Integrator, "params"):
             for s in range(k):
