@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import threading
 import time
 from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
@@ -75,6 +76,7 @@ class MDSimulator:
         self._writer = None      # one background thread writes the files in step order
         self._formatters = None  # threads formatting the blocks of one trajectory frame
         self._jobs = []
+        self._profile_lock = threading.Lock()   # output_time is added to from both threads
         if self.output_enabled:
             self.output_dir.mkdir(parents=True, exist_ok=True)
             if any_traj:
@@ -179,7 +181,8 @@ class MDSimulator:
                     f.write(part)
         if "f" in item:
             torch.save(item["f"].clone(), os.path.join(self._paths["forces_dir"], f"forces_{step_i:06d}.pt"))
-        self.sim_profile["output_time"] += time.perf_counter() - t0
+        with self._profile_lock:
+            self.sim_profile["output_time"] += time.perf_counter() - t0
 
     def _write_ready(self, wait: bool = False):
         """Hand every staged output whose copies have landed to the writer
@@ -251,7 +254,8 @@ class MDSimulator:
                 if self.verbose:
                     print(f"Step {step}/{self.num_steps}:Tot_E={pot + kin:.4f} ev, Pot_E = {pot:.4f} ev, "
                           f"Kin_E = {kin:.4f} ev, T = {temp:.4f} K")
-                self.sim_profile["output_time"] += time.perf_counter() - t_out
+                with self._profile_lock:
+                    self.sim_profile["output_time"] += time.perf_counter() - t_out
         if self.output_enabled:
             self._write_ready(wait=True)
         torch.cuda.synchronize(self.device)
