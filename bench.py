@@ -42,8 +42,8 @@ A_W, M_W = 3.165, 183.84
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=300)
-    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=40)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--n", type=int, default=80, help="BCC cells per side (atoms = 2 n^3)")
     p.add_argument("--graph-steps", type=int, default=20)
@@ -96,7 +96,12 @@ def mb_velocities(n_atoms, T, seed):
 
 
 class ClockSampler:
-    """nvidia-smi samples during the timed region (clocks, power, throttle reasons)."""
+    """nvidia-smi samples during the timed region (clocks, power, throttle reasons).
+
+    Entering waits (up to 3 s) for the first sample, so that sampling runs
+    before the timed work starts; the summary keeps the samples taken between
+    entering and leaving (the nearest later one if the region was shorter
+    than the 100 ms sampling interval, reported with "in_region": 0)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -110,20 +115,30 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", self.gpu_id], stdout=subprocess.PIPE,
+                                          "-lms", "100", "-i", self.gpu_id], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            give_up = time.monotonic() + 3.0
+            while not self.lines and self.proc.poll() is None and time.monotonic() < give_up:
+                time.sleep(0.005)
         except (OSError, ValueError):
             self.proc = None
+        self.t0 = time.monotonic()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def __exit__(self, *exc):
+        self.t1 = time.monotonic()
         if self.proc is not None:
+            # one more sample when the region was shorter than the interval
+            give_up = self.t1 + 0.3
+            while not any(t >= self.t1 for t, _ in self.lines) and self.proc.poll() is None \
+                    and time.monotonic() < give_up:
+                time.sleep(0.005)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -133,7 +148,10 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", float("inf"))
+        inside = [line for t, line in self.lines if t0 <= t <= t1]
+        later = [line for t, line in self.lines if t > t1][:1]
+        for line in inside or later:
             parts = [s.strip() for s in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -146,9 +164,9 @@ class ClockSampler:
                 if val.lower().startswith("active"):
                     reasons.add(name)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "in_region": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "in_region": len(sm) if inside else 0}
 
 
 def measured_peaks(key: str = "hbm_gbs"):

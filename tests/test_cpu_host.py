@@ -199,3 +199,28 @@ def test_package_references_resolve():
         val = int(re.search(rf"#define {name}\s+(\d+)", hdr).group(1))
         assert getattr(_lib, name) == val, name
     assert engine.TILE == int(re.search(r"#define SIM_TILE\s+(\d+)", hdr).group(1))
+
+
+def test_clock_summary_keeps_samples_of_the_timed_region():
+    """The bench's clock record: samples between entering and leaving the
+    timed region, the next later one when the region was shorter than the
+    sampling interval, throttle reasons from the "Active" columns."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+
+    def row(mhz, power_cap="Not Active", thermal="Not Active"):
+        return f"0, {mhz}, 1965, 700.0, 0x0, Not Active, Not Active, {thermal}, {power_cap}"
+
+    c = bench.ClockSampler("GPU-x")
+    c.t0, c.t1 = 10.0, 11.0
+    c.lines = [(9.9, row(300)), (10.2, row(1965)), (10.5, row(1900, power_cap="Active")), (10.8, row(1965)),
+               (11.1, row(300, thermal="Active"))]
+    s = c.summary()
+    assert s == {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3, "in_region": 3}
+    c.lines = [(9.9, row(300)), (11.05, row(1950)), (11.15, row(1000))]
+    s = c.summary()
+    assert s["sm_mhz"] == 1950.0 and s["samples"] == 1 and s["in_region"] == 0
+    c.lines = []
+    assert c.summary()["samples"] == 0
