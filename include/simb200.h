@@ -468,7 +468,8 @@ int sim_engine_half_count(const SimEngine* e, double rc2, int64_t* row_ptr, void
 int sim_engine_half_fill(const SimEngine* e, double rc2, const int64_t* row_ptr,
                          int64_t* edge_i, int64_t* edge_j, double* dist, void* stream);
 
-/* Exclusive scan helper used by the wrappers: out[0]=0, out[k+1]=sum in[0..k]. */
+/* Exclusive scan of int64 counts: out[0]=0, out[k+1]=sum in[0..k] (n+1 entries;
+ * in may be NULL when n = 0). */
 int sim_scan_i64(const int64_t* in, int64_t n, int64_t* out, void* stream);
 
 /* ==== group 3: batched replicas ========================================== *

@@ -731,7 +731,7 @@ extern "C" int sim_engine_half_fill(const SimEngine* ep, double rc2, const int64
 }
 
 extern "C" int sim_scan_i64(const int64_t* in, int64_t n, int64_t* out, void* stream) {
-    if (!in || !out || n < 0) return SIM_ERR_ARG;
+    if (!out || n < 0 || (n > 0 && !in)) return SIM_ERR_ARG;   // n = 0: out[0] = 0, in may be NULL
     k_scan_exclusive<int64_t><<<1, 1024, 0, (cudaStream_t)stream>>>(in, n, out, nullptr, nullptr);
     return launch_status("sim_scan_i64");
 }

@@ -58,6 +58,8 @@ def test_argument_errors_are_reported_without_gpu(lib):
     assert lib.sim_berendsen_mu(None, None, None, None) == _lib.SIM_ERR_ARG
     assert lib.sim_berendsen_scale_first(None, None, None, None, 0, None) == _lib.SIM_ERR_ARG
     assert lib.sim_eam_force_integrate_indenter(None, None, None, None, 1, None) == _lib.SIM_ERR_ARG
+    assert lib.sim_scan_i64(None, 5, None, None) == _lib.SIM_ERR_ARG
+    assert lib.sim_scan_i64(None, -1, None, None) == _lib.SIM_ERR_ARG
     e, p, ip = _lib.SimEngine(), _lib.SimLJParams(), _lib.SimIntegrator()
     e.n = 10
     for mode in (0, 3):   # only 1 (second half) and 2 (with the next first half)

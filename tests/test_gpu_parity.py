@@ -90,6 +90,20 @@ def test_engine_list_export_matches_oracle(sb):
     assert torch.equal(eng.gather("x").cpu(), torch.tensor(x))
 
 
+@pytest.mark.parametrize("n", [0, 1, 31, 8192, 8193, 100_003])
+def test_scan_i64_matches_cumsum(sb, n):
+    """sim_scan_i64: out[0] = 0, out[k+1] = in[0] + ... + in[k], exact in int64,
+    across the 8192-entry tiles of its one-block loop."""
+    from simulon_b200 import _lib
+    rng = np.random.default_rng(n)
+    counts = rng.integers(0, 1 << 40, size=n, dtype=np.int64)
+    src = torch.tensor(counts, device=DEV)
+    out = torch.full((n + 1,), -1, dtype=torch.int64, device=DEV)
+    _lib.call("sim_scan_i64", _lib.ptr(src), n, _lib.ptr(out), torch.cuda.current_stream().cuda_stream)
+    want = np.concatenate([[0], np.cumsum(counts)])
+    assert np.array_equal(out.cpu().numpy(), want)
+
+
 # ---------------------------------------------------------------- EAM
 def _eam_engine(sb, fsw_path, x, H, v=None):
     parser = sb.EAMParser(fsw_path)
