@@ -357,13 +357,15 @@ int sim_eam_step_drift(const SimEngine* e, const SimEAMTables* t, const SimInteg
  *   to the force pass, the reduction partials and the last-block counters come
  *   from one fixed 4,456,704-byte array inside the library; e->posfp,
  *   e->partials, e->red_counter and e->n_blocks_max are ignored (may be NULL /
- *   0).  Every other SimEngine buffer and the outputs (f32 or f64, red_out,
- *   flags) are the caller's, as for sim_eam_forces.
+ *   0).  e->cut_mask is ignored as well (neither read nor written; the force
+ *   pass tests every list entry against the cutoff instead, same results).
+ *   Every other SimEngine buffer and the outputs (f32 or f64, red_out, flags)
+ *   are the caller's, as for sim_eam_forces.
  *   Limit: e->n_pad <= SIM_STATIC_MAX_ATOMS; a larger system returns
  *   SIM_ERR_ARG before any CUDA call, with the reason in sim_last_cuda_error().
- *   Set-up: the first call on each device looks up the array's device address
- *   (cudaGetSymbolAddress, that device current); make it before any stream
- *   capture.  Each call zeroes the counters itself (cudaMemsetAsync on
+ *   Set-up: every call looks up the array's device address on the current
+ *   device (cudaGetSymbolAddress); the first call on a device also loads the
+ *   array there, so make it before any stream capture.  Each call zeroes the counters itself (cudaMemsetAsync on
  *   `stream`); nothing else has to start at zero.
  *   Concurrency: one array per device, shared by all calls -- calls that can
  *   overlap (other streams or host threads on the same device) race on it;

@@ -122,6 +122,59 @@ def write_fs_w_setfl(path, n_rho: int = 5000, d_rho: float = 0.012,
     return str(path)
 
 
+# Two-element Finnis-Sinclair variant (elements W and Li, the second a scaled
+# copy of the first): F_b(rho) = -A_b sqrt(rho); the density that a neighbour
+# of element a contributes to a host of element b is s[a][b] (r-d)^2, with an
+# asymmetric s so that a swapped [host, neighbour] index shows; pair terms
+# p_ab phi(r).  Used to check multi-element table indexing.
+FS_2E = dict(elements=("W", "Li"), A=(1.896373, 1.70673), s=((1.0, 0.85), (0.7, 0.9)),
+             p=((1.0, 0.9), (0.9, 0.8)))
+
+
+def write_fs_two_element_setfl(path, n_rho: int = 5000, d_rho: float = 0.012,
+                               n_r: int = 5000, d_r: float = 4.4 / 5000, cutoff: float = 4.4):
+    """Write the two-element FS potential of FS_2E in eam/fs layout (per
+    element b: F_b, then the density blocks for neighbour a = 0, 1; then the
+    pair blocks (0,0), (0,1), (1,1) as r*phi); returns the path."""
+    rk = np.arange(n_r) * d_r
+    rhok = np.arange(n_rho) * d_rho
+    f = fs_w_functions(r=rk)
+    sq = np.sqrt(rhok)
+    lines = ["synthetic two-element Finnis-Sinclair (eam/fs layout)",
+             "scaled copies of phi=(r-c)^2(c0+c1 r+c2 r^2), rho=(r-d)^2, F=-A sqrt(rho)",
+             "elements W, Li",
+             "2 W Li",
+             f"{n_rho} {d_rho!r} {n_r} {d_r!r} {cutoff!r}"]
+    blocks = []
+    for b, (el, mass) in enumerate(((FS_2E["elements"][0], W_MASS), (FS_2E["elements"][1], 6.94))):
+        lines_b = [f"{74 if b == 0 else 3} {mass} {W_A} bcc"]
+        data = [-FS_2E["A"][b] * sq] + [FS_2E["s"][a][b] * f["rho"] for a in range(2)]
+        blocks.append((lines_b, data))
+    for head, data in blocks:
+        lines += head
+        for blk in data:
+            for i in range(0, len(blk), 5):
+                lines.append(" ".join(f"{v:.16e}" for v in blk[i:i + 5]))
+    for a in range(2):
+        for b in range(a, 2):
+            blk = FS_2E["p"][a][b] * rk * f["phi"]
+            for i in range(0, len(blk), 5):
+                lines.append(" ".join(f"{v:.16e}" for v in blk[i:i + 5]))
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    return str(path)
+
+
+def write_xyz_symbols(path, coords, symbols):
+    """XYZ file with one symbol per atom (round-trip precision)."""
+    coords = np.asarray(coords, dtype=np.float64)
+    with open(path, "w") as fh:
+        fh.write(f"{coords.shape[0]}\nmixed synthetic\n")
+        for s, (x, y, z) in zip(symbols, coords):
+            fh.write(f"{s} {float(x)!r} {float(y)!r} {float(z)!r}\n")
+    return str(path)
+
+
 def perfect_bcc_known_answer(a: float = W_A, p=FS_W):
     """Analytic E/atom of the perfect BCC lattice for the synthetic FS-W form.
 

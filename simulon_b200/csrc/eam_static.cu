@@ -18,13 +18,20 @@
 // cudaMemsetAsync on the caller's stream.  The partials and records are written
 // before they are read within the call, so nothing else needs clearing.
 //
-// The device address of the array is looked up once per device, with that
-// device current, by cudaGetSymbolAddress on the first call made there; make
-// that first call before any stream capture.  The array is one per device and
-// shared by every call: two calls that may overlap in time (different streams
-// or host threads on one device) race on it, and the caller must serialise them.
+// The device address of the array is looked up on every call, with the
+// caller's device current, by cudaGetSymbolAddress (a host-side lookup with no
+// stream work), so a device reset or a re-created primary context that moves
+// the array is followed.  The first call on a device also loads the array's
+// module there: make that first call before any stream capture.  The array is
+// one per device and shared by every call: two calls that may overlap in time
+// (different streams or host threads on one device) race on it, and the caller
+// must serialise them.
+//
+// The in-cutoff mask (e->cut_mask) is per-atom scratch as well, so it is not
+// used here: the density pass writes no mask and the force pass tests every
+// list entry against the cutoff itself, which visits the same pairs in the
+// same order and gives the same results.
 #include <cstdio>
-#include <mutex>
 #include "common.cuh"
 
 namespace simb200 {
@@ -38,33 +45,15 @@ static_assert(kRecordOffset % 256 == 0, "per-atom records must stay 256-byte ali
 
 static __device__ __align__(256) unsigned char g_eam_scratch[kScratchBytes];
 
-static constexpr int kMaxDevices = 64;
-static std::mutex g_scratch_mutex;
-static void* g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of g_eam_scratch on the current device (looked up once).
+// Device address of g_eam_scratch on the current device.
 static int scratch_on_current_device(void** out) {
-    int dev = -1;
-    cudaError_t err = cudaGetDevice(&dev);
-    if (err != cudaSuccess) {
-        set_cuda_error(err, "sim_eam_forces_static: cudaGetDevice");
+    void* p = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&p, g_eam_scratch);
+    if (err != cudaSuccess || !p) {
+        set_cuda_error(err, "sim_eam_forces_static: cudaGetSymbolAddress of the scratch array");
         return SIM_ERR_CUDA;
     }
-    if (dev < 0 || dev >= kMaxDevices) {
-        set_error_text("sim_eam_forces_static: device ordinal outside the 64 devices this library tracks");
-        return SIM_ERR_ARG;
-    }
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        err = cudaGetSymbolAddress(&p, g_eam_scratch);
-        if (err != cudaSuccess || !p) {
-            set_cuda_error(err, "sim_eam_forces_static: cudaGetSymbolAddress of the scratch array");
-            return SIM_ERR_CUDA;
-        }
-        g_scratch_ptr[dev] = p;
-    }
-    *out = g_scratch_ptr[dev];
+    *out = p;
     return SIM_OK;
 }
 
@@ -91,6 +80,7 @@ extern "C" int sim_eam_forces_static(const SimEngine* ep, const SimEAMTables* tp
     e.red_counter = reinterpret_cast<uint32_t*>(b);
     e.partials = reinterpret_cast<double*>(b + kCounterBytes);
     e.posfp = reinterpret_cast<int32_t*>(b + kRecordOffset);
+    e.cut_mask = nullptr;
     e.n_blocks_max = kStaticMaxBlocks;
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t err = cudaMemsetAsync(e.red_counter, 0, kCounterBytes, st);

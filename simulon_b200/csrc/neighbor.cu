@@ -23,7 +23,7 @@ namespace simb200 {
 // ---------------------------------------------------------------------------
 // single-block exclusive scan (cell counts, row counts); out has n+1 entries
 template <typename T>
-__global__ void k_scan_exclusive(const T* __restrict__ in, int64_t n, T* __restrict__ out,
+__global__ void k_scan_exclusive(const T* in, int64_t n, T* out,
                                  T* zero_after, const int32_t* gate) {
     if (gate && __ldg(gate) == 0) return;
     __shared__ T warp_tot[32];

@@ -194,11 +194,18 @@ class AtomFileReader:
 
     # ---- velocities (reader.py:292-339) ----------------------------------
     def set_maxwell_boltzmann_velocity(self, temperature):
-        kB = 8.617333262e-5
-        m = (self.atom_mass.to(self.dtype) * 1.036427e-4).unsqueeze(-1)
-        sigma = torch.sqrt(kB * torch.as_tensor(temperature, device=self.device, dtype=self.dtype) / m)
+        """v ~ N(0, kB T / m) per component from torch's generator on this
+        device, centre-of-mass momentum removed; the operations and their
+        order are those of reader.py:319-339, so a seeded draw gives the
+        reference's velocities bit for bit."""
+        kB_eV = 8.617333262e-5
+        MASS_CONV = 1.036427e-4
+        m_internal = (self.atom_mass * MASS_CONV).unsqueeze(-1)
+        sigma = torch.sqrt(kB_eV * temperature / m_internal)
         v = torch.randn((self.atom_count, 3), device=self.device, dtype=self.dtype) * sigma
-        v = v - (v * m).sum(0) / m.sum()
+        total_p = (v * m_internal).sum(dim=0)
+        total_m = m_internal.sum()
+        v = v - total_p / total_m
         self.engine.set_velocities(v)
 
     def create_velocity_gaussian(self, temperature, seed):

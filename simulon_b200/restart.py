@@ -7,8 +7,9 @@ virial_cache -- so the reference's ``load_checkpoint`` can read it, plus the
 engine's Philox step counter (``philox_step``), with which the Langevin noise
 of the resumed run continues exactly (the noise is keyed by seed, original
 atom index and step).  ``load_checkpoint(model, path)`` reads either
-layout (tensors only: ``weights_only=True``), reloads positions, velocities
-and box into the device state (cell sort and list build), restores the RNG
+layout (tensors only: ``weights_only=True``; the box from ``box_H``, or from
+``box_length`` as a cubic box when the reference wrote that key instead),
+reloads positions, velocities and box into the device state (cell sort and list build), restores the RNG
 states and the step counter, and returns the next step.  The forces of the
 restored positions are recomputed on the first step (the reference restores
 its force cache instead; both give the same forces).
@@ -44,8 +45,14 @@ def load_checkpoint(model, path: str | Path) -> int:
     ckpt = torch.load(path, map_location="cpu", weights_only=True)
     mol = model.molecular
     eng = model.engine
+    H = None
     if "box_H" in ckpt:
         H = np.asarray(ckpt["box_H"], np.float64)
+    elif "box_length" in ckpt:
+        # the reference's layout for a molecular without a Box object
+        # (restart.py:55-58): a cubic box of that side
+        H = np.diag([float(ckpt["box_length"])] * 3)
+    if H is not None:
         eng.set_box(H)
         if hasattr(mol, "box"):
             mol.box.H = torch.as_tensor(H)

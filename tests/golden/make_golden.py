@@ -1,9 +1,9 @@
 """Generate golden vectors by running the reference implementation itself.
 
 Run from the repository root in a container where the reference checkout is
-available (default path below, or SIMULON_REFERENCE=<dir>):
+available, giving its path as the argument or in SIMULON_REFERENCE:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference checkout>
 
 The reference is imported unmodified; two third-party imports it makes at
 module level but does not use on this path (pymatgen.core and
@@ -25,7 +25,7 @@ import torch
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-REF = os.environ.get("SIMULON_REFERENCE", "/root/reference")
+REF = os.environ.get("SIMULON_REFERENCE", "")
 
 from oracle import inputs as oin  # noqa: E402
 from oracle.philox import langevin_normals  # noqa: E402
@@ -369,22 +369,224 @@ def crack_cases(tmp):
           lower=lo.numpy(), sigma=sigma, projected=proj, threshold=1.0, bins=160, **res)
 
 
+class _NativeRecorder(types.ModuleType):
+    """Stands in for the reference's native module ``simulon_cuda`` while the
+    reference's own wrappers run: each call's arguments are recorded as the
+    wrapper passed them, and the outputs the call must produce are supplied
+    from the reference's pure-PyTorch evaluation of the same quantities
+    (``expect``), so that the wrapper carries on exactly as it would with a
+    correct native module."""
+
+    def __init__(self):
+        super().__init__("simulon_cuda")
+        self.calls = []
+        self.expect = {}
+
+    def configure_lj_smoothing(self, mode, rc, rs):
+        self.calls.append(("configure_lj_smoothing", dict(mode=int(mode), rc=float(rc), rs=float(rs))))
+
+    def lj_energy_force_cuda(self, pos, edge_index, sigma, epsilon, box_length):
+        self.calls.append(("lj_energy_force_cuda", dict(pos=pos.clone(), edge_index=edge_index.clone(),
+                                                        sigma=sigma.clone(), epsilon=epsilon.clone(),
+                                                        box_length=float(box_length))))
+        return [self.expect["energy"].reshape(1).float(), self.expect["forces"].float()]
+
+    def density_pass(self, distances, row_index, col_index, atom_types, density_table, inv_dr, n_r, rho_out):
+        self.calls.append(("density_pass", dict(distances=distances.clone(), row=row_index.clone(),
+                                                col=col_index.clone(), types=atom_types.clone(),
+                                                table_shape=np.array(density_table.shape),
+                                                inv_dr=float(inv_dr), n_r=int(n_r))))
+        rho_out += self.expect["rho"]
+
+    def force_pass(self, distances, dist_vec, row_index, col_index, atom_types, density_deriv_table,
+                   pair_deriv_table, dF_drho, inv_dr, n_r, forces_out):
+        self.calls.append(("force_pass", dict(distances=distances.clone(), dist_vec=dist_vec.clone(),
+                                              row=row_index.clone(), col=col_index.clone(),
+                                              types=atom_types.clone(), dF=dF_drho.clone(),
+                                              inv_dr=float(inv_dr), n_r=int(n_r))))
+        forces_out += self.expect["forces"]
+
+
+def _table_digest(t):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(t.detach().cpu().numpy().astype(np.float32)).tobytes()).hexdigest()
+
+
+def legacy_cases(tmp):
+    """Calls the reference's own wrappers make into the native module
+    (core/force/eam_force_cu.py:496-505,551-564 -> density_pass / force_pass;
+    core/force/lennard_jones_force_cu.py:53,74 -> configure_lj_smoothing /
+    lj_energy_force_cuda), recorded with their arguments and with the values
+    the calls must produce, taken from the reference's PyTorch evaluation of
+    the same step (EAMForceCUDAExt(use_extension=False) for rho after pass 1,
+    F'(rho) and the pass-2 forces; core/force/lennard_jones_force.py in FP64
+    for the LJ energy and forces on the wrapper's in-cutoff edges)."""
+    from io_utils.eam_parser import EAMParser
+    from core.md_model import BackboneInterface, BaseModel, SumBackboneInterface
+    from core.integrator.integrator import VerletIntegrator
+
+    rec = _NativeRecorder()
+    sys.modules["simulon_cuda"] = rec
+    from core.force.eam_force_cu import EAMForceCUDAExt
+
+    class _Paired(BackboneInterface):
+        """The pure-PyTorch forward supplies rho, F'(rho) and the forces; the
+        extension-path forward of a second instance records its native calls."""
+
+        def __init__(self, parser, mol):
+            super().__init__()
+            self.pure = EAMForceCUDAExt(parser, mol, use_extension=False)
+            # the wrapper takes its extension branch only when CUDA is
+            # available (eam_force_cu.py:325); report it available while the
+            # instance is built -- its tensors stay on the CPU
+            avail = torch.cuda.is_available
+            torch.cuda.is_available = lambda: True
+            try:
+                self.ext = EAMForceCUDAExt(parser, mol, use_extension=True)
+            finally:
+                torch.cuda.is_available = avail
+            assert self.ext.ext_mod is rec
+            orig = self.pure._interp_rho
+            self.cap = {}
+            self.evals = []
+            idx = self.pure.atom_type_indices
+
+            def spy(rho_i, i_type, deriv=False):
+                out = orig(rho_i, i_type, deriv)
+                m = idx == i_type
+                self.cap.setdefault("rho", torch.zeros(idx.shape[0]))[m] = rho_i
+                self.cap.setdefault("dF" if deriv else "F", torch.zeros(idx.shape[0]))[m] = out
+                return out
+            self.pure._interp_rho = spy
+
+        def forward(self):
+            self.cap = {}
+            ref = self.pure()
+            rec.expect = {"rho": self.cap["rho"].clone(), "forces": ref["forces"].clone()}
+            out = self.ext()
+            assert torch.equal(out["forces"], ref["forces"]) and float(out["energy"]) == float(ref["energy"])
+            rec.expect["dF"] = self.cap["dF"].clone()
+            rec.expect["out"] = {k: out[k].detach().clone() for k in ("energy", "virial", "virial_tensor")}
+            self.evals.append(dict(rec.expect))
+            return out
+
+    def eam_record(name, pot, coords, symbols, steps):
+        parser = EAMParser(pot, torch.device("cpu"))
+        path = oin.write_xyz_symbols(os.path.join(tmp, name + ".xyz"), coords, symbols)
+        mol = AtomFileReader_ref(path, float(L), parser.cutoff)
+        bb = _Paired(parser, mol)
+        arrays = dict(density_table=_table_digest(bb.pure.density_table),
+                      density_deriv_table=_table_digest(bb.pure.density_deriv_table),
+                      pair_table=_table_digest(bb.pure.pair_table),
+                      pair_deriv_table=_table_digest(bb.pure.pair_deriv_table),
+                      embed_table=_table_digest(torch.stack([bb.pure.embed_table[t] for t in range(bb.pure.E)])),
+                      embed_deriv_table=_table_digest(torch.stack([bb.pure.embed_deriv_table[t]
+                                                                   for t in range(bb.pure.E)])),
+                      embed_rho_min=np.array([bb.pure.embed_rho_min[t] for t in range(bb.pure.E)]),
+                      embed_drho=np.array([bb.pure.embed_drho[t] for t in range(bb.pure.E)]),
+                      embed_n=np.array([bb.pure.embed_n[t] for t in range(bb.pure.E)]),
+                      r_max=float(bb.pure.r_max), md_steps=steps)
+        integ = VerletIntegrator(mol, dt=0.002, ensemble="NVE")
+        mol.atom_velocities = torch.tensor(oin.maxwell_boltzmann(mol.atom_mass.numpy(), 300.0, 21),
+                                           dtype=torch.float32)
+        model = BaseModel(SumBackboneInterface([bb], mol), integ, mol)
+        rec.calls.clear()
+        for _ in range(steps):
+            model()            # the first step evaluates the forces twice (md_model.py:89-103)
+        assert len(rec.calls) == 2 * len(bb.evals)
+        for s, ev in enumerate(bb.evals):
+            (n1, d), (n2, f) = rec.calls[2 * s:2 * s + 2]
+            assert (n1, n2) == ("density_pass", "force_pass")
+            for k in ("distances", "row", "col", "table_shape", "inv_dr", "n_r"):
+                arrays[f"s{s}_d_{k}"] = d[k]
+            for k in ("distances", "dist_vec", "row", "col", "dF"):
+                arrays[f"s{s}_f_{k}"] = f[k]
+            arrays[f"s{s}_rho"] = ev["rho"]
+            arrays[f"s{s}_forces"] = ev["forces"]
+            for k, v in ev["out"].items():
+                arrays[f"s{s}_{k}"] = v
+        arrays["evaluations"] = len(bb.evals)
+        arrays["types"] = d["types"]
+        _save(name, **arrays)
+
+    def AtomFileReader_ref(path, box_length, cutoff):
+        from io_utils.reader import AtomFileReader
+        return AtomFileReader(filename=path, box_length=box_length, cutoff=cutoff, device=torch.device("cpu"),
+                              skin_thickness=0.5, is_fs=True)
+
+    x, L = oin.bcc_lattice(5)
+    eam_record("legacy_eam_w250_f32", oin.write_fs_w_setfl(os.path.join(tmp, "W_synthetic.eam.fs")),
+               oin.jitter(x, 0.05, 11), ["W"] * len(x), steps=3)
+    rng = np.random.default_rng(12)
+    sym = np.where(rng.random(len(x)) < 0.4, "Li", "W").tolist()
+    sym[0] = "W"
+    eam_record("legacy_eam_wli250_f32", oin.write_fs_two_element_setfl(os.path.join(tmp, "WLi_synthetic.eam.fs")),
+               oin.jitter(x, 0.05, 13), sym, steps=1)
+
+    # LJ: the CUDA wrapper for a two-species mixture in each smoothing mode
+    # (argon and a lighter species with neon-like parameters, labelled Cl
+    # because the reference's element table carries no neon charge); the
+    # expected values are the reference's FP64 PyTorch LJ on the same system
+    from core.force.lennard_jones_force import LennardJonesForce as LJTorch
+    from core.force.lennard_jones_force_cu import LennardJonesForce as LJCuda
+    xa, La = oin.fcc_lattice(3)
+    xa = oin.jitter(xa, 0.05, 14)
+    rng = np.random.default_rng(15)
+    sym = np.where(rng.random(len(xa)) < 0.35, "Cl", "Ar").tolist()
+    sym[0] = "Ar"
+    e_ar, s_ar, e_ne, s_ne = 0.0104, 3.405, 0.0031, 2.74
+    mix = {"epsilon": float(np.sqrt(e_ar * e_ne)), "sigma": 0.5 * (s_ar + s_ne)}
+    params = {"[0 0]": {"epsilon": e_ar, "sigma": s_ar}, "[0 1]": mix, "[1 0]": mix,
+              "[1 1]": {"epsilon": e_ne, "sigma": s_ne}}
+    path = oin.write_xyz_symbols(os.path.join(tmp, "arcl108.xyz"), xa, sym)
+    torch.set_default_dtype(torch.float64)
+    try:
+        from io_utils.reader import AtomFileReader
+        for mode in ("raw", "fs", "switch"):
+            mol = AtomFileReader(filename=path, box_length=La, cutoff=7.0, device=torch.device("cpu"),
+                                 parameter=params, skin_thickness=0.5)
+            mol.is_fs = mode == "fs"
+            mol.is_switch = mode == "switch"
+            ref = LJTorch(mol)()
+            rec.calls.clear()
+            rec.expect = {"energy": ref["energy"].detach().clone(), "forces": ref["forces"].detach().clone()}
+            out = LJCuda(mol)()
+            calls = dict(rec.calls)
+            lj = calls["lj_energy_force_cuda"]
+            cfg = calls["configure_lj_smoothing"]
+            _save(f"legacy_lj_arcl108_{mode}_f32", pos=lj["pos"], edge_index=lj["edge_index"], sigma=lj["sigma"],
+                  epsilon=lj["epsilon"], box_length=lj["box_length"], mode=cfg["mode"], rc=cfg["rc"], rs=cfg["rs"],
+                  energy=ref["energy"], forces=ref["forces"], virial=out["virial"],
+                  virial_tensor=out["virial_tensor"], n_list_edges=mol.graph_data.edge_index.shape[1])
+    finally:
+        torch.set_default_dtype(torch.float32)
+    del sys.modules["simulon_cuda"]
+
+
+GROUPS = {"neighbor": "neighbor_cases", "lj": "lj_cases", "eam": "eam_cases", "md": "md_cases",
+          "mech": "mech_cases", "indenter": "indenter_cases", "crack": "crack_cases", "legacy": "legacy_cases"}
+
+
 def main():
-    if not os.path.isdir(REF):
-        raise SystemExit(f"reference checkout not found at {REF}")
+    """make_golden.py [<reference checkout>] [group ...]: every group by default."""
+    args = sys.argv[1:]
+    ref = args.pop(0) if args and os.path.isdir(args[0]) else REF
+    if not ref or not os.path.isdir(ref):
+        raise SystemExit("usage: make_golden.py <reference checkout> [group ...] (or set SIMULON_REFERENCE); "
+                         f"groups: {' '.join(GROUPS)}")
+    unknown = [a for a in args if a not in GROUPS]
+    if unknown:
+        raise SystemExit(f"unknown group(s) {unknown}; groups: {' '.join(GROUPS)}")
+    globals()["REF"] = ref
     _stub_imports()
     import builtins
     quiet = builtins.print
     with tempfile.TemporaryDirectory() as tmp:
-        builtins.print = lambda *a, **k: None if str(a[0] if a else "").startswith("[EAM") else quiet(*a, **k)
+        builtins.print = lambda *a, **k: None if str(a[0] if a else "").startswith(("[EAM", "[LJ")) else \
+            quiet(*a, **k)
         try:
-            neighbor_cases(tmp)
-            lj_cases(tmp)
-            eam_cases(tmp)
-            md_cases(tmp)
-            mech_cases(tmp)
-            indenter_cases(tmp)
-            crack_cases(tmp)
+            for g in (args or list(GROUPS)):
+                globals()[GROUPS[g]](tmp)
         finally:
             builtins.print = quiet
 

@@ -90,6 +90,22 @@ def test_engine_list_export_matches_oracle(sb):
     assert torch.equal(eng.gather("x").cpu(), torch.tensor(x))
 
 
+def test_engine_half_count_row_offsets_in_place_scan(sb):
+    """sim_engine_half_count scans its per-row counts in place (counts in
+    row_ptr[1:], offsets into row_ptr): for 16,000 atoms the scan crosses
+    the 8192-entry tiles; offsets equal the cumulative sum of the oracle's
+    per-row pair counts."""
+    from simulon_b200 import _lib
+    x, L = oin.bcc_lattice(20)
+    x = oin.jitter(x, 0.05, 31)
+    eng = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], np.diag([L] * 3), 4.4, 0.5, device=DEV)
+    row_ptr = torch.full((eng.n + 1,), -7, device=DEV, dtype=torch.int64)
+    _lib.call("sim_engine_half_count", eng.st_ref, 4.9 ** 2, _lib.ptr(row_ptr), eng.stream)
+    o = onb.half_list(x, OracleBox(L), 4.9 ** 2)
+    want = np.concatenate([[0], np.cumsum(np.bincount(o["i"], minlength=len(x)))])
+    assert np.array_equal(row_ptr.cpu().numpy(), want)
+
+
 @pytest.mark.parametrize("n", [0, 1, 31, 8192, 8193, 100_003])
 def test_scan_i64_matches_cumsum(sb, n):
     """sim_scan_i64: out[0] = 0, out[k+1] = in[0] + ... + in[k], exact in int64,
@@ -542,3 +558,40 @@ def test_neighbor_overflow_is_detected_and_grown(sb, fsw_path):
     eng = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], np.diag([L] * 3), 4.4, 0.5, device=DEV, nbr_cap=8)
     assert eng.nbr_cap >= 26 and eng.status() & sb._lib.SIM_STATUS_OVERFLOW == 0
     assert eng.neighbor_stats()["max"] == 26
+
+
+# ------------------------------------------------ Maxwell-Boltzmann velocities
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_maxwell_boltzmann_velocities_match_reference_formula(sb, dtype):
+    """AtomFileReader.set_maxwell_boltzmann_velocity against the reference's
+    formula (io_utils/reader.py:319-339) restated here with the same seeded
+    torch generator: bit-equal velocities; centre-of-mass momentum zero to
+    round-off; the per-species kinetic temperature within 5% of the target
+    for 54,000 atoms of two masses (6,000 of the lighter one)."""
+    old = torch.get_default_dtype()
+    torch.set_default_dtype(dtype)
+    try:
+        coords, L = oin.bcc_lattice(30)       # 54,000 sites, every ninth one a lighter species
+        symbols = ["Ar" if k % 9 == 0 else "W" for k in range(len(coords))]
+        mol = sb.AtomFileReader.from_arrays(symbols, coords, L, 4.4, device=DEV, skin_thickness=0.5)
+        T = 523.0
+        torch.manual_seed(1234)
+        mol.set_maxwell_boltzmann_velocity(T)
+        v = mol.atom_velocities
+        # the reference's formula, same generator state
+        torch.manual_seed(1234)
+        m_internal = (mol.atom_mass * 1.036427e-4).unsqueeze(-1)
+        sigma = torch.sqrt(8.617333262e-5 * T / m_internal)
+        ref = torch.randn((mol.atom_count, 3), device=DEV, dtype=dtype) * sigma
+        ref = ref - (ref * m_internal).sum(dim=0) / m_internal.sum()
+    finally:
+        torch.set_default_dtype(old)
+    assert v.dtype == dtype and torch.equal(v, ref)
+    m = m_internal.double()
+    p = (v.double() * m).sum(0)
+    assert float(p.abs().max()) < (1e-9 if dtype == torch.float64 else 1e-4) * float((v.double().abs() * m).sum())
+    light = torch.tensor([s == "Ar" for s in symbols], device=DEV)
+    for sel in (light, ~light):
+        ke = 0.5 * float((m[sel] * v[sel].double() ** 2).sum())
+        t_kin = 2.0 * ke / (3.0 * int(sel.sum())) / 8.617333262e-5
+        assert abs(t_kin / T - 1.0) < 0.05, t_kin

@@ -60,6 +60,34 @@ def test_restart_continues_the_run(sb, tmp_path):
         torch.set_default_dtype(torch.float32)
 
 
+def test_restart_reads_box_length_layout(sb, tmp_path):
+    """A checkpoint in the reference's layout for a molecular without a Box
+    (key 'box_length' instead of 'box_H', io_utils/restart.py:55-58) restores
+    a cubic box of that side along with the positions."""
+    from simulon_b200.restart import load_checkpoint, save_checkpoint
+    torch.set_default_dtype(torch.float64)
+    try:
+        x, L = oin.fcc_lattice(3)
+        x = oin.jitter(x, 0.05, 0)
+        v = oin.maxwell_boltzmann(np.full(len(x), oin.AR_MASS), 94.4, 1)
+        model, mol = _lj_model(sb, tmp_path, x, L, v)
+        model()
+        ck = str(tmp_path / "restart.pt")
+        save_checkpoint(model, 0, ck)
+        ckpt = torch.load(ck, map_location="cpu", weights_only=True)
+        del ckpt["box_H"]
+        ckpt["box_length"] = 1.02 * L
+        torch.save(ckpt, ck)
+        model2, mol2 = _lj_model(sb, tmp_path, x, L, np.zeros_like(v))
+        assert load_checkpoint(model2, ck) == 1
+        np.testing.assert_allclose(model2.engine.box_matrix(), np.diag([1.02 * L] * 3), rtol=1e-14, atol=0)
+        np.testing.assert_array_equal(mol2.coordinates.cpu().numpy(), ckpt["coordinates"].numpy())
+        model2()
+        assert model2.engine.status() == 0
+    finally:
+        torch.set_default_dtype(torch.float32)
+
+
 def test_simulator_output_files(sb, tmp_path):
     """traj.xyz every 5 steps, energies.csv every step, forces every 10, over
     a 20-step graph-captured run: contents equal the device log and state."""

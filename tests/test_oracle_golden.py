@@ -252,3 +252,68 @@ def test_indenter_backbone_matches_reference():
     assert n == list(g["contact_atoms"])
     np.testing.assert_allclose(md.x.numpy(), g["x"], atol=1e-10)
     np.testing.assert_allclose(md.v.numpy(), g["v"], atol=1e-9)
+
+
+# ------------------------------------------------ native-module call records
+def _edge_lerp(tab, a, b, r, inv_dr, n_r):
+    """The native kernels' table lookup (cuda source/eam_cuda_ext_kernel.cu:9-18):
+    floor, clamp to n_r - 2, one lerp, FP32."""
+    x = r.astype(np.float32) * np.float32(inv_dr)
+    i = np.clip(np.floor(x).astype(np.int64), 0, n_r - 2)
+    t = x - i.astype(np.float32)
+    return tab[a, b, i] + t * (tab[a, b, i + 1] - tab[a, b, i])
+
+
+@pytest.mark.parametrize("name,writer", [("legacy_eam_w250_f32", oin.write_fs_w_setfl),
+                                         ("legacy_eam_wli250_f32", oin.write_fs_two_element_setfl)])
+def test_native_call_records_match_oracle_tables(tmp_path, name, writer):
+    """The oracle's FP32 tables equal the reference's bit for bit (one and two
+    elements, digests recorded from the reference), and the recorded pass-1 /
+    pass-2 inputs give the recorded rho and forces through the native
+    kernels' arithmetic restated here (rho 1e-6 relative, forces 5e-6 eV/A)."""
+    import hashlib
+    g = load(name)
+    t = oeam.EAMTables(oeam.parse_eam(writer(str(tmp_path / "pot.eam.fs"))), dtype=torch.float32)
+    for key, tab in (("density_table", t.density), ("density_deriv_table", t.density_deriv),
+                     ("pair_table", t.pair), ("pair_deriv_table", t.pair_deriv), ("embed_table", t.embed),
+                     ("embed_deriv_table", t.embed_deriv)):
+        dig = hashlib.sha256(np.ascontiguousarray(tab.numpy().astype(np.float32)).tobytes()).hexdigest()
+        assert dig == str(g[key]), key
+    D, DD, PD = t.density.numpy(), t.density_deriv.numpy(), t.pair_deriv.numpy()
+    types = g["types"]
+    for s in range(int(g["evaluations"])):
+        r, row, col = g[f"s{s}_d_distances"], g[f"s{s}_d_row"], g[f"s{s}_d_col"]
+        inv_dr, n_r = float(g[f"s{s}_d_inv_dr"]), int(g[f"s{s}_d_n_r"])
+        a, b = types[row], types[col]
+        rho = np.zeros(len(types))
+        np.add.at(rho, row, _edge_lerp(D, a, b, r, inv_dr, n_r))
+        np.add.at(rho, col, _edge_lerp(D, b, a, r, inv_dr, n_r))
+        assert np.max(np.abs(rho - g[f"s{s}_rho"]) / g[f"s{s}_rho"]) < 1e-6
+        dF = g[f"s{s}_f_dF"]
+        sc = (dF[row] * _edge_lerp(DD, a, b, r, inv_dr, n_r) + dF[col] * _edge_lerp(DD, b, a, r, inv_dr, n_r)
+              + _edge_lerp(PD, a, b, r, inv_dr, n_r))
+        fv = -sc[:, None] * g[f"s{s}_f_dist_vec"] / (r[:, None] + 1e-8)
+        F = np.zeros((len(types), 3))
+        np.add.at(F, row, fv)
+        np.add.at(F, col, -fv)
+        assert np.max(np.abs(F - g[f"s{s}_forces"])) < 5e-6
+
+
+@pytest.mark.parametrize("mode", ["raw", "fs", "switch"])
+def test_native_lj_call_records_match_oracle(mode):
+    """The LJ calls the wrapper makes (in-cutoff edges, per-edge FP32 sigma
+    and epsilon, smoothing mode) give the recorded FP64 reference energy and
+    forces through the oracle's LJ (energy 1e-6 relative, forces 1e-6 eV/A:
+    the positions were recorded as the FP32 copies the wrapper passes)."""
+    g = load(f"legacy_lj_arcl108_{mode}_f32")
+    L = float(g["box_length"])
+    pos = g["pos"].astype(np.float64)
+    i, j = g["edge_index"]
+    rij = pos[i] - pos[j]
+    rij -= L * np.round(rij / L)
+    assert np.all(np.sqrt((rij ** 2).sum(1)) <= 7.0)
+    out = lj_forward(torch.tensor(pos), torch.tensor(i), torch.tensor(j), torch.tensor(g["epsilon"]),
+                     torch.tensor(g["sigma"]), OracleBox(np.diag([L, L, L])), 7.0,
+                     mode=["raw", "fs", "switch"][int(g["mode"])], rs=float(g["rs"]) or None)
+    assert abs(float(out["energy"]) - float(g["energy"])) < 1e-6 * abs(float(g["energy"]))
+    assert np.max(np.abs(out["forces"].numpy() - g["forces"])) < 1e-6
