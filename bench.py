@@ -181,12 +181,29 @@ def measured_peaks(key: str = "hbm_gbs"):
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle port)
-def cpu_baseline(seconds: float, n_cells: int = 20):
-    """The oracle's restatement of the reference CPU path (FP32 EAM, as the
-    reference's EAM path; torch CPU ops, all host threads) on a bounded sample."""
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(seconds: float, n_cells: int = 80):
+    """The oracle's restatement of the reference CPU path (FP32 EAM, the
+    reference EAM path's only precision; torch CPU ops on all host threads)
+    on the bench's own workload, BCC W 2 n^3 atoms: force + integrate steps
+    timed for about ``seconds`` (at least two), the list built by the
+    oracle's cell search (proven pair-set equal to the reference's search);
+    the reference's own O(N^2) search is timed on 16,000 atoms by its C
+    restatement and extrapolated by N^2, reported separately."""
     import torch
     from oracle import eam as oeam
     from oracle import inputs as oin
+    from oracle import neighbor as onb
     from oracle.box import OracleBox
     from oracle.integrator import OracleMD
     threads = os.cpu_count() or 1
@@ -197,35 +214,131 @@ def cpu_baseline(seconds: float, n_cells: int = 20):
     x, L = bcc(n_cells)
     box = OracleBox(L)
     types = np.zeros(len(x), np.int64)
+    t_setup = time.perf_counter()
     md = OracleMD(x.astype(np.float32), mb_velocities(len(x), 300.0, 5).astype(np.float32), np.full(len(x), M_W),
                   box, lambda xx, i, j: oeam.eam_forward(xx, i, j, types, box, tables), cutoff=4.4, skin=0.5,
                   dt=0.002, ensemble="NVE", dtype=torch.float32)
-    md.step()                                   # warm-up
+    t_list = time.perf_counter() - t_setup
+    md.step()                                   # warm-up (first call: two force evaluations)
     steps, t0 = 0, time.perf_counter()
-    while time.perf_counter() - t0 < seconds or steps < 3:
+    while time.perf_counter() - t0 < seconds or steps < 2:
         md.step()
         steps += 1
     dt = time.perf_counter() - t0
+    # the reference's O(N^2) search (gpu_kdtree.py:90-155), its C restatement on 16,000 atoms
+    xs, Ls = bcc(20)
+    tb = time.perf_counter()
+    onb.half_list(xs.astype(np.float32), OracleBox(Ls), onb.rc2_like_reference(4.4, 0.5, np.float32), mode="brute")
+    t_brute = time.perf_counter() - tb
     return {"value": len(x) * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"oracle FP32 restatement of the reference CPU path (torch CPU), BCC W {len(x)} atoms, "
-                      f"{steps} NVE steps incl. its own list rebuilds, {dt:.1f} s"}
+            "cpu": cpu_model(),
+            "sample": f"oracle FP32 restatement of the reference CPU path (torch CPU, {threads} threads), BCC W "
+                      f"{len(x):,} atoms (the bench workload), {steps} NVE force + integrate steps in {dt:.1f} s "
+                      f"after one warm-up step, list by the oracle's cell search ({t_list:.1f} s incl. setup; "
+                      f"{md.rebuilds - 1} rebuilds inside the timed steps)",
+            "rebuild_o_n2_extrapolated_s": t_brute * (len(x) / len(xs)) ** 2,
+            "rebuild_note": f"the reference's O(N^2) pair search restated in C, {t_brute:.2f} s on {len(xs):,} atoms, "
+                            f"scaled by (N/{len(xs):,})^2 (extrapolated, not run)"}
+
+
+def oracle_force_rmse(x, H, f_gpu, tables64, seed: int, radius: float = 20.0, cutoff: float = 4.4):
+    """RMSE of the GPU forces against the FP64 oracle on the atoms within
+    ``radius`` of a seeded random point of the box (~2,000 atoms in bulk W):
+    the oracle evaluates the atoms within radius + 2 cutoffs of that point, so
+    the densities of the sampled atoms' neighbours are complete."""
+    import torch
+    from oracle import eam as oeam
+    from oracle import neighbor as onb
+    from oracle.box import OracleBox
+    box = OracleBox(H)
+    x = np.asarray(x, np.float64)
+    rng = np.random.default_rng(seed)
+    c = rng.random(3) @ np.asarray(H, np.float64)
+    d = np.linalg.norm(box.minimum_image(torch.tensor(x - c)).numpy(), axis=1)
+    inner = np.nonzero(d < radius)[0]
+    outer = np.nonzero(d < radius + 2.0 * cutoff + 0.1)[0]
+    if len(inner) == 0:
+        return None, 0
+    xs = x[outer]
+    hl = onb.half_list(xs, box, (cutoff * (1.0 + 1e-9)) ** 2, mode="brute" if len(xs) < 4096 else "auto")
+    o = oeam.eam_forward(torch.tensor(xs), hl["i"], hl["j"], np.zeros(len(xs), np.int64), box, tables64)
+    pos_in_outer = np.searchsorted(outer, inner)
+    err = np.asarray(f_gpu, np.float64)[inner] - o["forces"].numpy()[pos_in_outer]
+    return float(np.sqrt((err ** 2).mean())), int(len(inner))
+
+
+def oracle_checks(pot, checks):
+    """The oracle as the checker of the forms' forces (this CPU leg only):
+    force RMSE against the FP64 oracle for each recorded state."""
+    import torch
+    from oracle import eam as oeam
+    t64 = oeam.EAMTables(oeam.parse_eam(pot), dtype=torch.float64)
+    out = {}
+    for name, c in checks.items():
+        if name == "batched":
+            per = []
+            for k, (x, H, f) in enumerate(c):
+                r, n = oracle_force_rmse(x, H, f, t64, seed=100 + k)
+                if r is not None:
+                    per.append((r, n))
+            out[name] = {"max_replica_rmse_ev_per_a": max(r for r, _ in per),
+                         "mean_replica_rmse_ev_per_a": float(np.mean([r for r, _ in per])),
+                         "replicas_checked": len(per), "atoms_checked": int(sum(n for _, n in per))}
+        else:
+            x, H, f = c
+            r, n = oracle_force_rmse(x, H, f, t64, seed=7)
+            out[name] = {"rmse_ev_per_a": r, "atoms_checked": n}
+    return out
+
+
+def config1_cpu():
+    """Config 1 on the CPU: LJ argon 108 atoms (FCC 3^3, a 5.26 A, jitter 0.05 A
+    seed 0), FP64, Langevin 94.4 K gamma 10/ps, dt 2 fs, 1,000 steps through
+    the oracle's restatement of the reference step (torch CPU)."""
+    import torch
+    from oracle import inputs as oin
+    from oracle.box import OracleBox
+    from oracle.integrator import OracleMD
+    from oracle.lj import lj_forward
+    torch.set_num_threads(os.cpu_count() or 1)
+    x, L = oin.fcc_lattice(3)
+    x = oin.jitter(x, 0.05, 0)
+    v = oin.maxwell_boltzmann(np.full(len(x), oin.AR_MASS), 94.4, 1)
+    box = OracleBox(L)
+    eps = torch.tensor(0.0104, dtype=torch.float32)
+    sig = torch.tensor(3.405, dtype=torch.float32)
+    md = OracleMD(x, v, np.full(len(x), oin.AR_MASS), box,
+                  lambda xx, i, j: lj_forward(xx, i, j, eps.expand(len(i)), sig.expand(len(i)), box, 7.0),
+                  cutoff=7.0, skin=0.5, dt=0.002, ensemble="NVT", temperature=94.4, gamma=10.0,
+                  dtype=torch.float64, noise_fn=lambda step: torch.randn(len(x), 3, dtype=torch.float64))
+    for _ in range(5):
+        md.step()
+    t0 = time.perf_counter()
+    for _ in range(1000):
+        md.step()
+    dt = time.perf_counter() - t0
+    return {"value": len(x) * 1000 / dt, "unit": UNIT, "steps_per_s": 1000 / dt, "ms_per_step": dt,
+            "steps": 1000, "atoms": len(x), "kind": "port", "cores": os.cpu_count() or 1,
+            "workload": "LJ Ar FCC 3^3 = 108 atoms, FP64, Langevin 94.4 K gamma 10/ps, dt 2 fs, rc 7.0 A, skin 0.5 A"}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    # the oracle port on a 16,000-atom sample of the same workload, timed over
-    # the timed steps' share of a fixed two-minute budget (at least 3 MD steps)
-    seconds = 120.0 * args.steps / max(1, args.steps + args.warmup)
-    base = cpu_baseline(seconds=seconds, n_cells=20)
+    # the oracle port on the GPU arm's workload, timed over the timed steps'
+    # share of a fixed two-minute budget (at least two MD steps)
+    seconds = 90.0 * args.steps / max(1, args.steps + args.warmup)
+    base = cpu_baseline(seconds=seconds, n_cells=args.n)
     line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "EAM-W bulk BCC, synthetic FS potential, NVE 300 K, dt 2 fs, skin 0.5 A",
-                       "atoms": 16000},
+            "warmup": args.warmup, "ms_per_step": 1e3 * 2 * args.n ** 3 / base["value"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"EAM-W bulk BCC 2*{args.n}^3 = {2 * args.n ** 3:,} atoms, synthetic FS potential, "
+                                   "NVE from 300 K, dt 2 fs, skin 0.5 A", "atoms": 2 * args.n ** 3},
             "impl": "reference", "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_extras:
+        line["config1"] = config1_cpu()
     print(json.dumps(line), flush=True)
 
 
@@ -235,6 +348,75 @@ def eng_state_bytes(eng) -> int:
     import torch
     return sum(t.numel() * t.element_size() for t in (eng.x, eng.v, eng.posq, eng.posfp, eng.xref, eng.f32, eng.nbr,
                                                        eng.nnbr) if isinstance(t, torch.Tensor))
+
+
+def energy_drift(model, first: int, k: int, n_atoms: int, dt_ps: float):
+    """Least-squares slope of the total energy per atom (eV/atom/ns) over the
+    logged steps [first, first + k) (at most the log's capacity)."""
+    count, k = int(k), min(int(k), model.engine.log_capacity)
+    if k < 2:
+        return None
+    rows = model.step_log(first + count - k, k).cpu().numpy()
+    etot = (rows[:, 0] + rows[:, 1] + rows[:, 9]) / n_atoms
+    t_ns = np.arange(k) * dt_ps * 1e-3
+    return float(np.polyfit(t_ns, etot, 1)[0])
+
+
+def clock_window(gpu_id: str, fn, seconds: float = 1.5):
+    """Clock samples over repeats of the timed work (fn) for about `seconds`
+    right after the timed region, for runs whose timed region is shorter than
+    the sampler's 100 ms interval."""
+    import torch
+    with ClockSampler(gpu_id) as clocks:
+        t0 = time.monotonic()
+        reps = 0
+        while time.monotonic() - t0 < seconds:
+            fn()
+            torch.cuda.synchronize()
+            reps += 1
+    out = clocks.summary()
+    out["repeats"] = reps
+    return out
+
+
+def config1_gpu(sb, dev, G):
+    """Config 1 on the GPU: LJ argon 108 atoms (FCC 3^3, a 5.26 A, jitter 0.05 A
+    seed 0), FP64, Langevin 94.4 K gamma 10/ps, dt 2 fs, 1,000 steps through
+    BaseModel.run (graphs of G steps), timed with events."""
+    import torch
+    a = 5.26
+    g = np.arange(3)
+    cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    x = ((cells[:, None, :] + basis[None]).reshape(-1, 3) * a).astype(np.float64)
+    x = x + np.random.default_rng(0).normal(0.0, 0.05, size=x.shape)
+    L = 3 * a
+    m = 39.948 * 1.036427e-4
+    rng = np.random.default_rng(1)
+    v = rng.standard_normal(x.shape) * np.sqrt(8.617333262e-5 * 94.4 / m)
+    v -= v.mean(0)
+    old = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        mol = sb.AtomFileReader.from_arrays(["Ar"] * len(x), x, L, 7.0, device=dev, skin_thickness=0.5,
+                                            parameter={"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}})
+        integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NVT", temperature=(94.4, 94.4), gamma=10.0, seed=1)
+        mol.atom_velocities = torch.tensor(v, device=dev)
+        model = sb.BaseModel(sb.SumBackboneInterface([sb.LennardJonesForce(mol)], mol), integ, mol)
+    finally:
+        torch.set_default_dtype(old)
+    model.run(5 * G, graph_steps=G)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = model.run(1000, graph_steps=G)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"value": len(x) * 1000 / (ms / 1e3), "unit": UNIT, "steps_per_s": 1000 / (ms / 1e3),
+            "ms_per_step": ms / 1000, "steps": 1000, "atoms": len(x), "temperature_k": float(out["temperature"]),
+            "status": mol.engine.status(),
+            "workload": "LJ Ar FCC 3^3 = 108 atoms, FP64, Langevin 94.4 K gamma 10/ps, dt 2 fs, rc 7.0 A, skin 0.5 A"}
 
 
 def launches_for(steps: int, graph_steps: int) -> int:
@@ -332,6 +514,11 @@ def run_b200(args):
     status = eng.status()
     rebuilds = int(eng.flags[3].item()) - rb0
     value = world * N * args.steps / (ms / 1e3)
+    drift = energy_drift(model, model.steps_done - args.steps, args.steps, N, 0.002)
+    window = clock_window(gpu_id, lambda: model.run(args.steps, graph_steps=G)) if ms < 300 else None
+    # state for the oracle's force check (CPU leg): forces recomputed at the current positions
+    eng.eam_forces(ff.tables)
+    checks = {"plain": (eng.gather("x").cpu().numpy(), eng.box_matrix(), eng.gather("f").cpu().numpy())}
     nbr = eng.neighbor_stats()
     nbar = nbr["mean"]
 
@@ -391,7 +578,12 @@ def run_b200(args):
             "step_roofline": {"bytes_per_atom_step": B_step, "achieved": step_achieved, "peak": peak,
                               "frac": step_achieved / peak, "unit": "GB/s"},
             "clocks": clocks.summary(),
+            "energy_drift_ev_per_atom_per_ns": drift,
+            "energy_drift_steps": min(args.steps, eng.log_capacity),
             "gpu_launches": launches_for(args.steps, G) + 10 * rebuilds}
+    if window is not None:
+        line["clocks_window"] = dict(window, note="repeats of the timed steps for 1.5 s right after the timed "
+                                                 "region (the timed region is shorter than the 100 ms sampling)")
 
     if not args.no_extras and rank == 0:
         line["e2e"] = e2e(model, mol, x, v, args, dev)
@@ -400,20 +592,30 @@ def run_b200(args):
     if not args.no_mlp and "mlp" in forms:
         line["mlp"] = mlp_form(args, sb, pot, dev, world)
     if not args.no_batched and "batched" in forms:
-        line["batched"] = batched_form(args, sb, pot, dev, world, rank, barrier)
+        line["batched"] = batched_form(args, sb, pot, dev, world, rank, barrier, checks)
     if "variants" in forms:
-        line["eam_variants"] = eam_variants_form(args, sb, pot, dev, world)
+        line["eam_variants"] = eam_variants_form(args, sb, pot, dev, world, checks)
     if "mechanics" in forms and world == 1:
         line["mechanics"] = mechanics_form(args, sb, pot, dev, world)
+    if not args.no_extras and world == 1:
+        line["config1"] = config1_gpu(sb, dev, G)
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
         if not args.no_extras and world == 1:
-            line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+            # CPU leg: the timed baseline, then the oracle as the checker of the forces
+            line["cpu_baseline"] = cpu_baseline(args.cpu_seconds, n_cells=args.n)
+            rm = oracle_checks(pot, checks)
+            line["force_rmse_vs_fp64_ev_per_a"] = rm["plain"]["rmse_ev_per_a"]
+            line["force_check"] = rm["plain"]
+            if "batched" in rm and "batched" in line:
+                line["batched"]["force_rmse_vs_fp64"] = rm["batched"]
+            if "triclinic_nve" in rm and "eam_variants" in line:
+                line["eam_variants"]["triclinic_nve"]["force_rmse_vs_fp64"] = rm["triclinic_nve"]
         print(json.dumps(line), flush=True)
 
 
-def batched_form(args, sb, pot, dev, world, rank, barrier):
+def batched_form(args, sb, pot, dev, world, rank, barrier, checks=None):
     """Batched form: seeded sweep of crack slabs (BCC W, sizes log-uniform in
     [2,000, 250,000], temperatures 50..1200 K, Langevin gamma 10/ps, dt 1 fs,
     grips opening 1e-4 A/step; list skin 0.75 A by default -- a neighbour-list
@@ -454,6 +656,11 @@ def batched_form(args, sb, pot, dev, world, rank, barrier):
     rebuilds = be.rebuild_counts() - rb0
     events = int(be.flags[3].item()) - ev0
     status = be.status()
+    if checks is not None:       # per-replica state for the oracle's force check (CPU leg)
+        be.eam_forces(tables)
+        X, F = be.gather("x").cpu().numpy(), be.gather("f").cpu().numpy()
+        checks["batched"] = [(X[be.replica_slice(k)], np.asarray(be.replicas[k].H, np.float64).reshape(3, 3),
+                              F[be.replica_slice(k)]) for k in range(be.n_rep)]
     T = be.temperature().cpu()
     table = gather_replica_table(mine, torch.stack([T, torch.tensor(rebuilds, dtype=torch.float64)], 1),
                                  len(reps))
@@ -471,15 +678,13 @@ def batched_form(args, sb, pot, dev, world, rank, barrier):
             "replica_rebuilds_in_timed": int(table[:, 1].sum()),
             "temperature_k_min_max": [float(table[:, 0].min()), float(table[:, 0].max())],
             "gpu_launches": launches,
-            "force_rmse": "same pair arithmetic as the plain form (per-replica forces bit-identical to the "
-                          "single-system engine, tests/test_gpu_batch.py); plain form <= 1e-5 eV/A vs FP64",
             "config": {"workload": f"{len(reps)} BCC-W crack slabs, sizes log-uniform 2,000-250,000 (seeded), "
                                    "precrack L_x/4, 3-layer grips opening 1e-4 A/step, T 50-1200 K Langevin "
                                    f"gamma 10/ps, dt 1 fs, skin {args.batch_skin} A",
                        "parallelism": f"LPT over {world} rank(s)", "graph_steps": G}}
 
 
-def eam_variants_form(args, sb, pot, dev, world):
+def eam_variants_form(args, sb, pot, dev, world, checks=None):
     """The other EAM-W bulk cases of the plain form, 2 n^3 = 1,024,000 atoms:
     NVE in a triclinic box (rows (L,0,0), (0.02 L, L, 0), (0,0,L), the BCC
     sites sheared with it) and Berendsen NPT at P0 = 0 bar with a 300 K
@@ -532,6 +737,12 @@ def eam_variants_form(args, sb, pot, dev, world):
         row = {"value": world * N * args.steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.steps,
                "status": eng.status(), "rebuilds_in_timed": int(eng.flags[3].item()) - rb0,
                "temperature_k": float(outs["temperature"])}
+        if baro is None:
+            row["energy_drift_ev_per_atom_per_ns"] = energy_drift(model, model.steps_done - args.steps, args.steps, N,
+                                                                  0.002)
+            if checks is not None:
+                ff.compute()
+                checks[name] = (eng.gather("x").cpu().numpy(), eng.box_matrix(), eng.gather("f").cpu().numpy())
         if baro is not None:
             row["pressure_bar"] = float(baro.pressure())
             row["volume_change"] = abs(float(np.linalg.det(eng.box_matrix()))) / V0 - 1.0

@@ -386,6 +386,12 @@ int sim_lj_forces(const SimEngine* e, const SimLJParams* p, int32_t precision, v
  * step_ctr[1] to this step like sim_eam_force_integrate_drift. */
 int sim_lj_forces_integrate(const SimEngine* e, const SimLJParams* p, const SimIntegrator* integ, int32_t mode,
                             void* stream);
+/* FP32-pair LJ as a further force field of a sum (SumBackboneInterface.forward,
+ * core/md_model.py:39-46, which adds each backbone's forces, energy, virial
+ * and virial tensor into shared buffers): atom i's LJ force is added to
+ * e->f32, the pair energy, scalar virial (sum F r) and virial tensor to
+ * red_out.  Run after the first force field's pass (e.g. sim_eam_forces). */
+int sim_lj_forces_add(const SimEngine* e, const SimLJParams* p, void* stream);
 
 /* first_half: v += 0.5 a dt; x += v dt; refresh posq; skin/2 trigger -> flags[0].
  * force_precision: 0 reads f32, 1 reads f64. */

@@ -95,7 +95,7 @@ def half_list(pos: np.ndarray, box: OracleBox, rc2: float, mode: str = "auto"):
     ncell = grid if grid is not None else np.ones(3, np.int32)
     n = pos.shape[0]
     fn = getattr(lib, f"oracle_half_list_{suf}")
-    cap = max(16, int(n) * 64)
+    cap = max(16, int(n) * 32)          # grown (and the search rerun) when a row set needs more
     while True:
         oi = np.empty(cap, np.int64)
         oj = np.empty(cap, np.int64)

@@ -162,6 +162,7 @@ SIGNATURES = {
                            ctypes.c_int32, c_p],
     "sim_lj_forces": [_P(SimEngine), _P(SimLJParams), ctypes.c_int32, c_p],
     "sim_lj_forces_integrate": [_P(SimEngine), _P(SimLJParams), _P(SimIntegrator), ctypes.c_int32, c_p],
+    "sim_lj_forces_add": [_P(SimEngine), _P(SimLJParams), c_p],
     "sim_integrate_first": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_integrate_second": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_integrate_second_first": [_P(SimEngine), _P(SimIntegrator), ctypes.c_int32, c_p],

@@ -221,7 +221,8 @@ __device__ __forceinline__ void block_partials(double (&vals)[NV], double* parti
 // 32 compensated sums combine in a fixed tree (TwoSum of the sums, the
 // compensations added): the order depends only on the grid size.
 template <int NV>
-__device__ __forceinline__ void partial_sums(const double* partials, int slot0, int stride, double* out, int out0) {
+__device__ __forceinline__ void partial_sums(const double* partials, int slot0, int stride, double* out, int out0,
+                                             bool accumulate = false) {
     const int lane = threadIdx.x & 31, nw = (int)(blockDim.x >> 5);
     for (int k = (int)(threadIdx.x >> 5); k < NV; k += nw) {
         double s = 0.0, c = 0.0;   // value s - c
@@ -240,7 +241,7 @@ __device__ __forceinline__ void partial_sums(const double* partials, int slot0, 
             c = c + c2 - err;
             s = t;
         }
-        if (lane == 0) out[out0 + k] = s - c;
+        if (lane == 0) out[out0 + k] = accumulate ? out[out0 + k] + (s - c) : s - c;
     }
 }
 
@@ -249,10 +250,13 @@ __device__ __forceinline__ void partial_sums(const double* partials, int slot0, 
 // k: lane l adds rows l, l+32, ... with Kahan compensation, then the 32
 // compensated sums combine in a fixed tree (TwoSum of the sums, the
 // compensations added): the order depends only on the grid size.  Must be
-// called by every thread of every block (blockDim.x a multiple of 32).
+// called by every thread of every block (blockDim.x a multiple of 32).  With
+// `accumulate` the sums are added to what `out` holds (a further force field
+// of a sum of force fields) instead of replacing it.
 template <int NV>
 __device__ __forceinline__ bool last_block_finalize(double* partials, uint32_t* counter,
-                                                    double* out, int slot0, int stride = SIM_RED_SLOTS) {
+                                                    double* out, int slot0, int stride = SIM_RED_SLOTS,
+                                                    bool accumulate = false) {
     __shared__ bool is_last;
     __threadfence();
     __syncthreads();
@@ -263,7 +267,7 @@ __device__ __forceinline__ bool last_block_finalize(double* partials, uint32_t* 
     __syncthreads();
     if (!is_last) return false;
     __threadfence();
-    partial_sums<NV>(partials, slot0, stride, out, slot0);
+    partial_sums<NV>(partials, slot0, stride, out, slot0, accumulate);
     if (threadIdx.x == 0) *counter = 0u;
     return true;
 }

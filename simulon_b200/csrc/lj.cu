@@ -66,7 +66,10 @@ __device__ __forceinline__ void lj_pair(const SimLJParams& p, const LJConst& c, 
 // second half of the step (Langevin O-step, half kick, K and K tensor), and
 // with 2 also the next step's first half (kick, drift, posq refresh, skin/2
 // trigger; step_ctr[0] advanced, step_ctr[1] = this step).
-template <bool ORTHO, bool SINGLE, int INTEG>
+// ACC (with INTEG 0): LJ as a further force field of a sum
+// (SumBackboneInterface, core/md_model.py:39-46): atom i's LJ force is added
+// to the force already in e.f32 and the energy and virial sums to red_out.
+template <bool ORTHO, bool SINGLE, int INTEG, bool ACC = false>
 __global__ void __launch_bounds__(SIM_THREADS, LJ_MIN_BLOCKS) k_lj_f32(SimEngine e, SimLJParams p, SimIntegrator ip) {
     pdl_trigger();
     pdl_wait();   // positions, box and list come from earlier kernels
@@ -107,6 +110,10 @@ __global__ void __launch_bounds__(SIM_THREADS, LJ_MIN_BLOCKS) k_lj_f32(SimEngine
             rvec<ORTHO>(b, qi, qj, r0, r1, r2);
             lj_pair(p, SINGLE ? c1 : lj_const(p, ti * p.n_types + qj.w), rc, rc2, rs, r0, r1, r2, fx, fy, fz, acc);
         }
+        if (ACC) {
+            const float4 f0 = reinterpret_cast<const float4*>(e.f32)[i];
+            fx = f0.x + fx; fy = f0.y + fy; fz = f0.z + fz;
+        }
         reinterpret_cast<float4*>(e.f32)[i] = make_float4(fx, fy, fz, 0.0f);
         bad |= !(isfinite(fx) && isfinite(fy) && isfinite(fz));
         if (INTEG) {
@@ -139,7 +146,7 @@ __global__ void __launch_bounds__(SIM_THREADS, LJ_MIN_BLOCKS) k_lj_f32(SimEngine
 #pragma unroll
         for (int s = 0; s < 8; ++s) vals[s] = 0.5 * (double)acc[s];
         block_partials<8>(vals, e.partials, SIM_RED_EPOT_PAIR);
-        last_block_finalize<8>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR);
+        last_block_finalize<8>(e.partials, e.red_counter + 1, e.red_out, SIM_RED_EPOT_PAIR, SIM_RED_SLOTS, ACC);
     }
 }
 
@@ -246,21 +253,24 @@ __global__ void k_zero_slot(double* out, int slot) { out[slot] = 0.0; }
 
 using namespace simb200;
 
-template <bool ORTHO, bool SINGLE, int INTEG>
+template <bool ORTHO, bool SINGLE, int INTEG, bool ACC>
 static int launch_lj_f32(const SimEngine& e, const SimLJParams& p, const SimIntegrator& ip, cudaStream_t st) {
-    const int g = persistent_grid((const void*)k_lj_f32<ORTHO, SINGLE, INTEG>, SIM_THREADS, 0, e.n);
+    const int g = persistent_grid((const void*)k_lj_f32<ORTHO, SINGLE, INTEG, ACC>, SIM_THREADS, 0, e.n);
     if (g > e.n_blocks_max) return SIM_ERR_ARG;
-    const cudaError_t err = launch_pdl(k_lj_f32<ORTHO, SINGLE, INTEG>, dim3(g), dim3(SIM_THREADS), 0, st, e, p, ip);
+    const cudaError_t err =
+        launch_pdl(k_lj_f32<ORTHO, SINGLE, INTEG, ACC>, dim3(g), dim3(SIM_THREADS), 0, st, e, p, ip);
     if (err != cudaSuccess) { set_cuda_error(err, "sim_lj_forces: launch"); return SIM_ERR_CUDA; }
     return SIM_OK;
 }
 
-template <int INTEG>
+template <int INTEG, bool ACC = false>
 static int lj_f32(const SimEngine& e, const SimLJParams& p, const SimIntegrator& ip, cudaStream_t st) {
     const bool single = p.n_types == 1;
     if (e.box_orthogonal)
-        return single ? launch_lj_f32<true, true, INTEG>(e, p, ip, st) : launch_lj_f32<true, false, INTEG>(e, p, ip, st);
-    return single ? launch_lj_f32<false, true, INTEG>(e, p, ip, st) : launch_lj_f32<false, false, INTEG>(e, p, ip, st);
+        return single ? launch_lj_f32<true, true, INTEG, ACC>(e, p, ip, st)
+                      : launch_lj_f32<true, false, INTEG, ACC>(e, p, ip, st);
+    return single ? launch_lj_f32<false, true, INTEG, ACC>(e, p, ip, st)
+                  : launch_lj_f32<false, false, INTEG, ACC>(e, p, ip, st);
 }
 
 extern "C" int sim_lj_forces(const SimEngine* ep, const SimLJParams* pp, int32_t precision, void* stream) {
@@ -295,3 +305,10 @@ extern "C" int sim_lj_forces_integrate(const SimEngine* ep, const SimLJParams* p
     return launch_status(mode == 1 ? "sim_lj_forces_integrate" : "sim_lj_forces_integrate (drift)");
 }
 
+
+extern "C" int sim_lj_forces_add(const SimEngine* ep, const SimLJParams* pp, void* stream) {
+    if (!ep || !pp || ep->n <= 0) return SIM_ERR_ARG;
+    const int rc = lj_f32<0, true>(*ep, *pp, SimIntegrator{}, (cudaStream_t)stream);
+    if (rc != SIM_OK) return rc;
+    return launch_status("sim_lj_forces_add");
+}

@@ -186,6 +186,16 @@ class LennardJonesForce(BackboneInterface):
     def compute(self):
         self.molecular.engine.lj_forces(self.params, self.force_precision)
 
+    def add_to_engine(self, force_precision: int = 0):
+        """As a further backbone of a SumBackboneInterface (md_model.py:39-46):
+        the LJ forces, energy and virials are added to the engine's, which the
+        first backbone wrote (FP32 pairs)."""
+        if force_precision != 0:
+            raise NotImplementedError("LJ is summed onto FP32 forces only (the first force field computes FP32 "
+                                      "forces)")
+        eng = self.molecular.engine
+        _lib.call("sim_lj_forces_add", eng.st_ref, self.params.ref, eng.stream)
+
     def compute_and_finish(self, integrator):
         """Forces plus the integrator's second half (one pass over the atoms for
         FP32 pairs; the FP64 path runs the two separately)."""

@@ -26,8 +26,11 @@ class SumBackboneInterface(nn.Module):
     """Sum of force-field backbones (md_model.py:19-52).  The first backbone
     is the device force field (it writes the engine's forces, energy and
     virial); each further one must add its terms on the device
-    (``add_to_engine``, e.g. ``SphericalIndenterForce``).  The outputs are
-    the engine's sums, as the reference's summed buffers."""
+    (``add_to_engine``: ``LennardJonesForce`` with FP32 pairs,
+    ``SphericalIndenterForce``).  The outputs are the engine's sums, as the
+    reference's summed buffers: the scalar virials are added as each force
+    field defines its own (EAM sum s r, LJ sum F r), as the reference adds
+    them."""
 
     def __init__(self, backbones, molecular):
         super().__init__()
@@ -79,7 +82,7 @@ class BaseModel(nn.Module):
         the integrator fused (one element type, FP32 pairs, no barostat)."""
         bb = self.sum_bone.backbones
         if (self.barostat is not None or len(bb) != 2 or not hasattr(bb[0], "compute_finish_with_indenter")
-                or not hasattr(bb[1], "add_to_engine") or not hasattr(self.Integrator, "params")
+                or not getattr(bb[1], "fusable_into_force_pass", False) or not hasattr(self.Integrator, "params")
                 or self.engine.use_tiles or getattr(bb[0], "E", 0) != 1 or bb[0].force_precision != 0):
             return None
         return bb[0], bb[1]

@@ -102,6 +102,10 @@ class SphericalIndenterForce(BackboneInterface):
     engine's virial tensor is symmetric: the indenter's F (x) x enters it with
     its upper triangle."""
 
+    # its force depends on the atom's own position only, so an EAM force pass
+    # can add it in its per-atom epilogue (sim_eam_force_integrate_indenter)
+    fusable_into_force_pass = True
+
     def __init__(self, molecular, radius: float, stiffness: float, center):
         super().__init__()
         self.molecular = molecular

@@ -369,6 +369,39 @@ def crack_cases(tmp):
           lower=lo.numpy(), sigma=sigma, projected=proj, threshold=1.0, bins=160, **res)
 
 
+def sum_cases(tmp):
+    """A sum of two force fields (core/md_model.py:19-52): EAM-W (the pure
+    PyTorch EAMForceCUDAExt) plus a raw LJ on the same W atoms and the same
+    cutoff, FP32 (the reference EAM path's precision): the summed outputs of
+    one evaluation, then 10 NVE steps through BaseModel."""
+    from io_utils.eam_parser import EAMParser
+    from core.force.eam_force_cu import EAMForceCUDAExt
+    from core.force.lennard_jones_force import LennardJonesForce
+    from core.integrator.integrator import VerletIntegrator
+    from core.md_model import BaseModel, SumBackboneInterface
+    pot = oin.write_fs_w_setfl(os.path.join(tmp, "W_synthetic.eam.fs"))
+    parser = EAMParser(pot, torch.device("cpu"))
+    x, L = oin.bcc_lattice(5)
+    x = oin.jitter(x, 0.05, 41)
+    v0 = oin.maxwell_boltzmann(np.full(len(x), oin.W_MASS), 300.0, 42)
+    params = {"[0 0]": {"epsilon": 0.02, "sigma": 2.3}}
+    mol = _reader(tmp, "w250sum", x, "W", L, parser.cutoff, 0.5, params=params, is_fs=False)
+    sb = SumBackboneInterface([EAMForceCUDAExt(parser, mol, use_extension=False), LennardJonesForce(mol)], mol)
+    out0 = {k: v.detach().clone() for k, v in sb().items()}
+    integ = VerletIntegrator(mol, dt=0.002, ensemble="NVE")
+    mol.atom_velocities = torch.tensor(v0, dtype=torch.float32)
+    model = BaseModel(sb, integ, mol)
+    rec = {k: [] for k in ("energy", "kinetic_energy", "virial")}
+    for _ in range(10):
+        out = model()
+        for k in rec:
+            rec[k].append(float(out[k]))
+    _save("sum_w250_eam_lj_f32", x0=x, v0=v0, box=L, dt=0.002, steps=10, epsilon=0.02, sigma=2.3,
+          forces0=out0["forces"], energy0=out0["energy"], virial0=out0["virial"],
+          virial_tensor0=out0["virial_tensor"], x=mol.coordinates, v=mol.atom_velocities,
+          **{k: np.array(v) for k, v in rec.items()})
+
+
 class _NativeRecorder(types.ModuleType):
     """Stands in for the reference's native module ``simulon_cuda`` while the
     reference's own wrappers run: each call's arguments are recorded as the
@@ -564,7 +597,8 @@ def legacy_cases(tmp):
 
 
 GROUPS = {"neighbor": "neighbor_cases", "lj": "lj_cases", "eam": "eam_cases", "md": "md_cases",
-          "mech": "mech_cases", "indenter": "indenter_cases", "crack": "crack_cases", "legacy": "legacy_cases"}
+          "mech": "mech_cases", "indenter": "indenter_cases", "crack": "crack_cases", "legacy": "legacy_cases",
+          "sum": "sum_cases"}
 
 
 def main():

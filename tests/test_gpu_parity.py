@@ -595,3 +595,33 @@ def test_maxwell_boltzmann_velocities_match_reference_formula(sb, dtype):
         ke = 0.5 * float((m[sel] * v[sel].double() ** 2).sum())
         t_kin = 2.0 * ke / (3.0 * int(sel.sum())) / 8.617333262e-5
         assert abs(t_kin / T - 1.0) < 0.05, t_kin
+
+
+# ------------------------------------------------ sum of force fields
+def test_sum_of_eam_and_lj_matches_reference(sb, fsw_path, tmp_path):
+    """SumBackboneInterface([EAM, LJ]) (core/md_model.py:19-52): the LJ pass
+    adds its forces, energy and virials to the EAM pass's on the device
+    (sim_lj_forces_add).  One evaluation against the reference's summed
+    outputs (forces 5e-5 eV/A, energy 2e-6 relative, virials 1e-5 relative),
+    then 10 NVE steps through BaseModel (energies 2e-5 relative, positions
+    5e-4 A; the reference integrates in FP32, the device in FP64)."""
+    g = load("sum_w250_eam_lj_f32")
+    path = oin.write_xyz(str(tmp_path / "w.xyz"), g["x0"], "W")
+    parser = sb.EAMParser(fsw_path)
+    params = {"[0 0]": {"epsilon": float(g["epsilon"]), "sigma": float(g["sigma"])}}
+    mol = sb.AtomFileReader(path, float(g["box"]), parser.cutoff, device=DEV, skin_thickness=0.5,
+                            parameter=params)
+    bone = sb.SumBackboneInterface([sb.EAMForceCUDAExt(parser, mol), sb.LennardJonesForce(mol)], mol)
+    out = bone()
+    assert np.max(np.abs(out["forces"].cpu().numpy() - g["forces0"])) < 5e-5
+    assert abs(float(out["energy"]) - float(g["energy0"])) < 2e-6 * abs(float(g["energy0"]))
+    assert abs(float(out["virial"]) - float(g["virial0"])) < 1e-5 * abs(float(g["virial0"]))
+    np.testing.assert_allclose(out["virial_tensor"].cpu().numpy(), g["virial_tensor0"], rtol=1e-5,
+                               atol=1e-5 * float(np.abs(g["virial_tensor0"]).max()))
+    integ = sb.VerletIntegrator(mol, dt=float(g["dt"]), ensemble="NVE")
+    mol.atom_velocities = torch.tensor(g["v0"].astype(np.float32), device=DEV)
+    model = sb.BaseModel(bone, integ, mol)
+    e = [float(model()["energy"]) for _ in range(int(g["steps"]))]
+    np.testing.assert_allclose(e, g["energy"], rtol=2e-5)
+    np.testing.assert_allclose(mol.coordinates.cpu().numpy(), g["x"], atol=5e-4)
+    assert mol.engine.status() == 0

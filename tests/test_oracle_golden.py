@@ -317,3 +317,21 @@ def test_native_lj_call_records_match_oracle(mode):
                      mode=["raw", "fs", "switch"][int(g["mode"])], rs=float(g["rs"]) or None)
     assert abs(float(out["energy"]) - float(g["energy"])) < 1e-6 * abs(float(g["energy"]))
     assert np.max(np.abs(out["forces"].numpy() - g["forces"])) < 1e-6
+
+
+def test_sum_of_eam_and_lj_oracle_matches_reference(fsw):
+    """The oracle's EAM (FP32 tables) plus its LJ on the same half list give the
+    reference's summed forces, energy and virials at FP32 round-off."""
+    g = load("sum_w250_eam_lj_f32")
+    box = OracleBox(float(g["box"]))
+    x = g["x0"].astype(np.float32)
+    hl = onb.half_list(x, box, onb.rc2_like_reference(4.4, 0.5, np.float32))
+    t32 = oeam.EAMTables(fsw, dtype=torch.float32)
+    e = oeam.eam_forward(torch.tensor(x), hl["i"], hl["j"], np.zeros(len(x), np.int64), box, t32)
+    n = len(hl["i"])
+    lj = lj_forward(torch.tensor(x), hl["i"], hl["j"], torch.full((n,), float(g["epsilon"]), dtype=torch.float32),
+                    torch.full((n,), float(g["sigma"]), dtype=torch.float32), box, 4.4)
+    F = e["forces"].numpy() + lj["forces"].numpy()
+    assert np.max(np.abs(F - g["forces0"])) < 2e-5
+    assert abs(float(e["energy"] + lj["energy"]) - float(g["energy0"])) < 2e-6 * abs(float(g["energy0"]))
+    assert abs(float(e["virial"] + lj["virial"]) - float(g["virial0"])) < 2e-5 * abs(float(g["virial0"]))
