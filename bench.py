@@ -760,8 +760,8 @@ def mechanics_form(args, sb, pot, dev, world):
     atoms (BCC W, synthetic FS potential, dt 2 fs, 300 K Maxwell-Boltzmann
     velocities): (1) uniaxial tension along x at 0.1 / ps with the anisotropic
     NPT barostat holding y and z at 0 bar (core/mechanics/loading.py:6-81,
-    core/barostat.py:78-208), one loader.step + model() per step as the
-    reference's loop does (eager launches); (2) a spherical indenter (radius
+    core/barostat.py:78-208), loader step + MD step per step as the
+    reference's loop, captured in CUDA graphs (UniaxialTensileLoader.run); (2) a spherical indenter (radius
     20 A, stiffness 0.05 eV/A^3) on the top layer as a second backbone
     (core/mechanics/indenter.py:7-68), its centre lowered 0.04 A between
     20-step graph replays.  Each timed with CUDA events like the plain line."""
@@ -786,11 +786,10 @@ def mechanics_form(args, sb, pot, dev, world):
             model = sb.BaseModel(sb.SumBackboneInterface([ff], mol), integ, mol, barostat=baro)
 
             def steps(k):
-                o = None
-                for _ in range(k):
-                    loader.step(0.002)
-                    o = model()
-                return o
+                # loader and MD steps captured together in CUDA graphs; the
+                # loader's bookkeeping runs on the device (no per-step host read)
+                loader.run(model, k, 0.002, graph_steps=args.graph_steps)
+                return model._outputs()
         else:
             top = float(x[:, 2].max())
             center = np.array([0.5 * L, 0.5 * L, top + 20.0 - 1.0])
@@ -819,7 +818,8 @@ def mechanics_form(args, sb, pot, dev, world):
         row = {"value": N * K / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K, "steps": K, "status": eng.status(),
                "rebuilds_in_timed": int(eng.flags[3].item()) - rb0, "temperature_k": float(o["temperature"])}
         if name == "tensile":
-            row["engineering_strain"] = float(loader.total_engineering_strain)
+            row["engineering_strain"] = float(loader.state[12])
+            row["regrids"] = int(loader.regrids)
             row["forced_rebuilds"] = int(loader.forced_rebuilds)
             row["pressure_bar"] = [float(p) for p in o["pressure"].reshape(-1)[:3]]
         else:
@@ -856,7 +856,8 @@ def mechanics_form(args, sb, pot, dev, world):
     del sim, model, ff, integ, mol
     torch.cuda.empty_cache()
     out["config"] = {"workload": f"EAM-W BCC 2*{args.n}^3 = {N:,} atoms, synthetic FS W, dt 2 fs, 300 K: uniaxial "
-                                 "tension 0.1/ps along x with anisotropic NPT at 0 bar on y, z (eager per-step loop); "
+                                 "tension 0.1/ps along x with anisotropic NPT at 0 bar on y, z (loader + MD steps in "
+                                 "CUDA graphs); "
                                  "spherical indenter r 20 A, k 0.05 eV/A^3, lowered 0.04 A per 20-step graph; "
                                  "MDSimulator NVE writing traj.xyz and energies.csv every 100 steps",
                      "parallelism": "replicas x1"}

@@ -224,6 +224,21 @@ typedef struct SimBoxScale {
     int32_t pad;
 } SimBoxScale;
 
+/* UniaxialTensileLoader bookkeeping on the device (sim_loader_check) */
+typedef struct SimLoaderCheck {
+    int32_t axis;              /* loading axis 0..2                                  */
+    int32_t pad;
+    double rebuild_strain;     /* max |H inv(H_list) - I| that forces a list rebuild */
+    double regrid_margin;      /* request a regrid when a cell is narrower than
+                                  x_rc (1 + margin)                                  */
+} SimLoaderCheck;
+/* state of sim_loader_check: SIM_LOADER_STATE doubles, host-initialised:
+ * [0..8] H at the list the rule last forced (set to the box at start),
+ * [9..11] initial row lengths; written by the device: [12] engineering strain
+ * of the loading axis, [13..15] current row lengths, [16] forced rebuilds,
+ * [17] 1 = regrid requested (the host clears it after MDEngine-style regrid). */
+#define SIM_LOADER_STATE 32
+
 /* ---- spherical indenter (core/mechanics/indenter.py:7-68) --------------- */
 typedef struct SimIndenter {
     const double* center;      /* [3] device (settable between graph replays)      */
@@ -438,6 +453,15 @@ int sim_aniso_npt(const SimEngine* e, const SimAniso* p, double* work, void* str
 /* UniaxialTensileLoader.step's box update (loading.py:41-80): H <- diag(scale) H
  * and the same position, velocity (vel_scale), posq and reference handling. */
 int sim_box_scale(const SimEngine* e, const SimBoxScale* p, double* work, void* stream);
+/* The rest of UniaxialTensileLoader.step (loading.py:41-80) on the device, to
+ * run after sim_box_scale so that the loop needs no host read per step: the
+ * box row lengths and the loading axis' engineering strain (state[12]); a
+ * list rebuild requested through flags[0] (taken by the next conditional
+ * rebuild) once the box has deformed by more than p->rebuild_strain since the
+ * list this rule last forced; state[17] = 1 when the cell grid comes within
+ * p->regrid_margin of the list cutoff (the host regrids between launches or
+ * graph replays).  One thread; graph-capturable. */
+int sim_loader_check(const SimEngine* e, const SimLoaderCheck* p, double* state, void* stream);
 
 /* SphericalIndenterForce.forward (indenter.py:40-68) added to the engine's
  * forces (force_precision 0: f32, 1: f64) after a force field's pass: for

@@ -100,6 +100,14 @@ class SimBoxScale(ctypes.Structure):
                 ("reset_reference", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
+class SimLoaderCheck(ctypes.Structure):
+    _fields_ = [("axis", ctypes.c_int32), ("pad", ctypes.c_int32), ("rebuild_strain", ctypes.c_double),
+                ("regrid_margin", ctypes.c_double)]
+
+
+LOADER_STATE = 32
+
+
 class SimIndenter(ctypes.Structure):
     _fields_ = [("center", ctypes.c_void_p), ("radius", ctypes.c_double), ("stiffness", ctypes.c_double),
                 ("out", ctypes.c_void_p)]
@@ -171,6 +179,7 @@ SIGNATURES = {
     "sim_berendsen_scale_first": [_P(SimEngine), _P(SimBerendsen), c_p, _P(SimIntegrator), ctypes.c_int32, c_p],
     "sim_aniso_npt": [_P(SimEngine), _P(SimAniso), c_p, c_p],
     "sim_box_scale": [_P(SimEngine), _P(SimBoxScale), c_p, c_p],
+    "sim_loader_check": [_P(SimEngine), _P(SimLoaderCheck), c_p, c_p],
     "sim_indenter_add": [_P(SimEngine), _P(SimIndenter), ctypes.c_int32, c_p],
     "sim_batch_crack_observe": [c_p, c_p, c_p, ctypes.c_int32, c_p, c_p, c_p, c_p],
     "sim_gather_original_f64": [_P(SimEngine), c_p, c_p, c_p],

@@ -318,6 +318,56 @@ __global__ void __launch_bounds__(SIM_THREADS) k_scale_atoms(SimEngine e, const 
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
 }
 
+// UniaxialTensileLoader.step's bookkeeping (loading.py:41-80) on the device,
+// after the box update: row lengths and the loading axis' engineering strain;
+// a list rebuild requested through flags[0] (taken at the next conditional
+// rebuild) when the box has deformed by more than rebuild_strain since the
+// list the rule last forced (the skin test compares fractional positions, so
+// it does not see an affine change); and a regrid request when a cell would
+// come within regrid_margin of the list cutoff across any axis of >= 3 cells
+// (the host regrids between graph replays, before the cells are too small).
+// state: SIM_LOADER_STATE doubles, see simb200.h.
+__global__ void k_loader_check(SimEngine e, SimLoaderCheck p, double* state) {
+    pdl_wait();
+    const double* H = e.box->H;
+    double len[3];
+    for (int a = 0; a < 3; ++a) {
+        const double* r = H + 3 * a;
+        len[a] = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        state[13 + a] = len[a];
+    }
+    state[12] = len[p.axis] / state[9 + p.axis] - 1.0;
+    // M = H inv(H_list); deviation from the identity
+    const double* L = state;
+    const double det = det3(L);
+    double inv[9];
+    inv[0] = (L[4] * L[8] - L[5] * L[7]) / det; inv[1] = (L[2] * L[7] - L[1] * L[8]) / det;
+    inv[2] = (L[1] * L[5] - L[2] * L[4]) / det; inv[3] = (L[5] * L[6] - L[3] * L[8]) / det;
+    inv[4] = (L[0] * L[8] - L[2] * L[6]) / det; inv[5] = (L[2] * L[3] - L[0] * L[5]) / det;
+    inv[6] = (L[3] * L[7] - L[4] * L[6]) / det; inv[7] = (L[1] * L[6] - L[0] * L[7]) / det;
+    inv[8] = (L[0] * L[4] - L[1] * L[3]) / det;
+    double dev = 0.0;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            const double m = H[3 * r] * inv[c] + H[3 * r + 1] * inv[3 + c] + H[3 * r + 2] * inv[6 + c];
+            dev = fmax(dev, fabs(m - (r == c ? 1.0 : 0.0)));
+        }
+    if (dev > p.rebuild_strain) {
+        e.flags[0] = 1;
+        for (int k = 0; k < 9; ++k) state[k] = H[k];
+        state[16] += 1.0;
+    }
+    const double V = fabs(det3(H));
+    for (int a = 0; a < 3; ++a) {
+        if (e.ncell[a] < 3) continue;
+        const double* u = H + 3 * ((a + 1) % 3);
+        const double* w = H + 3 * ((a + 2) % 3);
+        const double cx = u[1] * w[2] - u[2] * w[1], cy = u[2] * w[0] - u[0] * w[2], cz = u[0] * w[1] - u[1] * w[0];
+        if (V / sqrt(cx * cx + cy * cy + cz * cz) < e.x_rc * (1.0 + p.regrid_margin) * (double)e.ncell[a])
+            state[17] = 1.0;
+    }
+}
+
 __global__ void k_box_commit(SimEngine e, const double* work) {
     pdl_wait();
     *e.box = *reinterpret_cast<const SimBox*>(work + 16);
@@ -644,3 +694,12 @@ extern "C" int sim_indenter_add(const SimEngine* ep, const SimIndenter* p, int32
     return launch_status("sim_indenter_add");
 }
 
+
+extern "C" int sim_loader_check(const SimEngine* ep, const SimLoaderCheck* p, double* state, void* stream) {
+    if (!ep || !p || !state || p->axis < 0 || p->axis > 2 || !(p->rebuild_strain >= 0.0) ||
+        !(p->regrid_margin >= 0.0))
+        return SIM_ERR_ARG;
+    const cudaError_t err = launch_pdl(k_loader_check, dim3(1), dim3(1), 0, (cudaStream_t)stream, *ep, *p, state);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_loader_check: launch"); return SIM_ERR_CUDA; }
+    return launch_status("sim_loader_check");
+}

@@ -305,12 +305,14 @@ class MDEngine:
         w = perpendicular_widths(H)
         return all(int(n) < 3 or w[k] / int(n) >= self.x_rc for k, n in enumerate(self.ncell))
 
-    def regrid(self) -> bool:
+    def regrid(self, margin: float = 0.0) -> bool:
         """Cell grid for the current device box (after a barostat or a loader
-        shrank cells below rc + skin, SIM_STATUS_CELLS) and a full reload: the
-        list is rebuilt on the new grid.  Synchronises; True if the grid changed."""
+        shrank cells below rc + skin, SIM_STATUS_CELLS, or to within ``margin``
+        of it) and a full reload: the list is rebuilt on the new grid.  Cells
+        are chosen at least (rc + skin)(1 + margin) wide.  Synchronises; True
+        if the grid changed."""
         H = self.box_matrix()
-        nc = cell_grid(H, self.x_rc, self.n)
+        nc = cell_grid(H, self.x_rc * (1.0 + float(margin)), self.n)
         if np.array_equal(nc, self.ncell) and self.cells_valid(H):
             return False
         x, v = self.gather("x"), self.gather("v")

@@ -111,14 +111,21 @@ class BaseModel(nn.Module):
         return (self.barostat is None and self.sum_bone.single and hasattr(bone, "compute_finish_and_drift")
                 and hasattr(self.Integrator, "params") and not self.engine.use_tiles)
 
-    def _launch_steps(self, k: int):
-        """k steps, launches only.  For EAM without a barostat the first half of
+    def _launch_steps(self, k: int, pre_step=None):
+        """k steps, launches only.  ``pre_step`` (launches only, e.g.
+        UniaxialTensileLoader.launch) runs before each step; the steps then
+        run unfused.  For EAM without a barostat the first half of
         step s+1 runs inside step s's force pass (same arithmetic, one pass over
         the atoms fewer per step); the last step ends with full-step velocities.
         With a spherical indenter as EAM's second backbone, the indenter's force
         is added inside that pass.  With a Berendsen barostat the atoms'
         scaling of step s runs inside step s+1's first half; the last step
         scales them itself."""
+        if pre_step is not None:
+            for _ in range(k):
+                pre_step()
+                self._step_launches()
+            return
         if k > 1 and not self._drift_fusable() and callable(getattr(self.barostat, "deferred_first_half", None)) \
                 and hasattr(self.Integrator, "params"):
             for s in range(k):
@@ -195,36 +202,52 @@ class BaseModel(nn.Module):
         return self._outputs()
 
     # ---- graph-captured multi-step execution ------------------------------
-    def _graph(self, k: int):
+    def _graph(self, k: int, pre_step=None):
         if getattr(self, "_graph_generation", None) != self.engine.generation:
             self._graphs = {}   # the engine's buffers were reallocated (MDEngine.regrid)
             self._graph_generation = self.engine.generation
-        if k not in self._graphs:
+        key = (k, pre_step)
+        if key not in self._graphs:
+            if len(self._graphs) >= 8:                     # keep the cache bounded
+                self._graphs.pop(next(iter(self._graphs)))
             s = torch.cuda.Stream(self.engine.device)
             s.wait_stream(torch.cuda.current_stream(self.engine.device))
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=s):
-                self._launch_steps(k)
+                self._launch_steps(k, pre_step)
             torch.cuda.current_stream(self.engine.device).wait_stream(s)
-            self._graphs[k] = g
-        return self._graphs[k]
+            self._graphs[key] = g
+        return self._graphs[key]
 
-    def run(self, n_steps: int, graph_steps: int = 20):
+    def run(self, n_steps: int, graph_steps: int = 20, pre_step=None):
         """Advance n_steps with CUDA graphs (no host sync); returns the last outputs.
 
-        Capturing records launches without executing them, so the device state
-        is unchanged by the capture itself.
+        ``pre_step``: a callable that only launches device work (for example
+        UniaxialTensileLoader.launch with its dt bound), run before every step
+        and captured with it.  Capturing records launches without executing
+        them, so the device state is unchanged by the capture itself.
         """
+        n_steps = int(n_steps)
+        if pre_step is not None and n_steps > 0 and (self._first_call or not self.engine.forces_valid):
+            # as the reference's loop (loader.step(); model()): the first call's
+            # forces are those of the positions after the first pre-step
+            pre_step()
+            self._prime()
+            self._step_launches()
+            self.steps_done += 1
+            self.profile["pair_calls"] += 1
+            self.profile["integrate_calls"] += 1
+            n_steps -= 1
         self._prime()
-        full, rest = divmod(int(n_steps), int(graph_steps))
+        full, rest = divmod(n_steps, int(graph_steps))
         if full:
-            g = self._graph(int(graph_steps))
+            g = self._graph(int(graph_steps), pre_step)
             for _ in range(full):
                 g.replay()
-        self._launch_steps(rest)
-        self.steps_done += int(n_steps)
-        self.profile["pair_calls"] += int(n_steps)
-        self.profile["integrate_calls"] += int(n_steps)
+        self._launch_steps(rest, pre_step)
+        self.steps_done += n_steps
+        self.profile["pair_calls"] += n_steps
+        self.profile["integrate_calls"] += n_steps
         return self._outputs()
 
     def step_log(self, first_step: int, count: int) -> torch.Tensor:

@@ -10,15 +10,18 @@ rebuild, and the reference's reset of last_positions.  ``step`` returns the
 engineering strain of the loading axis as a Python float (it reads the
 device box, which also holds a barostat's changes of the other axes).
 
-Beyond the reference: the cell grid is rebuilt when the box shrinks below
-rc + skin per cell (``MDEngine.regrid``), and the list is rebuilt whenever
-the box has strained by more than a quarter of the skin over the list
-cutoff since the last such rebuild (the skin test compares fractional
-positions, which an affine box change leaves unchanged).
+Beyond the reference: the cell grid is rebuilt before the box shrinks below
+rc + skin per cell (``MDEngine.regrid``, asked for by the device with a
+margin), and the list is rebuilt whenever the box has strained by more than
+a quarter of the skin over the list cutoff since the last such rebuild (the
+skin test compares fractional positions, which an affine box change leaves
+unchanged).  That bookkeeping runs on the device, so loader and MD steps can
+be captured together in CUDA graphs.
 """
 from __future__ import annotations
 
 import ctypes
+import math
 
 import numpy as np
 import torch
@@ -28,14 +31,31 @@ from .forces import BackboneInterface, _force_outputs
 
 
 class UniaxialTensileLoader:
+    """Uniaxial loading (loading.py:6-81): each step scales the loading axis
+    of the box by 1 + strain_rate dt (and, with lateral_mode "poisson", the
+    other axes by the Poisson contraction) and maps the atoms through
+    fractional coordinates, on the device.  The step's bookkeeping runs on the
+    device too (``sim_loader_check``): the engineering strain, the list
+    rebuild forced after an affine strain of a quarter of the skin over the
+    list cutoff, and the request to regrid before the cells become narrower
+    than the list cutoff.
+
+    ``step(dt)`` keeps the reference's contract (returns the engineering
+    strain as a float, so it synchronises and regrids when asked).
+    ``launch(dt)`` only enqueues the work (returns the strain as a device
+    scalar), so ``model.run(n, pre_step=...)`` can capture loader and MD
+    steps together in CUDA graphs; ``run(model, n_steps, dt)`` does that in
+    chunks and regrids between them (``maintain``)."""
+
     def __init__(self, molecular, axis: int = 0, strain_rate: float = 1.0e-3, lateral_mode: str = "fixed",
-                 poisson_ratio: float = 0.28, max_lateral_scale_step: float = 2.0e-3):
+                 poisson_ratio: float = 0.28, max_lateral_scale_step: float = 2.0e-3, regrid_margin: float = 0.01):
         self.molecular = molecular
         self.axis = int(axis)
         self.strain_rate = float(strain_rate)
         self.lateral_mode = str(lateral_mode).lower()
         self.poisson_ratio = float(poisson_ratio)
         self.max_lateral_scale_step = float(max_lateral_scale_step)
+        self.regrid_margin = float(regrid_margin)
         if self.axis not in (0, 1, 2):
             raise ValueError(f"axis must be 0/1/2, got {axis}")
         if not hasattr(molecular, "engine"):
@@ -47,9 +67,19 @@ class UniaxialTensileLoader:
         self.initial_lengths = torch.tensor(np.linalg.norm(H, axis=1), dtype=torch.float64)
         self.total_engineering_strain = 0.0
         self.work = torch.zeros(_lib.BOXSCALE_WORK, dtype=torch.float64, device=eng.device)
-        self._H_list = H
-        self.forced_rebuilds = 0
+        self.state = torch.zeros(_lib.LOADER_STATE, dtype=torch.float64, device=eng.device)
+        self._reset_list_box(H)
+        self.state[9:12] = self.initial_lengths.to(eng.device)
+        skin = 2.0 * math.sqrt(float(eng.st.skin_half2))
+        self._check = _lib.SimLoaderCheck()
+        self._check.axis = self.axis
+        self._check.rebuild_strain = 0.25 * skin / float(eng.x_rc)
+        self._check.regrid_margin = self.regrid_margin
+        self._hooks = {}
         self.regrids = 0
+
+    def _reset_list_box(self, H):
+        self.state[0:9] = torch.as_tensor(np.asarray(H, np.float64).reshape(-1), dtype=torch.float64)
 
     def _scale_vector(self, dt: float) -> list:
         dstrain = self.strain_rate * float(dt)
@@ -62,30 +92,55 @@ class UniaxialTensileLoader:
                     scale[ax] = lat
         return scale
 
-    def step(self, dt: float) -> float:
-        mol = self.molecular
-        eng = mol.engine
+    def launch(self, dt: float) -> torch.Tensor:
+        """The box update and its bookkeeping, launches only (capturable)."""
+        eng = self.molecular.engine
         s = _lib.SimBoxScale()
         s.scale[:] = self._scale_vector(dt)
         s.vel_scale[:] = [1.0, 1.0, 1.0]
         s.reset_reference = 1
         _lib.call("sim_box_scale", eng.st_ref, ctypes.byref(s), _lib.ptr(self.work), eng.stream)
-        H = eng.box_matrix()
-        if not eng.cells_valid(H):
-            eng.regrid()
-            self.regrids += 1
-            self._H_list = H
-        else:
-            dev = np.abs(np.linalg.solve(self._H_list.T, H.T).T - np.eye(3)).max()
-            if dev * eng.x_rc > 0.25 * eng.skin:
-                eng.rebuild(only_if_flagged=False)
-                self.forced_rebuilds += 1
-                self._H_list = H
+        _lib.call("sim_loader_check", eng.st_ref, ctypes.byref(self._check), _lib.ptr(self.state), eng.stream)
+        return self.state[12]
+
+    def maintain(self) -> bool:
+        """Regrid when the device asked for it (synchronises); True if it did."""
+        if float(self.state[17].item()) == 0.0:
+            return False
+        eng = self.molecular.engine
+        eng.regrid(margin=self.regrid_margin)
+        self.regrids += 1
+        self.state[17] = 0.0
+        self._reset_list_box(eng.box_matrix())
+        return True
+
+    def step(self, dt: float) -> float:
+        self.launch(dt)
+        self.maintain()
+        mol = self.molecular
         if hasattr(mol, "box"):
-            mol.box.H = torch.as_tensor(H)
-        lengths = np.linalg.norm(H, axis=1)
-        self.total_engineering_strain = float(lengths[self.axis] / float(self.initial_lengths[self.axis]) - 1.0)
+            mol.box.H = torch.as_tensor(mol.engine.box_matrix())
+        self.total_engineering_strain = float(self.state[12].item())
         return self.total_engineering_strain
+
+    def run(self, model, n_steps: int, dt: float, graph_steps: int = 20) -> torch.Tensor:
+        """n_steps of (loader step, MD step) captured together in CUDA graphs of
+        graph_steps steps, regridding between graphs when asked; returns the
+        engineering strain as a device scalar."""
+        hook = self._hooks.get(float(dt))
+        if hook is None:
+            hook = self._hooks[float(dt)] = (lambda: self.launch(dt))
+        done = 0
+        while done < int(n_steps):
+            k = min(int(graph_steps), int(n_steps) - done)
+            model.run(k, graph_steps=graph_steps, pre_step=hook)
+            self.maintain()
+            done += k
+        return self.state[12]
+
+    @property
+    def forced_rebuilds(self) -> int:
+        return int(self.state[16].item())
 
     def current_lengths(self) -> torch.Tensor:
         return torch.tensor(np.linalg.norm(self.molecular.engine.box_matrix(), axis=1), dtype=torch.float64)

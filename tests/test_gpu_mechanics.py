@@ -6,7 +6,9 @@ tests/test_oracle_golden.py).  LJ argon 108 atoms, FP64 forces, NVE: energies
 and axis pressures to 1e-8 relative, box to 1e-12, strain rates to 1e-7,
 final wrapped positions to 1e-8 A and velocities to 1e-7 A/ps.  Also: the
 cell-grid guard reports a box that shrank below the list cutoff per cell, and
-MDEngine.regrid repairs it."""
+MDEngine.regrid repairs it.  The graph variants capture the whole run
+(loader steps included, UniaxialTensileLoader.run) and compare the final
+state."""
 import json
 
 import numpy as np
@@ -54,10 +56,14 @@ def test_tensile_and_aniso_npt_match_reference(sb, tmp_path, name, graph):
         loader = UniaxialTensileLoader(mol, **load_kw) if load_kw else None
         E, P, H, eta, strain = [], [], [], [], []
         for s in range(int(g["steps"])):
-            strain.append(loader.step(float(g["dt"])) if loader else 0.0)
-            if graph and loader is None and s == 0:
-                model.run(int(g["steps"]), graph_steps=5)    # whole run as CUDA graphs: no per-step record
+            if graph:     # whole run as CUDA graphs (loader and MD steps captured together): no per-step record
+                if loader is None:
+                    model.run(int(g["steps"]), graph_steps=5)
+                else:
+                    last = loader.run(model, int(g["steps"]), float(g["dt"]), graph_steps=5)
+                    np.testing.assert_allclose(float(last), g["strain"][-1], rtol=1e-12)
                 break
+            strain.append(loader.step(float(g["dt"])) if loader else 0.0)
             out = model()
             E.append(float(out["energy"]))
             P.append(out["pressure"].cpu().numpy().copy())
