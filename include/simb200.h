@@ -711,7 +711,8 @@ const char* sim_last_cuda_error(void);
 int sim_version(void);
 /* sizeof of SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator,
  * SimBerendsen, SimRep, SimBatch, SimMLP, SimAniso, SimBoxScale, SimIndenter,
- * SimCrack (host-only; lets bindings verify their struct layouts; n >= 13). */
+ * SimCrack, SimLoaderCheck (host-only; lets bindings verify their struct
+ * layouts; n >= 13, the first min(n, 14) are written). */
 int sim_struct_sizes(int64_t* out, int32_t n);
 
 #ifdef __cplusplus

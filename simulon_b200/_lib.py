@@ -221,7 +221,7 @@ SIGNATURES = {
     "sim_struct_sizes": [c_p, ctypes.c_int32],
 }
 STRUCTS = (SimBox, SimEngine, SimEAMTables, SimLJParams, SimIntegrator, SimBerendsen, SimRep, SimBatch, SimMLP,
-           SimAniso, SimBoxScale, SimIndenter, SimCrack)
+           SimAniso, SimBoxScale, SimIndenter, SimCrack, SimLoaderCheck)
 _RESTYPES = {"sim_last_cuda_error": ctypes.c_char_p, "sim_format_xyz_rows": ctypes.c_int64}
 
 _lib = None

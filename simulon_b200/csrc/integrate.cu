@@ -654,13 +654,14 @@ extern "C" const char* sim_last_cuda_error(void) { return g_err; }
 extern "C" int sim_version(void) { return 1; }
 
 extern "C" int sim_struct_sizes(int64_t* out, int32_t n) {
-    const int64_t sizes[13] = {(int64_t)sizeof(SimBox), (int64_t)sizeof(SimEngine), (int64_t)sizeof(SimEAMTables),
+    const int64_t sizes[14] = {(int64_t)sizeof(SimBox), (int64_t)sizeof(SimEngine), (int64_t)sizeof(SimEAMTables),
                                (int64_t)sizeof(SimLJParams), (int64_t)sizeof(SimIntegrator),
                                (int64_t)sizeof(SimBerendsen), (int64_t)sizeof(SimRep), (int64_t)sizeof(SimBatch),
                                (int64_t)sizeof(SimMLP), (int64_t)sizeof(SimAniso), (int64_t)sizeof(SimBoxScale),
-                               (int64_t)sizeof(SimIndenter), (int64_t)sizeof(SimCrack)};
+                               (int64_t)sizeof(SimIndenter), (int64_t)sizeof(SimCrack),
+                               (int64_t)sizeof(SimLoaderCheck)};
     if (!out || n < 13) return SIM_ERR_ARG;
-    for (int k = 0; k < 13; ++k) out[k] = sizes[k];
+    for (int k = 0; k < 14 && k < n; ++k) out[k] = sizes[k];
     return SIM_OK;
 }
 

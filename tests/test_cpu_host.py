@@ -65,6 +65,15 @@ def test_argument_errors_are_reported_without_gpu(lib):
     for mode in (0, 3):   # only 1 (second half) and 2 (with the next first half)
         assert lib.sim_lj_forces_integrate(ctypes.byref(e), ctypes.byref(p), ctypes.byref(ip), mode, None) == \
             _lib.SIM_ERR_ARG
+    # the summed-LJ and loader-bookkeeping entry points
+    assert lib.sim_lj_forces_add(None, None, None) == _lib.SIM_ERR_ARG
+    assert lib.sim_lj_forces_add(ctypes.byref(_lib.SimEngine()), ctypes.byref(p), None) == _lib.SIM_ERR_ARG
+    chk = _lib.SimLoaderCheck()
+    assert lib.sim_loader_check(None, ctypes.byref(chk), None, None) == _lib.SIM_ERR_ARG
+    for axis, strain, margin in ((3, 0.01, 0.01), (-1, 0.01, 0.01), (0, -1.0, 0.01), (0, 0.01, -0.5)):
+        chk.axis, chk.rebuild_strain, chk.regrid_margin = axis, strain, margin
+        assert lib.sim_loader_check(ctypes.byref(e), ctypes.byref(chk), ctypes.c_void_p(16), None) == \
+            _lib.SIM_ERR_ARG
     with pytest.raises(_lib.SimError):
         _lib.check(_lib.SIM_ERR_ARG, "probe")
 
