@@ -1034,16 +1034,15 @@ def e2e(model, mol, x, v, args, dev):
     v_out = torch.empty(N, 3, dtype=torch.float64).pin_memory()
 
     def one_pass(n_steps):
-        mol.update_coordinates(xh)          # H2D + cell sort + list build
-        mol.atom_velocities = vh            # H2D
+        mol.update_coordinates(xh, velocities=vh)     # H2D of both + cell sort + list build
         done = 0
         while done < n_steps:
             k = min(G * 5, n_steps - done)
             model.run(k, graph_steps=G)
             log_h[done:done + k].copy_(model.step_log(model.steps_done - k, k), non_blocking=True)
             done += k
-        x_out.copy_(mol.coordinates)
-        v_out.copy_(mol.atom_velocities)
+        x_out.copy_(mol.coordinates, non_blocking=True)
+        v_out.copy_(mol.atom_velocities, non_blocking=True)
         torch.cuda.synchronize()
     one_pass(min(K, G * 5))
     t0 = time.perf_counter()
@@ -1053,7 +1052,8 @@ def e2e(model, mol, x, v, args, dev):
     row_bytes = log_h.shape[1] * 8
     return {"value": N * K / dt, "unit": UNIT, "h2d_bytes_per_step": 2 * N * 24 / K,
             "d2h_bytes_per_step": row_bytes + 2 * N * 24 / K, "seconds": dt,
-            "path": "AtomFileReader.update_coordinates / atom_velocities -> BaseModel.run -> coordinates/velocities + step log"}
+            "path": "AtomFileReader.update_coordinates(x, velocities=v) -> BaseModel.run -> coordinates/velocities + "
+                    "step log"}
 
 
 if __name__ == "__main__":

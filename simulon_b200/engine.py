@@ -220,9 +220,12 @@ class MDEngine:
 
     # ---- state in/out ------------------------------------------------------
     def load(self, positions, velocities=None):
-        """Load original-order rows, sort into cells and build the list."""
-        pos = torch.as_tensor(positions).to(self.device, torch.float64).contiguous()
-        vel = None if velocities is None else torch.as_tensor(velocities).to(self.device, torch.float64).contiguous()
+        """Load original-order rows, sort into cells and build the list.  The
+        copies from pinned host rows are asynchronous; the capacity check at
+        the end synchronises, so they have landed when this returns."""
+        pos = torch.as_tensor(positions).to(self.device, torch.float64, non_blocking=True).contiguous()
+        vel = None if velocities is None else \
+            torch.as_tensor(velocities).to(self.device, torch.float64, non_blocking=True).contiguous()
         _lib.call("sim_engine_load", self.st_ref, _lib.ptr(pos), _lib.ptr(vel), _lib.ptr(self.types), self.stream)
         self.rebuilds_host += 1
         self.forces_valid = False
@@ -286,10 +289,10 @@ class MDEngine:
         dst = {"x": self.x, "v": self.v}[which]
         _lib.call("sim_scatter_original_f64", self.st_ref, _lib.ptr(rows), _lib.ptr(dst), self.stream)
 
-    def set_positions(self, rows):
-        """New coordinates: reload (re-sorts cells, rebuilds the list, resets the skin reference)."""
-        v = self.gather("v")
-        self.load(rows, v)
+    def set_positions(self, rows, velocities=None):
+        """New coordinates (and, if given, velocities): reload (re-sorts cells,
+        rebuilds the list, resets the skin reference)."""
+        self.load(rows, self.gather("v") if velocities is None else velocities)
 
     def set_velocities(self, rows):
         self.scatter("v", rows)

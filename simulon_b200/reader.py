@@ -158,9 +158,11 @@ class AtomFileReader:
     def update_velocities(self, velocities):
         self.engine.set_velocities(velocities)
 
-    def update_coordinates(self, coordinates):
-        """Replace the coordinates (re-sorts, rebuilds the list, resets the skin reference)."""
-        self.engine.set_positions(coordinates)
+    def update_coordinates(self, coordinates, velocities=None):
+        """Replace the coordinates (re-sorts, rebuilds the list, resets the skin
+        reference); ``velocities`` (beyond the reference's signature) replaces
+        the velocities in the same load."""
+        self.engine.set_positions(coordinates, velocities)
 
     def update_neighbor_list(self):
         t0 = time.perf_counter()
