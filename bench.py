@@ -515,7 +515,17 @@ def run_b200(args):
     rebuilds = int(eng.flags[3].item()) - rb0
     value = world * N * args.steps / (ms / 1e3)
     drift = energy_drift(model, model.steps_done - args.steps, args.steps, N, 0.002)
-    window = clock_window(gpu_id, lambda: model.run(args.steps, graph_steps=G)) if ms < 300 else None
+    drift_steps = args.steps
+    window = None
+    if ms < 300:
+        # short timed region: clock samples over repeats of the same steps, and
+        # the NVE drift over the longest window the step log holds
+        first = model.steps_done
+        window = clock_window(gpu_id, lambda: model.run(args.steps, graph_steps=G))
+        done = model.steps_done - first
+        if done > args.steps:
+            drift_steps = min(done, eng.log_capacity)
+            drift = energy_drift(model, model.steps_done - drift_steps, drift_steps, N, 0.002)
     # state for the oracle's force check (CPU leg): forces recomputed at the current positions
     eng.eam_forces(ff.tables)
     checks = {"plain": (eng.gather("x").cpu().numpy(), eng.box_matrix(), eng.gather("f").cpu().numpy())}
@@ -579,7 +589,9 @@ def run_b200(args):
                               "frac": step_achieved / peak, "unit": "GB/s"},
             "clocks": clocks.summary(),
             "energy_drift_ev_per_atom_per_ns": drift,
-            "energy_drift_steps": min(args.steps, eng.log_capacity),
+            "energy_drift_steps": min(drift_steps, eng.log_capacity),
+            "energy_drift_window": "timed steps" if drift_steps == args.steps else
+                                   "the NVE steps of the timed region and of the clock window after it",
             "gpu_launches": launches_for(args.steps, G) + 10 * rebuilds}
     if window is not None:
         line["clocks_window"] = dict(window, note="repeats of the timed steps for 1.5 s right after the timed "
@@ -738,8 +750,14 @@ def eam_variants_form(args, sb, pot, dev, world, checks=None):
                "status": eng.status(), "rebuilds_in_timed": int(eng.flags[3].item()) - rb0,
                "temperature_k": float(outs["temperature"])}
         if baro is None:
-            row["energy_drift_ev_per_atom_per_ns"] = energy_drift(model, model.steps_done - args.steps, args.steps, N,
-                                                                  0.002)
+            # short timed regions: continue the same NVE run (untimed) so the
+            # drift is fitted over at least 2,000 steps
+            extra = max(0, 2000 - args.steps) // args.graph_steps * args.graph_steps
+            if extra:
+                model.run(extra, graph_steps=args.graph_steps)
+            k = min(args.steps + extra, eng.log_capacity)
+            row["energy_drift_ev_per_atom_per_ns"] = energy_drift(model, model.steps_done - k, k, N, 0.002)
+            row["energy_drift_steps"] = k
             if checks is not None:
                 ff.compute()
                 checks[name] = (eng.gather("x").cpu().numpy(), eng.box_matrix(), eng.gather("f").cpu().numpy())
@@ -804,7 +822,9 @@ def mechanics_form(args, sb, pot, dev, world):
                     ind.set_center(center - np.array([0.0, 0.0, depth[0]]))
                     o = model.run(args.graph_steps, graph_steps=args.graph_steps)
                 return o
-        steps(max(args.warmup, args.graph_steps))
+        # two graphs' worth of warm-up: the first step runs eagerly (the first
+        # call's forces), so the graph of graph_steps steps is captured here
+        steps(max(args.warmup, 2 * args.graph_steps))
         torch.cuda.synchronize()
         rb0 = int(eng.flags[3].item())
         K = (args.steps // args.graph_steps) * args.graph_steps
