@@ -19,6 +19,7 @@ ranks and the value is the total atom-steps of all ranks per second.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -167,6 +168,15 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "in_region": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
                 "samples": len(sm), "in_region": len(sm) if inside else 0}
+
+
+def settle():
+    """Before a timed region: collect garbage (so that the destruction of an
+    earlier form's CUDA graphs and buffers cannot fall inside the region) and
+    drain the device."""
+    import torch
+    gc.collect()
+    torch.cuda.synchronize()
 
 
 def measured_peaks(key: str = "hbm_gbs"):
@@ -408,6 +418,7 @@ def config1_gpu(sb, dev, G):
     model.run(5 * G, graph_steps=G)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    settle()
     e0.record()
     out = model.run(1000, graph_steps=G)
     e1.record()
@@ -501,6 +512,7 @@ def run_b200(args):
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(gpu_id) as clocks:
+        settle()
         e0.record(stream)
         model.run(args.steps, graph_steps=G)
         e1.record(stream)
@@ -655,6 +667,7 @@ def batched_form(args, sb, pot, dev, world, rank, barrier, checks=None):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
+    settle()
     e0.record(stream)
     be.run(tables, integ, args.steps, graph_steps=G)
     e1.record(stream)
@@ -737,6 +750,7 @@ def eam_variants_form(args, sb, pot, dev, world, checks=None):
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+        settle()
         e0.record()
         outs = model.run(args.steps, graph_steps=args.graph_steps)
         e1.record()
@@ -830,6 +844,7 @@ def mechanics_form(args, sb, pot, dev, world):
         K = (args.steps // args.graph_steps) * args.graph_steps
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
+        settle()
         e0.record()
         o = steps(K)
         e1.record()
@@ -864,6 +879,7 @@ def mechanics_form(args, sb, pot, dev, world):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
+        settle()
         e0.record()
         sim.run()
         e1.record()
@@ -930,6 +946,7 @@ def lj_form(args, sb, dev, world):
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+        settle()
         e0.record(stream)
         model.run(args.steps, graph_steps=G)
         e1.record(stream)
@@ -990,6 +1007,7 @@ def mlp_form(args, sb, pot, dev, world):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    settle()
     e0.record(stream)
     run.run(K)
     e1.record(stream)

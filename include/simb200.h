@@ -453,6 +453,23 @@ int sim_aniso_npt(const SimEngine* e, const SimAniso* p, double* work, void* str
 /* UniaxialTensileLoader.step's box update (loading.py:41-80): H <- diag(scale) H
  * and the same position, velocity (vel_scale), posq and reference handling. */
 int sim_box_scale(const SimEngine* e, const SimBoxScale* p, double* work, void* stream);
+/* The controller half of sim_aniso_npt (AnisotropicNPTBarostat.step,
+ * barostat.py:137-208): axis pressures, the strain-rate update and the new box
+ * prepared in `work`, without moving the atoms (sim_box_scale_after_first
+ * moves them together with the next step's loader update and first half). */
+int sim_aniso_control(const SimEngine* e, const SimAniso* p, double* work, void* stream);
+/* The end of a tensile step and the start of the next in one pass over the
+ * atoms (run_scripts/w_tensile.py's loop: barostat.step after model(), then
+ * loader.step and the next model()'s first_half, integrator.py:91-99): the box
+ * update prepared in work_prev (sim_aniso_control), then the loader's box
+ * update p prepared on that box into `work`, then the first half of the next
+ * step in the new box; the same operations in the same order as
+ * sim_box_scale (or sim_aniso_npt's scaling), sim_box_scale and
+ * sim_integrate_first launched one after another, so the same bits.  The box
+ * is committed; sim_loader_check follows as after sim_box_scale.  work:
+ * SIM_BOXSCALE_WORK doubles. */
+int sim_box_scale_after_first(const SimEngine* e, const double* work_prev, int32_t reset_prev, const SimBoxScale* p,
+                              double* work, const SimIntegrator* integ, int32_t force_precision, void* stream);
 /* The rest of UniaxialTensileLoader.step (loading.py:41-80) on the device, to
  * run after sim_box_scale so that the loop needs no host read per step: the
  * box row lengths and the loading axis' engineering strain (state[12]); a

@@ -180,6 +180,9 @@ SIGNATURES = {
     "sim_aniso_npt": [_P(SimEngine), _P(SimAniso), c_p, c_p],
     "sim_box_scale": [_P(SimEngine), _P(SimBoxScale), c_p, c_p],
     "sim_loader_check": [_P(SimEngine), _P(SimLoaderCheck), c_p, c_p],
+    "sim_aniso_control": [_P(SimEngine), _P(SimAniso), c_p, c_p],
+    "sim_box_scale_after_first": [_P(SimEngine), c_p, ctypes.c_int32, _P(SimBoxScale), c_p, _P(SimIntegrator),
+                                  ctypes.c_int32, c_p],
     "sim_indenter_add": [_P(SimEngine), _P(SimIndenter), ctypes.c_int32, c_p],
     "sim_batch_crack_observe": [c_p, c_p, c_p, ctypes.c_int32, c_p, c_p, c_p, c_p],
     "sim_gather_original_f64": [_P(SimEngine), c_p, c_p, c_p],

@@ -130,6 +130,15 @@ class AnisotropicNPTBarostat:
         _lib.call("sim_aniso_npt", eng.st_ref, self._ref, _lib.ptr(self.work), eng.stream)
         return self.work[0:3]
 
+    def controller(self, dt: float):
+        """step() without moving the atoms: the axis pressures, the strain-rate
+        update and the new box are prepared in ``work``; a loader's next
+        update moves the atoms for both (UniaxialTensileLoader.launch_after)."""
+        eng = self.molecular.engine
+        self._st.dt = float(dt)
+        _lib.call("sim_aniso_control", eng.st_ref, self._ref, _lib.ptr(self.work), eng.stream)
+        return self.work[0:3]
+
     def pressure(self) -> torch.Tensor:
         """Axis pressures (bar) of the last step (device tensor)."""
         return self.work[0:3]

@@ -400,7 +400,8 @@ __global__ void __launch_bounds__(BATCH_DENSITY_THREADS, 3) k_bb_density(SimBatc
     const float rc2 = t.cutoff * t.cutoff;
     const bool use_mask = e.cut_mask != nullptr && e.nbr_cap <= 64;
     const int lane = threadIdx.x & 31;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const BlockRange br = block_range(e.n);   // warp-aligned: a warp's 32 slots stay in one replica
+    for (int64_t i = br.begin + threadIdx.x; i < br.end; i += blockDim.x) {
         bool real;
         const int k = slot_replica(B, i, real);
         const BoxF b(B.rep[k].box);
@@ -486,7 +487,8 @@ __global__ void __launch_bounds__(BATCH_FORCE_THREADS, 1) k_bb_force(SimBatch B,
     const int lane = threadIdx.x & 31;
     bool bad = false;
     const uint64_t step = MODE && ip.step_ctr ? *ip.step_ctr : 0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const BlockRange br = block_range(e.n);   // warp-aligned: a warp's 32 slots stay in one replica
+    for (int64_t i = br.begin + threadIdx.x; i < br.end; i += blockDim.x) {
         bool real;
         const int k = slot_replica(B, i, real);
         const SimRep& R = B.rep[k];

@@ -34,6 +34,21 @@ int launch_eam_force_tiled(const SimEngine& e, const SimEAMTables& t, const SimI
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// This block's share of [0, n) for the persistent per-atom passes: one
+// contiguous range per block, the ranges equal to within a warp's 32 slots
+// (ceil(n / blocks) rounded up to whole warps).  Against a grid-stride walk
+// of blockDim-sized tiles, every SM gets the same work (a tile left over for
+// some blocks held their SMs for a whole extra tile) and consecutive
+// iterations of a block gather from overlapping neighbourhoods.
+struct BlockRange {
+    int64_t begin, end;
+};
+__device__ __forceinline__ BlockRange block_range(int64_t n) {
+    const int64_t c = ((n + gridDim.x - 1) / gridDim.x + 31) / 32 * 32;
+    const int64_t b = (int64_t)blockIdx.x * c;
+    return BlockRange{b < n ? b : n, b + c < n ? b + c : n};
+}
+
 // Loads of data read once per pass (neighbour-list rows, in-cutoff masks):
 // evict-first in L1 and L2, so the caches keep the gathered neighbour
 // positions instead.

@@ -10,8 +10,10 @@
 //
 // Design: one thread per atom over the full ELL list (no atomics, bitwise
 // reproducible).  Persistent grids: each block stages its tables in shared
-// memory once.  Tables are stored as value + forward difference so each
-// interpolation is one FMA, and pass 2 fetches {f', phi', df', dphi'} with one
+// memory once and walks one contiguous, warp-aligned share of the atoms
+// (block_range), so every SM gets the same work.  Tables are stored as value
+// + forward difference so each interpolation is one FMA, and pass 2 fetches
+// {f', phi', df', dphi'} with one
 // 16-byte load and interpolates f' and phi' with one packed FP32x2 FMA.
 // Pass 1 writes a 16-byte record {fixed-point x, y, z, F'} per atom so pass 2
 // gathers a neighbour's position and F'(rho) together.  Rows of the list are
@@ -28,13 +30,13 @@ namespace simb200 {
 #define EAM_DENSITY_THREADS 512
 #endif
 #ifndef EAM_DENSITY_MIN_BLOCKS
-#define EAM_DENSITY_MIN_BLOCKS 3  // 3 x 512 threads per SM (<= 40 registers)
+#define EAM_DENSITY_MIN_BLOCKS 2  // 2 x 512 threads per SM (<= 64 registers)
 #endif
 #ifndef EAM_CARVEOUT_PCT
 #define EAM_CARVEOUT_PCT -1       // shared-memory carveout hint in percent (-1: driver default)
 #endif
 #ifndef EAM_DENSITY_UNROLL
-#define EAM_DENSITY_UNROLL 4      // list entries gathered together in pass 1 (divides 32)
+#define EAM_DENSITY_UNROLL 8      // list entries gathered together in pass 1 (divides 32)
 #endif
 #ifndef EAM_FORCE_THREADS
 #define EAM_FORCE_THREADS 1024
@@ -67,8 +69,8 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k
     const float rc2 = t.cutoff * t.cutoff;
     const bool use_mask = e.cut_mask != nullptr && e.nbr_cap <= 64;
     double acc = 0.0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += stride) {
+    const BlockRange br = block_range(e.n);
+    for (int64_t i = br.begin + threadIdx.x; i < br.end; i += blockDim.x) {
         const int4 qi = posq[i];
         const int ti = qi.w;
         const int nn = e.nnbr[i];
@@ -166,7 +168,8 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
     bool bad = false, trig = false;
     const uint64_t step = INTEG && ip.step_ctr ? *ip.step_ctr : 0;
     double iv[IND ? 11 : 1] = {0};     // indenter: energy, force (3), contacts, virial xx yy zz xy xz yz
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const BlockRange br = block_range(e.n);
+    for (int64_t i = br.begin + threadIdx.x; i < br.end; i += blockDim.x) {
         const int4 pi = posfp[i];
         const float fpi = __int_as_float(pi.w);
         const int nn = e.nnbr[i];

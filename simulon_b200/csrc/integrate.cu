@@ -373,6 +373,103 @@ __global__ void k_box_commit(SimEngine e, const double* work) {
     *e.box = *reinterpret_cast<const SimBox*>(work + 16);
 }
 
+// A loader's box update prepared on the box that an earlier update in the
+// same step (the barostat's, work_prev) is about to commit: as k_box_prepare
+// with work_prev's new box in place of *e.box.
+__global__ void k_box_prepare_after(SimBoxScale p, const double* work_prev, double* work) {
+    pdl_wait();
+    for (int a = 0; a < 3; ++a) {
+        work[a] = 0.0;
+        work[3 + a] = p.scale[a];
+        work[6 + a] = p.vel_scale[a];
+    }
+    prepare_scaled_box(*reinterpret_cast<const SimBox*>(work_prev + 16), p.scale, work_box(work));
+}
+
+// One box update of an atom held in registers, with k_scale_atoms' arithmetic:
+// position through fractional coordinates of box ob into nb and wrapped,
+// velocity scaled, the skin test against the reference code xr, and (reset)
+// the reference moved to the new code.
+__device__ __forceinline__ bool scale_atom_regs(const SimEngine& e, const SimBox& ob, const SimBox& nb,
+                                                const double* vs, double* x, double* v, uint32_t* xr, int reset,
+                                                bool& bad) {
+    double s[3], xn[3];
+    cart_to_frac(ob, x[0], x[1], x[2], s);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) xn[c] = fma(s[2], nb.H[6 + c], fma(s[1], nb.H[3 + c], s[0] * nb.H[c]));
+    if (nb.orthogonal) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double d = nb.H[4 * c];
+            xn[c] = xn[c] - floor(xn[c] / d) * d;
+        }
+    } else {
+        double t[3];
+        cart_to_frac(nb, xn[0], xn[1], xn[2], t);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) t[c] -= floor(t[c]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) xn[c] = fma(t[2], nb.H[6 + c], fma(t[1], nb.H[3 + c], t[0] * nb.H[c]));
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        x[c] = xn[c];
+        v[c] = v[c] * vs[c];
+        bad |= !isfinite(xn[c]) || !isfinite(v[c]);
+    }
+    // place_atom's code and skin test, in registers
+    double f[3];
+    cart_to_frac(nb, xn[0], xn[1], xn[2], f);
+    const uint32_t q[3] = {to_fixed(f[0]), to_fixed(f[1]), to_fixed(f[2])};
+    const double t0 = (double)(int32_t)(q[0] - xr[0]) * 2.3283064365386963e-10;
+    const double t1 = (double)(int32_t)(q[1] - xr[1]) * 2.3283064365386963e-10;
+    const double t2 = (double)(int32_t)(q[2] - xr[2]) * 2.3283064365386963e-10;
+    const double d0 = t0 * nb.H[0] + t1 * nb.H[3] + t2 * nb.H[6];
+    const double d1 = t0 * nb.H[1] + t1 * nb.H[4] + t2 * nb.H[7];
+    const double d2 = t0 * nb.H[2] + t1 * nb.H[5] + t2 * nb.H[8];
+    if (reset) {
+        xr[0] = q[0]; xr[1] = q[1]; xr[2] = q[2];
+    }
+    return d0 * d0 + d1 * d1 + d2 * d2 > e.skin_half2;
+}
+
+// Two box updates in sequence -- the barostat's of step s (w1) then a
+// loader's of step s+1 (w2, prepared by k_box_prepare_after) -- followed by
+// the first half of step s+1 (as k_first_half, in box w2), in one pass over
+// the atoms: the operations and their order are those of k_scale_atoms twice
+// and k_first_half, so the results are the same bits.  The box is committed
+// by k_box_commit(w2) afterwards.
+__global__ void __launch_bounds__(SIM_THREADS) k_two_scales_first(SimEngine e, const double* w1, const double* w2,
+                                                                  int reset1, int reset2, SimIntegrator p, int prec) {
+    pdl_trigger();
+    pdl_wait();
+    const int64_t P = e.n_pad;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool trig = false, bad = false;
+    if (i == 0 && p.step_ctr) *p.step_ctr += 1;   // as k_first_half
+    if (i < e.n) {
+        const SimBox& ob = *e.box;
+        const SimBox& nb1 = *reinterpret_cast<const SimBox*>(w1 + 16);
+        const SimBox& nb2 = *reinterpret_cast<const SimBox*>(w2 + 16);
+        double x[3], v[3];
+        uint32_t xr[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            x[c] = e.x[c * P + i];
+            v[c] = e.v[c * P + i];
+            xr[c] = (uint32_t)e.xref[c * P + i];
+        }
+        trig |= scale_atom_regs(e, ob, nb1, w1 + 6, x, v, xr, reset1, bad);
+        trig |= scale_atom_regs(e, nb1, nb2, w2 + 6, x, v, xr, reset2, bad);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) e.xref[c * P + i] = (int32_t)xr[c];
+        const double f[3] = {load_force(e, prec, i, 0), load_force(e, prec, i, 1), load_force(e, prec, i, 2)};
+        trig |= first_half_atom(e, nb2, p, i, e.posq[4 * i + 3], f, v, bad, x);
+    }
+    if (__any_sync(0xffffffffu, trig) && (threadIdx.x & 31) == 0) e.flags[0] = 1;
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+}
+
 static int launch_box_scale(const SimEngine& e, double* work, int reset, cudaStream_t st, const char* what) {
     cudaError_t err = launch_pdl(k_scale_atoms, dim3((unsigned)ceil_div(e.n, SIM_THREADS)), dim3(SIM_THREADS), 0, st,
                                  e, (const double*)work, reset);
@@ -703,4 +800,29 @@ extern "C" int sim_loader_check(const SimEngine* ep, const SimLoaderCheck* p, do
     const cudaError_t err = launch_pdl(k_loader_check, dim3(1), dim3(1), 0, (cudaStream_t)stream, *ep, *p, state);
     if (err != cudaSuccess) { set_cuda_error(err, "sim_loader_check: launch"); return SIM_ERR_CUDA; }
     return launch_status("sim_loader_check");
+}
+
+extern "C" int sim_aniso_control(const SimEngine* ep, const SimAniso* p, double* work, void* stream) {
+    if (!ep || !p || !work || ep->n <= 0 || !p->eta_dot || (p->stochastic && !p->counter)) return SIM_ERR_ARG;
+    const cudaError_t err = launch_pdl(k_aniso_control, dim3(1), dim3(1), 0, (cudaStream_t)stream, *ep, *p, work);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_aniso_control: launch"); return SIM_ERR_CUDA; }
+    return launch_status("sim_aniso_control");
+}
+
+extern "C" int sim_box_scale_after_first(const SimEngine* ep, const double* work_prev, int32_t reset_prev,
+                                         const SimBoxScale* p, double* work, const SimIntegrator* integ,
+                                         int32_t force_precision, void* stream) {
+    if (!ep || !work_prev || !p || !work || !integ || ep->n <= 0 || (force_precision == 1 && !ep->f64))
+        return SIM_ERR_ARG;
+    for (int a = 0; a < 3; ++a)
+        if (!(p->scale[a] > 0.0) || !(p->vel_scale[a] > 0.0)) return SIM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t err = launch_pdl(k_box_prepare_after, dim3(1), dim3(1), 0, st, *p, work_prev, work);
+    if (err == cudaSuccess)
+        err = launch_pdl(k_two_scales_first, dim3((unsigned)ceil_div(ep->n, SIM_THREADS)), dim3(SIM_THREADS), 0, st,
+                         *ep, work_prev, (const double*)work, (int)reset_prev, (int)p->reset_reference, *integ,
+                         (int)force_precision);
+    if (err == cudaSuccess) err = launch_pdl(k_box_commit, dim3(1), dim3(1), 0, st, *ep, (const double*)work);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_box_scale_after_first: launch"); return SIM_ERR_CUDA; }
+    return launch_status("sim_box_scale_after_first");
 }

@@ -82,8 +82,8 @@ __global__ void __launch_bounds__(SIM_THREADS, LJ_MIN_BLOCKS) k_lj_f32(SimEngine
     float acc[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};   // as k_eam_force's
     bool bad = false, trig = false;
     const uint64_t step = INTEG && ip.step_ctr ? *ip.step_ctr : 0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += stride) {
+    const BlockRange br = block_range(e.n);
+    for (int64_t i = br.begin + threadIdx.x; i < br.end; i += blockDim.x) {
         const int4 qi = posq[i];
         const int ti = qi.w;
         const int nn = e.nnbr[i];
@@ -215,8 +215,8 @@ __global__ void __launch_bounds__(SIM_THREADS) k_lj_f64(SimEngine e, SimLJParams
     const double rc = p.rc, rs = p.rs;
     const LJConst64 c1 = SINGLE ? lj_const64(p, 0) : LJConst64{0, 0, 0, 0, 0};
     double vals[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += stride) {
+    const BlockRange br = block_range(e.n);
+    for (int64_t i = br.begin + threadIdx.x; i < br.end; i += blockDim.x) {
         const double xi0 = e.x[i], xi1 = e.x[P + i], xi2 = e.x[2 * P + i];
         const int ti = e.posq[4 * i + 3];
         const int nn = e.nnbr[i];

@@ -122,6 +122,25 @@ class BaseModel(nn.Module):
         scaling of step s runs inside step s+1's first half; the last step
         scales them itself."""
         if pre_step is not None:
+            loader = getattr(pre_step, "loader", None)
+            baro = self.barostat
+            if (k > 1 and loader is not None and callable(getattr(loader, "launch_after", None))
+                    and callable(getattr(baro, "controller", None)) and hasattr(baro, "work")
+                    and hasattr(self.Integrator, "params")):
+                # tensile loop: the barostat's atom scaling of step s, the
+                # loader's update and the first half of step s+1 in one pass
+                pre_step()
+                self.Integrator.first_half()
+                for s in range(k):
+                    self._forces_and_second_half()
+                    if s < k - 1:
+                        baro.controller(self.Integrator.dt)
+                        self.engine.log_step()
+                        loader.launch_after(baro, self.Integrator, pre_step.dt)
+                    else:
+                        baro.step(self.Integrator.dt)
+                        self.engine.log_step()
+                return
             for _ in range(k):
                 pre_step()
                 self._step_launches()

@@ -45,7 +45,10 @@ class UniaxialTensileLoader:
     ``launch(dt)`` only enqueues the work (returns the strain as a device
     scalar), so ``model.run(n, pre_step=...)`` can capture loader and MD
     steps together in CUDA graphs; ``run(model, n_steps, dt)`` does that in
-    chunks and regrids between them (``maintain``)."""
+    chunks and regrids between them (``maintain``).  With an anisotropic
+    barostat the model then runs the barostat's atom scaling of step s, the
+    loader's update and the first half of step s+1 as one pass
+    (``launch_after``)."""
 
     def __init__(self, molecular, axis: int = 0, strain_rate: float = 1.0e-3, lateral_mode: str = "fixed",
                  poisson_ratio: float = 0.28, max_lateral_scale_step: float = 2.0e-3, regrid_margin: float = 0.01):
@@ -103,6 +106,33 @@ class UniaxialTensileLoader:
         _lib.call("sim_loader_check", eng.st_ref, ctypes.byref(self._check), _lib.ptr(self.state), eng.stream)
         return self.state[12]
 
+    def launch_after(self, barostat, integrator, dt: float) -> torch.Tensor:
+        """The next step's start in one pass: the barostat's box update prepared
+        by barostat.controller(), this loader's update, and integrator's
+        first half (sim_box_scale_after_first), then the bookkeeping and the
+        conditional rebuild; the same bits as barostat.step(), launch(dt) and
+        integrator.first_half() one after another."""
+        eng = self.molecular.engine
+        s = _lib.SimBoxScale()
+        s.scale[:] = self._scale_vector(dt)
+        s.vel_scale[:] = [1.0, 1.0, 1.0]
+        s.reset_reference = 1
+        _lib.call("sim_box_scale_after_first", eng.st_ref, _lib.ptr(barostat.work), int(barostat._st.reset_reference),
+                  ctypes.byref(s), _lib.ptr(self.work), integrator.params.ref, int(integrator.force_precision),
+                  eng.stream)
+        _lib.call("sim_loader_check", eng.st_ref, ctypes.byref(self._check), _lib.ptr(self.state), eng.stream)
+        eng.rebuild_if_needed()
+        return self.state[12]
+
+    def hook(self, dt: float):
+        """The per-step callable for BaseModel.run(pre_step=...): launch(dt),
+        marked so that the model can fuse it with a barostat's scaling and
+        the first half-step (launch_after)."""
+        h = self._hooks.get(float(dt))
+        if h is None:
+            h = self._hooks[float(dt)] = _LoaderHook(self, float(dt))
+        return h
+
     def maintain(self) -> bool:
         """Regrid when the device asked for it (synchronises); True if it did."""
         if float(self.state[17].item()) == 0.0:
@@ -127,9 +157,7 @@ class UniaxialTensileLoader:
         """n_steps of (loader step, MD step) captured together in CUDA graphs of
         graph_steps steps, regridding between graphs when asked; returns the
         engineering strain as a device scalar."""
-        hook = self._hooks.get(float(dt))
-        if hook is None:
-            hook = self._hooks[float(dt)] = (lambda: self.launch(dt))
+        hook = self.hook(dt)
         done = 0
         while done < int(n_steps):
             k = min(int(graph_steps), int(n_steps) - done)
@@ -144,6 +172,16 @@ class UniaxialTensileLoader:
 
     def current_lengths(self) -> torch.Tensor:
         return torch.tensor(np.linalg.norm(self.molecular.engine.box_matrix(), axis=1), dtype=torch.float64)
+
+
+class _LoaderHook:
+    """UniaxialTensileLoader.launch(dt) as a BaseModel.run pre-step."""
+
+    def __init__(self, loader, dt: float):
+        self.loader, self.dt = loader, float(dt)
+
+    def __call__(self):
+        return self.loader.launch(self.dt)
 
 
 class SphericalIndenterForce(BackboneInterface):

@@ -74,6 +74,14 @@ def test_argument_errors_are_reported_without_gpu(lib):
         chk.axis, chk.rebuild_strain, chk.regrid_margin = axis, strain, margin
         assert lib.sim_loader_check(ctypes.byref(e), ctypes.byref(chk), ctypes.c_void_p(16), None) == \
             _lib.SIM_ERR_ARG
+    # the fused tensile pieces
+    assert lib.sim_aniso_control(None, None, None, None) == _lib.SIM_ERR_ARG
+    bs = _lib.SimBoxScale()
+    bs.scale[:] = [1.0, 1.0, 1.0]
+    bs.vel_scale[:] = [1.0, 0.0, 1.0]     # a non-positive factor
+    assert lib.sim_box_scale_after_first(ctypes.byref(e), ctypes.c_void_p(16), 1, ctypes.byref(bs),
+                                         ctypes.c_void_p(16), ctypes.byref(ip), 0, None) == _lib.SIM_ERR_ARG
+    assert lib.sim_box_scale_after_first(None, None, 1, None, None, None, 0, None) == _lib.SIM_ERR_ARG
     with pytest.raises(_lib.SimError):
         _lib.check(_lib.SIM_ERR_ARG, "probe")
 

@@ -22,6 +22,11 @@ DEV = torch.device("cuda")
 
 
 @pytest.fixture(scope="module")
+def fsw_path(tmp_path_factory):
+    return oin.write_fs_w_setfl(str(tmp_path_factory.mktemp("pot") / "W_synthetic.eam.fs"))
+
+
+@pytest.fixture(scope="module")
 def sb():
     import simulon_b200
     simulon_b200._lib.load()
@@ -83,6 +88,63 @@ def test_tensile_and_aniso_npt_match_reference(sb, tmp_path, name, graph):
         assert mol.engine.status() == 0
     finally:
         torch.set_default_dtype(torch.float32)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_fused_tensile_steps_equal_per_step_calls(sb, tmp_path, fsw_path, precision):
+    """loader.run (CUDA graphs; the barostat's atom scaling of step s, the
+    loader's update and the first half of step s+1 in one pass,
+    sim_box_scale_after_first) against the reference-shaped loop
+    loader.step(dt); model() with separate launches: positions, velocities,
+    box, strain rates and step-log rows bit for bit.  LJ argon with FP64 forces
+    and EAM tungsten with FP32 forces."""
+    from simulon_b200.barostat import AnisotropicNPTBarostat
+    from simulon_b200.mechanics import UniaxialTensileLoader
+    old = torch.get_default_dtype()
+    res = []
+    for mode in ("calls", "run"):
+        if precision == "f64":
+            torch.set_default_dtype(torch.float64)
+            x, L = oin.fcc_lattice(3)
+            x = oin.jitter(x, 0.05, 0)
+            v = oin.maxwell_boltzmann(np.full(len(x), oin.AR_MASS), 94.4, 1)
+            mol = sb.AtomFileReader.from_arrays(["Ar"] * len(x), x, L, 7.0, device=DEV, skin_thickness=0.5,
+                                                parameter={"[0 0]": {"epsilon": 0.0104, "sigma": 3.405}})
+            ff = sb.LennardJonesForce(mol)
+            T = 94.4
+        else:
+            x, L = oin.bcc_lattice(8)
+            x = oin.jitter(x, 0.05, 71)
+            v = oin.maxwell_boltzmann(np.full(len(x), oin.W_MASS), 300.0, 72)
+            parser = sb.EAMParser(fsw_path)
+            mol = sb.AtomFileReader.from_arrays(["W"] * len(x), x, L, parser.cutoff, device=DEV, skin_thickness=0.5,
+                                                is_fs=True)
+            ff = sb.EAMForceCUDAExt(parser, mol)
+            T = 300.0
+        try:
+            integ = sb.VerletIntegrator(mol, dt=0.002, ensemble="NVE")
+            mol.atom_velocities = torch.tensor(v, device=DEV)
+            baro = AnisotropicNPTBarostat(mol, [0.0, 0.0, 0.0], temperature_k=T, control_axes=(False, True, True),
+                                          compressibility_bar_inv=3.2e-5)
+            model = sb.BaseModel(sb.SumBackboneInterface([ff], mol), integ, mol, barostat=baro)
+            loader = UniaxialTensileLoader(mol, axis=0, strain_rate=2.0)
+            if mode == "calls":
+                for _ in range(12):
+                    loader.step(0.002)
+                    model()
+            else:
+                loader.run(model, 12, 0.002, graph_steps=5)
+            torch.cuda.synchronize()
+            eng = mol.engine
+            res.append((eng.gather("x").cpu().numpy(), eng.gather("v").cpu().numpy(), eng.box_matrix(),
+                        baro.eta_dot.cpu().numpy(), model.step_log(0, 12).cpu().numpy(), float(loader.state[12])))
+            assert eng.status() == 0
+        finally:
+            torch.set_default_dtype(old)
+    a, b = res
+    for k in range(5):
+        np.testing.assert_array_equal(a[k], b[k])
+    assert a[5] == b[5]
 
 
 def test_cell_guard_and_regrid(sb, tmp_path):
