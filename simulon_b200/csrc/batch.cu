@@ -267,10 +267,10 @@ __global__ void k_bb_slot_cells(SimBatch B, int only_flagged) {
 }
 
 #define BATCH_ELL_WARPS 4
-__global__ void __launch_bounds__(BATCH_ELL_WARPS * 32) k_bb_build_ell(SimBatch B, float rc2_list, int only_flagged) {
-    __shared__ uint64_t keys[BATCH_ELL_WARPS][ELL_SORT_MAX];
-    __shared__ int4 cq[BATCH_ELL_WARPS][ELL_CELL_CAND];
-    __shared__ int cj[BATCH_ELL_WARPS][ELL_CELL_CAND];
+template <bool ORTH>
+__global__ void __launch_bounds__(BATCH_ELL_WARPS * 32, ORTH ? 5 : 4) k_bb_build_ell(SimBatch B, float rc2_list,
+                                                                                   int only_flagged) {
+    __shared__ uint64_t keys[BATCH_ELL_WARPS][ELL_KEYS];
     const SimEngine& e = B.e;
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
     const int warp = threadIdx.x >> 5;
@@ -299,8 +299,8 @@ __global__ void __launch_bounds__(BATCH_ELL_WARPS * 32) k_bb_build_ell(SimBatch 
         const SimRep& R = B.rep[W.ids[f]];
         const int32_t* rank = e.cell_rank + 2 * R.cell_off;
         const CellGrid g{&R.box, R.ncell[0], R.ncell[1], R.ncell[2], rank, e.cell_start + R.cell_off};
-        ell_cell_warp(posq, t - W.cells[f], rank + R.n_cells, g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr,
-                      e.flags, keys[warp], cq[warp], cj[warp]);
+        ell_cell_warp<ORTH>(posq, t - W.cells[f], rank + R.n_cells, g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr,
+                            e.flags, keys[warp]);
     }
 }
 
@@ -337,7 +337,11 @@ static int batch_rebuild(const SimBatch& B, int only_flagged, cudaStream_t st) {
     k_bb_slot_cells<<<g, SIM_THREADS, 0, st>>>(B, only_flagged);
     const float rc2_list = (float)(B.e.x_rc * B.e.x_rc * (1.0 + 4e-6));
     const int64_t ge = ceil_div(B.n_cell_entries, BATCH_ELL_WARPS);
-    k_bb_build_ell<<<(int)(ge > 148 * 64 ? 148 * 64 : ge), BATCH_ELL_WARPS * 32, 0, st>>>(B, rc2_list, only_flagged);
+    const int gb = (int)(ge > 148 * 64 ? 148 * 64 : ge);
+    if (B.e.box_orthogonal)
+        k_bb_build_ell<true><<<gb, BATCH_ELL_WARPS * 32, 0, st>>>(B, rc2_list, only_flagged);
+    else
+        k_bb_build_ell<false><<<gb, BATCH_ELL_WARPS * 32, 0, st>>>(B, rc2_list, only_flagged);
     k_bb_finish<<<1, 256, 0, st>>>(B, only_flagged);
     return launch_status("sim_batch_rebuild");
 }

@@ -56,7 +56,8 @@ __device__ __forceinline__ void warp_sort_cell(int32_t* perm, const int32_t* ori
 }
 
 #define ELL_SORT_MAX 128    // rows up to this length are sorted by distance
-#define ELL_CELL_CAND 384   // candidates of one cell's stencil kept in shared memory
+#define ELL_REG_ROUNDS 8    // stencil candidates a warp holds in registers: 32 per round
+#define ELL_KEYS (2 * ELL_SORT_MAX)   // shared key buffer of one warp (two rows)
 
 // One periodic box's cells: linear cell index -> rank (visiting order) ->
 // first slot of the cell (start has one entry more than there are cells).
@@ -67,32 +68,42 @@ struct CellGrid {
     const int32_t* start;
 };
 
-// The FP32 box terms in registers (read once, not per candidate).
+// The FP32 box terms in registers (read once, not per candidate), each
+// scaled by 2^-32: a fixed-point difference converted to float times a
+// scaled term is the same float as the difference in box units
+// (fixed_delta) times the term, since a power-of-two scaling is exact, so
+// the distances below are those of frac_to_cart_f.
 struct ListBox {
     float h[9];
     bool orth;
     __device__ __forceinline__ explicit ListBox(const SimBox& b) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) h[k] = b.Hf[k];
+        for (int k = 0; k < 9; ++k) h[k] = b.Hf[k] * 2.3283064365386963e-10f;
         orth = b.orthogonal != 0;
     }
 };
 
 // Squared minimum-image distance of two fixed-point positions, with the
 // arithmetic of frac_to_cart_f and an unfused sum of squares.
-__device__ __forceinline__ float list_d2(const ListBox& b, const int4& qi, const int4& qj) {
-    const float t0 = fixed_delta(qi.x, qj.x), t1 = fixed_delta(qi.y, qj.y), t2 = fixed_delta(qi.z, qj.z);
+template <bool ORTH>
+__device__ __forceinline__ float list_d2_t(const ListBox& b, const int4& qi, const int4& qj) {
+    const float t0 = __int2float_rn((int32_t)((uint32_t)qi.x - (uint32_t)qj.x));
+    const float t1 = __int2float_rn((int32_t)((uint32_t)qi.y - (uint32_t)qj.y));
+    const float t2 = __int2float_rn((int32_t)((uint32_t)qi.z - (uint32_t)qj.z));
     float r0, r1, r2;
-    if (b.orth) {
-        r0 = t0 * b.h[0];
-        r1 = t1 * b.h[4];
-        r2 = t2 * b.h[8];
+    if (ORTH) {
+        r0 = __fmul_rn(t0, b.h[0]);
+        r1 = __fmul_rn(t1, b.h[4]);
+        r2 = __fmul_rn(t2, b.h[8]);
     } else {
-        r0 = fmaf(t2, b.h[6], fmaf(t1, b.h[3], t0 * b.h[0]));
-        r1 = fmaf(t2, b.h[7], fmaf(t1, b.h[4], t0 * b.h[1]));
-        r2 = fmaf(t2, b.h[8], fmaf(t1, b.h[5], t0 * b.h[2]));
+        r0 = fmaf(t2, b.h[6], fmaf(t1, b.h[3], __fmul_rn(t0, b.h[0])));
+        r1 = fmaf(t2, b.h[7], fmaf(t1, b.h[4], __fmul_rn(t0, b.h[1])));
+        r2 = fmaf(t2, b.h[8], fmaf(t1, b.h[5], __fmul_rn(t0, b.h[2])));
     }
     return __fadd_rn(__fadd_rn(__fmul_rn(r0, r0), __fmul_rn(r1, r1)), __fmul_rn(r2, r2));
+}
+__device__ __forceinline__ float list_d2(const ListBox& b, const int4& qi, const int4& qj) {
+    return b.orth ? list_d2_t<true>(b, qi, qj) : list_d2_t<false>(b, qi, qj);
 }
 
 // Sort key of a list entry: d^2 bits (non-negative floats order like their
@@ -229,67 +240,154 @@ __device__ __forceinline__ void ell_row_warp(const int4* __restrict__ posq, int6
     ell_row_done(i, cnt, cap, nnbr, flags);
 }
 
-// All rows of the atoms in cell `r` (visiting rank), built by one warp: the
-// candidates of the cell's stencil are gathered once into shared memory (cq,
-// cj: ELL_CELL_CAND entries) and tested against each atom of the cell in turn,
-// so a candidate's position is read from global memory once per cell instead
-// of once per atom.  Rows come out equal to ell_row_warp's; cells whose
-// stencil holds more than ELL_CELL_CAND atoms, and rows longer than
-// ELL_SORT_MAX, are built by ell_row_warp.
-__device__ __forceinline__ void ell_cell_warp(const int4* __restrict__ posq, int r, const int32_t* lin_of_rank,
-                                              const CellGrid& g, float rc2_list, int32_t* nbr, int64_t P, int cap,
-                                              int32_t* nnbr, int32_t* flags, uint64_t* keys, int4* cq, int* cj) {
+// Sorted writes of two rows at once (i1's row empty when n1 is 0), each of up
+// to 32 entries held one per lane: an entry's rank counts the row's entries
+// with a smaller d^2 (shuffled from their lanes; d^2 bits are below 2^31, so
+// the sign of their difference is the comparison) plus, among the entries of
+// equal d^2 (__match_any_sync; a perfect lattice has many), those with a
+// smaller slot -- the order of list_key.  Every lane of the warp must call
+// this.
+__device__ __forceinline__ void ell_write_sorted2(int64_t i0, int n0, const uint64_t* k0, int64_t i1, int n1,
+                                                  const uint64_t* k1, int32_t* nbr, int64_t P) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    const bool on0 = lane < n0, on1 = lane < n1;
+    const uint64_t e0 = on0 ? k0[lane] : 0x7fffffff00000000ull, e1 = on1 ? k1[lane] : 0x7fffffff00000000ull;
+    const int32_t d0 = (int32_t)(e0 >> 32), d1 = (int32_t)(e1 >> 32);   // padded lanes: 2^31 - 1, above every d^2
+    const int j0 = (int32_t)(uint32_t)e0, j1 = (int32_t)(uint32_t)e1;
+    const int n = n0 > n1 ? n0 : n1;
+    int r0 = 0, r1 = 0;
+#pragma unroll 4
+    for (int f = 0; f < n; ++f) {
+        r0 += (int)((uint32_t)(__shfl_sync(FULL, d0, f) - d0) >> 31);
+        r1 += (int)((uint32_t)(__shfl_sync(FULL, d1, f) - d1) >> 31);
+    }
+    const unsigned self = 1u << lane;
+    const unsigned g0 = __match_any_sync(FULL, d0), g1 = __match_any_sync(FULL, d1);
+    unsigned t0 = on0 ? g0 & ~self : 0u;
+    unsigned t1 = on1 ? g1 & ~self : 0u;
+    while (__any_sync(FULL, (t0 | t1) != 0u)) {
+        const int f0 = t0 ? __ffs(t0) - 1 : lane, f1 = t1 ? __ffs(t1) - 1 : lane;
+        r0 += __shfl_sync(FULL, j0, f0) < j0 ? 1 : 0;
+        r1 += __shfl_sync(FULL, j1, f1) < j1 ? 1 : 0;
+        t0 &= t0 - 1u;
+        t1 &= t1 - 1u;
+    }
+    if (on0) nbr[(int64_t)r0 * P + i0] = j0;
+    if (on1) nbr[(int64_t)r1 * P + i1] = j1;
+}
+
+// Candidates of a stencil chunk in registers: lane l holds candidates
+// base + l + 32 m (m < ELL_REG_ROUNDS) of the flattened stencil; slot -1 past
+// its end.  Every lane of the warp must call this.
+struct CellCands {
+    int4 q[ELL_REG_ROUNDS];
+    int j[ELL_REG_ROUNDS];
+};
+__device__ __forceinline__ void load_cands(const int4* __restrict__ posq, const Stencil& st, int base,
+                                           CellCands& c) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int m = 0; m < ELL_REG_ROUNDS; ++m) {
+        c.j[m] = -1;
+        c.q[m] = make_int4(0, 0, 0, 0);
+        if (base + m * 32 < st.total) {                  // uniform
+            const int t = base + m * 32 + lane;
+            const int j = stencil_slot(st, t);
+            if (t < st.total) {
+                c.j[m] = j;
+                c.q[m] = posq[j];
+            }
+        }
+    }
+}
+
+// One chunk's candidates tested against two atoms (i0, i1; i1's results
+// dropped unless `two`): accepted entries are compacted in visiting order
+// through ballots into the rows' key buffers (k0, k1), counts in c0, c1.
+template <bool ORTH>
+__device__ __forceinline__ void sweep2(const ListBox& b, const CellCands& c, int rem, int i0, int i1, int4 q0,
+                                       int4 q1, bool two, float rc2_list, uint64_t* k0, uint64_t* k1, int& c0,
+                                       int& c1) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned below = (1u << (threadIdx.x & 31)) - 1u;
+#pragma unroll
+    for (int m = 0; m < ELL_REG_ROUNDS; ++m) {
+        if (m * 32 >= rem) break;                        // uniform
+        const int j = c.j[m];
+        const float d0 = list_d2_t<ORTH>(b, q0, c.q[m]);
+        const float d1 = list_d2_t<ORTH>(b, q1, c.q[m]);
+        const bool a0 = j >= 0 && j != i0 && d0 < rc2_list;
+        const bool a1 = two && j >= 0 && j != i1 && d1 < rc2_list;
+        const unsigned m0 = __ballot_sync(FULL, a0), m1 = __ballot_sync(FULL, a1);
+        const int p0 = c0 + __popc(m0 & below), p1 = c1 + __popc(m1 & below);
+        if (a0 && p0 < ELL_SORT_MAX) k0[p0] = list_key(d0, j);
+        if (a1 && p1 < ELL_SORT_MAX) k1[p1] = list_key(d1, j);
+        c0 += __popc(m0);
+        c1 += __popc(m1);
+    }
+}
+
+template <bool ORTH>
+__device__ __forceinline__ void ell_cell_rows(const int4* __restrict__ posq, int a0, int a1, int lin,
+                                              const Stencil& st, const ListBox& b, const CellGrid& g,
+                                              float rc2_list, int32_t* nbr, int64_t P, int cap, int32_t* nnbr,
+                                              int32_t* flags, uint64_t* keys) {
+    uint64_t* k0 = keys;
+    uint64_t* k1 = keys + ELL_SORT_MAX;
+    const int chunk = ELL_REG_ROUNDS * 32;
+    const bool one_chunk = st.total <= chunk;
+    CellCands c;
+    if (one_chunk) load_cands(posq, st, 0, c);
+    for (int i = a0; i < a1; i += 2) {
+        const bool two = i + 1 < a1;
+        const int i1 = two ? i + 1 : i;
+        const int4 q0 = posq[i], q1 = posq[i1];
+        int c0 = 0, c1 = 0;
+        for (int base = 0; base < st.total; base += chunk) {
+            if (!one_chunk) load_cands(posq, st, base, c);
+            sweep2<ORTH>(b, c, st.total - base, i, i1, q0, q1, two, rc2_list, k0, k1, c0, c1);
+        }
+        __syncwarp();
+        const int kept0 = c0 < cap ? c0 : cap;
+        const int kept1 = two ? (c1 < cap ? c1 : cap) : 0;
+        // rows longer than the sort buffer: built again by ell_row_warp (visiting order)
+        if (kept0 > ELL_SORT_MAX) ell_row_warp(posq, i, lin, g, rc2_list, nbr, P, cap, nnbr, flags, k0);
+        if (kept1 > ELL_SORT_MAX) ell_row_warp(posq, i1, lin, g, rc2_list, nbr, P, cap, nnbr, flags, k1);
+        const int s0 = kept0 <= ELL_SORT_MAX ? kept0 : 0;
+        const int s1 = kept1 <= ELL_SORT_MAX ? kept1 : 0;
+        if (s0 <= 32 && s1 <= 32) {
+            ell_write_sorted2(i, s0, k0, i1, s1, k1, nbr, P);
+        } else {
+            ell_write_sorted(i, s0, k0, nbr, P);
+            ell_write_sorted(i1, s1, k1, nbr, P);
+        }
+        if (kept0 <= ELL_SORT_MAX) ell_row_done(i, c0, cap, nnbr, flags);
+        if (two && kept1 <= ELL_SORT_MAX) ell_row_done(i1, c1, cap, nnbr, flags);
+        __syncwarp();
+    }
+}
+
+// All rows of the atoms in cell `r` (visiting rank), built by one warp: the
+// cell's stencil candidates are held in registers (ELL_REG_ROUNDS per lane;
+// larger stencils are swept in chunks, reloaded per pair of atoms) and each
+// candidate is tested against two of the cell's atoms per sweep.  Rows come
+// out equal to ell_row_warp's.  keys: ELL_KEYS entries of shared memory.
+// ORTH_ONLY: every box is orthogonal (the triclinic arithmetic is left out,
+// which keeps the kernel's register count down).
+template <bool ORTH_ONLY>
+__device__ __forceinline__ void ell_cell_warp(const int4* __restrict__ posq, int r, const int32_t* lin_of_rank,
+                                              const CellGrid& g, float rc2_list, int32_t* nbr, int64_t P, int cap,
+                                              int32_t* nnbr, int32_t* flags, uint64_t* keys) {
     const int a0 = g.start[r], a1 = g.start[r + 1];
     if (a0 == a1) return;
     const int lin = lin_of_rank[r];
     const Stencil st = stencil_of(g, lin);
-    if (st.total > ELL_CELL_CAND) {
-        for (int i = a0; i < a1; ++i) ell_row_warp(posq, i, lin, g, rc2_list, nbr, P, cap, nnbr, flags, keys);
-        return;
-    }
-    for (int base = 0; base < st.total; base += 32) {
-        const int t = base + lane;
-        const int j = stencil_slot(st, t);
-        if (t < st.total) {
-            cq[t] = posq[j];
-            cj[t] = j;
-        }
-    }
-    __syncwarp();
     const ListBox b(*g.box);
-    const unsigned below = (1u << lane) - 1u;
-    for (int i = a0; i < a1; ++i) {
-        const int4 qi = posq[i];
-        int cnt = 0;
-        for (int base = 0; base < st.total; base += 32) {
-            const int t = base + lane;
-            bool acc = false;
-            float d2 = 0.0f;
-            int j = 0;
-            if (t < st.total) {
-                j = cj[t];
-                if (j != i) {
-                    d2 = list_d2(b, qi, cq[t]);
-                    acc = d2 < rc2_list;
-                }
-            }
-            const unsigned m = __ballot_sync(FULL, acc);
-            const int pos = cnt + __popc(m & below);
-            if (acc && pos < ELL_SORT_MAX) keys[pos] = list_key(d2, j);
-            cnt += __popc(m);
-        }
-        __syncwarp();
-        const int kept = cnt < cap ? cnt : cap;
-        if (kept > ELL_SORT_MAX) {
-            ell_row_warp(posq, i, lin, g, rc2_list, nbr, P, cap, nnbr, flags, keys);
-        } else {
-            ell_write_sorted(i, kept, keys, nbr, P);
-            ell_row_done(i, cnt, cap, nnbr, flags);
-        }
-        __syncwarp();
-    }
+    if (ORTH_ONLY || b.orth)
+        ell_cell_rows<true>(posq, a0, a1, lin, st, b, g, rc2_list, nbr, P, cap, nnbr, flags, keys);
+    else
+        ell_cell_rows<false>(posq, a0, a1, lin, st, b, g, rc2_list, nbr, P, cap, nnbr, flags, keys);
 }
 
 }  // namespace simb200

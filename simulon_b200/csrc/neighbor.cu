@@ -267,19 +267,19 @@ __global__ void k_slot_cells(SimEngine e, const int32_t* gate) {
 }
 
 // Full list in ELL layout, one warp per cell (row builders in grid.cuh).
+// ORTH: the engine's box is and stays orthogonal (5 blocks of 4 warps per SM
+// at 96 registers).
 #define ELL_WARPS 4
-__global__ void __launch_bounds__(ELL_WARPS * 32) k_build_ell(SimEngine e, const int32_t* cell_lin,
-                                                             float rc2_list, const int32_t* gate) {
+template <bool ORTH>
+__global__ void __launch_bounds__(ELL_WARPS * 32, ORTH ? 5 : 4) k_build_ell(SimEngine e, const int32_t* cell_lin,
+                                                                           float rc2_list, const int32_t* gate) {
     if (gate && __ldg(gate) == 0) return;
-    __shared__ uint64_t keys[ELL_WARPS][ELL_SORT_MAX];
-    __shared__ int4 cq[ELL_WARPS][ELL_CELL_CAND];
-    __shared__ int cj[ELL_WARPS][ELL_CELL_CAND];
+    __shared__ uint64_t keys[ELL_WARPS][ELL_KEYS];
     const CellGrid g{e.box, e.ncell[0], e.ncell[1], e.ncell[2], e.cell_rank, e.cell_start};
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
     const int warp = threadIdx.x >> 5;
     for (int r = blockIdx.x * ELL_WARPS + warp; r < e.n_cells; r += gridDim.x * ELL_WARPS)
-        ell_cell_warp(posq, r, cell_lin, g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags, keys[warp], cq[warp],
-                      cj[warp]);
+        ell_cell_warp<ORTH>(posq, r, cell_lin, g, rc2_list, e.nbr, e.n_pad, e.nbr_cap, e.nnbr, e.flags, keys[warp]);
 }
 
 // Count the rebuild (flags[3]) when it ran and clear the request.
@@ -536,7 +536,10 @@ extern "C" int sim_rebuild(const SimEngine* ep, int32_t only_if_flagged, void* s
     k_slot_cells<<<g, SIM_THREADS, 0, st>>>(e, gate);
     const float rc2_list = (float)(e.x_rc * e.x_rc * (1.0 + 4e-6));
     // cell_lin (rank -> linear index) is stored right after cell_rank
-    k_build_ell<<<ell_grid(e.n_cells), ELL_WARPS * 32, 0, st>>>(e, e.cell_rank + e.n_cells, rc2_list, gate);
+    if (e.box_orthogonal)
+        k_build_ell<true><<<ell_grid(e.n_cells), ELL_WARPS * 32, 0, st>>>(e, e.cell_rank + e.n_cells, rc2_list, gate);
+    else
+        k_build_ell<false><<<ell_grid(e.n_cells), ELL_WARPS * 32, 0, st>>>(e, e.cell_rank + e.n_cells, rc2_list, gate);
     launch_build_halo(e, gate, st);
     k_finish_rebuild<<<1, 1, 0, st>>>(e.flags, only_if_flagged ? 1 : 0);
     return launch_status("sim_rebuild");
