@@ -36,7 +36,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "atom-steps/s (EAM-W, 1 B200): plain vs batched vs MLP at stated force RMSE"
 UNIT = "atom-steps/s"
-PASS2_DRAM_BYTES_PER_ATOM = (66263040 + 1362176) / 524288   # k_eam_force<1,1,1>, ncu --set full
+PASS2_DRAM_BYTES_PER_ATOM = (66266112 + 2173696) / 524288   # k_eam_force<1,1,1>, ncu --set full
 A_W, M_W = 3.165, 183.84
 
 
@@ -1059,17 +1059,22 @@ def mlp_form(args, sb, pot, dev, world):
 def e2e(model, mol, x, v, args, dev):
     """Same metric through the public API with host buffers: pinned H2D of the
     state, K steps, D2H of every step's scalars and of the final state into
-    pinned buffers.  One untimed pass of the same path first (it loads the
-    kernels this path uses that the device-resident run does not)."""
+    pinned buffers.  The state crosses in the API's dtype (the reader's
+    ``dtype``, torch's default as in the reference reader: float32 here),
+    which is what ``update_coordinates`` takes and ``coordinates`` /
+    ``atom_velocities`` return.  One untimed pass of the same path first (it
+    loads the kernels this path uses that the device-resident run does
+    not)."""
     import torch
     N = len(x)
-    xh = torch.tensor(x).pin_memory()
-    vh = torch.tensor(v).pin_memory()
+    io = mol.dtype
+    xh = torch.tensor(x, dtype=io).pin_memory()
+    vh = torch.tensor(v, dtype=io).pin_memory()
     K = args.steps
     G = args.graph_steps
     log_h = torch.empty(K, model.engine.log.shape[1], dtype=torch.float64).pin_memory()
-    x_out = torch.empty(N, 3, dtype=torch.float64).pin_memory()
-    v_out = torch.empty(N, 3, dtype=torch.float64).pin_memory()
+    x_out = torch.empty(N, 3, dtype=io).pin_memory()
+    v_out = torch.empty(N, 3, dtype=io).pin_memory()
 
     def one_pass(n_steps):
         mol.update_coordinates(xh, velocities=vh)     # H2D of both + cell sort + list build
@@ -1088,8 +1093,9 @@ def e2e(model, mol, x, v, args, dev):
     dt = time.perf_counter() - t0
     assert torch.isfinite(x_out).all() and torch.isfinite(v_out).all() and torch.isfinite(log_h).all()
     row_bytes = log_h.shape[1] * 8
-    return {"value": N * K / dt, "unit": UNIT, "h2d_bytes_per_step": 2 * N * 24 / K,
-            "d2h_bytes_per_step": row_bytes + 2 * N * 24 / K, "seconds": dt,
+    state_bytes = 2 * N * 3 * x_out.element_size()
+    return {"value": N * K / dt, "unit": UNIT, "h2d_bytes_per_step": state_bytes / K,
+            "d2h_bytes_per_step": row_bytes + state_bytes / K, "seconds": dt, "io_dtype": str(io).split(".")[-1],
             "path": "AtomFileReader.update_coordinates(x, velocities=v) -> BaseModel.run -> coordinates/velocities + "
                     "step log"}
 

@@ -222,14 +222,36 @@ class MDEngine:
     def load(self, positions, velocities=None):
         """Load original-order rows, sort into cells and build the list.  The
         copies from pinned host rows are asynchronous; the capacity check at
-        the end synchronises, so they have landed when this returns."""
+        the end synchronises, so they have landed when this returns.  Host
+        velocities cross on a side stream while the cell sort and the list
+        build run on the positions, and are scattered into the sorted slots
+        afterwards (the same slots' values as loading them together)."""
         pos = torch.as_tensor(positions).to(self.device, torch.float64, non_blocking=True).contiguous()
-        vel = None if velocities is None else \
-            torch.as_tensor(velocities).to(self.device, torch.float64, non_blocking=True).contiguous()
-        _lib.call("sim_engine_load", self.st_ref, _lib.ptr(pos), _lib.ptr(vel), _lib.ptr(self.types), self.stream)
+        vel = None if velocities is None else torch.as_tensor(velocities)
+        late_v = vel is not None and vel.device.type == "cpu"
+        if late_v:
+            main = torch.cuda.current_stream(self.device)
+            side = self._copy_stream()
+            side.wait_stream(main)
+            with torch.cuda.stream(side):
+                vel = vel.to(self.device, torch.float64, non_blocking=True).contiguous()
+            vel.record_stream(main)
+            ready = side.record_event()
+        elif vel is not None:
+            vel = vel.to(self.device, torch.float64).contiguous()
+        _lib.call("sim_engine_load", self.st_ref, _lib.ptr(pos), _lib.ptr(None if late_v else vel),
+                  _lib.ptr(self.types), self.stream)
+        if late_v:
+            main.wait_event(ready)
+            _lib.call("sim_scatter_original_f64", self.st_ref, _lib.ptr(vel), _lib.ptr(self.v), self.stream)
         self.rebuilds_host += 1
         self.forces_valid = False
         self.ensure_capacity()
+
+    def _copy_stream(self):
+        if getattr(self, "_side_stream", None) is None:
+            self._side_stream = torch.cuda.Stream(self.device)
+        return self._side_stream
 
     def _alloc_lists(self):
         dev, P = self.device, self.n_pad
