@@ -51,7 +51,8 @@ class UniaxialTensileLoader:
     (``launch_after``)."""
 
     def __init__(self, molecular, axis: int = 0, strain_rate: float = 1.0e-3, lateral_mode: str = "fixed",
-                 poisson_ratio: float = 0.28, max_lateral_scale_step: float = 2.0e-3, regrid_margin: float = 0.01):
+                 poisson_ratio: float = 0.28, max_lateral_scale_step: float = 2.0e-3, regrid_margin: float = 0.01,
+                 regrid_headroom: float = 0.06):
         self.molecular = molecular
         self.axis = int(axis)
         self.strain_rate = float(strain_rate)
@@ -59,6 +60,7 @@ class UniaxialTensileLoader:
         self.poisson_ratio = float(poisson_ratio)
         self.max_lateral_scale_step = float(max_lateral_scale_step)
         self.regrid_margin = float(regrid_margin)
+        self.regrid_headroom = max(float(regrid_headroom), self.regrid_margin)
         if self.axis not in (0, 1, 2):
             raise ValueError(f"axis must be 0/1/2, got {axis}")
         if not hasattr(molecular, "engine"):
@@ -134,11 +136,16 @@ class UniaxialTensileLoader:
         return h
 
     def maintain(self) -> bool:
-        """Regrid when the device asked for it (synchronises); True if it did."""
+        """Regrid when the device asked for it (synchronises); True if it did.
+        The device asks once the cells come within regrid_margin of the list
+        cutoff; the new cells are at least regrid_headroom wider than it, so
+        a box that keeps shrinking regrids about once per
+        regrid_headroom - regrid_margin of strain rather than at every cell
+        it loses (a regrid reloads the engine and recaptures its graphs)."""
         if float(self.state[17].item()) == 0.0:
             return False
         eng = self.molecular.engine
-        eng.regrid(margin=self.regrid_margin)
+        eng.regrid(margin=self.regrid_headroom)
         self.regrids += 1
         self.state[17] = 0.0
         self._reset_list_box(eng.box_matrix())

@@ -322,12 +322,8 @@ def indenter_cases(tmp):
         torch.set_default_dtype(torch.float32)
 
 
-def crack_cases(tmp):
-    """Crack observables of run_scripts/w_crack.py (_select_mouth_groups,
-    _estimate_crack_length, _project_to_lattice_axes) on a precracked BCC-W
-    slab as built and with its upper half opened (a smooth opening profile
-    around the crack plus seeded jitter), and the stress projection of a
-    seeded symmetric tensor."""
+def _stub_matplotlib():
+    """run_scripts/w_crack.py imports matplotlib at module level for its plots."""
     for name in ("matplotlib", "matplotlib.pyplot"):
         if name not in sys.modules:
             m = types.ModuleType(name)
@@ -335,6 +331,15 @@ def crack_cases(tmp):
             m.rcParams = {}
             sys.modules[name] = m
     sys.modules["matplotlib"].pyplot = sys.modules["matplotlib.pyplot"]
+
+
+def crack_cases(tmp):
+    """Crack observables of run_scripts/w_crack.py (_select_mouth_groups,
+    _estimate_crack_length, _project_to_lattice_axes) on a precracked BCC-W
+    slab as built and with its upper half opened (a smooth opening profile
+    around the crack plus seeded jitter), and the stress projection of a
+    seeded symmetric tensor."""
+    _stub_matplotlib()
     from run_scripts.w_crack import _estimate_crack_length, _project_to_lattice_axes, _select_mouth_groups
     from simulon_b200.batch import crack_slab
 
@@ -367,6 +372,62 @@ def crack_cases(tmp):
     proj = _project_to_lattice_axes(sigma, types.SimpleNamespace(H=H))
     _save("crack_obs_w3000", x0=x0, x1=x1, H=H, crack_plane_y=yc, half_length=half, upper=up.numpy(),
           lower=lo.numpy(), sigma=sigma, projected=proj, threshold=1.0, bins=160, **res)
+
+
+def crack_md_cases(tmp):
+    """Two precracked BCC-W slabs (simulon_b200.batch.crack_slab: 1,200 and
+    2,000 target atoms) each run through the grip loop of
+    run_scripts/w_crack.py:384-394,456-471 with the reference's own
+    pure-PyTorch EAMForceCUDAExt, VerletIntegrator (NVE, dt 1 fs) and
+    BaseModel: before and after every model() call the grip atoms are put at
+    their starting positions -/+ half the opening along y with zero velocity,
+    update_coordinates runs and the skin reference is reset; the opening of
+    loop step s is (s + 1) * rate.  20 steps; the final state and every
+    step's potential energy are saved."""
+    from core.force.eam_force_cu import EAMForceCUDAExt
+    from core.integrator.integrator import VerletIntegrator
+    from core.md_model import BaseModel, SumBackboneInterface
+    from io_utils.eam_parser import EAMParser
+    from simulon_b200.batch import crack_slab
+    _stub_matplotlib()
+    from run_scripts.w_crack import _axis_unit
+
+    pot = oin.write_fs_w_setfl(os.path.join(tmp, "W_synthetic.eam.fs"))
+    parser = EAMParser(pot, torch.device("cpu"))
+    rate, steps, dt = 2e-3, 20, 0.001
+    for k, (n, T, seed) in enumerate(((1200, 300.0, 11), (2000, 900.0, 12))):
+        rep = crack_slab(n, temperature=T, grip_rate=rate, seed=seed)
+        mol = _reader(tmp, f"slab{k}", rep.positions, "W", rep.H, parser.cutoff, 0.5, is_fs=True)
+        integ = VerletIntegrator(mol, dt=dt, ensemble="NVE")
+        mol.atom_velocities = torch.tensor(rep.velocities, dtype=torch.float32)
+        model = BaseModel(SumBackboneInterface([EAMForceCUDAExt(parser, mol, use_extension=False)], mol), integ, mol)
+        y_unit = _axis_unit(mol.box.H, 1, torch.device("cpu"), mol.coordinates.dtype)    # w_crack.py:341
+        lower = torch.tensor(rep.grip == 1)
+        upper = torch.tensor(rep.grip == 2)
+        lower_ref = mol.coordinates[lower].detach().clone()
+        upper_ref = mol.coordinates[upper].detach().clone()
+
+        def apply_grips(total_opening):
+            shift = 0.5 * float(total_opening) * y_unit
+            with torch.no_grad():
+                mol.coordinates[lower] = lower_ref - shift
+                mol.coordinates[upper] = upper_ref + shift
+                mol.atom_velocities[lower] = 0.0
+                mol.atom_velocities[upper] = 0.0
+                mol.update_coordinates(mol.coordinates)
+                mol.last_positions = mol.coordinates.detach().clone()
+
+        apply_grips(0.0)
+        epot = []
+        for s in range(steps):
+            opening = (s + 1) * rate
+            apply_grips(opening)
+            out = model()
+            apply_grips(opening)
+            epot.append(float(out["energy"]))
+        _save(f"crack_md_w{n}", x0=rep.positions, v0=rep.velocities, grip=rep.grip, H=rep.H, T=T, seed=seed,
+              rate=rate, dt=dt, steps=steps, x=mol.coordinates, v=mol.atom_velocities, epot=np.array(epot),
+              rebuilds=mol.profile["neighbor_builds"])
 
 
 def sum_cases(tmp):
@@ -598,7 +659,7 @@ def legacy_cases(tmp):
 
 GROUPS = {"neighbor": "neighbor_cases", "lj": "lj_cases", "eam": "eam_cases", "md": "md_cases",
           "mech": "mech_cases", "indenter": "indenter_cases", "crack": "crack_cases", "legacy": "legacy_cases",
-          "sum": "sum_cases"}
+          "sum": "sum_cases", "crack_md": "crack_md_cases"}
 
 
 def main():

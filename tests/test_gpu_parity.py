@@ -597,6 +597,35 @@ def test_maxwell_boltzmann_velocities_match_reference_formula(sb, dtype):
         assert abs(t_kin / T - 1.0) < 0.05, t_kin
 
 
+def test_update_coordinates_from_pinned_host_rows(sb, fsw_path):
+    """update_coordinates(x, velocities=v) from pinned float32 host rows (the
+    velocities cross on a side stream while the cell sort and list build run)
+    reads back the same rows, and 10 MD steps from it are bit-equal to the
+    same steps after a load of the same rows from device tensors."""
+    coords, L = oin.bcc_lattice(8)
+    rng = np.random.default_rng(11)
+    x = np.minimum(np.mod(oin.jitter(coords, 0.08, 5) + 0.3 * L, L), L - 1e-3)[rng.permutation(len(coords))]
+    v = rng.normal(0.0, 0.01, x.shape)
+    xh = torch.tensor(x, dtype=torch.float32).pin_memory()
+    vh = torch.tensor(v, dtype=torch.float32).pin_memory()
+    parser = sb.EAMParser(fsw_path)
+    states = []
+    for host in (True, False):
+        mol = sb.AtomFileReader.from_arrays(["W"] * len(x), coords, L, parser.cutoff, device=DEV, skin_thickness=0.5,
+                                            is_fs=True)
+        model = sb.BaseModel(sb.SumBackboneInterface([sb.EAMForceCUDAExt(parser, mol)], mol),
+                             sb.VerletIntegrator(mol, dt=0.002, ensemble="NVE"), mol)
+        model.run(3, graph_steps=3)
+        if host:
+            mol.update_coordinates(xh, velocities=vh)
+        else:
+            mol.update_coordinates(xh.to(DEV), velocities=vh.to(DEV))
+        assert torch.equal(mol.coordinates.cpu(), xh) and torch.equal(mol.atom_velocities.cpu(), vh)
+        model.run(10, graph_steps=5)
+        states.append((mol.engine.gather("x").cpu(), mol.engine.gather("v").cpu()))
+    assert torch.equal(states[0][0], states[1][0]) and torch.equal(states[0][1], states[1][1])
+
+
 # ------------------------------------------------ sum of force fields
 def test_sum_of_eam_and_lj_matches_reference(sb, fsw_path, tmp_path):
     """SumBackboneInterface([EAM, LJ]) (core/md_model.py:19-52): the LJ pass
