@@ -349,6 +349,14 @@ int sim_eam_force_integrate_drift(const SimEngine* e, const SimEAMTables* t, con
  * persistent grid in n_blocks_max (a second set of block partials). */
 int sim_eam_force_integrate_indenter(const SimEngine* e, const SimEAMTables* t, const SimIntegrator* p,
                                      const SimIndenter* ind, int32_t mode, void* stream);
+/* sim_eam_force_integrate_indenter in mode 2, sim_log_step on step_ctr[1] and
+ * sim_rebuild_if_needed, with the log row and (while the stream is captured)
+ * the rebuild's IF-node value written by the force pass's last block, as
+ * sim_eam_step_drift does for EAM alone: the same bits, two kernels fewer
+ * per step.  One element type, untiled kernels. */
+int sim_eam_step_drift_indenter(const SimEngine* e, const SimEAMTables* t, const SimIntegrator* integ,
+                                const SimIndenter* ind, const double* extra, int32_t n_extra, double* log,
+                                int32_t log_capacity, void* stream);
 /* One whole MD step of the drift-fused form ended on the device: EAM pass 1,
  * then pass 2 as sim_eam_force_integrate_drift, whose last block also appends
  * the step's log row (as sim_log_step on &step_ctr[1]) and decides the
@@ -479,6 +487,22 @@ int sim_box_scale_after_first(const SimEngine* e, const double* work_prev, int32
  * p->regrid_margin of the list cutoff (the host regrids between launches or
  * graph replays).  One thread; graph-capturable. */
 int sim_loader_check(const SimEngine* e, const SimLoaderCheck* p, double* state, void* stream);
+/* One tensile MD step's end and the next one's start with an anisotropic
+ * barostat (run_scripts/w_tensile.py's loop, barostat.py:137-208,
+ * loading.py:41-80): what sim_aniso_control(baro, work_baro),
+ * sim_log_step(step_ctr, extra, n_extra, log, capacity),
+ * sim_box_scale_after_first(work_baro, baro->reset_reference, load,
+ * work_load, integ, force_precision), sim_loader_check(check, state) and
+ * sim_rebuild_if_needed do one after another, in three kernels (the
+ * controller, the log row and the loader's box prepared on one thread; the
+ * pass over the atoms; the box committed, the loader's bookkeeping and, while
+ * the stream is captured, the value of the rebuild's IF node on one thread)
+ * and the rebuild's IF node instead of seven kernels: the same operations in
+ * the same order, so the same bits.  Arguments as in those calls. */
+int sim_tensile_link(const SimEngine* e, const SimAniso* baro, double* work_baro, const uint64_t* step_ctr,
+                     const double* extra, int32_t n_extra, double* log, int32_t capacity, const SimBoxScale* load,
+                     double* work_load, const SimIntegrator* integ, int32_t force_precision,
+                     const SimLoaderCheck* check, double* state, void* stream);
 
 /* SphericalIndenterForce.forward (indenter.py:40-68) added to the engine's
  * forces (force_precision 0: f32, 1: f64) after a force field's pass: for

@@ -166,6 +166,8 @@ SIGNATURES = {
     "sim_eam_force_integrate_drift": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), c_p],
     "sim_eam_force_integrate_indenter": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), _P(SimIndenter),
                                          ctypes.c_int32, c_p],
+    "sim_eam_step_drift_indenter": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), _P(SimIndenter), c_p,
+                                    ctypes.c_int32, c_p, ctypes.c_int32, c_p],
     "sim_eam_step_drift": [_P(SimEngine), _P(SimEAMTables), _P(SimIntegrator), c_p, ctypes.c_int32, c_p,
                            ctypes.c_int32, c_p],
     "sim_lj_forces": [_P(SimEngine), _P(SimLJParams), ctypes.c_int32, c_p],
@@ -183,6 +185,8 @@ SIGNATURES = {
     "sim_aniso_control": [_P(SimEngine), _P(SimAniso), c_p, c_p],
     "sim_box_scale_after_first": [_P(SimEngine), c_p, ctypes.c_int32, _P(SimBoxScale), c_p, _P(SimIntegrator),
                                   ctypes.c_int32, c_p],
+    "sim_tensile_link": [_P(SimEngine), _P(SimAniso), c_p, c_p, c_p, ctypes.c_int32, c_p, ctypes.c_int32,
+                         _P(SimBoxScale), c_p, _P(SimIntegrator), ctypes.c_int32, _P(SimLoaderCheck), c_p, c_p],
     "sim_indenter_add": [_P(SimEngine), _P(SimIndenter), ctypes.c_int32, c_p],
     "sim_batch_crack_observe": [c_p, c_p, c_p, ctypes.c_int32, c_p, c_p, c_p, c_p],
     "sim_gather_original_f64": [_P(SimEngine), c_p, c_p, c_p],

@@ -531,6 +531,49 @@ extern "C" int sim_eam_force_integrate_indenter(const SimEngine* ep, const SimEA
     return launch_status("sim_eam_force_integrate_indenter");
 }
 
+namespace {
+struct StepIndCtx {
+    const SimEngine* e;
+    const SimEAMTables* t;
+    const SimIntegrator* ip;
+    const SimIndenter* ind;
+    StepEnd end;
+};
+int step_ind_pass2(const void* ctx, cudaStream_t st, const cudaGraphConditionalHandle* h) {
+    const StepIndCtx& c = *static_cast<const StepIndCtx*>(ctx);
+    StepEnd end = c.end;
+    end.set_cond = h != nullptr;
+    if (h) end.h = *h;
+    const SimEngine& e = *c.e;
+    const int rc = e.box_orthogonal ? launch_force<true, 2, true, true>(e, *c.t, *c.ip, end, st, *c.ind)
+                                    : launch_force<true, 2, false, true>(e, *c.t, *c.ip, end, st, *c.ind);
+    return rc != SIM_OK ? rc : launch_status("sim_eam_step_drift_indenter");
+}
+int step_ind_body(const void* ctx, cudaStream_t s) { return rebuild_body(static_cast<const StepIndCtx*>(ctx)->e, s); }
+int step_ind_eager(const void* ctx, cudaStream_t s) {
+    return rebuild_eager(static_cast<const StepIndCtx*>(ctx)->e, s);
+}
+}  // namespace
+
+extern "C" int sim_eam_step_drift_indenter(const SimEngine* ep, const SimEAMTables* tp, const SimIntegrator* ip,
+                                           const SimIndenter* ind, const double* extra, int32_t n_extra, double* log,
+                                           int32_t log_capacity, void* stream) {
+    if (!ep || !ep->box || !tp || !ip || !ind || ep->n <= 0 || !ep->posfp || !valid_tables(*tp)) return SIM_ERR_ARG;
+    if (!ind->center || !ind->out || !(ind->radius >= 0.0) || !ip->step_ctr || (ip->langevin && !ip->rff))
+        return SIM_ERR_ARG;
+    if (!log || log_capacity <= 0 || n_extra < 0 || n_extra > 32 || (n_extra > 0 && !extra)) return SIM_ERR_ARG;
+    if (tp->n_types != 1 || smem_pass2(*tp) > kSmemLimit || tiled_eam_usable(*ep, *tp)) {
+        set_error_text("sim_eam_step_drift_indenter: one element type, untiled kernels only");
+        return SIM_ERR_ARG;
+    }
+    int rc = sim_eam_density(ep, tp, stream);
+    if (rc != SIM_OK) return rc;
+    eam_set_attributes();
+    StepIndCtx c{ep, tp, ip, ind, StepEnd{extra, log, (int)n_extra, (int)log_capacity, 0, 0}};
+    return launch_if_cond((cudaStream_t)stream, step_ind_pass2, step_ind_body, step_ind_eager, &c,
+                          "sim_eam_step_drift_indenter");
+}
+
 extern "C" int sim_eam_forces(const SimEngine* ep, const SimEAMTables* tp, void* stream) {
     int rc = sim_eam_density(ep, tp, stream);
     if (rc != SIM_OK) return rc;

@@ -210,8 +210,7 @@ __device__ void prepare_scaled_box(const SimBox& b, const double* scale, SimBox&
     nb.pad[0] = nb.pad[1] = nb.pad[2] = 0;
 }
 
-__global__ void k_aniso_control(SimEngine e, SimAniso p, double* work) {
-    pdl_wait();
+__device__ void aniso_control(const SimEngine& e, SimAniso p, double* work) {
     const SimBox& b = *e.box;
     const double* H = b.H;
     const double* r = e.red_out;
@@ -258,6 +257,11 @@ __global__ void k_aniso_control(SimEngine e, SimAniso p, double* work) {
     }
     if (p.stochastic) *p.counter += 1;
     prepare_scaled_box(b, scale, work_box(work));
+}
+
+__global__ void k_aniso_control(SimEngine e, SimAniso p, double* work) {
+    pdl_wait();
+    aniso_control(e, p, work);
 }
 
 __global__ void k_box_prepare(SimEngine e, SimBoxScale p, double* work) {
@@ -327,8 +331,7 @@ __global__ void __launch_bounds__(SIM_THREADS) k_scale_atoms(SimEngine e, const 
 // come within regrid_margin of the list cutoff across any axis of >= 3 cells
 // (the host regrids between graph replays, before the cells are too small).
 // state: SIM_LOADER_STATE doubles, see simb200.h.
-__global__ void k_loader_check(SimEngine e, SimLoaderCheck p, double* state) {
-    pdl_wait();
+__device__ void loader_check(const SimEngine& e, const SimLoaderCheck& p, double* state) {
     const double* H = e.box->H;
     double len[3];
     for (int a = 0; a < 3; ++a) {
@@ -368,6 +371,11 @@ __global__ void k_loader_check(SimEngine e, SimLoaderCheck p, double* state) {
     }
 }
 
+__global__ void k_loader_check(SimEngine e, SimLoaderCheck p, double* state) {
+    pdl_wait();
+    loader_check(e, p, state);
+}
+
 __global__ void k_box_commit(SimEngine e, const double* work) {
     pdl_wait();
     *e.box = *reinterpret_cast<const SimBox*>(work + 16);
@@ -376,14 +384,17 @@ __global__ void k_box_commit(SimEngine e, const double* work) {
 // A loader's box update prepared on the box that an earlier update in the
 // same step (the barostat's, work_prev) is about to commit: as k_box_prepare
 // with work_prev's new box in place of *e.box.
-__global__ void k_box_prepare_after(SimBoxScale p, const double* work_prev, double* work) {
-    pdl_wait();
+__device__ void box_prepare_after(const SimBoxScale& p, const double* work_prev, double* work) {
     for (int a = 0; a < 3; ++a) {
         work[a] = 0.0;
         work[3 + a] = p.scale[a];
         work[6 + a] = p.vel_scale[a];
     }
     prepare_scaled_box(*reinterpret_cast<const SimBox*>(work_prev + 16), p.scale, work_box(work));
+}
+__global__ void k_box_prepare_after(SimBoxScale p, const double* work_prev, double* work) {
+    pdl_wait();
+    box_prepare_after(p, work_prev, work);
 }
 
 // One box update of an atom held in registers, with k_scale_atoms' arithmetic:
@@ -468,6 +479,33 @@ __global__ void __launch_bounds__(SIM_THREADS) k_two_scales_first(SimEngine e, c
     }
     if (__any_sync(0xffffffffu, trig) && (threadIdx.x & 31) == 0) e.flags[0] = 1;
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+}
+
+// The end of tensile step s and the start of step s+1 with an anisotropic
+// barostat (sim_tensile_link): k_link_control does on one thread what
+// k_aniso_control, k_log_step and k_box_prepare_after do, in that order;
+// k_two_scales_first follows; then k_link_commit does what k_box_commit,
+// k_loader_check and (while capturing) k_set_rebuild_condition do.  The same
+// operations in the same order as the seven launches, so the same bits.
+__global__ void k_link_control(SimEngine e, SimAniso a, double* wb, const uint64_t* ctr, const double* extra,
+                               int n_extra, double* log, int cap, SimBoxScale q, double* wl) {
+    pdl_trigger();
+    pdl_wait();
+    aniso_control(e, a, wb);
+    const int w = SIM_RED_SLOTS + n_extra + 1;
+    double* row = log + (size_t)((ctr ? *ctr : 0) % (uint64_t)cap) * w;
+    for (int k = 0; k < SIM_RED_SLOTS; ++k) row[k] = e.red_out[k];
+    for (int k = 0; k < n_extra; ++k) row[SIM_RED_SLOTS + k] = extra[k];
+    row[SIM_RED_SLOTS + n_extra] = (double)e.flags[1];
+    box_prepare_after(q, wb, wl);
+}
+
+__global__ void k_link_commit(SimEngine e, const double* wl, SimLoaderCheck c, double* state,
+                              cudaGraphConditionalHandle h, int set_cond) {
+    pdl_wait();
+    *e.box = *reinterpret_cast<const SimBox*>(wl + 16);
+    loader_check(e, c, state);
+    if (set_cond) cudaGraphSetConditional(h, e.flags[0] != 0 ? 1u : 0u);
 }
 
 static int launch_box_scale(const SimEngine& e, double* work, int reset, cudaStream_t st, const char* what) {
@@ -792,6 +830,61 @@ extern "C" int sim_indenter_add(const SimEngine* ep, const SimIndenter* p, int32
     return launch_status("sim_indenter_add");
 }
 
+
+namespace {
+struct LinkCtx {
+    const SimEngine* e;
+    const SimAniso* a;
+    double* wb;
+    const uint64_t* ctr;
+    const double* extra;
+    int n_extra;
+    double* log;
+    int cap;
+    const SimBoxScale* q;
+    double* wl;
+    const SimIntegrator* ip;
+    int prec;
+    const SimLoaderCheck* c;
+    double* state;
+};
+
+int link_cond(const void* ctx, cudaStream_t st, const cudaGraphConditionalHandle* h) {
+    const LinkCtx& c = *static_cast<const LinkCtx*>(ctx);
+    const SimEngine& e = *c.e;
+    cudaError_t err = launch_pdl(k_link_control, dim3(1), dim3(1), 0, st, e, *c.a, c.wb, c.ctr, c.extra, c.n_extra,
+                                 c.log, c.cap, *c.q, c.wl);
+    if (err == cudaSuccess)
+        err = launch_pdl(k_two_scales_first, dim3((unsigned)ceil_div(e.n, SIM_THREADS)), dim3(SIM_THREADS), 0, st, e,
+                         (const double*)c.wb, (const double*)c.wl, (int)c.a->reset_reference,
+                         (int)c.q->reset_reference, *c.ip, c.prec);
+    if (err == cudaSuccess)
+        err = launch_pdl(k_link_commit, dim3(1), dim3(1), 0, st, e, (const double*)c.wl, *c.c, c.state,
+                         h ? *h : (cudaGraphConditionalHandle)0, h ? 1 : 0);
+    if (err != cudaSuccess) { set_cuda_error(err, "sim_tensile_link: launch"); return SIM_ERR_CUDA; }
+    return SIM_OK;
+}
+int link_body(const void* ctx, cudaStream_t s) { return sim_rebuild(static_cast<const LinkCtx*>(ctx)->e, 0, s); }
+int link_eager(const void* ctx, cudaStream_t s) { return sim_rebuild(static_cast<const LinkCtx*>(ctx)->e, 1, s); }
+}  // namespace
+
+extern "C" int sim_tensile_link(const SimEngine* ep, const SimAniso* baro, double* work_baro, const uint64_t* step_ctr,
+                                const double* extra, int32_t n_extra, double* log, int32_t capacity,
+                                const SimBoxScale* load, double* work_load, const SimIntegrator* integ,
+                                int32_t force_precision, const SimLoaderCheck* check, double* state, void* stream) {
+    if (!ep || !ep->box || ep->n <= 0 || !baro || !work_baro || !baro->eta_dot || (baro->stochastic && !baro->counter))
+        return SIM_ERR_ARG;
+    if (!log || capacity <= 0 || n_extra < 0 || n_extra > 32 || (n_extra > 0 && !extra)) return SIM_ERR_ARG;
+    if (!load || !work_load || !integ || (force_precision == 1 && !ep->f64)) return SIM_ERR_ARG;
+    for (int a = 0; a < 3; ++a)
+        if (!(load->scale[a] > 0.0) || !(load->vel_scale[a] > 0.0)) return SIM_ERR_ARG;
+    if (!check || !state || check->axis < 0 || check->axis > 2 || !(check->rebuild_strain >= 0.0) ||
+        !(check->regrid_margin >= 0.0))
+        return SIM_ERR_ARG;
+    const LinkCtx c{ep, baro, work_baro, step_ctr, extra, (int)n_extra, log, (int)capacity, load, work_load, integ,
+                    (int)force_precision, check, state};
+    return launch_if_cond((cudaStream_t)stream, link_cond, link_body, link_eager, &c, "sim_tensile_link");
+}
 
 extern "C" int sim_loader_check(const SimEngine* ep, const SimLoaderCheck* p, double* state, void* stream) {
     if (!ep || !p || !state || p->axis < 0 || p->axis > 2 || !(p->rebuild_strain >= 0.0) ||

@@ -391,6 +391,15 @@ class MDEngine:
         self._last_force_precision = 0
         self.forces_valid = True
 
+    def eam_step_drift_indenter(self, tables, integ, indenter_ref):
+        """eam_forces_integrate_indenter (mode 2) + log_step(after_drift=True)
+        + rebuild_if_needed, with the log row and the rebuild decision made by
+        pass 2's last block."""
+        _lib.call("sim_eam_step_drift_indenter", self.st_ref, tables.ref, integ.ref, indenter_ref, _lib.ptr(self.extra),
+                  LOG_EXTRA, _lib.ptr(self.log), self.log_capacity, self.stream)
+        self._last_force_precision = 0
+        self.forces_valid = True
+
     def eam_step_drift(self, tables, integ):
         """eam_forces_integrate_drift + log_step(after_drift=True) +
         rebuild_if_needed, with the log row and the rebuild decision made by

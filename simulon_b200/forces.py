@@ -101,6 +101,11 @@ class EAMForceCUDAExt(BackboneInterface):
         integrator's second half (mode 1) or both half-steps (mode 2)."""
         self.molecular.engine.eam_forces_integrate_indenter(self.tables, integrator.params, indenter._ref, mode)
 
+    def step_drift_with_indenter(self, integrator, indenter):
+        """compute_finish_with_indenter(mode 2), the step's log row and the
+        conditional list rebuild, the last two decided inside the force pass."""
+        self.molecular.engine.eam_step_drift_indenter(self.tables, integrator.params, indenter._ref)
+
     def step_and_drift(self, integrator):
         """compute_finish_and_drift, the step's log row and the conditional
         list rebuild, with the last two decided inside the force pass."""

@@ -124,7 +124,7 @@ class BaseModel(nn.Module):
         if pre_step is not None:
             loader = getattr(pre_step, "loader", None)
             baro = self.barostat
-            if (k > 1 and loader is not None and callable(getattr(loader, "launch_after", None))
+            if (k > 1 and loader is not None and callable(getattr(loader, "link", None))
                     and callable(getattr(baro, "controller", None)) and hasattr(baro, "work")
                     and hasattr(self.Integrator, "params")):
                 # tensile loop: the barostat's atom scaling of step s, the
@@ -134,9 +134,7 @@ class BaseModel(nn.Module):
                 for s in range(k):
                     self._forces_and_second_half()
                     if s < k - 1:
-                        baro.controller(self.Integrator.dt)
-                        self.engine.log_step()
-                        loader.launch_after(baro, self.Integrator, pre_step.dt)
+                        loader.link(baro, self.Integrator, pre_step.dt)
                     else:
                         baro.step(self.Integrator.dt)
                         self.engine.log_step()
@@ -164,10 +162,11 @@ class BaseModel(nn.Module):
             eam, ind = pair
             self.Integrator.first_half()
             for s in range(k):
-                eam.compute_finish_with_indenter(self.Integrator, ind, 2 if s < k - 1 else 1)
-                self.engine.log_step(after_drift=s < k - 1)
                 if s < k - 1:
-                    self.engine.rebuild_if_needed()
+                    eam.step_drift_with_indenter(self.Integrator, ind)
+                else:
+                    eam.compute_finish_with_indenter(self.Integrator, ind, 1)
+                    self.engine.log_step()
             return
         if k <= 1 or not self._drift_fusable():
             for _ in range(k):

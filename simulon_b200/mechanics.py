@@ -126,6 +126,25 @@ class UniaxialTensileLoader:
         eng.rebuild_if_needed()
         return self.state[12]
 
+    def link(self, barostat, integrator, dt: float) -> torch.Tensor:
+        """The end of this step and the start of the next with an anisotropic
+        barostat, in one call (sim_tensile_link): the barostat's controller,
+        the step's log row, then launch_after's work; the same bits as
+        barostat.controller(dt), the engine's log_step() and
+        launch_after(barostat, integrator, dt) one after another, in three
+        kernels instead of seven."""
+        eng = self.molecular.engine
+        barostat._st.dt = float(integrator.dt)
+        s = _lib.SimBoxScale()
+        s.scale[:] = self._scale_vector(dt)
+        s.vel_scale[:] = [1.0, 1.0, 1.0]
+        s.reset_reference = 1
+        _lib.call("sim_tensile_link", eng.st_ref, barostat._ref, _lib.ptr(barostat.work), _lib.ptr(eng.step_ctr),
+                  _lib.ptr(eng.extra), int(eng.extra.numel()), _lib.ptr(eng.log), eng.log_capacity, ctypes.byref(s),
+                  _lib.ptr(self.work), integrator.params.ref, int(integrator.force_precision),
+                  ctypes.byref(self._check), _lib.ptr(self.state), eng.stream)
+        return self.state[12]
+
     def hook(self, dt: float):
         """The per-step callable for BaseModel.run(pre_step=...): launch(dt),
         marked so that the model can fuse it with a barostat's scaling and

@@ -58,6 +58,7 @@ def test_argument_errors_are_reported_without_gpu(lib):
     assert lib.sim_berendsen_mu(None, None, None, None) == _lib.SIM_ERR_ARG
     assert lib.sim_berendsen_scale_first(None, None, None, None, 0, None) == _lib.SIM_ERR_ARG
     assert lib.sim_eam_force_integrate_indenter(None, None, None, None, 1, None) == _lib.SIM_ERR_ARG
+    assert lib.sim_eam_step_drift_indenter(None, None, None, None, None, 0, None, 0, None) == _lib.SIM_ERR_ARG
     assert lib.sim_scan_i64(None, 5, None, None) == _lib.SIM_ERR_ARG
     assert lib.sim_scan_i64(None, -1, None, None) == _lib.SIM_ERR_ARG
     e, p, ip = _lib.SimEngine(), _lib.SimLJParams(), _lib.SimIntegrator()
@@ -82,6 +83,13 @@ def test_argument_errors_are_reported_without_gpu(lib):
     assert lib.sim_box_scale_after_first(ctypes.byref(e), ctypes.c_void_p(16), 1, ctypes.byref(bs),
                                          ctypes.c_void_p(16), ctypes.byref(ip), 0, None) == _lib.SIM_ERR_ARG
     assert lib.sim_box_scale_after_first(None, None, 1, None, None, None, 0, None) == _lib.SIM_ERR_ARG
+    # the linked tensile step: a missing piece, a bad loader scale or a bad loader check, before any launch
+    an = _lib.SimAniso()
+    assert lib.sim_tensile_link(None, None, None, None, None, 0, None, 0, None, None, None, 0, None, None,
+                                None) == _lib.SIM_ERR_ARG
+    assert lib.sim_tensile_link(ctypes.byref(e), ctypes.byref(an), ctypes.c_void_p(16), None, None, 0,
+                                ctypes.c_void_p(16), 8, ctypes.byref(bs), ctypes.c_void_p(16), ctypes.byref(ip), 0,
+                                ctypes.byref(chk), ctypes.c_void_p(16), None) == _lib.SIM_ERR_ARG
     with pytest.raises(_lib.SimError):
         _lib.check(_lib.SIM_ERR_ARG, "probe")
 
