@@ -90,6 +90,21 @@ def test_engine_list_export_matches_oracle(sb):
     assert torch.equal(eng.gather("x").cpu(), torch.tensor(x))
 
 
+def test_engine_long_rows_match_oracle(sb):
+    """The list builder's long forms: FCC Ar within 11.5 A (~174 neighbours
+    per row, beyond the 128-entry sorted-row buffer, so rows are written in
+    visiting order) in a 2x2x2 cell grid (500 candidates per stencil, two
+    register chunks); the engine's export equals the oracle's pair set."""
+    x, L = oin.fcc_lattice(5)
+    x = oin.jitter(x, 0.05, 41)
+    eng = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.AR_MASS], np.diag([L] * 3), 11.0, 0.5, device=DEV)
+    assert list(eng.ncell) == [2, 2, 2] and eng.neighbor_stats()["max"] > 128
+    ei, _ = eng.half_list(11.5 ** 2)
+    o = onb.half_list(x, OracleBox(L), 11.5 ** 2)
+    assert np.array_equal(ei[0].cpu().numpy(), o["i"]) and np.array_equal(ei[1].cpu().numpy(), o["j"])
+    assert eng.status() == 0
+
+
 def test_engine_half_count_row_offsets_in_place_scan(sb):
     """sim_engine_half_count scans its per-row counts in place (counts in
     row_ptr[1:], offsets into row_ptr): for 16,000 atoms the scan crosses
