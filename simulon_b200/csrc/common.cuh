@@ -356,11 +356,12 @@ __device__ __forceinline__ void second_half_atom(const SimEngine& e, const SimIn
 // moved more than skin/2 from its position at the last rebuild
 // (reader.py:136-163).  v_in / x_in: the velocity to kick and the position to
 // drift (read from e.v / e.x when NULL).
-__device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, int64_t i, int type, const double* xn);
+__device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, int64_t i, int type, const double* xn,
+                                           int32_t* q_out = nullptr);
 
 __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimBox& b, const SimIntegrator& p, int64_t i,
                                                 int type, const double* f, const double* v_in, bool& bad,
-                                                const double* x_in = nullptr) {
+                                                const double* x_in = nullptr, int32_t* q_out = nullptr) {
     const int64_t P = e.n_pad;
     const double m = e.mass[type];
     double xn[3];
@@ -373,7 +374,7 @@ __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimBox
         st_state(&e.v[c * P + i], vh);
         bad |= !isfinite(xn[c]) || !isfinite(vh);
     }
-    return place_atom(e, b, i, type, xn);
+    return place_atom(e, b, i, type, xn, q_out);
 }
 
 __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimIntegrator& p, int64_t i, int type,
@@ -381,10 +382,12 @@ __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimInt
     return first_half_atom(e, *e.box, p, i, type, f, v_in, bad);
 }
 
-// Store position xn of slot i, refresh its fixed-point code in posq, and
-// report whether it is more than skin/2 from its position at the last rebuild
-// (reader.py:136-163).
-__device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, int64_t i, int type, const double* xn) {
+// Store position xn of slot i, refresh its fixed-point code in posq (in
+// q_out instead when given: a pass that still gathers posq must not see it
+// change), and report whether it is more than skin/2 from its position at the
+// last rebuild (reader.py:136-163).
+__device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, int64_t i, int type, const double* xn,
+                                           int32_t* q_out) {
     const int64_t P = e.n_pad;
 #pragma unroll
     for (int c = 0; c < 3; ++c) st_state(&e.x[c * P + i], xn[c]);
@@ -395,7 +398,7 @@ __device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, 
     q.y = (int32_t)to_fixed(s[1]);
     q.z = (int32_t)to_fixed(s[2]);
     q.w = type;
-    reinterpret_cast<int4*>(e.posq)[i] = q;
+    reinterpret_cast<int4*>(q_out ? q_out : e.posq)[i] = q;
     // displacement since the last rebuild, minimum image in fractional space
     const double t0 = (double)(int32_t)((uint32_t)q.x - (uint32_t)ld_state(&e.xref[i])) * 2.3283064365386963e-10;
     const double t1 = (double)(int32_t)((uint32_t)q.y - (uint32_t)ld_state(&e.xref[P + i])) * 2.3283064365386963e-10;

@@ -124,8 +124,10 @@ __global__ void __launch_bounds__(SIM_THREADS, LJ_MIN_BLOCKS) k_lj_f32(SimEngine
             acc[9] += (float)(m * v[0] * v[0]); acc[10] += (float)(m * v[1] * v[1]); acc[11] += (float)(m * v[2] * v[2]);
             acc[12] += (float)(m * v[0] * v[1]); acc[13] += (float)(m * v[0] * v[2]); acc[14] += (float)(m * v[1] * v[2]);
             if (INTEG == 2) {
+                // the new fixed-point record goes to posfp: other threads of this
+                // pass still gather posq; k_copy_records moves it after the pass
                 const double f[3] = {(double)fx, (double)fy, (double)fz};
-                trig |= first_half_atom(e, ip, i, ti, f, v, bad);
+                trig |= first_half_atom(e, *e.box, ip, i, ti, f, v, bad, nullptr, e.posfp);
             }
         }
     }
@@ -249,6 +251,16 @@ __global__ void __launch_bounds__(SIM_THREADS) k_lj_f64(SimEngine e, SimLJParams
 
 // zero the embedding slot for pair-only force fields
 __global__ void k_zero_slot(double* out, int slot) { out[slot] = 0.0; }
+
+// posq <- posfp for the atoms (the records a mode-2 pass wrote aside)
+__global__ void k_copy_records(SimEngine e) {
+    pdl_trigger();
+    pdl_wait();
+    const int4* __restrict__ src = reinterpret_cast<const int4*>(e.posfp);
+    int4* __restrict__ dst = reinterpret_cast<int4*>(e.posq);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
 }  // namespace simb200
 
 using namespace simb200;
@@ -300,8 +312,15 @@ extern "C" int sim_lj_forces_integrate(const SimEngine* ep, const SimLJParams* p
     if (ip->langevin && !ip->rff) return SIM_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     k_zero_slot<<<1, 1, 0, st>>>(ep->red_out, SIM_RED_EPOT_EMBED);
+    if (mode == 2 && !ep->posfp) return SIM_ERR_ARG;
     const int rc = mode == 1 ? lj_f32<1>(*ep, *pp, *ip, st) : lj_f32<2>(*ep, *pp, *ip, st);
     if (rc != SIM_OK) return rc;
+    if (mode == 2) {
+        const int64_t blocks = ceil_div(ep->n, SIM_THREADS);
+        const cudaError_t err = launch_pdl(k_copy_records, dim3((unsigned)(blocks > 148 * 16 ? 148 * 16 : blocks)),
+                                           dim3(SIM_THREADS), 0, st, *ep);
+        if (err != cudaSuccess) { set_cuda_error(err, "sim_lj_forces_integrate: copy"); return SIM_ERR_CUDA; }
+    }
     return launch_status(mode == 1 ? "sim_lj_forces_integrate" : "sim_lj_forces_integrate (drift)");
 }
 

@@ -286,14 +286,17 @@ def test_lj_fp32_pairs_match_reference(sb, tmp_path, mode):
     assert np.sqrt(((f - g["forces"]) ** 2).mean()) < 2e-6
 
 
-@pytest.mark.parametrize("mode", ["raw", "switch"])
-def test_lj_fused_integrator_equals_separate_kernels(sb, tmp_path, mode):
+@pytest.mark.parametrize("mode,n", [("raw", 6), ("switch", 6), ("raw", 48)])
+def test_lj_fused_integrator_equals_separate_kernels(sb, tmp_path, mode, n):
     """FP32 LJ with the integrator in the force pass (second half; second half
     plus the next first half) against the separate force and integrator
     kernels: positions and velocities bit for bit after 40 Langevin steps,
-    triggered rebuilds included; energies and virials to FP32 sum order."""
+    triggered rebuilds included; energies and virials to FP32 sum order.  At
+    n = 48 (442,368 atoms) each thread of the persistent grid takes three
+    atoms, so a pass whose first half moved atoms that later iterations still
+    gather would show here."""
     from simulon_b200.engine import integrator_params
-    x, L = oin.fcc_lattice(6)
+    x, L = oin.fcc_lattice(n)
     x = oin.jitter(x, 0.05, 91)
     res = []
     for fused in ("separate", "second", "drift"):
