@@ -406,7 +406,9 @@ int sim_lj_forces(const SimEngine* e, const SimLJParams* p, int32_t precision, v
  * integrator.py:102-124); mode 2 adds the next step's first half as well
  * (as sim_integrate_first, integrator.py:91-99: kick with the new forces,
  * drift, posq refresh, skin/2 trigger), advancing p->step_ctr[0] and setting
- * step_ctr[1] to this step like sim_eam_force_integrate_drift. */
+ * step_ctr[1] to this step like sim_eam_force_integrate_drift.  Mode 2 writes
+ * the new fixed-point records to e->posfp (required; the pass still gathers
+ * posq) and copies them to posq after the pass. */
 int sim_lj_forces_integrate(const SimEngine* e, const SimLJParams* p, const SimIntegrator* integ, int32_t mode,
                             void* stream);
 /* FP32-pair LJ as a further force field of a sum (SumBackboneInterface.forward,
