@@ -463,6 +463,40 @@ def _lib_red_slots():
     return _lib.RED_SLOTS
 
 
+def test_eam_drift_fused_equals_separate_at_scale(sb, fsw_path):
+    """BCC W 2*64^3 = 524,288 atoms, where each thread of the persistent pass 2
+    takes three or four atoms: 30 Langevin steps with the next first half
+    fused into pass 2 (sim_eam_step_drift) against separate force, second-half
+    and first-half kernels, positions and velocities bit for bit (pass 2
+    gathers pass 1's copy of the positions, so atoms that its epilogue has
+    moved are never seen by the same pass)."""
+    from simulon_b200.engine import integrator_params
+    x, L = oin.bcc_lattice(64)
+    x = oin.jitter(x, 0.05, 52)
+    v = oin.maxwell_boltzmann(np.full(len(x), oin.W_MASS), 600.0, 53)
+    res = []
+    for fused in (False, True):
+        eng, tables, _ = _eam_engine(sb, fsw_path, x, np.diag([L] * 3), v)
+        integ = integrator_params(eng, 0.002, langevin=True, temperature=600.0, gamma=10.0, seed=7)
+        eng.eam_forces(tables)
+        eng.integrate_first(integ, 0)
+        eng.rebuild_if_needed()
+        for s in range(30):
+            if fused and s < 29:
+                eng.eam_step_drift(tables, integ)
+                continue
+            eng.eam_forces(tables)
+            eng.integrate_second(integ, 0)
+            if s < 29:
+                eng.integrate_first(integ, 0)
+                eng.rebuild_if_needed()
+        torch.cuda.synchronize()
+        assert eng.status() == 0
+        res.append((eng.gather("x").cpu(), eng.gather("v").cpu(), int(eng.flags[3])))
+    assert torch.equal(res[0][0], res[1][0]) and torch.equal(res[0][1], res[1][1])
+    assert res[0][2] == res[1][2]
+
+
 def test_graph_run_matches_eager_steps(sb, fsw_path):
     x, L = oin.bcc_lattice(10)
     x = oin.jitter(x, 0.05, 50)
