@@ -85,6 +85,37 @@ def _single_drift_run(eng, tables, integ, k):
             eng.eam_forces_integrate(tables, integ)
 
 
+def test_batch_nve_trajectory_matches_single_engines_at_scale(sb, fsw):
+    """A 351,232-atom replica (each thread of the persistent batched passes
+    takes two or three atoms) next to a 250-atom one: 30 NVE steps in
+    graphs of 10, positions and velocities bit for bit against the single
+    engine, so no pass of the batch sees atoms that its own epilogue moved."""
+    from simulon_b200.batch import BatchedEngine, Replica
+    from simulon_b200.engine import integrator_params
+    parser, tables = fsw
+    reps = []
+    for k, n in enumerate((56, 5)):
+        x, L = oin.bcc_lattice(n)
+        x = oin.jitter(x, 0.06, 170 + k)
+        v = oin.maxwell_boltzmann(np.full(len(x), oin.W_MASS), 600.0, 180 + k)
+        reps.append(Replica(positions=x, H=np.diag([L] * 3), velocities=v, temperature=600.0))
+    be = BatchedEngine(reps, oin.W_MASS, parser.cutoff, 0.5, device=DEV)
+    integ = be.integrator(0.002, langevin=False)
+    be.run(tables, integ, 30, graph_steps=10)
+    torch.cuda.synchronize()
+    assert be.status() == 0
+    xb, vb = be.gather("x").cpu(), be.gather("v").cpu()
+    for k, rp in enumerate(reps):
+        eng = _single(sb, rp, parser, rp.velocities)
+        ip = integrator_params(eng, 0.002)
+        eng.eam_forces(tables)
+        for _ in range(3):
+            _single_drift_run(eng, tables, ip, 10)
+        sl = be.replica_slice(k)
+        assert torch.equal(xb[sl], eng.gather("x").cpu()), k
+        assert torch.equal(vb[sl], eng.gather("v").cpu()), k
+
+
 def test_batch_nve_trajectory_matches_single_engines(sb, fsw):
     from simulon_b200.batch import BatchedEngine
     from simulon_b200.engine import integrator_params
