@@ -565,6 +565,7 @@ __global__ void __launch_bounds__(BATCH_FORCE_THREADS, 1) k_bb_force(SimBatch B,
             B.rep_flags[k] = 1;
             e.flags[0] = 1;
         }
+        virial_trace(acc);
         double* out = B.chunk_red + (i >> 5) * SIM_RED_SLOTS;
 #pragma unroll
         for (int s = 0; s < 15; ++s) {

@@ -273,6 +273,7 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
             }
         }
     }
+    virial_trace(acc);
     if (INTEG == 2 && __any_sync(0xffffffffu, trig) && (threadIdx.x & 31) == 0) e.flags[0] = 1;
     if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
     if (INTEG) {

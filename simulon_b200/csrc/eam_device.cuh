@@ -97,14 +97,17 @@ __device__ __forceinline__ int pop_slot(uint64_t& m) {
 // ---------------------------------------------------------------------------
 // pass 2.  Per-thread accumulators: acc[0] pair energy, acc[1] scalar virial,
 // acc[2..7] virial tensor (xx yy zz xy xz yz), acc[8] K, acc[9..14] K tensor;
-// only the three force components are per atom.
+// only the three force components are per atom.  The scalar virial sum s r is
+// minus the tensor's trace (f = -s r/|r|, so f.r = -s |r|): it is not summed
+// per pair but set from the thread's trace before the reduction (virial_trace).
+__device__ __forceinline__ void virial_trace(float (&acc)[15]) { acc[1] = -(acc[2] + acc[3] + acc[4]); }
+
 __device__ __forceinline__ void pair_force(float s, float phi, float r, float inv_r, float r0, float r1, float r2,
                                            float& fx, float& fy, float& fz, float (&acc)[15]) {
     const float c = -s * inv_r;            // force on i = c * r_ij
     const float ax = c * r0, ay = c * r1, az = c * r2;
     fx += ax; fy += ay; fz += az;
     acc[0] += phi;
-    acc[1] = fmaf(s, r, acc[1]);
     acc[2] = fmaf(ax, r0, acc[2]); acc[3] = fmaf(ay, r1, acc[3]); acc[4] = fmaf(az, r2, acc[4]);
     acc[5] = fmaf(ax, r1, acc[5]); acc[6] = fmaf(ax, r2, acc[6]); acc[7] = fmaf(ay, r2, acc[7]);
 }

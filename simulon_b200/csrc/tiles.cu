@@ -323,7 +323,6 @@ __global__ void __launch_bounds__(SIM_TILE, 1) k_eam_force_tiled(SimEngine e, Si
                 const float ax = c * r0, ay = c * r1, az = c * r2;
                 fx += ax; fy += ay; fz += az;
                 acc[0] += phi;
-                acc[1] = fmaf(s, r, acc[1]);
                 acc[2] = fmaf(ax, r0, acc[2]); acc[3] = fmaf(ay, r1, acc[3]); acc[4] = fmaf(az, r2, acc[4]);
                 acc[5] = fmaf(ax, r1, acc[5]); acc[6] = fmaf(ax, r2, acc[6]); acc[7] = fmaf(ay, r2, acc[7]);
             }
@@ -342,6 +341,7 @@ __global__ void __launch_bounds__(SIM_TILE, 1) k_eam_force_tiled(SimEngine e, Si
     }
     cp_async_wait<0>();
     if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);
+    acc[1] = -(acc[2] + acc[3] + acc[4]);   // scalar virial s r = minus the tensor's trace
     if (INTEG) {
         double vals[15];
 #pragma unroll
