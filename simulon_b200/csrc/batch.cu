@@ -385,7 +385,7 @@ __global__ void k_bb_flag_all(SimBatch B) {
 }
 
 // ---------------------------------------------------------------------------
-// EAM pass 1: as k_eam_density, with the replica's box per warp and per-warp
+// EAM pass 1: as k_eam_density (one element type), with the replica's box per warp and per-warp
 // embedding-energy sums
 
 template <bool ORTHO>
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(BATCH_DENSITY_THREADS, 3) k_bb_density(SimBatc
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     bool in;
-                    rho += density_term<true, ORTHO>(b, qi, q[u], rc2, dens, s_dens, w, t, in);
+                    rho += density_term<true, ORTHO, true>(b, qi, q[u], rc2, dens, s_dens, w, t, in);
                     bits |= (uint32_t)in << u;
                 }
                 if (kk < 32) in_lo |= bits << kk;
@@ -435,8 +435,8 @@ __global__ void __launch_bounds__(BATCH_DENSITY_THREADS, 3) k_bb_density(SimBatc
             }
             for (; kk < nn; ++kk) {
                 bool in;
-                rho += density_term<true, ORTHO>(b, qi, __ldg(&posq[ld_stream(&nbr[(int64_t)kk * P + i])]), rc2, dens,
-                                                 s_dens, w, t, in);
+                rho += density_term<true, ORTHO, true>(b, qi, __ldg(&posq[ld_stream(&nbr[(int64_t)kk * P + i])]), rc2,
+                                                       dens, s_dens, w, t, in);
                 if (kk < 32) in_lo |= (uint32_t)in << kk;
                 else in_hi |= (uint32_t)in << (kk - 32);
             }
@@ -714,7 +714,7 @@ static Window batch_window(const SimEAMTables& t) {
 }
 
 static bool batch_tables_ok(const SimEAMTables* t) {
-    return t && t->n_types == 1 && t->n_r >= 2 && t->n_rho >= 2 && t->dens_vd && t->deriv_vd && t->pair_vd &&
+    return t && t->n_types == 1 && t->n_r >= 2 && t->n_r < kMaxTableRows && t->n_rho >= 2 && t->dens_vd && t->deriv_vd && t->pair_vd &&
            t->embed && t->embed_deriv && t->rho_min && t->inv_drho && t->rho_clamp_hi;
 }
 

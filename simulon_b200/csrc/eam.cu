@@ -48,12 +48,13 @@ namespace simb200 {
 #define EAM_WINDOW_ROWS 4096
 #endif
 
-template <bool SMEM, bool ORTHO>
+// ONE: engine and tables hold a single element type.
+template <bool SMEM, bool ORTHO, bool ONE>
 __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k_eam_density(SimEngine e, SimEAMTables t, Window w) {
     extern __shared__ float2 s_dens[];
     pdl_trigger();
     const float2* dens = reinterpret_cast<const float2*>(t.dens_vd);
-    const int nt = t.n_types;
+    const int nt = ONE ? 1 : t.n_types;
     if (SMEM) {
         for (int tt = 0; tt < nt * nt; ++tt)
             for (int k = threadIdx.x; k < w.n_win; k += blockDim.x)
@@ -72,7 +73,7 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k
     const BlockRange br = block_range(e.n);
     for (int64_t i = br.begin + threadIdx.x; i < br.end; i += blockDim.x) {
         const int4 qi = posq[i];
-        const int ti = qi.w;
+        const int ti = ONE ? 0 : qi.w;
         const int nn = e.nnbr[i];
         const float2* g_i = dens + (size_t)ti * nt * t.n_r;
         const float2* s_i = s_dens + (size_t)ti * nt * w.n_win;
@@ -91,7 +92,7 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 bool in;
-                rho += density_term<SMEM, ORTHO>(b, qi, q[u], rc2, g_i, s_i, w, t, in);
+                rho += density_term<SMEM, ORTHO, ONE>(b, qi, q[u], rc2, g_i, s_i, w, t, in);
                 bits |= (uint32_t)in << u;
             }
             if (k < 32) in_lo |= bits << k;
@@ -99,8 +100,8 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k
         }
         for (; k < nn; ++k) {
             bool in;
-            rho += density_term<SMEM, ORTHO>(b, qi, __ldg(&posq[ld_stream(&nbr[(int64_t)k * P + i])]), rc2, g_i, s_i,
-                                             w, t, in);
+            rho += density_term<SMEM, ORTHO, ONE>(b, qi, __ldg(&posq[ld_stream(&nbr[(int64_t)k * P + i])]), rc2, g_i,
+                                                  s_i, w, t, in);
             if (k < 32) in_lo |= (uint32_t)in << k;
             else in_hi |= (uint32_t)in << (k - 32);
         }
@@ -353,8 +354,10 @@ static void allow_smem(K kernel) {
 static void eam_set_attributes() {
     static bool done = false;   // the first call happens before any stream capture
     if (!done) {
-        allow_smem(k_eam_density<true, true>);
-        allow_smem(k_eam_density<true, false>);
+        allow_smem(k_eam_density<true, true, true>);
+        allow_smem(k_eam_density<true, false, true>);
+        allow_smem(k_eam_density<true, true, false>);
+        allow_smem(k_eam_density<true, false, false>);
         allow_smem(k_eam_force<true, 0, true>);
         allow_smem(k_eam_force<true, 1, true>);
         allow_smem(k_eam_force<true, 2, true>);
@@ -370,7 +373,7 @@ static void eam_set_attributes() {
 }
 
 static bool valid_tables(const SimEAMTables& t) {
-    return t.n_types >= 1 && t.n_r >= 2 && t.n_rho >= 2 && t.embed && t.embed_deriv && t.rho_min && t.inv_drho &&
+    return t.n_types >= 1 && t.n_r >= 2 && t.n_r < kMaxTableRows && t.n_rho >= 2 && t.embed && t.embed_deriv && t.rho_min && t.inv_drho &&
            t.rho_clamp_hi && t.dens_vd && t.deriv_vd && t.pair_vd;
 }
 
@@ -385,16 +388,21 @@ static int force_threads(const SimEngine& e) {
     return t == 0 ? EAM_FORCE_THREADS : (t == 256 || t == 512 || t == EAM_FORCE_THREADS) && t <= EAM_FORCE_THREADS ? t : -1;
 }
 
-template <bool SMEM, bool ORTHO>
-static int launch_density(const SimEngine& e, const SimEAMTables& t, size_t smem, cudaStream_t st) {
+template <bool SMEM, bool ORTHO, bool ONE>
+static int launch_density1(const SimEngine& e, const SimEAMTables& t, size_t smem, cudaStream_t st) {
     const int threads = density_threads(e);
     if (threads < 0) return SIM_ERR_ARG;
-    const int g = persistent_grid((const void*)k_eam_density<SMEM, ORTHO>, threads, smem, e.n);
+    const int g = persistent_grid((const void*)k_eam_density<SMEM, ORTHO, ONE>, threads, smem, e.n);
     if (g > e.n_blocks_max) return SIM_ERR_ARG;
-    const cudaError_t err = launch_pdl(k_eam_density<SMEM, ORTHO>, dim3(g), dim3(threads), smem, st, e, t,
+    const cudaError_t err = launch_pdl(k_eam_density<SMEM, ORTHO, ONE>, dim3(g), dim3(threads), smem, st, e, t,
                                        table_window(t));
     if (err != cudaSuccess) { set_cuda_error(err, "sim_eam_density: launch"); return SIM_ERR_CUDA; }
     return SIM_OK;
+}
+template <bool SMEM, bool ORTHO>
+static int launch_density(const SimEngine& e, const SimEAMTables& t, size_t smem, cudaStream_t st) {
+    return e.n_types == 1 && t.n_types == 1 ? launch_density1<SMEM, ORTHO, true>(e, t, smem, st)
+                                            : launch_density1<SMEM, ORTHO, false>(e, t, smem, st);
 }
 
 extern "C" int sim_eam_density(const SimEngine* ep, const SimEAMTables* tp, void* stream) {

@@ -56,10 +56,18 @@ struct Lerp {
     int k;
     float frac;
 };
+// Tables hold fewer rows than this (checked by every entry point that takes
+// SimEAMTables), so lerp_r's truncation below is exact.
+constexpr int kMaxTableRows = 1 << 22;
+
+// trunc(idx_f) without the conversion unit: for 0 <= idx_f < 2^23 the sum
+// 2^23 + idx_f rounded toward zero is 2^23 + trunc(idx_f), held in the low
+// mantissa bits, and subtracting 2^23 back is exact -- the same k and fraction
+// as (int)idx_f and idx_f - (float)k (tables have fewer than 2^22 rows).
 __device__ __forceinline__ Lerp lerp_r(float r, const SimEAMTables& t) {
     const float idx_f = fminf(r, t.r_clamp_hi) * t.inv_dr;
-    const int k = (int)idx_f;
-    return Lerp{k, idx_f - (float)k};
+    const float s = __fadd_rz(idx_f, 8388608.0f);
+    return Lerp{__float_as_int(s) - 0x4B000000, idx_f - (s - 8388608.0f)};
 }
 
 // ---------------------------------------------------------------------------
@@ -70,7 +78,9 @@ struct Window {
     int k_lo, n_win;
 };
 
-template <bool SMEM, bool ORTHO>
+// ONE: a single element type (type 0 throughout), so the table row needs no
+// type index.
+template <bool SMEM, bool ORTHO, bool ONE = false>
 __device__ __forceinline__ float density_term(const BoxF& b, const int4& qi, const int4& qj, float rc2,
                                               const float2* g_i, const float2* s_i, Window w,
                                               const SimEAMTables& t, bool& inside) {
@@ -80,9 +90,10 @@ __device__ __forceinline__ float density_term(const BoxF& b, const int4& qi, con
     inside = d2 < rc2;
     if (!inside) return 0.0f;
     const Lerp l = lerp_r(d2 * rsqrt_approx(d2), t);
+    const int tj = ONE ? 0 : qj.w;
     float2 v;
-    if (SMEM && l.k >= w.k_lo) v = s_i[qj.w * w.n_win + (l.k - w.k_lo)];
-    else v = __ldg(&g_i[(size_t)qj.w * t.n_r + l.k]);
+    if (SMEM && l.k >= w.k_lo) v = s_i[tj * w.n_win + (l.k - w.k_lo)];
+    else v = __ldg(&g_i[(size_t)tj * t.n_r + l.k]);
     return fmaf(l.frac, v.y, v.x);
 }
 

@@ -1366,7 +1366,9 @@ extern "C" int sim_autotune_mlp(const SimEngine* e, const float* dEdG, float* G,
 }
 
 extern "C" int sim_eam_atom_energy(const SimEngine* e, const SimEAMTables* t, float* e_atom, void* stream) {
-    if (!e || !t || !e_atom || e->n <= 0 || t->n_types != 1 || !t->dens_vd || !t->pair_vd) return SIM_ERR_ARG;
+    if (!e || !t || !e_atom || e->n <= 0 || t->n_types != 1 || t->n_r < 2 || t->n_r >= kMaxTableRows || !t->dens_vd ||
+        !t->pair_vd)
+        return SIM_ERR_ARG;
     const int g = (int)((e->n + 255) / 256 < 148 * 8 ? (e->n + 255) / 256 : 148 * 8);
     k_eam_atom_energy<<<g, 256, 0, (cudaStream_t)stream>>>(*e, *t, e_atom);
     return launch_status("sim_eam_atom_energy");

@@ -90,6 +90,15 @@ def test_argument_errors_are_reported_without_gpu(lib):
     assert lib.sim_tensile_link(ctypes.byref(e), ctypes.byref(an), ctypes.c_void_p(16), None, None, 0,
                                 ctypes.c_void_p(16), 8, ctypes.byref(bs), ctypes.c_void_p(16), ctypes.byref(ip), 0,
                                 ctypes.byref(chk), ctypes.c_void_p(16), None) == _lib.SIM_ERR_ARG
+    # EAM tables of 2^22 rows or more are refused (the kernels' row truncation is exact below that)
+    tb = _lib.SimEAMTables()
+    for name in ("density", "density_deriv", "pair", "pair_deriv", "embed", "embed_deriv", "rho_min", "inv_drho",
+                 "rho_clamp_hi", "dens_vd", "deriv_vd", "pair_vd"):
+        setattr(tb, name, 16)
+    tb.n_types, tb.n_r, tb.n_rho = 1, 1 << 22, 100
+    e.n_types, e.posfp = 1, 16
+    assert lib.sim_eam_density(ctypes.byref(e), ctypes.byref(tb), None) == _lib.SIM_ERR_ARG
+    assert lib.sim_eam_atom_energy(ctypes.byref(e), ctypes.byref(tb), ctypes.c_void_p(16), None) == _lib.SIM_ERR_ARG
     with pytest.raises(_lib.SimError):
         _lib.check(_lib.SIM_ERR_ARG, "probe")
 
