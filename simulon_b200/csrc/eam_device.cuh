@@ -97,13 +97,26 @@ __device__ __forceinline__ float density_term(const BoxF& b, const int4& qi, con
     return fmaf(l.frac, v.y, v.x);
 }
 
-// Lowest set bit of m as a list slot (clearing it), or -1 when m is empty.
-__device__ __forceinline__ int pop_slot(uint64_t& m) {
-    if (m == 0) return -1;
-    const int k = __ffsll((long long)m) - 1;
-    m &= m - 1;
-    return k;
-}
+// A row's in-cutoff slots (bit k: slot k) as two 32-bit words, since slots of
+// 32 and above are rare; pop() returns the lowest one left and clears it, or
+// -1 when none is left (the slots come out in increasing order).
+struct SlotMask {
+    uint32_t lo, hi;
+    __device__ __forceinline__ explicit SlotMask(uint64_t m) : lo((uint32_t)m), hi((uint32_t)(m >> 32)) {}
+    __device__ __forceinline__ int pop() {
+        if (lo) {
+            const int k = __ffs((int)lo) - 1;
+            lo &= lo - 1;
+            return k;
+        }
+        if (hi) {
+            const int k = __ffs((int)hi) + 31;
+            hi &= hi - 1;
+            return k;
+        }
+        return -1;
+    }
+};
 
 // ---------------------------------------------------------------------------
 // pass 2.  Per-thread accumulators: acc[0] pair energy, acc[1] scalar virial,
