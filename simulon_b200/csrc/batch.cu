@@ -506,14 +506,14 @@ __global__ void __launch_bounds__(BATCH_FORCE_THREADS, 1) k_bb_force(SimBatch B,
             if (use_mask) {
                 // in-cutoff slots only; the next two list entries are fetched
                 // while the current pair is gathered and evaluated
-                SlotMask m(ld_stream(&e.cut_mask[i]));
-                int ka = m.pop(), kb = m.pop();
+                SlotSeq m(ld_stream(&e.cut_mask[i]));
+                int ka = m.next(), kb = m.next();
                 int ja = ka >= 0 ? ld_stream(&nbr[(int64_t)ka * P + i]) : 0;
                 int jb = kb >= 0 ? ld_stream(&nbr[(int64_t)kb * P + i]) : 0;
                 while (kb >= 0) {
                     const int j0 = ja, j1 = jb;
-                    ka = m.pop();
-                    kb = m.pop();
+                    ka = m.next();
+                    kb = m.next();
                     if (ka >= 0) ja = ld_stream(&nbr[(int64_t)ka * P + i]);
                     if (kb >= 0) jb = ld_stream(&nbr[(int64_t)kb * P + i]);
                     const int4 q0 = __ldg(&posfp[j0]);

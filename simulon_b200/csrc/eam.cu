@@ -179,14 +179,14 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
         if (SINGLE && use_mask) {
             // only the slots pass 1 found inside the cutoff; the next two list
             // entries are fetched while the current pair is gathered and evaluated
-            SlotMask m(ld_stream(&e.cut_mask[i]));
-            int ka = m.pop(), kb = m.pop();
+            SlotSeq m(ld_stream(&e.cut_mask[i]));
+            int ka = m.next(), kb = m.next();
             int ja = ka >= 0 ? ld_stream(&nbr[(int64_t)ka * P + i]) : 0;
             int jb = kb >= 0 ? ld_stream(&nbr[(int64_t)kb * P + i]) : 0;
             while (kb >= 0) {
                 const int j0 = ja, j1 = jb;
-                ka = m.pop();
-                kb = m.pop();
+                ka = m.next();
+                kb = m.next();
                 if (ka >= 0) ja = ld_stream(&nbr[(int64_t)ka * P + i]);
                 if (kb >= 0) jb = ld_stream(&nbr[(int64_t)kb * P + i]);
                 const int4 q0 = __ldg(&posfp[j0]);
@@ -219,8 +219,8 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
             const float4* gd = reinterpret_cast<const float4*>(t.deriv_vd);
             const float2* gp = reinterpret_cast<const float2*>(t.pair_vd);
             ti = posq[i].w;
-            SlotMask m(use_mask ? ld_stream(&e.cut_mask[i]) : 0);
-            for (int k = use_mask ? m.pop() : 0; use_mask ? k >= 0 : k < nn; k = use_mask ? m.pop() : k + 1) {
+            SlotSeq m(use_mask ? ld_stream(&e.cut_mask[i]) : 0);
+            for (int k = use_mask ? m.next() : 0; use_mask ? k >= 0 : k < nn; k = use_mask ? m.next() : k + 1) {
                 const int j = ld_stream(&nbr[(int64_t)k * P + i]);
                 const int4 qj = __ldg(&posfp[j]);
                 float r0, r1, r2;

@@ -118,6 +118,19 @@ struct SlotMask {
     }
 };
 
+// The same slots in the same order, the leading run of set bits (slots 0 ..
+// p-1, usually most of the in-cutoff set since rows are sorted by distance at
+// rebuild) taken by counting instead of bit scans.
+struct SlotSeq {
+    SlotMask m;
+    int k, p;
+    __device__ __forceinline__ explicit SlotSeq(uint64_t bits) : m(bits), k(0) {
+        p = m.lo == 0xFFFFFFFFu ? 32 : __ffs((int)~m.lo) - 1;
+        m.lo &= m.lo + 1u;     // clears the leading run (all of lo when p = 32)
+    }
+    __device__ __forceinline__ int next() { return k < p ? k++ : m.pop(); }
+};
+
 // ---------------------------------------------------------------------------
 // pass 2.  Per-thread accumulators: acc[0] pair energy, acc[1] scalar virial,
 // acc[2..7] virial tensor (xx yy zz xy xz yz), acc[8] K, acc[9..14] K tensor;
