@@ -535,11 +535,11 @@ __global__ void __launch_bounds__(BATCH_FORCE_THREADS, 1) k_bb_force(SimBatch B,
                 const int64_t a = e.orig[i];
                 const int code = B.grip[a];
                 const double m = e.mass[0];
-                double v[3] = {0.0, 0.0, 0.0};
+                double v[3] = {0.0, 0.0, 0.0}, acl[3];
                 if (code == 0) {
                     SimIntegrator ipk = ip;
                     ipk.rff = B.rep_rff + k;          // one element type: rff[0] of this replica
-                    second_half_atom(e, ipk, i, 0, step, (double)fx, (double)fy, (double)fz, v, bad, MODE == 1);
+                    second_half_atom(e, ipk, i, 0, step, (double)fx, (double)fy, (double)fz, v, bad, MODE == 1, acl);
                 } else if (MODE == 1) {
 #pragma unroll
                     for (int c = 0; c < 3; ++c) e.v[c * P + i] = 0.0;
@@ -550,7 +550,7 @@ __global__ void __launch_bounds__(BATCH_FORCE_THREADS, 1) k_bb_force(SimBatch B,
                 if (MODE == 2) {
                     if (code == 0) {
                         const double f[3] = {(double)fx, (double)fy, (double)fz};
-                        trig = first_half_atom(e, R.box, ip, i, 0, f, v, bad);
+                        trig = first_half_atom(e, R.box, ip, i, 0, f, v, bad, nullptr, nullptr, acl);
                     } else {
                         double xn[3];
                         grip_position(B, R, code, a, step + 1, xn);

@@ -327,9 +327,9 @@ __device__ __forceinline__ void langevin_normals(uint32_t a, uint64_t step, uint
 // Writes e.v and returns the new velocity in v_out.
 __device__ __forceinline__ void second_half_atom(const SimEngine& e, const SimIntegrator& p, int64_t i, int type,
                                                  uint64_t step, double f0, double f1, double f2, double* v_out,
-                                                 bool& bad, bool store = true) {
+                                                 bool& bad, bool store = true, double* a_out = nullptr) {
     const int64_t P = e.n_pad;
-    const double m = e.mass[type];
+    const double inv_m = e.inv_mass[type];
     double z[3] = {0.0, 0.0, 0.0};
     double rff = 0.0;
     if (p.langevin) {
@@ -343,7 +343,8 @@ __device__ __forceinline__ void second_half_atom(const SimEngine& e, const SimIn
     for (int c = 0; c < 3; ++c) {
         double vel = ld_state(&e.v[c * P + i]);
         if (p.langevin) vel = __dadd_rn(__dmul_rn(vel, p.damp), __dmul_rn(z[c], rff));
-        const double a = __ddiv_rn(f[c], m);
+        const double a = __dmul_rn(f[c], inv_m);   // F (1/m): within 1 ulp of F/m, without a divide
+        if (a_out) a_out[c] = a;
         vel = __dadd_rn(vel, __dmul_rn(__dmul_rn(0.5, a), p.dt));
         if (store) st_state(&e.v[c * P + i], vel);
         v_out[c] = vel;
@@ -355,19 +356,23 @@ __device__ __forceinline__ void second_half_atom(const SimEngine& e, const SimIn
 // x += v dt, refresh the fixed-point code in posq, and report whether the atom
 // moved more than skin/2 from its position at the last rebuild
 // (reader.py:136-163).  v_in / x_in: the velocity to kick and the position to
-// drift (read from e.v / e.x when NULL).
+// drift (read from e.v / e.x when NULL); a_in: the acceleration when the
+// caller already formed it (second_half_atom's a_out for the same forces).
+// Both half-steps form F/m as F times the stored 1/m, which is within one
+// ulp of the reference's quotient and spares an FP64 divide per component.
 __device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, int64_t i, int type, const double* xn,
                                            int32_t* q_out = nullptr);
 
 __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimBox& b, const SimIntegrator& p, int64_t i,
                                                 int type, const double* f, const double* v_in, bool& bad,
-                                                const double* x_in = nullptr, int32_t* q_out = nullptr) {
+                                                const double* x_in = nullptr, int32_t* q_out = nullptr,
+                                                const double* a_in = nullptr) {
     const int64_t P = e.n_pad;
-    const double m = e.mass[type];
+    const double inv_m = e.inv_mass[type];
     double xn[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const double a = __ddiv_rn(f[c], m);
+        const double a = a_in ? a_in[c] : __dmul_rn(f[c], inv_m);
         const double v0 = v_in ? v_in[c] : ld_state(&e.v[c * P + i]);
         const double vh = __dadd_rn(v0, __dmul_rn(__dmul_rn(0.5, a), p.dt));
         xn[c] = __dadd_rn(x_in ? x_in[c] : ld_state(&e.x[c * P + i]), __dmul_rn(vh, p.dt));

@@ -128,10 +128,10 @@ __global__ void __launch_bounds__(SIM_THREADS) k_second_first(SimEngine e, SimIn
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < e.n; i += (int64_t)gridDim.x * blockDim.x) {
         const int type = e.posq[4 * i + 3];
         const double f[3] = {load_force(e, prec, i, 0), load_force(e, prec, i, 1), load_force(e, prec, i, 2)};
-        double v[3];
-        second_half_atom(e, p, i, type, step, f[0], f[1], f[2], v, bad, false);
+        double v[3], a[3];
+        second_half_atom(e, p, i, type, step, f[0], f[1], f[2], v, bad, false, a);
         ke_terms(e.mass[type], v, vals);
-        trig |= first_half_atom(e, p, i, type, f, v, bad);
+        trig |= first_half_atom(e, *e.box, p, i, type, f, v, bad, nullptr, nullptr, a);
     }
     if (__any_sync(0xffffffffu, trig) && (threadIdx.x & 31) == 0) e.flags[0] = 1;
     if (bad) atomicOr(&e.flags[1], SIM_STATUS_NONFINITE);

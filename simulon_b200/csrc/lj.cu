@@ -117,8 +117,8 @@ __global__ void __launch_bounds__(SIM_THREADS, LJ_MIN_BLOCKS) k_lj_f32(SimEngine
         reinterpret_cast<float4*>(e.f32)[i] = make_float4(fx, fy, fz, 0.0f);
         bad |= !(isfinite(fx) && isfinite(fy) && isfinite(fz));
         if (INTEG) {
-            double v[3];
-            second_half_atom(e, ip, i, ti, step, (double)fx, (double)fy, (double)fz, v, bad, INTEG == 1);
+            double v[3], a[3];
+            second_half_atom(e, ip, i, ti, step, (double)fx, (double)fy, (double)fz, v, bad, INTEG == 1, a);
             const double m = e.mass[ti];
             acc[8] += (float)(0.5 * m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
             acc[9] += (float)(m * v[0] * v[0]); acc[10] += (float)(m * v[1] * v[1]); acc[11] += (float)(m * v[2] * v[2]);
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(SIM_THREADS, LJ_MIN_BLOCKS) k_lj_f32(SimEngine
                 // the new fixed-point record goes to posfp: other threads of this
                 // pass still gather posq; k_copy_records moves it after the pass
                 const double f[3] = {(double)fx, (double)fy, (double)fz};
-                trig |= first_half_atom(e, *e.box, ip, i, ti, f, v, bad, nullptr, e.posfp);
+                trig |= first_half_atom(e, *e.box, ip, i, ti, f, v, bad, nullptr, e.posfp, a);
             }
         }
     }
