@@ -165,6 +165,7 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
     const int64_t P = e.n_pad;
     const float rc2 = t.cutoff * t.cutoff;
     const bool use_mask = e.cut_mask != nullptr && e.nbr_cap <= 64;
+    const bool spec2 = e.nbr_cap >= 2;
     float acc[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     bool bad = false, trig = false;
     const uint64_t step = INTEG && ip.step_ctr ? *ip.step_ctr : 0;
@@ -179,10 +180,15 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
         if (SINGLE && use_mask) {
             // only the slots pass 1 found inside the cutoff; the next two list
             // entries are fetched while the current pair is gathered and evaluated
+            // slots 0 and 1 are nearly always the first two inside the cutoff:
+            // their entries are loaded before the mask arrives and replaced
+            // when the mask says otherwise (rows 0 and 1 exist: nbr_cap >= 2)
+            int ja = ld_stream(&nbr[i]);
+            int jb = spec2 ? ld_stream(&nbr[P + i]) : 0;
             SlotSeq m(ld_stream(&e.cut_mask[i]));
             int ka = m.next(), kb = m.next();
-            int ja = ka >= 0 ? ld_stream(&nbr[(int64_t)ka * P + i]) : 0;
-            int jb = kb >= 0 ? ld_stream(&nbr[(int64_t)kb * P + i]) : 0;
+            if (ka != 0) ja = ka >= 0 ? ld_stream(&nbr[(int64_t)ka * P + i]) : 0;
+            if (kb != 1 || !spec2) jb = kb >= 0 ? ld_stream(&nbr[(int64_t)kb * P + i]) : 0;
             while (kb >= 0) {
                 const int j0 = ja, j1 = jb;
                 ka = m.next();
