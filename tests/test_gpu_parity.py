@@ -220,17 +220,27 @@ def test_eam_tiled_equals_untiled(sb, fsw_path, tri):
     np.testing.assert_allclose(out[1][1][:9], out[0][1][:9], rtol=1e-6, atol=1e-6)
 
 
-@pytest.mark.parametrize("tri", [False, True])
-def test_eam_cutoff_mask_equals_full_scan(sb, fsw_path, tri):
+@pytest.mark.parametrize("kind", ["ortho", "tri", "dense"])
+def test_eam_cutoff_mask_equals_full_scan(sb, fsw_path, kind):
     """Pass 2 over the in-cutoff slots recorded by pass 1 gives the same forces,
-    energies and virial, bit for bit, as pass 2 testing every list slot."""
-    if tri:
+    energies and virial, bit for bit, as pass 2 testing every list slot.
+    "dense": BCC compressed to a = 2.75 A, ~34 neighbours inside the cutoff
+    and ~47 list entries per row, so rows whose leading run of in-cutoff
+    slots fills the mask's low word, and slots of 32 and above, are walked."""
+    if kind == "tri":
         x, H = oin.bcc_triclinic(12)
     else:
-        x, L = oin.bcc_lattice(14)
+        x, L = oin.bcc_lattice(14, 2.75) if kind == "dense" else oin.bcc_lattice(14)
         H = np.diag([L] * 3)
     x = oin.jitter(x, 0.09, 43)
-    eng, tables, _ = _eam_engine(sb, fsw_path, x, H)
+    if kind == "dense":   # rows of <= 58 entries: a 64-slot list keeps the mask path
+        parser = sb.EAMParser(fsw_path)
+        tables = sb.EAMDeviceTables(parser, DEV)
+        eng = sb.MDEngine(x, np.zeros(len(x), np.int32), [oin.W_MASS], H, parser.cutoff, 0.5, nbr_cap=64,
+                          device=DEV)
+        assert eng.neighbor_stats()["max"] > 40 and eng.status() == 0
+    else:
+        eng, tables, _ = _eam_engine(sb, fsw_path, x, H)
     assert eng.cut_mask is not None
     out = []
     for masked in (True, False):
