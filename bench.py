@@ -36,7 +36,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "atom-steps/s (EAM-W, 1 B200): plain vs batched vs MLP at stated force RMSE"
 UNIT = "atom-steps/s"
-PASS2_DRAM_BYTES_PER_ATOM = (66266112 + 2173696) / 524288   # k_eam_force<1,1,1>, ncu --set full
+PASS2_DRAM_BYTES_PER_ATOM = (67890176 + 1833216) / 524288   # k_eam_force<1,1,1>, ncu --set full
 A_W, M_W = 3.165, 183.84
 
 
