@@ -361,12 +361,22 @@ __device__ __forceinline__ void second_half_atom(const SimEngine& e, const SimIn
 // Both half-steps form F/m as F times the stored 1/m, which is within one
 // ulp of the reference's quotient and spares an FP64 divide per component.
 __device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, int64_t i, int type, const double* xn,
-                                           int32_t* q_out = nullptr);
+                                           int32_t* q_out = nullptr, bool diag = false);
+
+// H and H^-1 with off-diagonal entries exactly zero: place_atom may then skip
+// the off-diagonal products (adding exact zeros changes no rounded value).
+__device__ __forceinline__ bool box_is_diagonal(const SimBox& b) {
+    bool z = true;
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+        if (k % 4 != 0) z = z && b.H[k] == 0.0 && b.Hinv[k] == 0.0;
+    return z;
+}
 
 __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimBox& b, const SimIntegrator& p, int64_t i,
                                                 int type, const double* f, const double* v_in, bool& bad,
                                                 const double* x_in = nullptr, int32_t* q_out = nullptr,
-                                                const double* a_in = nullptr) {
+                                                const double* a_in = nullptr, bool diag = false) {
     const int64_t P = e.n_pad;
     const double inv_m = e.inv_mass[type];
     double xn[3];
@@ -379,7 +389,7 @@ __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimBox
         st_state(&e.v[c * P + i], vh);
         bad |= !isfinite(xn[c]) || !isfinite(vh);
     }
-    return place_atom(e, b, i, type, xn, q_out);
+    return place_atom(e, b, i, type, xn, q_out, diag);
 }
 
 __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimIntegrator& p, int64_t i, int type,
@@ -392,12 +402,17 @@ __device__ __forceinline__ bool first_half_atom(const SimEngine& e, const SimInt
 // change), and report whether it is more than skin/2 from its position at the
 // last rebuild (reader.py:136-163).
 __device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, int64_t i, int type, const double* xn,
-                                           int32_t* q_out) {
+                                           int32_t* q_out, bool diag) {
     const int64_t P = e.n_pad;
 #pragma unroll
     for (int c = 0; c < 3; ++c) st_state(&e.x[c * P + i], xn[c]);
     double s[3];
-    cart_to_frac(b, xn[0], xn[1], xn[2], s);
+    if (diag) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s[k] = xn[k] * b.Hinv[4 * k];
+    } else {
+        cart_to_frac(b, xn[0], xn[1], xn[2], s);
+    }
     int4 q;
     q.x = (int32_t)to_fixed(s[0]);
     q.y = (int32_t)to_fixed(s[1]);
@@ -408,6 +423,10 @@ __device__ __forceinline__ bool place_atom(const SimEngine& e, const SimBox& b, 
     const double t0 = (double)(int32_t)((uint32_t)q.x - (uint32_t)ld_state(&e.xref[i])) * 2.3283064365386963e-10;
     const double t1 = (double)(int32_t)((uint32_t)q.y - (uint32_t)ld_state(&e.xref[P + i])) * 2.3283064365386963e-10;
     const double t2 = (double)(int32_t)((uint32_t)q.z - (uint32_t)ld_state(&e.xref[2 * P + i])) * 2.3283064365386963e-10;
+    if (diag) {
+        const double d0 = t0 * b.H[0], d1 = t1 * b.H[4], d2 = t2 * b.H[8];
+        return d0 * d0 + d1 * d1 + d2 * d2 > e.skin_half2;
+    }
     const double d0 = t0 * b.H[0] + t1 * b.H[3] + t2 * b.H[6];
     const double d1 = t0 * b.H[1] + t1 * b.H[4] + t2 * b.H[7];
     const double d2 = t0 * b.H[2] + t1 * b.H[5] + t2 * b.H[8];

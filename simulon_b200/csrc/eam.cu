@@ -159,6 +159,12 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
         __syncthreads();
     }
     pdl_wait();   // pass 1's posfp and F', the box and the list come from earlier kernels
+    __shared__ SimBox s_box;            // the box for the integrator epilogue, read once per block
+    if (INTEG == 2) {
+        if (threadIdx.x == 0) s_box = *e.box;
+        __syncthreads();
+    }
+    const bool diag = INTEG == 2 && box_is_diagonal(s_box);
     const BoxF b(*e.box);
     const int4* __restrict__ posfp = reinterpret_cast<const int4*>(e.posfp);
     const int32_t* __restrict__ nbr = e.nbr;
@@ -276,7 +282,7 @@ __global__ void __launch_bounds__(EAM_FORCE_THREADS, EAM_FORCE_MIN_BLOCKS) k_eam
             acc[12] += (float)(m * v[0] * v[1]); acc[13] += (float)(m * v[0] * v[2]); acc[14] += (float)(m * v[1] * v[2]);
             if (INTEG == 2) {
                 const double f[3] = {(double)fx, (double)fy, (double)fz};
-                trig |= first_half_atom(e, *e.box, ip, i, ti, f, v, bad, nullptr, nullptr, a);   // the same F/m
+                trig |= first_half_atom(e, s_box, ip, i, ti, f, v, bad, nullptr, nullptr, a, diag);   // the same F/m
             }
         }
     }
