@@ -171,7 +171,7 @@ typedef struct SimEAMTables {
     const float* dens_vd;        /* [E][E][n_r] float2 {f_k, df_k}                 */
     const float* deriv_vd;       /* [E][E][n_r] float4 {f'_k, phi'_k, df'_k, dphi'_k} */
     const float* pair_vd;        /* [E][E][n_r] float2 {phi_k, dphi_k}             */
-    int32_t n_types, n_r, n_rho, pad;
+    int32_t n_types, n_r, n_rho, pad;   /* 2 <= n_r < 2^22 (larger tables: SIM_ERR_ARG) */
     float cutoff, inv_dr, r_clamp_hi, pad2;   /* r_clamp_hi = r_max (1-1e-7) */
 } SimEAMTables;
 
