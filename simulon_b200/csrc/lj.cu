@@ -73,6 +73,12 @@ template <bool ORTHO, bool SINGLE, int INTEG, bool ACC = false>
 __global__ void __launch_bounds__(SIM_THREADS, LJ_MIN_BLOCKS) k_lj_f32(SimEngine e, SimLJParams p, SimIntegrator ip) {
     pdl_trigger();
     pdl_wait();   // positions, box and list come from earlier kernels
+    __shared__ SimBox s_box;            // the box for the integrator epilogue, read once per block
+    if (INTEG == 2) {
+        if (threadIdx.x == 0) s_box = *e.box;
+        __syncthreads();
+    }
+    const bool diag = INTEG == 2 && box_is_diagonal(s_box);
     const BoxF b(*e.box);
     const int4* __restrict__ posq = reinterpret_cast<const int4*>(e.posq);
     const int32_t* __restrict__ nbr = e.nbr;
@@ -127,7 +133,7 @@ __global__ void __launch_bounds__(SIM_THREADS, LJ_MIN_BLOCKS) k_lj_f32(SimEngine
                 // the new fixed-point record goes to posfp: other threads of this
                 // pass still gather posq; k_copy_records moves it after the pass
                 const double f[3] = {(double)fx, (double)fy, (double)fz};
-                trig |= first_half_atom(e, *e.box, ip, i, ti, f, v, bad, nullptr, e.posfp, a);
+                trig |= first_half_atom(e, s_box, ip, i, ti, f, v, bad, nullptr, e.posfp, a, diag);
             }
         }
     }
