@@ -70,6 +70,10 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k
     const float rc2 = t.cutoff * t.cutoff;
     const bool use_mask = e.cut_mask != nullptr && e.nbr_cap <= 64;
     double acc = 0.0;
+    // one element type: the embedding grid's constants read once per thread
+    // (the pass's own stores would make the compiler reload them per atom)
+    float grid1[3] = {0.f, 0.f, 0.f};
+    if (ONE) { grid1[0] = t.rho_min[0]; grid1[1] = t.rho_clamp_hi[0]; grid1[2] = t.inv_drho[0]; }
     const BlockRange br = block_range(e.n);
     for (int64_t i = br.begin + threadIdx.x; i < br.end; i += blockDim.x) {
         const int4 qi = posq[i];
@@ -106,7 +110,7 @@ __global__ void __launch_bounds__(EAM_DENSITY_THREADS, EAM_DENSITY_MIN_BLOCKS) k
             else in_hi |= (uint32_t)in << (k - 32);
         }
         float F, Fp;
-        embed_lookup(t, ti, rho, F, Fp);
+        embed_lookup(t, ti, rho, F, Fp, ONE ? grid1 : nullptr);
         posfp[i] = make_int4(qi.x, qi.y, qi.z, __float_as_int(Fp));
         if (use_mask) e.cut_mask[i] = ((uint64_t)in_hi << 32) | in_lo;
         acc += (double)F;

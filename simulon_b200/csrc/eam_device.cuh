@@ -13,11 +13,13 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
     return y;
 }
 
-// _interp_rho for F and F' of type ti
-__device__ __forceinline__ void embed_lookup(const SimEAMTables& t, int ti, float rho, float& F, float& Fp) {
-    const float lo = t.rho_min[ti];
-    const float rc = fminf(fmaxf(rho, lo), t.rho_clamp_hi[ti]);
-    const float idx_f = (rc - lo) * t.inv_drho[ti];
+// _interp_rho for F and F' of type ti; the grid's lower end, clamp and
+// inverse spacing may come from the caller (read once per thread)
+__device__ __forceinline__ void embed_lookup(const SimEAMTables& t, int ti, float rho, float& F, float& Fp,
+                                             const float* grid = nullptr) {
+    const float lo = grid ? grid[0] : t.rho_min[ti];
+    const float rc = fminf(fmaxf(rho, lo), grid ? grid[1] : t.rho_clamp_hi[ti]);
+    const float idx_f = (rc - lo) * (grid ? grid[2] : t.inv_drho[ti]);
     const int i = (int)idx_f;
     const int i1 = min(i + 1, t.n_rho - 1);
     const float frac = idx_f - (float)i;
